@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""FLIP steps/s on the 128^3 dam break, one B200 per rank.
+
+Workload (the 3D dam break of the benchmark table): 128^3 MAC grid, dx = 1/128,
+one-cell SOLID walls, water box x < 0.4, y < 0.6, z < 1 seeded with 8
+particles per cell (3,830,400 particles, octant-jittered, seed 1), zero initial
+velocity, gravity -9.81, dt = 0.002, FLIP 0.95 (PIC weight 0.05), RK2
+advection, 7-point PCG pressure solve (FP32 stencil and vectors, FP64
+reductions) to a 1e-6 relative residual.  Synthetic data; the particle state
+(2 x 61 MB float4 arrays) and the grids exceed nothing reusable across steps in
+L2 beyond what a real run keeps there, and the particle arrays alone are larger
+than the 126 MB L2.
+
+One JSON line on rank 0.  `--impl reference` times the reference's algorithm
+on the host cores instead (the CPU oracle port; the reference's own GPU binary
+needs cuDSS, which is not installed).  With torchrun (N > 1) each rank runs an
+independent replica of the scene on its own GPU (the solver is single-GPU by
+design); value = total steps/s, timing = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FLIP steps/s & PCG time-to-1e-6 at 128³, learned+mixed vs plain on one B200"
+N_GRID, DX, DT, PPC, SEED, PIC = 128, 1.0 / 128, 0.002, 8, 1, 0.05
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_GRID)
+    ap.add_argument("--ppc", type=int, default=PPC)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/), scaled as documented there; None if absent."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"fp_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_scene(n, ppc):
+    from fluidprjct_b200 import scenes
+    return scenes.dam_break_3d(n)
+
+
+def new_solver(lab, device, solver="pcg", n=N_GRID, ppc=PPC):
+    from fluidprjct_b200 import capi
+    s = capi.Solver(dx=1.0 / n, dt=DT, pic_weight=PIC, advection="rk2", solver=solver, tol=1e-6, max_iters=20000,
+                    device=device, output_format=capi.OUT_NONE)
+    s.set_labels(lab)
+    s.seed_particles(ppc, SEED)
+    return s
+
+
+def event_timer(stream_ptr):
+    import torch
+    st = torch.cuda.ExternalStream(stream_ptr)
+    return st, (lambda: torch.cuda.Event(enable_timing=True))
+
+
+def algorithmic_bytes(np_, nc, nf):
+    """Per-phase algorithmic HBM bytes (FP32 values, uint8 labels; each array
+    read or written once per phase)."""
+    return {
+        "label": 16 * np_ * 2 + 8 * np_ + 4 * nc * 3 + 2 * nc,   # read pos/vel, write sorted copies, keys/ranks, counts
+        "p2g": 32 * np_ + 24 * (nc * 1.0) + 4 * nc,              # particles in, u,v,w + u*,v*,w* out
+        "project": 29 * nc,
+        "g2p_advect": 64 * np_ + 24 * nc,                         # pos/vel in+out, u,v,w,u*,v*,w* in
+    }
+
+
+def run_ours(args, rank, local, world):
+    import torch
+    from fluidprjct_b200 import capi
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    lab = make_scene(args.n, args.ppc)
+    s = new_solver(lab, local, "pcg", args.n, args.ppc)
+    np_ = s.num_particles
+    nc = args.n ** 3
+    stream, Ev = event_timer(s.stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        s.step(1)
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    time.sleep(0.3)
+    l0 = s.stats()["kernel_launches"]
+    e0, e1 = Ev(), Ev()
+    e0.record(stream)
+    per = []
+    for _ in range(args.steps):
+        s.step(1)
+        per.append(s.stats())
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    launches = per[-1]["kernel_launches"] - l0
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms / 1000.0)
+
+    # ---- roofline of the dominant kernel (the persistent PCG) ----
+    nf = statistics.mean(p["num_fluid_cells"] for p in per)
+    iters = [p["pcg_iters"] for p in per]
+    pcg_ms = [p["t_pcg"] for p in per]
+    pcg_bytes = [41.0 * p["num_fluid_cells"] * p["pcg_iters"] + 17.0 * p["num_fluid_cells"] for p in per]
+    peak, peak_kind = load_peaks()
+    pcg_gbs = sum(pcg_bytes) / (sum(pcg_ms) / 1000.0) / 1e9
+    traffic = load_traffic()
+    phase_ms = {k: statistics.mean(p[k] for p in per) for k in ("t_label", "t_p2g", "t_pressure", "t_project",
+                                                                 "t_advect", "t_total")}
+    ab = algorithmic_bytes(np_, nc, nf)
+    phases = {
+        "label": {"ms": phase_ms["t_label"], "gbs": ab["label"] / phase_ms["t_label"] / 1e6},
+        "p2g+save+forces": {"ms": phase_ms["t_p2g"], "gbs": ab["p2g"] / phase_ms["t_p2g"] / 1e6},
+        "pressure": {"ms": phase_ms["t_pressure"], "pcg_ms": statistics.mean(pcg_ms), "pcg_iters": statistics.mean(iters)},
+        "project": {"ms": phase_ms["t_project"], "gbs": ab["project"] / phase_ms["t_project"] / 1e6},
+        "g2p+advect": {"ms": phase_ms["t_advect"], "gbs": ab["g2p_advect"] / phase_ms["t_advect"] / 1e6},
+    }
+    roofline = {"kernel": "k_pcg (persistent cooperative PCG)", "bound": "hbm", "achieved": round(pcg_gbs, 1),
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(pcg_gbs / peak, 4),
+                "traffic": (traffic or {}).get("k_pcg_bytes_per_launch"),
+                "algorithmic_bytes_per_launch": statistics.mean(pcg_bytes),
+                "note": "41 B per fluid cell per iteration + 17 B per fluid cell; working set is L2-resident at 128^3"}
+
+    out = {"metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 (FP64 reductions)", "data": "synthetic",
+           "config": {"workload": f"3D dam break {args.n}^3, dx=1/{args.n}, fluid x<0.4 y<0.6 z<1, {args.ppc} ppc",
+                      "particles": int(np_), "fluid_cells_mean": nf, "dt": DT, "flip": 1 - PIC, "advection": "rk2",
+                      "solver": "pcg (Jacobi, FP32 vectors, FP64 reductions)", "tol": 1e-6,
+                      "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                      "l2": "inputs larger than L2 (particle arrays 2 x 61 MB + grids 58 MB per step)"},
+           "ns_per_particle_step": round(ms_step * 1e6 / np_, 3),
+           "clocks": clk, "gpu_launches": int(launches), "roofline": roofline, "phases": phases}
+
+    # ---- PCG time-to-1e-6: plain vs mixed (refinement) on the same scene ----
+    if not args.no_variants and rank == 0:
+        var = {}
+        for name in ("pcg", "pcg_mixed", "pcg_mg", "pcg_learned"):
+            try:
+                v = new_solver(lab, local, name, args.n, args.ppc)
+            except Exception as e:  # variant not available in this build
+                var[name] = {"unavailable": str(e)}
+                continue
+            try:
+                for _ in range(3):
+                    v.step(1)
+                st = []
+                for _ in range(6):
+                    v.step(1)
+                    st.append(v.stats())
+                var[name] = {"pcg_ms": round(statistics.mean(x["t_pcg"] for x in st), 4),
+                             "pressure_ms": round(statistics.mean(x["t_pressure"] for x in st), 4),
+                             "iters": statistics.mean(x["pcg_iters"] for x in st),
+                             "outer": statistics.mean(x["outer_iters"] for x in st),
+                             "residual_max": max(x["residual"] for x in st),
+                             "fallback": sum(x["fallback"] for x in st)}
+            except Exception as e:
+                var[name] = {"error": str(e)}
+            v.close()
+        out["pcg_time_to_1e-6"] = var
+
+    # ---- end to end through the public API with host buffers ----
+    if not args.no_e2e:
+        pos, vel = s.particles()
+        hp = torch.from_numpy(pos).pin_memory()
+        hv = torch.from_numpy(vel).pin_memory()
+        hpn, hvn = hp.numpy(), hv.numpy()
+        k = max(3, min(args.steps, 10))
+        barrier()
+        a0, a1 = Ev(), Ev()
+        a0.record(stream)
+        for _ in range(k):
+            s.set_particles(hpn, hvn)                      # H2D of the step's input state
+            s.step(1)
+            p2, v2 = s.particles()                         # D2H of the step's result
+            hpn[:] = p2
+            hvn[:] = v2
+        a1.record(stream)
+        a1.synchronize()
+        ems = a0.elapsed_time(a1)
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        out["e2e"] = {"value": round(world * k / (ems / 1000.0), 3), "unit": "steps/s",
+                      "h2d_bytes_per_step": int(np_ * 24), "d2h_bytes_per_step": int(np_ * 24), "steps": k,
+                      "path": "fp_set_particles(pinned host pos, vel) + fp_step + fp_get_particles"}
+
+    # ---- CPU baseline (rank 0, N = 1) ----
+    if not args.no_cpu and rank == 0 and world == 1:
+        out["cpu_baseline"] = cpu_baseline(lab, args.n, args.ppc, args.cpu_seconds)
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    s.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def cpu_baseline(lab, n, ppc, seconds):
+    """The oracle port of the reference step, all host cores, bounded sample."""
+    from oracle import oracle as O
+    pos = O.seed3d(lab, 1.0 / n, ppc, SEED)
+    sim = O.Sim3(n, n, n, 1.0 / n, DT, fp64=False, pic_weight=PIC, tol=1e-6, rk2=True)
+    sim.set_labels(lab)
+    sim.set_particles(pos)
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < 1 or (time.perf_counter() - t0 < seconds and steps < 50):
+        sim.step(1)
+        steps += 1
+    el = time.perf_counter() - t0
+    return {"value": round(steps / el, 4), "unit": "steps/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{steps} full steps of the same scene ({len(pos)} particles) from the seeded state, "
+                      f"FP32 oracle with FP64 Jacobi-PCG to 1e-6, {el:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's algorithm on the host cores (oracle port)."""
+    if rank != 0:
+        return
+    lab = make_scene(args.n, args.ppc)
+    from oracle import oracle as O
+    pos = O.seed3d(lab, 1.0 / args.n, args.ppc, SEED)
+    sim = O.Sim3(args.n, args.n, args.n, 1.0 / args.n, DT, fp64=False, pic_weight=PIC, tol=1e-6, rk2=True)
+    sim.set_labels(lab)
+    sim.set_particles(pos)
+    budget = 150.0
+    t_start = time.perf_counter()
+    for _ in range(min(args.warmup, 1)):
+        sim.step(1)
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < args.steps and (steps < 2 or time.perf_counter() - t_start < budget):
+        sim.step(1)
+        steps += 1
+    el = time.perf_counter() - t0
+    v = steps / el
+    sample = (f"{steps} of {args.steps} requested steps (time-boxed to {budget:.0f} s) of the same scene, "
+              f"{len(pos)} particles, FP32 oracle port with FP64 Jacobi-PCG to 1e-6")
+    out = {"metric": METRIC, "value": round(v, 4), "unit": "steps/s", "n_gpus": world, "steps": steps,
+           "warmup": min(args.warmup, 1), "ms_per_step": round(1000 * el / steps, 2), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 solve)", "data": "synthetic",
+           "impl": "reference",
+           "config": {"workload": f"3D dam break {args.n}^3, dx=1/{args.n}, fluid x<0.4 y<0.6 z<1, {args.ppc} ppc",
+                      "particles": int(len(pos)), "parallelism": "host cores (OpenMP)"},
+           "cpu_baseline": {"value": round(v, 4), "unit": "steps/s", "cores": O.num_threads(), "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": round(v, 4), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "note": "the reference's own binary needs cuDSS (absent here); this arm runs the CPU restatement of its step"}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank, local, world = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, local, world)
+
+
+if __name__ == "__main__":
+    main()

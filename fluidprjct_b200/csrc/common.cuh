@@ -1,0 +1,130 @@
+// common.cuh -- shared device helpers of the PIC/FLIP kernels (sm_100a).
+//
+// Arithmetic follows the reference functors of src/FluidSim/FluidSolver3D.cu
+// expression by expression (IEEE division, no fast-math), so that integer
+// results (cell keys, labels) are bit-identical and floating-point ones agree
+// to rounding.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fp {
+
+constexpr uint8_t SOLID = 0, FLUID = 1, AIR = 2, BODY = 3;
+
+// Grid geometry passed by value to every kernel.
+struct Dims {
+    int W, H, D;
+    float dx;
+    __host__ __device__ int64_t nc() const { return int64_t(W) * H * D; }
+    __host__ __device__ int64_t nu() const { return int64_t(W + 1) * H * D; }
+    __host__ __device__ int64_t nv() const { return int64_t(W) * (H + 1) * D; }
+    __host__ __device__ int64_t nw() const { return int64_t(W) * H * (D + 1); }
+};
+
+// Rigid-body kinematics seen by the RHS and the projection
+// (RHSCalculator3D / UFunctor members, FluidSolver3D.cu:1368-1370, 2081-2083).
+struct BodyKin {
+    float3 vel, omega, com;
+    int active;
+};
+
+__device__ __forceinline__ int clampi(int a, int lo, int hi) { return min(max(a, lo), hi); }
+__device__ __forceinline__ float clamp01(float f) { return fminf(fmaxf(f, 0.0f), 1.0f); }
+
+// Cell of a particle: floorf(p/dx) clamped to the grid (MarkFluidCellsFunctor,
+// FluidSolver3D.cu:316-331).
+__device__ __forceinline__ int cell_key(float x, float y, float z, const Dims& g) {
+    int i = int(floorf(x / g.dx)), j = int(floorf(y / g.dx)), k = int(floorf(z / g.dx));
+    i = clampi(i, 0, g.W - 1);
+    j = clampi(j, 0, g.H - 1);
+    k = clampi(k, 0, g.D - 1);
+    return i + j * g.W + k * g.W * g.H;
+}
+
+__device__ __forceinline__ float3 body_vel_at(const BodyKin& b, float3 pos) {
+    float3 r = make_float3(pos.x - b.com.x, pos.y - b.com.y, pos.z - b.com.z);
+    return make_float3(b.vel.x + b.omega.y * r.z - b.omega.z * r.y,
+                       b.vel.y + b.omega.z * r.x - b.omega.x * r.z,
+                       b.vel.z + b.omega.x * r.y - b.omega.y * r.x);
+}
+
+// trilinearInterpolation (FluidSolver3D.cu:783-801).
+__device__ __forceinline__ float trilin(float xd, float yd, float zd, float c000, float c100, float c001, float c101,
+                                        float c010, float c110, float c011, float c111) {
+    float c00 = c000 * (1.0f - xd) + c100 * xd;
+    float c01 = c001 * (1.0f - xd) + c101 * xd;
+    float c10 = c010 * (1.0f - xd) + c110 * xd;
+    float c11 = c011 * (1.0f - xd) + c111 * xd;
+    float c0 = c00 * (1.0f - yd) + c10 * yd;
+    float c1 = c01 * (1.0f - yd) + c11 * yd;
+    return c0 * (1.0f - zd) + c1 * zd;
+}
+
+// MAC sample stencil: base corner index and fractions.  Base indices are
+// clamped so that base+1 stays inside the face grid; for positions inside
+// [0, (N-1)*dx] (where advection keeps particles) these are the reference's
+// clamps of interpVelDevice3D (FluidSolver3D.cu:1059-1140).
+struct Stencil {
+    int base;
+    float fx, fy, fz;
+};
+__device__ __forceinline__ Stencil stencil_u(float rx, float ry, float rz, const Dims& g) {
+    int i = int(floorf(rx)), j = int(floorf(ry - 0.5f)), k = int(floorf(rz - 0.5f));
+    i = clampi(i, 0, g.W - 1); j = clampi(j, 0, g.H - 2); k = clampi(k, 0, g.D - 2);
+    Stencil s;
+    s.fx = clamp01(rx - float(i)); s.fy = clamp01((ry - 0.5f) - float(j)); s.fz = clamp01((rz - 0.5f) - float(k));
+    s.base = i + j * (g.W + 1) + k * (g.W + 1) * g.H;
+    return s;
+}
+__device__ __forceinline__ Stencil stencil_v(float rx, float ry, float rz, const Dims& g) {
+    int i = int(floorf(rx - 0.5f)), j = int(floorf(ry)), k = int(floorf(rz - 0.5f));
+    i = clampi(i, 0, g.W - 2); j = clampi(j, 0, g.H - 1); k = clampi(k, 0, g.D - 2);
+    Stencil s;
+    s.fx = clamp01((rx - 0.5f) - float(i)); s.fy = clamp01(ry - float(j)); s.fz = clamp01((rz - 0.5f) - float(k));
+    s.base = i + j * g.W + k * g.W * (g.H + 1);
+    return s;
+}
+__device__ __forceinline__ Stencil stencil_w(float rx, float ry, float rz, const Dims& g) {
+    int i = int(floorf(rx - 0.5f)), j = int(floorf(ry - 0.5f)), k = int(floorf(rz));
+    i = clampi(i, 0, g.W - 2); j = clampi(j, 0, g.H - 2); k = clampi(k, 0, g.D - 1);
+    Stencil s;
+    s.fx = clamp01((rx - 0.5f) - float(i)); s.fy = clamp01((ry - 0.5f) - float(j)); s.fz = clamp01(rz - float(k));
+    s.base = i + j * g.W + k * g.W * g.H;
+    return s;
+}
+
+__device__ __forceinline__ float sample(const float* __restrict__ f, const Stencil& s, int sx, int sxy) {
+    const float* b = f + s.base;
+    return trilin(s.fx, s.fy, s.fz, __ldg(b), __ldg(b + 1), __ldg(b + sxy), __ldg(b + 1 + sxy), __ldg(b + sx),
+                  __ldg(b + 1 + sx), __ldg(b + sx + sxy), __ldg(b + 1 + sx + sxy));
+}
+// Sample of (f - g) per corner, the FLIP delta grid of gridToParticles
+// (FluidSolver3D.cu:995-1012) without materialising it.
+__device__ __forceinline__ float sample_delta(const float* __restrict__ f, const float* __restrict__ g, const Stencil& s,
+                                              int sx, int sxy) {
+    const float* a = f + s.base;
+    const float* b = g + s.base;
+    auto d = [&](int o) { return __ldg(a + o) - __ldg(b + o); };
+    return trilin(s.fx, s.fy, s.fz, d(0), d(1), d(sxy), d(1 + sxy), d(sx), d(1 + sx), d(sx + sxy), d(1 + sx + sxy));
+}
+
+__device__ __forceinline__ float3 interp_vel(const float* __restrict__ u, const float* __restrict__ v,
+                                             const float* __restrict__ w, const Dims& g, float3 pos) {
+    float rx = pos.x / g.dx, ry = pos.y / g.dx, rz = pos.z / g.dx;
+    return make_float3(sample(u, stencil_u(rx, ry, rz, g), g.W + 1, (g.W + 1) * g.H),
+                       sample(v, stencil_v(rx, ry, rz, g), g.W, g.W * (g.H + 1)),
+                       sample(w, stencil_w(rx, ry, rz, g), g.W, g.W * g.H));
+}
+
+// Labels with out-of-domain cells reading as SOLID.
+__device__ __forceinline__ uint8_t label_at(const uint8_t* __restrict__ lab, const Dims& g, int i, int j, int k) {
+    if (i < 0 || i >= g.W || j < 0 || j >= g.H || k < 0 || k >= g.D) return SOLID;
+    return lab[i + j * g.W + k * g.W * g.H];
+}
+
+// Device status word written by kernels that can fail without trapping.
+enum : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_NAN = 2, DEV_BREAKDOWN = 3, DEV_MAXIT = 4 };
+
+}  // namespace fp

@@ -1,0 +1,160 @@
+// kernels_advect.cu -- fused grid-to-particle transfer and advection.
+//
+// One thread per particle, particles in cell order (so the 48 + 72*substeps
+// grid gathers of neighbouring threads hit the same L1/L2 lines):
+//   G2P  (GridToParticleFunctor, FluidSolver3D.cu:803-980):
+//        v = alpha*I(u) + (1-alpha)*(v + I(u - u*)), the FLIP delta sampled
+//        corner by corner from u and u* instead of a materialised delta grid
+//        (:983-1012 allocates three per step);
+//   advection (AdvectParticlesFunctor, :1241-1330): adaptive substeps
+//        dT = C*dx/(|v| + 1e-37 + sqrt(5*dx*9.8)), halved when within 2*dT of
+//        the end; Ralston RK3 (weights 2/9, 3/9, 4/9) or midpoint RK2; clamp to
+//        [0, (N-1)*dx]; a particle that lands in SOLID/BODY is nudged half a
+//        cell toward the nearest FLUID cell centre among 34 offsets
+//        (projectParticleDevice3D, :1161-1239); at most 1000 substeps.
+#include "kernels.hpp"
+
+namespace fp {
+
+namespace {
+
+// Offsets searched by projectParticleDevice3D (:1164-1181); entry 9 is the
+// reference's {-1,-1} which value-initialises to {-1,-1,0}.
+__constant__ signed char c_off[34][3] = {
+    {1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1},
+    {1, 1, 0}, {-1, 1, 0}, {1, -1, 0}, {-1, -1, 0},
+    {1, 0, 1}, {-1, 0, 1}, {1, 0, -1}, {-1, 0, -1},
+    {0, 1, 1}, {0, -1, 1}, {0, 1, -1}, {0, -1, -1},
+    {1, 1, 1}, {-1, 1, 1}, {1, -1, 1}, {1, 1, -1},
+    {-1, -1, 1}, {-1, 1, -1}, {1, -1, -1}, {-1, -1, -1},
+    {-2, -1, 0}, {0, -1, -2}, {-2, -2, 0}, {0, -2, -2},
+    {-2, -2, -2}, {-2, 0, -2}, {2, -1, 0}, {0, -1, 2}};
+
+__device__ __forceinline__ bool project_particle(float3& pos, const uint8_t* __restrict__ lab, const Dims& g) {
+    const float dx = g.dx;
+    const int cx = int(floorf(pos.x / dx)), cy = int(floorf(pos.y / dx)), cz = int(floorf(pos.z / dx));
+    float best = 1e10f;
+    int bn = -1;
+#pragma unroll 2
+    for (int n = 0; n < 34; ++n) {
+        const int nx = cx + c_off[n][0], ny = cy + c_off[n][1], nz = cz + c_off[n][2];
+        if (nx < 0 || nx >= g.W || ny < 0 || ny >= g.H || nz < 0 || nz >= g.D) continue;
+        if (__ldg(lab + nx + ny * g.W + nz * g.W * g.H) != FLUID) continue;
+        const float ccx = (float(nx) + 0.5f) * dx, ccy = (float(ny) + 0.5f) * dx, ccz = (float(nz) + 0.5f) * dx;
+        const float d = (ccx - pos.x) * (ccx - pos.x) + (ccy - pos.y) * (ccy - pos.y) + (ccz - pos.z) * (ccz - pos.z);
+        if (d < best) { best = d; bn = n; }
+    }
+    if (bn < 0) return false;
+    pos.x = pos.x + (float(c_off[bn][0]) * 0.5f) * dx;
+    pos.y = pos.y + (float(c_off[bn][1]) * 0.5f) * dx;
+    pos.z = pos.z + (float(c_off[bn][2]) * 0.5f) * dx;
+    return true;
+}
+
+__global__ void __launch_bounds__(256) k_g2p_advect(float4* __restrict__ pos, float4* __restrict__ vel, int64_t np,
+                                                    const float* __restrict__ u, const float* __restrict__ v,
+                                                    const float* __restrict__ w, const float* __restrict__ us,
+                                                    const float* __restrict__ vs, const float* __restrict__ ws,
+                                                    const uint8_t* __restrict__ lab, Dims g, float alpha, float dt,
+                                                    float C, int do_g2p, int do_advect, int rk2) {
+    const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= np) return;
+    const float4 P = pos[q];
+    float3 p = make_float3(P.x, P.y, P.z);
+    const float dx = g.dx;
+    if (do_g2p) {
+        const float4 V = vel[q];
+        const float rx = p.x / dx, ry = p.y / dx, rz = p.z / dx;
+        const Stencil su = stencil_u(rx, ry, rz, g), sv = stencil_v(rx, ry, rz, g), sw = stencil_w(rx, ry, rz, g);
+        const int sxu = g.W + 1, sxyu = (g.W + 1) * g.H, sxv = g.W, sxyv = g.W * (g.H + 1), sxw = g.W, sxyw = g.W * g.H;
+        const float uP = sample(u, su, sxu, sxyu), dU = sample_delta(u, us, su, sxu, sxyu);
+        const float vP = sample(v, sv, sxv, sxyv), dV = sample_delta(v, vs, sv, sxv, sxyv);
+        const float wP = sample(w, sw, sxw, sxyw), dW = sample_delta(w, ws, sw, sxw, sxyw);
+        float4 out;
+        out.x = alpha * uP + (1.0f - alpha) * (V.x + dU);
+        out.y = alpha * vP + (1.0f - alpha) * (V.y + dV);
+        out.z = alpha * wP + (1.0f - alpha) * (V.z + dW);
+        out.w = V.w;
+        vel[q] = out;
+    }
+    if (!do_advect) return;
+    float subT = 0.0f;
+    bool finished = false;
+    int iter = 0;
+    const float floor_speed = sqrtf((5.0f * dx) * 9.8f);
+    const float xmax = float(g.W - 1) * dx, ymax = float(g.H - 1) * dx, zmax = float(g.D - 1) * dx;
+    while (!finished && iter++ < 1000) {
+        const float3 vel0 = interp_vel(u, v, w, g, p);
+        const float speed = sqrtf(vel0.x * vel0.x + vel0.y * vel0.y + vel0.z * vel0.z) + 1e-37f + floor_speed;
+        float dT = (C * dx) / speed;
+        if (subT + dT >= dt) { dT = dt - subT; finished = true; }
+        else if (subT + 2.0f * dT >= dt) { dT *= 0.5f; }
+        if (rk2) {
+            const float3 mid = make_float3(p.x + (vel0.x * 0.5f) * dT, p.y + (vel0.y * 0.5f) * dT, p.z + (vel0.z * 0.5f) * dT);
+            const float3 k2 = interp_vel(u, v, w, g, mid);
+            p = make_float3(p.x + k2.x * dT, p.y + k2.y * dT, p.z + k2.z * dT);
+        } else {
+            const float3 k1 = vel0;
+            const float3 k2 = interp_vel(u, v, w, g, make_float3(p.x + (k1.x * 0.5f) * dT, p.y + (k1.y * 0.5f) * dT,
+                                                                 p.z + (k1.z * 0.5f) * dT));
+            const float3 k3 = interp_vel(u, v, w, g, make_float3(p.x + (k2.x * 0.75f) * dT, p.y + (k2.y * 0.75f) * dT,
+                                                                 p.z + (k2.z * 0.75f) * dT));
+            const float a1 = (2.0f / 9.0f) * dT, a2 = (3.0f / 9.0f) * dT, a3 = (4.0f / 9.0f) * dT;
+            p = make_float3(p.x + k1.x * a1 + k2.x * a2 + k3.x * a3, p.y + k1.y * a1 + k2.y * a2 + k3.y * a3,
+                            p.z + k1.z * a1 + k2.z * a2 + k3.z * a3);
+        }
+        subT += dT;
+        p.x = fminf(fmaxf(p.x, 0.0f), xmax);
+        p.y = fminf(fmaxf(p.y, 0.0f), ymax);
+        p.z = fminf(fmaxf(p.z, 0.0f), zmax);
+        const int cx = int(floorf(p.x / dx)), cy = int(floorf(p.y / dx)), cz = int(floorf(p.z / dx));
+        if (cx >= 0 && cx < g.W && cy >= 0 && cy < g.H && cz >= 0 && cz < g.D) {
+            const uint8_t l = __ldg(lab + cx + cy * g.W + cz * g.W * g.H);
+            if (l == SOLID || l == BODY) {
+                if (!project_particle(p, lab, g)) break;
+            }
+        }
+        if (p.x < 0.0f || p.y < 0.0f || p.z < 0.0f || isnan(p.x) || isnan(p.y) || isnan(p.z)) break;
+    }
+    pos[q] = make_float4(p.x, p.y, p.z, P.w);
+}
+
+__global__ void k_unsort(const float4* __restrict__ pos, const float4* __restrict__ vel, int64_t np,
+                         float* __restrict__ pos_out, float* __restrict__ vel_out) {
+    const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= np) return;
+    const float4 P = pos[q];
+    const int64_t id = __float_as_int(P.w);
+    if (pos_out) { pos_out[3 * id] = P.x; pos_out[3 * id + 1] = P.y; pos_out[3 * id + 2] = P.z; }
+    if (vel_out) { const float4 V = vel[q]; vel_out[3 * id] = V.x; vel_out[3 * id + 1] = V.y; vel_out[3 * id + 2] = V.z; }
+}
+
+__global__ void k_pack(const float* __restrict__ pos, const float* __restrict__ vel, int64_t np, float4* __restrict__ p4,
+                       float4* __restrict__ v4) {
+    const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= np) return;
+    p4[q] = make_float4(pos[3 * q], pos[3 * q + 1], pos[3 * q + 2], __int_as_float(int(q)));
+    v4[q] = vel ? make_float4(vel[3 * q], vel[3 * q + 1], vel[3 * q + 2], 0.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+}  // namespace
+
+void launch_g2p_advect(float4* pos, float4* vel, int64_t np, const float* u, const float* v, const float* w,
+                       const float* us, const float* vs, const float* ws, const uint8_t* labels, Dims g, float alpha,
+                       float dt, float cfl, int do_g2p, int do_advect, int rk2, cudaStream_t st) {
+    if (np == 0) return;
+    k_g2p_advect<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, u, v, w, us, vs, ws, labels, g, alpha, dt,
+                                                             cfl, do_g2p, do_advect, rk2);
+}
+
+void launch_unsort(const float4* pos, const float4* vel, int64_t np, float* pos_out, float* vel_out, cudaStream_t st) {
+    if (np == 0) return;
+    k_unsort<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, pos_out, vel_out);
+}
+
+void launch_pack(const float* pos, const float* vel, int64_t np, float4* pos4, float4* vel4, cudaStream_t st) {
+    if (np == 0) return;
+    k_pack<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, pos4, vel4);
+}
+
+}  // namespace fp

@@ -1,0 +1,623 @@
+// kernels_pressure.cu -- pressure projection: RHS, matrix-free PCG, projection.
+//
+// Replaces pressureSolve (FluidSolver3D.cu:1815-2062) and applyPressure
+// (:2072-2464).  The reference assembles an upper-triangle CSR of the unit
+// 7-point Laplacian over FLUID cells (MatrixBuilder3D/MatrixFiller3D,
+// :1598-1777) and hands it to cuDSS every step.  Here the operator is never
+// stored: A*d at a FLUID cell is diag*d - sum of d over FLUID neighbours, with
+// diag = number of in-domain FLUID or AIR neighbours (SOLID, BODY and
+// out-of-domain neighbours are Neumann walls; AIR is Dirichlet p = 0).
+//
+// Layout: FLUID cells are compacted once per solve (fidx: padded dense index of
+// the n-th FLUID cell, in i-fastest order, the reference's fluidNumbers order);
+// x, r, q, b and diag are compact; the search direction dd lives on a dense
+// grid with a one-cell zero halo so that the stencil needs no bounds tests.
+//
+// The PCG is one persistent cooperative kernel: FP32 stencil and vector
+// updates, FP64 dot products reduced per CTA and then summed by every CTA in
+// a fixed order (deterministic, no host round trip per iteration), and a
+// bounded software grid barrier that reports a timeout instead of hanging.
+#include <cstdio>
+
+#include "kernels.hpp"
+#include "scan.cuh"
+
+namespace fp {
+
+namespace {
+
+constexpr int SCAN_BLOCK = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
+constexpr int PCG_THREADS = 512;
+
+__device__ __forceinline__ int64_t padded_index(int i, int j, int k, const Dims& g) {
+    return int64_t(i + 1) + int64_t(j + 1) * (g.W + 2) + int64_t(k + 1) * (g.W + 2) * (g.H + 2);
+}
+
+__device__ __forceinline__ bool solidish(uint8_t l) { return l == SOLID || l == BODY; }
+
+// Pass 1 of the fluid compaction: tile counts of FLUID cells; zero p.
+__global__ void __launch_bounds__(SCAN_BLOCK) k_fluid_tiles(const uint8_t* __restrict__ labels, int64_t nc,
+                                                            float* __restrict__ p, int* __restrict__ tile_sums) {
+    int64_t e0 = int64_t(blockIdx.x) * SCAN_TILE + int64_t(threadIdx.x) * SCAN_ITEMS;
+    int s = 0;
+#pragma unroll
+    for (int t = 0; t < SCAN_ITEMS; ++t) {
+        int64_t e = e0 + t;
+        if (e < nc) {
+            s += labels[e] == FLUID;
+            p[e] = 0.0f;
+        }
+    }
+    int total;
+    block_exclusive_scan<SCAN_BLOCK>(s, total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// RHSCalculator3D (FluidSolver3D.cu:1371-1456) at FLUID cell (i,j,k).
+__device__ __forceinline__ float rhs_at(const uint8_t* __restrict__ lab, const float* __restrict__ u,
+                                        const float* __restrict__ v, const float* __restrict__ w, const Dims& g,
+                                        int i, int j, int k, float scale, const BodyKin& body) {
+    const int W = g.W, H = g.H;
+    const float dx = g.dx;
+    const int64_t ui = int64_t(i) + int64_t(j) * (W + 1) + int64_t(k) * (W + 1) * H;
+    const int64_t vi = int64_t(i) + int64_t(j) * W + int64_t(k) * W * (H + 1);
+    const int64_t wi = int64_t(i) + int64_t(j) * W + int64_t(k) * W * H;
+    const float u0 = u[ui], u1 = u[ui + 1], v0 = v[vi], v1 = v[vi + W], w0 = w[wi], w1 = w[wi + int64_t(W) * H];
+    float div = u1 - u0 + v1 - v0 + w1 - w0;
+    float rhs = -scale * div;
+    uint8_t l;
+    l = label_at(lab, g, i - 1, j, k);
+    if (solidish(l)) {
+        float s = l == BODY ? body_vel_at(body, make_float3(float(i) * dx, (float(j) + 0.5f) * dx, (float(k) + 0.5f) * dx)).x : 0.0f;
+        rhs -= scale * (u0 - s);
+    }
+    l = label_at(lab, g, i + 1, j, k);
+    if (solidish(l)) {
+        float s = l == BODY ? body_vel_at(body, make_float3(float(i + 1) * dx, (float(j) + 0.5f) * dx, (float(k) + 0.5f) * dx)).x : 0.0f;
+        rhs += scale * (u1 - s);
+    }
+    l = label_at(lab, g, i, j - 1, k);
+    if (solidish(l)) {
+        float s = l == BODY ? body_vel_at(body, make_float3((float(i) + 0.5f) * dx, float(j) * dx, (float(k) + 0.5f) * dx)).y : 0.0f;
+        rhs -= scale * (v0 - s);
+    }
+    l = label_at(lab, g, i, j + 1, k);
+    if (solidish(l)) {
+        float s = l == BODY ? body_vel_at(body, make_float3((float(i) + 0.5f) * dx, float(j + 1) * dx, (float(k) + 0.5f) * dx)).y : 0.0f;
+        rhs += scale * (v1 - s);
+    }
+    l = label_at(lab, g, i, j, k - 1);
+    if (solidish(l)) {
+        float s = l == BODY ? body_vel_at(body, make_float3((float(i) + 0.5f) * dx, (float(j) + 0.5f) * dx, float(k) * dx)).z : 0.0f;
+        rhs -= scale * (w0 - s);
+    }
+    l = label_at(lab, g, i, j, k + 1);
+    if (solidish(l)) {
+        float s = l == BODY ? body_vel_at(body, make_float3((float(i) + 0.5f) * dx, (float(j) + 0.5f) * dx, float(k + 1) * dx)).z : 0.0f;
+        rhs += scale * (w1 - s);
+    }
+    return rhs;
+}
+
+// Pass 3: write the compact system (fidx, diag, b) of every FLUID cell.
+__global__ void __launch_bounds__(SCAN_BLOCK) k_fluid_build(const uint8_t* __restrict__ labels,
+                                                            const float* __restrict__ u, const float* __restrict__ v,
+                                                            const float* __restrict__ w, Dims g, float scale,
+                                                            BodyKin body, const float* __restrict__ rhs_dense,
+                                                            const int* __restrict__ tile_off, int* __restrict__ fidx,
+                                                            uint8_t* __restrict__ diag, float* __restrict__ b) {
+    const int64_t nc = g.nc();
+    int64_t e0 = int64_t(blockIdx.x) * SCAN_TILE + int64_t(threadIdx.x) * SCAN_ITEMS;
+    uint8_t lab[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int t = 0; t < SCAN_ITEMS; ++t) {
+        int64_t e = e0 + t;
+        lab[t] = e < nc ? labels[e] : SOLID;
+        s += lab[t] == FLUID;
+    }
+    int total;
+    int n = block_exclusive_scan<SCAN_BLOCK>(s, total) + tile_off[blockIdx.x];
+#pragma unroll
+    for (int t = 0; t < SCAN_ITEMS; ++t) {
+        if (lab[t] != FLUID) continue;
+        int64_t e = e0 + t;
+        int i = int(e % g.W), j = int((e / g.W) % g.H), k = int(e / (int64_t(g.W) * g.H));
+        fidx[n] = int(padded_index(i, j, k, g));
+        int d = 0;
+        const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+#pragma unroll
+        for (int o = 0; o < 6; ++o) {
+            uint8_t l = label_at(labels, g, i + off[o][0], j + off[o][1], k + off[o][2]);
+            d += (l == FLUID || l == AIR);
+        }
+        diag[n] = uint8_t(d);
+        b[n] = rhs_dense ? rhs_dense[e] : rhs_at(labels, u, v, w, g, i, j, k, scale, body);
+        ++n;
+    }
+}
+
+// ---------------------------------------------------------------- grid barrier
+// Sense-free generation barrier for a cooperative launch.  The wait is bounded:
+// after ~2^26 polls the block records DEV_TIMEOUT and leaves; every caller
+// checks the status after the barrier and returns, so no block waits forever.
+__device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* status) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = &bar->gen;
+        unsigned gen0 = *vgen;
+        __threadfence();
+        unsigned arrived = atomicAdd(&bar->count, 1u);
+        if (arrived == nblocks - 1) {
+            atomicExch(&bar->count, 0u);
+            __threadfence();
+            atomicAdd(&bar->gen, 1u);
+        } else {
+            long long polls = 0;
+            while (*vgen == gen0) {
+                if (++polls > (1ll << 26)) {
+                    atomicExch(status, DEV_TIMEOUT);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int*)status == DEV_OK;
+}
+
+// Block sum of two doubles (fixed tree, deterministic); result valid in thread 0.
+__device__ __forceinline__ double2 block_sum2(double a, double b) {
+    __shared__ double2 sh[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = make_double2(a, b);
+    __syncthreads();
+    double2 r = make_double2(0.0, 0.0);
+    if (wid == 0) {
+        r = lane < int(blockDim.x >> 5) ? sh[lane] : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            r.x += __shfl_down_sync(0xffffffffu, r.x, o);
+            r.y += __shfl_down_sync(0xffffffffu, r.y, o);
+        }
+    }
+    __syncthreads();
+    return r;
+}
+
+// Sum of per-block partials part[0..nb) (pairs), identical in every block.
+__device__ __forceinline__ double2 grid_sum2(const double2* part, int nb) {
+    __shared__ double2 res;
+    if (threadIdx.x < 32) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int t = threadIdx.x; t < nb; t += 32) {
+            // Written by other CTAs in this launch: read through L2.
+            double2 v = __ldcg(part + t);
+            s.x += v.x;
+            s.y += v.y;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s.x += __shfl_down_sync(0xffffffffu, s.x, o);
+            s.y += __shfl_down_sync(0xffffffffu, s.y, o);
+        }
+        if (threadIdx.x == 0) res = s;
+    }
+    __syncthreads();
+    double2 r = res;
+    __syncthreads();
+    return r;
+}
+
+struct PcgArgs {
+    Dims g;
+    const int* nf;
+    const int* fidx;
+    const uint8_t* diag;
+    const float* b;
+    float* x;
+    float* r;
+    float* q;
+    float* dd;
+    double2* part;  // [3 * nblocks]
+    GridBar* bar;
+    int* status;
+    PcgOut* out;
+    double tol;
+    int maxit;
+};
+
+__global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs a) {
+    const int nf = *a.nf;
+    const unsigned nb = gridDim.x;
+    const int stride = int(nb) * PCG_THREADS;
+    const int t0 = blockIdx.x * PCG_THREADS + threadIdx.x;
+    const int sx = 1, sy = a.g.W + 2, sz = (a.g.W + 2) * (a.g.H + 2);
+    double2* partA = a.part;
+    double2* partB = a.part + nb;
+    double2* partI = a.part + 2 * nb;
+
+    // x0 = 0, r0 = b, z0 = r0/diag, d0 = z0.
+    double rz_l = 0.0, rr_l = 0.0;
+    for (int n = t0; n < nf; n += stride) {
+        float rv = a.b[n];
+        float dg = float(a.diag[n]);
+        float z = dg > 0.0f ? rv / dg : 0.0f;
+        a.x[n] = 0.0f;
+        a.r[n] = rv;
+        a.dd[a.fidx[n]] = z;
+        rz_l += double(rv) * double(z);
+        rr_l += double(rv) * double(rv);
+    }
+    double2 bs = block_sum2(rz_l, rr_l);
+    if (threadIdx.x == 0) partI[blockIdx.x] = bs;
+    if (!grid_barrier(a.bar, nb, a.status)) return;
+    double2 tot = grid_sum2(partI, nb);
+    double rz = tot.x, rr = tot.y;
+    const double bb = tot.y;
+    const double thr = a.tol * a.tol * bb;
+    int it = 0;
+    int st = DEV_OK;
+    while (rr > thr && bb > 0.0) {
+        if (it >= a.maxit) { st = DEV_MAXIT; break; }
+        // Phase A: q = A d, partial d.q
+        double dq_l = 0.0;
+        for (int n = t0; n < nf; n += stride) {
+            const int c = a.fidx[n];
+            const float* d = a.dd + c;
+            // Neighbours were written by other CTAs in this launch: read through L2.
+            float dc = __ldcg(d);
+            float nbs = (__ldcg(d + sx) + __ldcg(d - sx)) + (__ldcg(d + sy) + __ldcg(d - sy)) +
+                        (__ldcg(d + sz) + __ldcg(d - sz));
+            float qv = float(a.diag[n]) * dc - nbs;
+            a.q[n] = qv;
+            dq_l += double(dc) * double(qv);
+        }
+        bs = block_sum2(dq_l, 0.0);
+        if (threadIdx.x == 0) partA[blockIdx.x] = bs;
+        if (!grid_barrier(a.bar, nb, a.status)) return;
+        const double dq = grid_sum2(partA, nb).x;
+        if (!(dq > 0.0) || isnan(dq)) { st = isnan(dq) ? DEV_NAN : DEV_BREAKDOWN; break; }
+        const float alpha = float(rz / dq);
+        // Phase B: x += alpha d, r -= alpha q, z = r/diag; partial r.z, r.r
+        double rz_n = 0.0, rr_n = 0.0;
+        for (int n = t0; n < nf; n += stride) {
+            const int c = a.fidx[n];
+            float dc = a.dd[c];
+            a.x[n] += alpha * dc;
+            float rv = a.r[n] - alpha * a.q[n];
+            a.r[n] = rv;
+            float dg = float(a.diag[n]);
+            float z = dg > 0.0f ? rv / dg : 0.0f;
+            rz_n += double(rv) * double(z);
+            rr_n += double(rv) * double(rv);
+        }
+        bs = block_sum2(rz_n, rr_n);
+        if (threadIdx.x == 0) partB[blockIdx.x] = bs;
+        if (!grid_barrier(a.bar, nb, a.status)) return;
+        tot = grid_sum2(partB, nb);
+        ++it;
+        if (isnan(tot.x) || isnan(tot.y)) { st = DEV_NAN; rr = tot.y; break; }
+        const float beta = float(tot.x / rz);
+        rz = tot.x;
+        rr = tot.y;
+        if (rr <= thr) break;
+        // Phase C: d = z + beta d
+        for (int n = t0; n < nf; n += stride) {
+            const int c = a.fidx[n];
+            float dg = float(a.diag[n]);
+            float z = dg > 0.0f ? a.r[n] / dg : 0.0f;
+            a.dd[c] = z + beta * a.dd[c];
+        }
+        if (!grid_barrier(a.bar, nb, a.status)) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.out->iters = it;
+        atomicCAS(a.status, DEV_OK, st);  // never masks a timeout recorded by another CTA
+        a.out->rr = rr;
+        a.out->bb = bb;
+        a.out->rz = rz;
+    }
+}
+
+__global__ void k_reset_pcg(GridBar* bar, int* status) {
+    bar->count = 0;
+    bar->gen = 0;
+    *status = DEV_OK;
+}
+
+__global__ void k_scatter_p(const int* __restrict__ nf_p, const int* __restrict__ fidx, const float* __restrict__ x,
+                            const double* __restrict__ x64, int use64, Dims g, float* __restrict__ p) {
+    const int nf = *nf_p;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) {
+        int cp = fidx[n];
+        int i = cp % (g.W + 2) - 1, j = (cp / (g.W + 2)) % (g.H + 2) - 1, k = cp / ((g.W + 2) * (g.H + 2)) - 1;
+        p[int64_t(i) + int64_t(j) * g.W + int64_t(k) * g.W * g.H] = use64 ? float(x64[n]) : x[n];
+    }
+}
+
+// Fill the padded dense grid dd (float) or xd (double) from a compact vector.
+__global__ void k_to_dense_f(const int* __restrict__ nf_p, const int* __restrict__ fidx, const float* __restrict__ x,
+                             float* __restrict__ dd) {
+    const int nf = *nf_p;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) dd[fidx[n]] = x[n];
+}
+
+// Partials of ||b - A x||^2 and ||b||^2 over the padded dense x (float or double).
+template <class T>
+__global__ void __launch_bounds__(256) k_residual(const int* __restrict__ nf_p, const int* __restrict__ fidx,
+                                                  const uint8_t* __restrict__ diag, const float* __restrict__ b,
+                                                  const T* __restrict__ xd, Dims g, double2* __restrict__ part,
+                                                  float* __restrict__ r_out, double* __restrict__ r64_out) {
+    const int nf = *nf_p;
+    const int sx = 1, sy = g.W + 2, sz = (g.W + 2) * (g.H + 2);
+    double e2 = 0.0, b2 = 0.0;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) {
+        const T* x = xd + fidx[n];
+        double ax = double(diag[n]) * double(x[0]) -
+                    (double(x[sx]) + double(x[-sx]) + double(x[sy]) + double(x[-sy]) + double(x[sz]) + double(x[-sz]));
+        double e = double(b[n]) - ax;
+        if (r_out) r_out[n] = float(e);
+        if (r64_out) r64_out[n] = e;
+        e2 += e * e;
+        b2 += double(b[n]) * double(b[n]);
+    }
+    double2 s = block_sum2(e2, b2);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void k_sum_partials(const double2* __restrict__ part, int nb, double* __restrict__ out) {
+    double2 s = grid_sum2(part, nb);
+    if (threadIdx.x == 0) { out[0] = s.x; out[1] = s.y; }
+}
+
+__global__ void k_ir_update(const int* __restrict__ nf_p, const int* __restrict__ fidx, const float* __restrict__ c,
+                            double* __restrict__ x64, double* __restrict__ xd) {
+    const int nf = *nf_p;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) {
+        double v = x64[n] + double(c[n]);
+        x64[n] = v;
+        xd[fidx[n]] = v;
+    }
+}
+
+// ---------------------------------------------------------------- projection
+// UFunctor/VFunctor/WFunctor (FluidSolver3D.cu:2072-2336) for one face between
+// cells L and R: a SOLID/BODY side gets a ghost pressure that makes the face
+// velocity equal to the wall velocity (0 or the rigid-body velocity).
+__device__ __forceinline__ float project_face(float vel, uint8_t lL, uint8_t lR, float pL, float pR, float vb,
+                                              float scale, float inv) {
+    const bool fL = (lL == FLUID || lL == AIR), fR = (lR == FLUID || lR == AIR);
+    float p0, p1;
+    if (fL && fR) { p0 = pL; p1 = pR; }
+    else if (solidish(lL)) { float s = lL == BODY ? vb : 0.0f; p0 = pR - inv * (vel - s); p1 = pR; }
+    else if (solidish(lR)) { float s = lR == BODY ? vb : 0.0f; p0 = pL; p1 = pL + inv * (vel - s); }
+    else { p0 = pL; p1 = pR; }
+    return vel - scale * (p1 - p0);
+}
+
+__device__ __forceinline__ float p_at(const float* __restrict__ p, const Dims& g, int i, int j, int k) {
+    if (i < 0 || i >= g.W || j < 0 || j >= g.H || k < 0 || k >= g.D) return 0.0f;
+    return p[i + j * g.W + k * g.W * g.H];
+}
+
+__global__ void k_project(float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+                          const float* __restrict__ p, const uint8_t* __restrict__ lab, Dims g, float scale, float inv,
+                          BodyKin body) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int W = g.W, H = g.H, D = g.D;
+    if (i > W || j > H || k > D) return;
+    const float dx = g.dx;
+    const uint8_t lc = label_at(lab, g, i, j, k);
+    const float pc = p_at(p, g, i, j, k);
+    if (j < H && k < D) {
+        int64_t id = int64_t(i) + int64_t(j) * (W + 1) + int64_t(k) * (W + 1) * H;
+        float vb = body.active ? body_vel_at(body, make_float3(float(i) * dx, (float(j) + 0.5f) * dx, (float(k) + 0.5f) * dx)).x : 0.0f;
+        u[id] = project_face(u[id], label_at(lab, g, i - 1, j, k), lc, p_at(p, g, i - 1, j, k), pc, vb, scale, inv);
+    }
+    if (i < W && k < D) {
+        int64_t id = int64_t(i) + int64_t(j) * W + int64_t(k) * W * (H + 1);
+        float vb = body.active ? body_vel_at(body, make_float3((float(i) + 0.5f) * dx, float(j) * dx, (float(k) + 0.5f) * dx)).y : 0.0f;
+        v[id] = project_face(v[id], label_at(lab, g, i, j - 1, k), lc, p_at(p, g, i, j - 1, k), pc, vb, scale, inv);
+    }
+    if (i < W && j < H) {
+        int64_t id = int64_t(i) + int64_t(j) * W + int64_t(k) * W * H;
+        float vb = body.active ? body_vel_at(body, make_float3((float(i) + 0.5f) * dx, (float(j) + 0.5f) * dx, float(k) * dx)).z : 0.0f;
+        w[id] = project_face(w[id], label_at(lab, g, i, j, k - 1), lc, p_at(p, g, i, j, k - 1), pc, vb, scale, inv);
+    }
+}
+
+// ---------------------------------------------------------------- CSR CG (FP64)
+// Symmetric matrix from its upper triangle: y = U x + U^T x - diag(U) x.
+__global__ void k_csr_sym_spmv(int n, const int* __restrict__ off, const int* __restrict__ cols,
+                               const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int e = off[i]; e < off[i + 1]; ++e) {
+        int c = cols[e];
+        s += vals[e] * x[c];
+        if (c != i) atomicAdd(&y[c], vals[e] * x[i]);
+    }
+    atomicAdd(&y[i], s);
+}
+__global__ void k_csr_diag(int n, const int* __restrict__ off, const int* __restrict__ cols,
+                           const double* __restrict__ vals, double* __restrict__ dg) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 1.0;
+    for (int e = off[i]; e < off[i + 1]; ++e) if (cols[e] == i) d = vals[e];
+    dg[i] = d;
+}
+__global__ void k_dot(int n, const double* __restrict__ a, const double* __restrict__ b, double2* part) {
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
+    double2 r = block_sum2(s, 0.0);
+    if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+__global__ void k_axpy2(int n, double alpha, const double* __restrict__ d, const double* __restrict__ q,
+                        double* __restrict__ x, double* __restrict__ r, const double* __restrict__ dg,
+                        double* __restrict__ z) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] += alpha * d[i];
+    r[i] -= alpha * q[i];
+    z[i] = r[i] / dg[i];
+}
+__global__ void k_xpby(int n, const double* __restrict__ z, double beta, double* __restrict__ d) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) d[i] = z[i] + beta * d[i];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers
+
+void launch_pressure_setup(const uint8_t* labels, const float* u, const float* v, const float* w, Dims g, float dt,
+                           BodyKin body, const float* rhs_dense, float* p, PressureBufs& pb, cudaStream_t st) {
+    const int64_t nc = g.nc();
+    const int ntiles = int((nc + SCAN_TILE - 1) / SCAN_TILE);
+    const float scale = (1000.0f * g.dx) / dt;  // rho*dx/dt, FluidSolver3D.cu:1520
+    k_fluid_tiles<<<ntiles, SCAN_BLOCK, 0, st>>>(labels, nc, p, pb.tile_sums);
+    k_scan_single_block<<<1, 1024, 0, st>>>(pb.tile_sums, ntiles, pb.nf);
+    k_fluid_build<<<ntiles, SCAN_BLOCK, 0, st>>>(labels, u, v, w, g, scale, body, rhs_dense, pb.tile_sums, pb.fidx,
+                                                 pb.diag, pb.b);
+}
+
+int pcg_max_blocks() {
+    static int cached = 0;
+    if (cached) return cached;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, PCG_THREADS, 0);
+    cached = sms * (per_sm > 0 ? per_sm : 1);
+    return cached;
+}
+
+int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, double tol, int maxit, int max_blocks, cudaStream_t st) {
+    int nb = pcg_max_blocks();
+    if (max_blocks > 0 && max_blocks < nb) nb = max_blocks;
+    int* status = &pb.out->status;
+    k_reset_pcg<<<1, 1, 0, st>>>(pb.bar, status);
+    PcgArgs a;
+    a.g = g; a.nf = pb.nf; a.fidx = pb.fidx; a.diag = pb.diag; a.b = rhs;
+    a.x = pb.x; a.r = pb.r; a.q = pb.q; a.dd = pb.dd;
+    a.part = reinterpret_cast<double2*>(pb.part); a.bar = pb.bar; a.status = status; a.out = pb.out;
+    a.tol = tol; a.maxit = maxit;
+    void* args[] = {&a};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(nb), dim3(PCG_THREADS), args, 0, st);
+    return e == cudaSuccess ? 0 : int(e);
+}
+
+void launch_scatter_p(const PressureBufs& pb, float* p, int use64, Dims g, cudaStream_t st) {
+    k_scatter_p<<<592, 256, 0, st>>>(pb.nf, pb.fidx, pb.x, pb.x64, use64, g, p);
+}
+
+void launch_true_residual(const PressureBufs& pb, const float* p, Dims g, cudaStream_t st) {
+    // Rebuild the padded dense x from the compact solution, then reduce.
+    k_to_dense_f<<<592, 256, 0, st>>>(pb.nf, pb.fidx, pb.x, pb.dd);
+    const int nb = 592;
+    k_residual<float><<<nb, 256, 0, st>>>(pb.nf, pb.fidx, pb.diag, pb.b, pb.dd, g,
+                                          reinterpret_cast<double2*>(pb.part), nullptr, nullptr);
+    k_sum_partials<<<1, 32, 0, st>>>(reinterpret_cast<double2*>(pb.part), nb, pb.red);
+    (void)p;
+}
+
+void launch_ir_residual(PressureBufs& pb, double* xd, Dims g, cudaStream_t st) {
+    // r = b - A x64 in FP64; the inner right-hand side is r rounded to FP32.
+    const int nb = 592;
+    k_residual<double><<<nb, 256, 0, st>>>(pb.nf, pb.fidx, pb.diag, pb.b, xd, g, reinterpret_cast<double2*>(pb.part),
+                                           pb.bin, nullptr);
+    k_sum_partials<<<1, 32, 0, st>>>(reinterpret_cast<double2*>(pb.part), nb, pb.red);
+}
+
+void launch_ir_update(PressureBufs& pb, double* xd, Dims g, cudaStream_t st) {
+    k_ir_update<<<592, 256, 0, st>>>(pb.nf, pb.fidx, pb.x, pb.x64, xd);
+    (void)g;
+}
+
+void launch_project(float* u, float* v, float* w, const float* p, const uint8_t* labels, Dims g, float dt, BodyKin b,
+                    cudaStream_t st) {
+    const float scale = dt / (1000.0f * g.dx);  // dt/(rho*dx), FluidSolver3D.cu:2341
+    const float inv = 1.0f / scale;
+    dim3 blk(32, 8, 1);
+    dim3 grd((g.W + 1 + 31) / 32, (g.H + 1 + 7) / 8, g.D + 1);
+    k_project<<<grd, blk, 0, st>>>(u, v, w, p, labels, g, scale, inv, b);
+}
+
+int csr_cg_solve(int n, const int* offsets, const int* cols, const double* vals, const double* b, double* x, double tol,
+                 int maxit, int* iters, double* relres, cudaStream_t st) {
+    if (n <= 0) return -1;
+    int nnz = offsets[n];
+    int *d_off = nullptr, *d_cols = nullptr;
+    double *d_vals = nullptr, *d_x = nullptr, *d_r = nullptr, *d_d = nullptr, *d_q = nullptr, *d_z = nullptr,
+           *d_dg = nullptr;
+    double2* d_part = nullptr;
+    cudaError_t e = cudaSuccess;
+    auto ck = [&](cudaError_t r) { if (r != cudaSuccess && e == cudaSuccess) e = r; };
+    ck(cudaMalloc(&d_off, sizeof(int) * (n + 1)));
+    ck(cudaMalloc(&d_cols, sizeof(int) * nnz));
+    ck(cudaMalloc(&d_vals, sizeof(double) * nnz));
+    for (double** p : {&d_x, &d_r, &d_d, &d_q, &d_z, &d_dg}) ck(cudaMalloc(p, sizeof(double) * n));
+    ck(cudaMalloc(&d_part, sizeof(double2) * 65));
+    if (e != cudaSuccess) goto done;
+    ck(cudaMemcpyAsync(d_off, offsets, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
+    ck(cudaMemcpyAsync(d_cols, cols, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
+    ck(cudaMemcpyAsync(d_vals, vals, sizeof(double) * nnz, cudaMemcpyHostToDevice, st));
+    ck(cudaMemcpyAsync(d_r, b, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    ck(cudaMemsetAsync(d_x, 0, sizeof(double) * n, st));
+    {
+        const int blk = 128, grd = (n + blk - 1) / blk;
+        k_csr_diag<<<grd, blk, 0, st>>>(n, d_off, d_cols, d_vals, d_dg);
+        auto dot = [&](const double* a, const double* bb) {
+            double h[2];
+            k_dot<<<64, 128, 0, st>>>(n, a, bb, d_part);
+            k_sum_partials<<<1, 32, 0, st>>>(d_part, 64, reinterpret_cast<double*>(d_part + 64));
+            cudaMemcpyAsync(h, reinterpret_cast<double*>(d_part + 64), sizeof(double) * 2, cudaMemcpyDeviceToHost, st);
+            cudaStreamSynchronize(st);
+            return h[0];
+        };
+        // z = r/diag, d = z
+        k_axpy2<<<grd, blk, 0, st>>>(n, 0.0, d_d, d_d, d_x, d_r, d_dg, d_z);
+        ck(cudaMemcpyAsync(d_d, d_z, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        const double bb = dot(d_r, d_r);
+        double rz = dot(d_r, d_z), rr = bb;
+        int it = 0;
+        while (bb > 0 && rr > tol * tol * bb && it < maxit) {
+            ck(cudaMemsetAsync(d_q, 0, sizeof(double) * n, st));
+            k_csr_sym_spmv<<<grd, blk, 0, st>>>(n, d_off, d_cols, d_vals, d_d, d_q);
+            double dq = dot(d_d, d_q);
+            if (!(dq > 0)) break;
+            double alpha = rz / dq;
+            k_axpy2<<<grd, blk, 0, st>>>(n, alpha, d_d, d_q, d_x, d_r, d_dg, d_z);
+            double rz2 = dot(d_r, d_z);
+            rr = dot(d_r, d_r);
+            k_xpby<<<grd, blk, 0, st>>>(n, d_z, rz2 / rz, d_d);
+            rz = rz2;
+            ++it;
+        }
+        if (iters) *iters = it;
+        if (relres) *relres = bb > 0 ? sqrt(rr / bb) : 0.0;
+        ck(cudaMemcpyAsync(x, d_x, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        ck(cudaStreamSynchronize(st));
+    }
+done:
+    cudaFree(d_off); cudaFree(d_cols); cudaFree(d_vals);
+    for (double* p : {d_x, d_r, d_d, d_q, d_z, d_dg}) cudaFree(p);
+    cudaFree(d_part);
+    return e == cudaSuccess ? 0 : int(e);
+}
+
+}  // namespace fp

@@ -1,0 +1,737 @@
+// solver.cu -- host runtime of the B200 PIC/FLIP solver and its C ABI.
+//
+// One fp_solver per scene: it owns a CUDA stream and every device buffer,
+// allocated once when the labels (grid) and particles are set, so a step
+// performs no allocation (the reference allocates ~15 Thrust temporaries per
+// step).  The step is the reference's frameStep (FluidSolver3D.cu:3030-3098)
+// with its phases fused into fewer kernels:
+//   label   : bin + label/scan + scatter  (labelGrid, and the cell sort)
+//   p2g     : brick-tiled P2G with normalise, u* save and gravity fused
+//   pressure: fluid compaction + RHS, persistent PCG, scatter, residual check
+//   project : one kernel over all faces
+//   g2p+adv : one kernel per particle
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fluidprjct.h"
+#include "io.hpp"
+#include "kernels.hpp"
+
+using namespace fp;
+
+namespace {
+
+constexpr float kGravity[3] = {0.0f, -9.81f, 0.0f};  // FluidSolver3D.cuh:78
+
+template <class T>
+cudaError_t dalloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    return cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+}
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+}  // namespace
+
+struct fp_solver {
+    fp_config cfg{};
+    std::string err;
+    int W = 0, H = 0, D = 0;
+    Dims g{};
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[10]{};
+    cudaEvent_t ev_pcg[2]{};
+    int64_t launches = 0;   // kernels launched by this solver
+    float pcg_ms = 0.0f;
+    bool have_grid = false;
+
+    // grids
+    uint8_t *d_base = nullptr, *d_labels = nullptr, *d_bodymark = nullptr;
+    float *d_u = nullptr, *d_v = nullptr, *d_w = nullptr, *d_us = nullptr, *d_vs = nullptr, *d_ws = nullptr,
+          *d_p = nullptr, *d_scratch = nullptr;
+    int *d_counts = nullptr, *d_start = nullptr, *d_tiles = nullptr;
+    // particles (cell order; pid in pos.w)
+    float4 *d_pos = nullptr, *d_vel = nullptr, *d_pos2 = nullptr, *d_vel2 = nullptr;
+    int *d_key = nullptr, *d_rank = nullptr;
+    float* d_io = nullptr;  // n*3 staging for unsort/pack
+    int64_t np = 0, cap = 0;
+    bool sorted = false;
+    // pressure
+    PressureBufs pb{};
+    double* d_xd = nullptr;
+    int64_t padded = 0;
+    // pinned result mirrors
+    PcgOut* h_out = nullptr;
+    double* h_red = nullptr;
+    int* h_nf = nullptr;
+    // body
+    BodyKin body{};
+    // stats
+    fp_step_stats stats{};
+    int64_t steps = 0;
+
+    int fail(int code, const std::string& m) {
+        err = m;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* where) {
+        err = std::string(where) + ": " + cudaGetErrorString(e);
+        return FP_ERR_CUDA;
+    }
+};
+
+namespace {
+
+void free_grid(fp_solver* s) {
+    dfree(s->d_base); dfree(s->d_labels); dfree(s->d_bodymark);
+    dfree(s->d_u); dfree(s->d_v); dfree(s->d_w); dfree(s->d_us); dfree(s->d_vs); dfree(s->d_ws);
+    dfree(s->d_p); dfree(s->d_scratch);
+    dfree(s->d_counts); dfree(s->d_start); dfree(s->d_tiles);
+    PressureBufs& pb = s->pb;
+    dfree(pb.nf); dfree(pb.fidx); dfree(pb.diag); dfree(pb.b); dfree(pb.bin); dfree(pb.x); dfree(pb.r); dfree(pb.q);
+    dfree(pb.dd); dfree(pb.x64); dfree(pb.part); dfree(pb.bar); dfree(pb.out); dfree(pb.red);
+    dfree(s->d_xd);
+    s->have_grid = false;
+}
+
+void free_particles(fp_solver* s) {
+    dfree(s->d_pos); dfree(s->d_vel); dfree(s->d_pos2); dfree(s->d_vel2);
+    dfree(s->d_key); dfree(s->d_rank); dfree(s->d_io);
+    s->np = s->cap = 0;
+}
+
+int alloc_grid(fp_solver* s, int W, int H, int D) {
+    free_grid(s);
+    s->W = W; s->H = H; s->D = D;
+    s->g = Dims{W, H, D, s->cfg.dx};
+    const int64_t nc = s->g.nc();
+    s->padded = int64_t(W + 2) * (H + 2) * (D + 2);
+    const int ntiles = int((nc + 4095) / 4096) + 1;
+    const int maxb = pcg_max_blocks();
+    cudaError_t e = cudaSuccess;
+    auto ck = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    ck(dalloc(&s->d_base, nc)); ck(dalloc(&s->d_labels, nc)); ck(dalloc(&s->d_bodymark, nc));
+    ck(dalloc(&s->d_u, s->g.nu())); ck(dalloc(&s->d_us, s->g.nu()));
+    ck(dalloc(&s->d_v, s->g.nv())); ck(dalloc(&s->d_vs, s->g.nv()));
+    ck(dalloc(&s->d_w, s->g.nw())); ck(dalloc(&s->d_ws, s->g.nw()));
+    ck(dalloc(&s->d_p, nc)); ck(dalloc(&s->d_scratch, nc));
+    ck(dalloc(&s->d_counts, nc + 1)); ck(dalloc(&s->d_start, nc + 1)); ck(dalloc(&s->d_tiles, ntiles));
+    PressureBufs& pb = s->pb;
+    ck(dalloc(&pb.nf, 1)); ck(dalloc(&pb.fidx, nc)); ck(dalloc(&pb.diag, nc)); ck(dalloc(&pb.b, nc));
+    ck(dalloc(&pb.bin, nc)); ck(dalloc(&pb.x, nc)); ck(dalloc(&pb.r, nc)); ck(dalloc(&pb.q, nc));
+    ck(dalloc(&pb.dd, s->padded)); ck(dalloc(&pb.x64, nc));
+    ck(dalloc(&pb.part, size_t(6) * std::max(maxb, 1024)));
+    ck(dalloc(&pb.bar, 1)); ck(dalloc(&pb.out, 1)); ck(dalloc(&pb.red, 2));
+    ck(dalloc(&s->d_xd, s->padded));
+    pb.tile_sums = s->d_tiles;
+    if (e != cudaSuccess) { free_grid(s); return s->cuda_fail(e, "device allocation of the grid"); }
+    for (float* a : {s->d_u, s->d_us}) ck(cudaMemsetAsync(a, 0, sizeof(float) * s->g.nu(), s->st));
+    for (float* a : {s->d_v, s->d_vs}) ck(cudaMemsetAsync(a, 0, sizeof(float) * s->g.nv(), s->st));
+    for (float* a : {s->d_w, s->d_ws}) ck(cudaMemsetAsync(a, 0, sizeof(float) * s->g.nw(), s->st));
+    ck(cudaMemsetAsync(s->d_p, 0, sizeof(float) * nc, s->st));
+    ck(cudaMemsetAsync(s->d_bodymark, 0, nc, s->st));
+    ck(cudaMemsetAsync(pb.dd, 0, sizeof(float) * s->padded, s->st));
+    ck(cudaMemsetAsync(pb.bar, 0, sizeof(GridBar), s->st));
+    if (e != cudaSuccess) { free_grid(s); return s->cuda_fail(e, "grid initialisation"); }
+    s->have_grid = true;
+    s->sorted = false;
+    return FP_OK;
+}
+
+int alloc_particles(fp_solver* s, int64_t n) {
+    if (n <= s->cap) { s->np = n; return FP_OK; }
+    free_particles(s);
+    cudaError_t e = cudaSuccess;
+    auto ck = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    ck(dalloc(&s->d_pos, n)); ck(dalloc(&s->d_vel, n)); ck(dalloc(&s->d_pos2, n)); ck(dalloc(&s->d_vel2, n));
+    ck(dalloc(&s->d_key, n)); ck(dalloc(&s->d_rank, n)); ck(dalloc(&s->d_io, size_t(n) * 6));
+    if (e != cudaSuccess) { free_particles(s); return s->cuda_fail(e, "device allocation of particles"); }
+    s->cap = n;
+    s->np = n;
+    return FP_OK;
+}
+
+float3 gravity3() { return make_float3(kGravity[0], kGravity[1], kGravity[2]); }
+
+// ---------------------------------------------------------------- phases
+void phase_label(fp_solver* s) {
+    s->launches += 5;  // bin, label tiles, tile scan, start tiles, scatter
+    cudaMemsetAsync(s->d_counts, 0, sizeof(int) * (s->g.nc() + 1), s->st);
+    launch_bin(s->d_pos, s->np, s->g, s->d_counts, s->d_key, s->d_rank, s->st);
+    launch_label_scan(s->d_base, s->cfg.active_body ? s->d_bodymark : nullptr, s->d_counts, s->d_labels, s->d_start,
+                      s->d_tiles, s->g, s->st);
+    launch_scatter(s->d_pos, s->d_vel, s->d_key, s->d_rank, s->d_start, s->np, s->d_pos2, s->d_vel2, s->st);
+    std::swap(s->d_pos, s->d_pos2);
+    std::swap(s->d_vel, s->d_vel2);
+    s->sorted = true;
+}
+
+void phase_p2g(fp_solver* s, int fused) {
+    if (!s->sorted) phase_label(s);
+    s->launches += 1;
+    launch_p2g(s->d_pos, s->d_vel, s->d_start, s->g, s->cfg.dt, gravity3(), s->d_u, s->d_v, s->d_w, s->d_us, s->d_vs,
+               s->d_ws, fused, s->st);
+}
+
+void phase_save(fp_solver* s) {
+    s->launches += 3;
+    launch_copy(s->d_u, s->d_us, s->g.nu(), s->st);
+    launch_copy(s->d_v, s->d_vs, s->g.nv(), s->st);
+    launch_copy(s->d_w, s->d_ws, s->g.nw(), s->st);
+}
+
+// Pressure solve of the system already set up in s->pb; leaves the solution in
+// p and the diagnostics in the pinned mirrors.  Returns FP_OK or an error.
+int solve_system(fp_solver* s, float* p_out) {
+    PressureBufs& pb = s->pb;
+    const double tol = s->cfg.tol;
+    const int maxit = s->cfg.max_iters;
+    int outer = 0, inner_total = 0;
+    int dev_status = DEV_OK;
+    const int solver = s->cfg.solver;
+    float pcg_ms = 0.0f;
+    if (solver == FP_SOLVER_PCG) {
+        cudaEventRecord(s->ev_pcg[0], s->st);
+        int e = launch_pcg(s->g, pb, pb.b, tol, maxit, 0, s->st);
+        cudaEventRecord(s->ev_pcg[1], s->st);
+        if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
+        s->launches += 2 + 1 + 3;  // reset + pcg, scatter, residual (3)
+        launch_scatter_p(pb, p_out, 0, s->g, s->st);
+        launch_true_residual(pb, p_out, s->g, s->st);
+        cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
+        cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+        cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+        cudaError_t ce = cudaStreamSynchronize(s->st);
+        if (ce != cudaSuccess) return s->cuda_fail(ce, "pressure solve");
+        inner_total = s->h_out->iters;
+        dev_status = s->h_out->status;
+        outer = 1;
+        cudaEventElapsedTime(&pcg_ms, s->ev_pcg[0], s->ev_pcg[1]);
+    } else {
+        // FP64 iterative refinement around FP32-vector PCG (FP64 reductions).
+        cudaMemsetAsync(pb.x64, 0, sizeof(double) * s->g.nc(), s->st);
+        cudaMemsetAsync(s->d_xd, 0, sizeof(double) * s->padded, s->st);
+        launch_ir_residual(pb, s->d_xd, s->g, s->st);
+        s->launches += 2;
+        cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+        cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+        cudaError_t ce = cudaStreamSynchronize(s->st);
+        if (ce != cudaSuccess) return s->cuda_fail(ce, "refinement residual");
+        const double bb = s->h_red[1];
+        double relres = bb > 0 ? std::sqrt(s->h_red[0] / bb) : 0.0;
+        while (relres > tol && outer < 12 && inner_total < maxit) {
+            double inner_tol = std::min(0.1, std::max(1e-4, 0.5 * tol / relres));
+            cudaEventRecord(s->ev_pcg[0], s->st);
+            int e = launch_pcg(s->g, pb, pb.bin, inner_tol, maxit - inner_total, 0, s->st);
+            cudaEventRecord(s->ev_pcg[1], s->st);
+            if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
+            s->launches += 2 + 1 + 2;  // reset + pcg, update, residual (2)
+            launch_ir_update(pb, s->d_xd, s->g, s->st);
+            launch_ir_residual(pb, s->d_xd, s->g, s->st);
+            cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
+            cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+            ce = cudaStreamSynchronize(s->st);
+            if (ce != cudaSuccess) return s->cuda_fail(ce, "refinement step");
+            inner_total += s->h_out->iters;
+            ++outer;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, s->ev_pcg[0], s->ev_pcg[1]);
+            pcg_ms += ms;
+            if (s->h_out->status == DEV_TIMEOUT || s->h_out->status == DEV_NAN) { dev_status = s->h_out->status; break; }
+            double nr = bb > 0 ? std::sqrt(s->h_red[0] / bb) : 0.0;
+            if (!(nr < relres)) { relres = nr; dev_status = DEV_BREAKDOWN; break; }  // stalled refinement
+            relres = nr;
+        }
+        launch_scatter_p(pb, p_out, 1, s->g, s->st);
+        s->launches += 1;
+        s->h_red[0] = relres * relres * bb;
+        s->h_red[1] = bb;
+        if (relres > tol && dev_status == DEV_OK) dev_status = DEV_MAXIT;
+    }
+    s->pcg_ms = pcg_ms;
+    s->stats.t_pcg = pcg_ms;
+    s->stats.num_fluid_cells = *s->h_nf;
+    s->stats.pcg_iters = inner_total;
+    s->stats.outer_iters = outer;
+    s->stats.fallback = 0;
+    s->stats.residual = s->h_red[1] > 0 ? std::sqrt(s->h_red[0] / s->h_red[1]) : 0.0;
+    int status = FP_OK;
+    if (*s->h_nf == 0) status = FP_ERR_NO_FLUID;
+    else if (dev_status == DEV_TIMEOUT) status = FP_ERR_TIMEOUT;
+    else if (dev_status == DEV_NAN || dev_status == DEV_BREAKDOWN) status = FP_ERR_SOLVER;
+    else if (dev_status == DEV_MAXIT) status = FP_ERR_SOLVER;
+    s->stats.solve_status = status;
+    if (status == FP_ERR_TIMEOUT) return s->fail(status, "PCG grid barrier timed out");
+    if (dev_status == DEV_NAN) return s->fail(status, "PCG produced NaN");
+    return FP_OK;  // no-fluid, breakdown and iteration cap are reported in stats, as the step continues
+}
+
+int phase_pressure(fp_solver* s) {
+    s->launches += 3;  // fluid tiles, tile scan, fluid build
+    cudaMemsetAsync(s->pb.dd, 0, sizeof(float) * s->padded, s->st);
+    BodyKin b = s->body;
+    b.active = s->cfg.active_body;
+    launch_pressure_setup(s->d_labels, s->d_u, s->d_v, s->d_w, s->g, s->cfg.dt, b, nullptr, s->d_p, s->pb, s->st);
+    return solve_system(s, s->d_p);
+}
+
+void phase_project(fp_solver* s) {
+    BodyKin b = s->body;
+    b.active = s->cfg.active_body;
+    s->launches += 1;
+    launch_project(s->d_u, s->d_v, s->d_w, s->d_p, s->d_labels, s->g, s->cfg.dt, b, s->st);
+}
+
+void phase_g2p_advect(fp_solver* s, int do_g2p, int do_adv) {
+    s->launches += 1;
+    launch_g2p_advect(s->d_pos, s->d_vel, s->np, s->d_u, s->d_v, s->d_w, s->d_us, s->d_vs, s->d_ws, s->d_labels, s->g,
+                      s->cfg.pic_weight, s->cfg.dt, s->cfg.cfl, do_g2p, do_adv, s->cfg.advection == FP_ADVECT_RK2,
+                      s->st);
+    if (do_adv) s->sorted = false;
+}
+
+int check_ready(fp_solver* s) {
+    if (!s) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "labels not loaded");
+    if (s->cfg.dim != 3) return s->fail(FP_ERR_ARG, "only dim = 3 is supported by this entry point");
+    if (s->W < 2 || s->H < 2 || s->D < 2) return s->fail(FP_ERR_ARG, "grid must be at least 2 cells on every axis");
+    return FP_OK;
+}
+
+int one_step(fp_solver* s) {
+    cudaEventRecord(s->ev[0], s->st);
+    phase_label(s);
+    cudaEventRecord(s->ev[1], s->st);
+    phase_p2g(s, 1);  // P2G + save + forces
+    cudaEventRecord(s->ev[2], s->st);
+    cudaEventRecord(s->ev[3], s->st);
+    int rc = phase_pressure(s);
+    cudaEventRecord(s->ev[4], s->st);
+    if (rc != FP_OK) return rc;
+    phase_project(s);
+    cudaEventRecord(s->ev[5], s->st);
+    cudaEventRecord(s->ev[6], s->st);  // body coupling slot
+    cudaEventRecord(s->ev[7], s->st);
+    phase_g2p_advect(s, 1, 1);
+    cudaEventRecord(s->ev[8], s->st);
+    cudaError_t e = cudaEventSynchronize(s->ev[8]);
+    if (e != cudaSuccess) return s->cuda_fail(e, "step");
+    float t[8];
+    for (int i = 0; i < 8; ++i) cudaEventElapsedTime(&t[i], s->ev[i], s->ev[i + 1]);
+    s->stats.t_label = t[0];
+    s->stats.t_p2g = t[1];
+    s->stats.t_forces = t[2];
+    s->stats.t_pressure = t[3];
+    s->stats.t_project = t[4];
+    s->stats.t_body = t[5];
+    s->stats.t_g2p = 0.0f;
+    s->stats.t_advect = t[7];
+    cudaEventElapsedTime(&s->stats.t_total, s->ev[0], s->ev[8]);
+    ++s->steps;
+    s->stats.step = s->steps;
+    s->stats.num_particles = s->np;
+    s->stats.kernel_launches = s->launches;
+    return FP_OK;
+}
+
+std::string frame_dir(const std::string& tmpl) {
+    size_t p = tmpl.find_last_of('/');
+    return p == std::string::npos ? std::string(".") : tmpl.substr(0, p);
+}
+
+}  // namespace
+
+// ======================================================================== C ABI
+extern "C" {
+
+const char* fp_version(void) { return "fluidprjct_b200 0.1 (sm_100a)"; }
+
+int fp_read_label_file(const char* path, int dim, int* dims, uint8_t* out) {
+    if (!path || !dims || (dim != 2 && dim != 3)) return FP_ERR_ARG;
+    std::vector<uint8_t> lab;
+    std::string err;
+    int W = 0, H = 0, D = 1;
+    bool ok = dim == 2 ? io::read_labels2d(path, W, H, lab, err) : io::read_labels3d(path, W, H, D, lab, err);
+    if (!ok) {
+        std::fprintf(stderr, "fp_read_label_file: %s\n", err.c_str());
+        return FP_ERR_IO;
+    }
+    dims[0] = W; dims[1] = H; dims[2] = D;
+    if (out) std::memcpy(out, lab.data(), lab.size());
+    return FP_OK;
+}
+
+int fp_read_ply_file(const char* path, int64_t* n, float* pos, float* vel, int* has_vel) {
+    if (!path || !n) return FP_ERR_ARG;
+    std::vector<float> p, v;
+    bool hv = false;
+    std::string err;
+    if (!io::read_ply(path, p, v, hv, err)) {
+        std::fprintf(stderr, "fp_read_ply_file: %s\n", err.c_str());
+        return FP_ERR_IO;
+    }
+    *n = int64_t(p.size() / 3);
+    if (has_vel) *has_vel = hv ? 1 : 0;
+    if (pos) std::memcpy(pos, p.data(), p.size() * sizeof(float));
+    if (vel && hv) std::memcpy(vel, v.data(), v.size() * sizeof(float));
+    return FP_OK;
+}
+
+int fp_config_default(fp_config* c) {
+    if (!c) return FP_ERR_ARG;
+    std::memset(c, 0, sizeof *c);
+    c->dim = 3;
+    c->dx = 0.1f;            // main.cpp:19
+    c->dt = 0.02f;           // main.cpp:18
+    c->pic_weight = 0.01f;   // main.cpp:23
+    c->iter_per_frame = 1;   // main.cpp:24
+    c->output_format = FP_OUT_PLY;
+    std::snprintf(c->output_template, sizeof c->output_template, "%s", "InputData/particles_");  // main.cpp:33
+    c->active_body = 0;
+    c->body_pos[0] = c->body_pos[1] = c->body_pos[2] = 0.5f;  // main.cpp:44-46
+    c->body_mass = 50.0f;    // main.cpp:48
+    c->ppc = 4;              // FluidSolver3D.cuh:72
+    c->seed = 0;
+    c->solver = FP_SOLVER_PCG;
+    c->advection = FP_ADVECT_RK3REF;
+    c->cfl = 0.1f;           // FluidSolver3D.cu:3092
+    c->tol = 1e-6;
+    c->max_iters = 20000;
+    c->body_radius = 0.0f;
+    c->body_density = 0.5f;
+    c->device = -1;
+    return FP_OK;
+}
+
+int fp_config_load_json(const char* path, fp_config* cfg, char* label_path, size_t label_path_len, int* frames) {
+    if (!path || !cfg) return FP_ERR_ARG;
+    std::string lp, err;
+    if (!io::load_config_json(path, *cfg, &lp, frames, err)) {
+        std::fprintf(stderr, "fp_config_load_json: %s\n", err.c_str());
+        return FP_ERR_IO;
+    }
+    if (label_path && label_path_len) std::snprintf(label_path, label_path_len, "%s", lp.c_str());
+    return FP_OK;
+}
+
+int fp_create(const fp_config* cfg, fp_solver** out) {
+    if (!out) return FP_ERR_ARG;
+    *out = nullptr;
+    auto* s = new (std::nothrow) fp_solver();
+    if (!s) return FP_ERR_ARG;
+    if (cfg) s->cfg = *cfg; else fp_config_default(&s->cfg);
+    if (!(s->cfg.dx > 0) || !(s->cfg.dt > 0) || (s->cfg.dim != 2 && s->cfg.dim != 3)) { delete s; return FP_ERR_ARG; }
+    if (s->cfg.solver != FP_SOLVER_PCG && s->cfg.solver != FP_SOLVER_PCG_MIXED) {
+        std::fprintf(stderr, "fp_create: solver %d is not available in this build\n", s->cfg.solver);
+        delete s;
+        return FP_ERR_ARG;
+    }
+    cudaError_t e = cudaSuccess;
+    if (s->cfg.device >= 0) e = cudaSetDevice(s->cfg.device);  // the calling thread's device from here on
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    for (auto& ev : s->ev) if (e == cudaSuccess) e = cudaEventCreate(&ev);
+    for (auto& ev : s->ev_pcg) if (e == cudaSuccess) e = cudaEventCreate(&ev);
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_out, sizeof(PcgOut));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_red, sizeof(double) * 2);
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_nf, sizeof(int));
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "fp_create: %s\n", cudaGetErrorString(e));
+        fp_destroy(s);
+        return FP_ERR_CUDA;
+    }
+    s->body.com = make_float3(s->cfg.body_pos[0], s->cfg.body_pos[1], s->cfg.body_pos[2]);
+    *out = s;
+    return FP_OK;
+}
+
+int fp_destroy(fp_solver* s) {
+    if (!s) return FP_OK;
+    if (s->st) cudaStreamSynchronize(s->st);
+    free_grid(s);
+    free_particles(s);
+    for (auto& ev : s->ev) if (ev) cudaEventDestroy(ev);
+    for (auto& ev : s->ev_pcg) if (ev) cudaEventDestroy(ev);
+    if (s->h_out) cudaFreeHost(s->h_out);
+    if (s->h_red) cudaFreeHost(s->h_red);
+    if (s->h_nf) cudaFreeHost(s->h_nf);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+    return FP_OK;
+}
+
+const char* fp_last_error(const fp_solver* s) { return s ? s->err.c_str() : "null solver"; }
+
+int fp_set_labels(fp_solver* s, const uint8_t* labels, int W, int H, int D) {
+    if (!s || !labels || W <= 0 || H <= 0 || D <= 0) return s ? s->fail(FP_ERR_ARG, "bad labels") : FP_ERR_ARG;
+    const int64_t nc = int64_t(W) * H * D;
+    for (int64_t c = 0; c < nc; ++c)
+        if (labels[c] > FP_BODY) return s->fail(FP_ERR_ARG, "label value out of range at cell " + std::to_string(c));
+    int rc = alloc_grid(s, W, H, D);
+    if (rc) return rc;
+    // The SOLID map is fixed for the run; BODY cells of an input are re-derived
+    // from the body every step, other non-SOLID cells from the particles.
+    std::vector<uint8_t> base(labels, labels + nc);
+    for (auto& l : base) if (l == FP_BODY) l = FP_AIR;
+    cudaError_t e = cudaMemcpyAsync(s->d_base, base.data(), size_t(nc), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_labels, labels, size_t(nc), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "label upload");
+    return FP_OK;
+}
+
+int fp_load_labels(fp_solver* s, const char* path) {
+    if (!s || !path) return FP_ERR_ARG;
+    std::vector<uint8_t> lab;
+    int W, H, D = 1;
+    bool ok = s->cfg.dim == 2 ? io::read_labels2d(path, W, H, lab, s->err) : io::read_labels3d(path, W, H, D, lab, s->err);
+    if (!ok) return FP_ERR_IO;
+    return fp_set_labels(s, lab.data(), W, H, D);
+}
+
+int fp_get_dims(const fp_solver* s, int* W, int* H, int* D) {
+    if (!s) return FP_ERR_ARG;
+    if (W) *W = s->W;
+    if (H) *H = s->H;
+    if (D) *D = s->D;
+    return FP_OK;
+}
+
+int fp_load_sdf(fp_solver* s, const char* path) {
+    if (!s) return FP_ERR_ARG;
+    (void)path;
+    return s->fail(FP_ERR_STATE, "rigid-body coupling is not enabled in this build");
+}
+
+int fp_set_particles(fp_solver* s, const float* pos, const float* vel, int64_t n) {
+    if (!s || n < 0 || (n > 0 && !pos)) return s ? s->fail(FP_ERR_ARG, "bad particle arrays") : FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "labels must be set before particles");
+    if (n >= (int64_t(1) << 31)) return s->fail(FP_ERR_ARG, "too many particles");
+    for (int64_t q = 0; q < 3 * n; ++q)
+        if (!std::isfinite(pos[q]) || (vel && !std::isfinite(vel[q])))
+            return s->fail(FP_ERR_ARG, "non-finite particle value at index " + std::to_string(q / 3));
+    int rc = alloc_particles(s, n);
+    if (rc) return rc;
+    if (n == 0) return FP_OK;
+    float* dpos = s->d_io;
+    float* dvel = s->d_io + 3 * n;
+    cudaError_t e = cudaMemcpyAsync(dpos, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess && vel) e = cudaMemcpyAsync(dvel, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "particle upload");
+    launch_pack(dpos, vel ? dvel : nullptr, n, s->d_pos, s->d_vel, s->st);
+    e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "particle upload");
+    s->sorted = false;
+    return FP_OK;
+}
+
+int fp_seed_particles(fp_solver* s, int ppc, uint32_t seed) {
+    if (!s || ppc < 0) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "labels must be loaded before seeding");
+    std::vector<uint8_t> lab(size_t(s->g.nc()));
+    cudaError_t e = cudaMemcpy(lab.data(), s->d_labels, lab.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return s->cuda_fail(e, "label download");
+    std::vector<float> pos;
+    io::seed_particles(lab.data(), s->W, s->H, s->D, s->cfg.dx, ppc, seed, pos);
+    return fp_set_particles(s, pos.data(), nullptr, int64_t(pos.size() / 3));
+}
+
+int fp_load_ply(fp_solver* s, const char* path) {
+    if (!s || !path) return FP_ERR_ARG;
+    std::vector<float> pos, vel;
+    bool hv = false;
+    if (!io::read_ply(path, pos, vel, hv, s->err)) return FP_ERR_IO;
+    return fp_set_particles(s, pos.data(), hv ? vel.data() : nullptr, int64_t(pos.size() / 3));
+}
+
+int64_t fp_num_particles(const fp_solver* s) { return s ? s->np : -1; }
+
+int fp_get_particles(fp_solver* s, float* pos, float* vel, int64_t n) {
+    if (!s || n != s->np) return s ? s->fail(FP_ERR_ARG, "particle count mismatch") : FP_ERR_ARG;
+    if (n == 0) return FP_OK;
+    launch_unsort(s->d_pos, s->d_vel, n, s->d_io, s->d_io + 3 * n, s->st);
+    cudaError_t e = cudaSuccess;
+    if (pos) e = cudaMemcpyAsync(pos, s->d_io, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess && vel) e = cudaMemcpyAsync(vel, s->d_io + 3 * n, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "particle download");
+    return FP_OK;
+}
+
+int fp_save_ply(fp_solver* s, const char* path, int format) {
+    if (!s || !path) return FP_ERR_ARG;
+    std::vector<float> pos(size_t(s->np) * 3), vel(size_t(s->np) * 3);
+    int rc = fp_get_particles(s, pos.data(), vel.data(), s->np);
+    if (rc) return rc;
+    if (!io::write_particles(path, pos.data(), vel.data(), s->np, format, s->err)) return FP_ERR_IO;
+    return FP_OK;
+}
+
+int fp_step(fp_solver* s, int n) {
+    int rc = check_ready(s);
+    if (rc) return rc;
+    for (int i = 0; i < n; ++i) {
+        rc = one_step(s);
+        if (rc) return rc;
+    }
+    return FP_OK;
+}
+
+int fp_run(fp_solver* s, int frames) {
+    int rc = check_ready(s);
+    if (rc) return rc;
+    const int ipf = std::max(1, s->cfg.iter_per_frame);
+    const std::string tmpl = s->cfg.output_template;
+    FILE* csv = nullptr;
+    if (s->cfg.active_body) {
+        std::string cp = frame_dir(tmpl) + "/csvRes.csv";
+        csv = std::fopen(cp.c_str(), "w");
+        if (csv) std::fprintf(csv, "frame,centerX1,centerX2,centerX3,angleX1,angleX2,angleX3\n");
+    }
+    phase_label(s);  // run() labels once before the loop (FluidSolver3D.cu:3110)
+    std::vector<float> pos, vel;
+    for (int64_t i = 0; i <= int64_t(frames) * ipf; ++i) {  // inclusive bound, :3111
+        rc = one_step(s);
+        if (rc) break;
+        if (i % ipf == 0 && s->cfg.output_format != FP_OUT_NONE) {
+            pos.resize(size_t(s->np) * 3);
+            vel.resize(size_t(s->np) * 3);
+            rc = fp_get_particles(s, pos.data(), vel.data(), s->np);
+            if (rc) break;
+            const char* ext = s->cfg.output_format == FP_OUT_OFF ? ".off" : ".ply";
+            std::string path = tmpl + std::to_string(i / ipf) + ext;
+            if (!io::write_particles(path, pos.data(), vel.data(), s->np, s->cfg.output_format, s->err)) {
+                rc = FP_ERR_IO;
+                break;
+            }
+            if (csv) {
+                std::fprintf(csv, "%lld,%g,%g,%g,%g,%g,%g\n", (long long)(i / ipf), s->stats.body_pos[0],
+                             s->stats.body_pos[1], s->stats.body_pos[2], s->stats.body_angles[0],
+                             s->stats.body_angles[1], s->stats.body_angles[2]);
+                std::fflush(csv);
+            }
+        }
+    }
+    if (csv) std::fclose(csv);
+    return rc;
+}
+
+int fp_run_phase(fp_solver* s, int phase) {
+    int rc = check_ready(s);
+    if (rc) return rc;
+    switch (phase) {
+        case FP_PHASE_LABEL: phase_label(s); break;
+        case FP_PHASE_P2G: phase_p2g(s, 0); break;
+        case FP_PHASE_SAVE: phase_save(s); break;
+        case FP_PHASE_FORCES: launch_forces(s->d_u, s->d_v, s->d_w, s->g, s->cfg.dt, gravity3(), s->st); break;
+        case FP_PHASE_PRESSURE: rc = phase_pressure(s); break;
+        case FP_PHASE_PROJECT: phase_project(s); break;
+        case FP_PHASE_BODY: break;
+        case FP_PHASE_G2P: phase_g2p_advect(s, 1, 0); break;
+        case FP_PHASE_ADVECT: phase_g2p_advect(s, 0, 1); break;
+        default: return s->fail(FP_ERR_ARG, "unknown phase");
+    }
+    cudaError_t e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "phase");
+    return rc;
+}
+
+static int64_t grid_len(const fp_solver* s, int which) {
+    switch (which) {
+        case FP_GRID_U: case FP_GRID_U_SAVED: return s->g.nu();
+        case FP_GRID_V: case FP_GRID_V_SAVED: return s->g.nv();
+        case FP_GRID_W: case FP_GRID_W_SAVED: return s->g.nw();
+        case FP_GRID_P: return s->g.nc();
+    }
+    return -1;
+}
+static float* grid_ptr(fp_solver* s, int which) {
+    float* a[7] = {s->d_u, s->d_v, s->d_w, s->d_us, s->d_vs, s->d_ws, s->d_p};
+    return (which >= 0 && which < 7) ? a[which] : nullptr;
+}
+
+int fp_get_grid(fp_solver* s, int which, float* out, int64_t n) {
+    if (!s || !out) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "no grid");
+    if (grid_len(s, which) != n) return s->fail(FP_ERR_ARG, "grid size mismatch");
+    cudaError_t e = cudaMemcpyAsync(out, grid_ptr(s, which), sizeof(float) * n, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    return e == cudaSuccess ? FP_OK : s->cuda_fail(e, "grid download");
+}
+
+int fp_set_grid(fp_solver* s, int which, const float* in, int64_t n) {
+    if (!s || !in) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "no grid");
+    if (grid_len(s, which) != n) return s->fail(FP_ERR_ARG, "grid size mismatch");
+    cudaError_t e = cudaMemcpyAsync(grid_ptr(s, which), in, sizeof(float) * n, cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    return e == cudaSuccess ? FP_OK : s->cuda_fail(e, "grid upload");
+}
+
+int fp_get_labels(fp_solver* s, uint8_t* out, int64_t n) {
+    if (!s || !out) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "no grid");
+    if (n != s->g.nc()) return s->fail(FP_ERR_ARG, "label size mismatch");
+    cudaError_t e = cudaMemcpyAsync(out, s->d_labels, size_t(n), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    return e == cudaSuccess ? FP_OK : s->cuda_fail(e, "label download");
+}
+
+int fp_set_body_state(fp_solver* s, const float* pos, const float* vel, const float* omega) {
+    if (!s) return FP_ERR_ARG;
+    if (pos) s->body.com = make_float3(pos[0], pos[1], pos[2]);
+    if (vel) s->body.vel = make_float3(vel[0], vel[1], vel[2]);
+    if (omega) s->body.omega = make_float3(omega[0], omega[1], omega[2]);
+    return FP_OK;
+}
+
+int fp_stats(const fp_solver* s, fp_step_stats* out) {
+    if (!s || !out) return FP_ERR_ARG;
+    *out = s->stats;
+    out->kernel_launches = s->launches;
+    return FP_OK;
+}
+
+void* fp_cuda_stream(const fp_solver* s) { return s ? static_cast<void*>(s->st) : nullptr; }
+
+int fp_pressure_solve(fp_solver* s, const float* rhs, float* x, int64_t n, int* iters, double* relres) {
+    if (!s || !rhs || !x) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "no grid");
+    if (n != s->g.nc()) return s->fail(FP_ERR_ARG, "rhs size mismatch");
+    cudaError_t e = cudaMemcpyAsync(s->d_scratch, rhs, sizeof(float) * n, cudaMemcpyHostToDevice, s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "rhs upload");
+    cudaMemsetAsync(s->pb.dd, 0, sizeof(float) * s->padded, s->st);
+    BodyKin b{};
+    // The solution goes to pb.q reused as a dense float scratch of nc entries.
+    launch_pressure_setup(s->d_labels, s->d_u, s->d_v, s->d_w, s->g, s->cfg.dt, b, s->d_scratch, s->pb.q, s->pb, s->st);
+    int rc = solve_system(s, s->d_scratch);
+    if (rc) return rc;
+    e = cudaMemsetAsync(s->d_scratch, 0, sizeof(float) * n, s->st);
+    launch_scatter_p(s->pb, s->d_scratch, s->cfg.solver != FP_SOLVER_PCG, s->g, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(x, s->d_scratch, sizeof(float) * n, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "solution download");
+    if (iters) *iters = s->stats.pcg_iters;
+    if (relres) *relres = s->stats.residual;
+    return s->stats.solve_status;
+}
+
+int fp_solve_csr_upper(int n, const int* offsets, const int* cols, const double* vals, const double* b, double* x,
+                       double tol, int max_iters, int* iters, double* relres) {
+    if (n <= 0 || !offsets || !cols || !vals || !b || !x) return FP_ERR_ARG;
+    for (int i = 0; i < n; ++i)
+        if (offsets[i + 1] < offsets[i]) return FP_ERR_ARG;
+    for (int e = 0; e < offsets[n]; ++e)
+        if (cols[e] < 0 || cols[e] >= n) return FP_ERR_ARG;
+    int rc = csr_cg_solve(n, offsets, cols, vals, b, x, tol, max_iters, iters, relres, 0);
+    return rc ? FP_ERR_CUDA : FP_OK;
+}
+
+}  // extern "C"

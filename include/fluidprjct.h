@@ -1,0 +1,212 @@
+/*
+ * fluidprjct.h -- C ABI of the B200-native PIC/FLIP solver.
+ *
+ * Drop-in replacement for the per-step solve path of Ship-Vano/FluidPrjct,
+ * whose interface is the C++ class FluidSolver3D
+ * (src/FluidSim/FluidSolver3D.cuh:13-186) driven by main.cpp:9-58.
+ * The class becomes an opaque handle; its public knobs become fp_config
+ * fields; init()/run()/frameStep() become fp_load_labels()+fp_seed_particles()
+ * / fp_run() / fp_step().
+ *
+ * Conventions
+ *   - Every entry point returns an int status (FP_OK = 0) and never throws.
+ *     fp_last_error() gives the message of the last failure on a handle.
+ *   - One solver per host thread; each solver owns one CUDA stream and all of
+ *     its device memory.  Buffers passed in or out are host memory owned by
+ *     the caller and are copied.
+ *   - Grids use the reference's layouts: cell (i,j,k) at i + j*W + k*W*H;
+ *     u is (W+1) x H x D, v is W x (H+1) x D, w is W x H x (D+1), each with
+ *     i fastest.  Labels: FP_SOLID 0, FP_FLUID 1, FP_AIR 2, FP_BODY 3
+ *     (utility.cuh:65-68).
+ *   - Particles are n x 3 interleaved float32 (x y z), returned in the order
+ *     they were given (the solver keeps them sorted by cell internally).
+ *   - Cells outside the grid count as SOLID walls.
+ */
+#ifndef FLUIDPRJCT_H
+#define FLUIDPRJCT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference's pressureSolve returns -1 (no fluid cells),
+ * -2 (empty matrix) and -4 (matrix creation failure)
+ * (FluidSolver3D.cu:1875-1951); those map to FP_ERR_NO_FLUID / FP_ERR_SOLVER. */
+enum {
+    FP_OK = 0,
+    FP_ERR_ARG = -1,        /* bad argument or size                        */
+    FP_ERR_IO = -2,         /* file missing, truncated or malformed        */
+    FP_ERR_CUDA = -3,       /* CUDA runtime error                          */
+    FP_ERR_STATE = -4,      /* call out of order (e.g. step before labels) */
+    FP_ERR_NO_FLUID = -5,   /* pressure solve found no FLUID cell          */
+    FP_ERR_SOLVER = -6,     /* PCG breakdown, NaN, or iteration cap        */
+    FP_ERR_TIMEOUT = -7     /* a bounded device-side wait gave up          */
+};
+
+enum { FP_SOLID = 0, FP_FLUID = 1, FP_AIR = 2, FP_BODY = 3 };
+
+/* Frame output format of fp_run (FileOutputFormat, utility.cuh:58-61, plus
+ * binary little-endian PLY and "no output"). */
+enum { FP_OUT_PLY = 0, FP_OUT_OFF = 1, FP_OUT_PLY_BINARY = 2, FP_OUT_NONE = 3 };
+
+/* Pressure solver variants (all matrix-free 7-point PCG on the GPU):
+ *   FP_SOLVER_PCG         FP32 stencil and vectors, FP64 reductions, Jacobi
+ *                         preconditioner ("plain" PCG);
+ *   FP_SOLVER_PCG_MIXED   the same inner PCG inside an FP64 iterative-refinement
+ *                         loop (true residual recomputed in FP64);
+ *   FP_SOLVER_PCG_MG      geometric-multigrid V-cycle preconditioner;
+ *   FP_SOLVER_PCG_LEARNED learned U-Net preconditioner, plain PCG fallback. */
+enum { FP_SOLVER_PCG = 0, FP_SOLVER_PCG_MIXED = 1, FP_SOLVER_PCG_MG = 2, FP_SOLVER_PCG_LEARNED = 3 };
+
+/* Advection: the reference's adaptive Ralston RK3 (AdvectParticlesFunctor,
+ * FluidSolver3D.cu:1241-1330) or midpoint RK2 with the same substepping. */
+enum { FP_ADVECT_RK3REF = 0, FP_ADVECT_RK2 = 1 };
+
+/* Grid selectors for fp_get_grid / fp_set_grid. */
+enum { FP_GRID_U = 0, FP_GRID_V = 1, FP_GRID_W = 2, FP_GRID_U_SAVED = 3, FP_GRID_V_SAVED = 4,
+       FP_GRID_W_SAVED = 5, FP_GRID_P = 6 };
+
+/* Step phases for fp_run_phase, in frameStep order (FluidSolver3D.cu:3030-3098). */
+enum { FP_PHASE_LABEL = 0, FP_PHASE_P2G = 1, FP_PHASE_SAVE = 2, FP_PHASE_FORCES = 3, FP_PHASE_PRESSURE = 4,
+       FP_PHASE_PROJECT = 5, FP_PHASE_BODY = 6, FP_PHASE_G2P = 7, FP_PHASE_ADVECT = 8 };
+
+/* Solver configuration.  Keys and defaults follow main.cpp:17-52 and the
+ * member initialisers of FluidSolver3D.cuh:72-80,160-166; the fields after
+ * body_mass are additions whose defaults reproduce the reference's behaviour. */
+typedef struct fp_config {
+    int      dim;                  /* 3 (FluidSolver3D) or 2 (FluidSolver2D)        */
+    float    dx;                   /* "dx"            default 0.1                   */
+    float    dt;                   /* "dt"            default 0.02                  */
+    float    pic_weight;           /* "PIC_WEIGHT"    default 0.01 (alpha)          */
+    int      iter_per_frame;       /* "iterPerFrame"  default 1                     */
+    int      output_format;        /* "outputFormat"  FP_OUT_PLY                    */
+    char     output_template[256]; /* "outputTemplate" "InputData/particles_"       */
+    int      active_body;          /* "activeBody"    default 0                     */
+    float    body_pos[3];          /* "body_x/y/z"    default 0.5                   */
+    float    body_mass;            /* "body_mass"     default 50                    */
+    /* additions */
+    int      ppc;                  /* particles per cell at seeding (reference 4)  */
+    uint32_t seed;                 /* mt19937 seed (the reference: random_device)  */
+    int      solver;               /* FP_SOLVER_*                                   */
+    int      advection;            /* FP_ADVECT_*                                   */
+    float    cfl;                  /* advection C (reference 0.1)                   */
+    double   tol;                  /* relative residual target (default 1e-6)      */
+    int      max_iters;            /* PCG iteration cap (default 20000)            */
+    float    body_radius;          /* analytic sphere SDF radius; 0 = SDF file     */
+    float    body_density;         /* sphere density relative to water            */
+    int      device;               /* CUDA device ordinal; -1 = current device     */
+} fp_config;
+
+/* Per-step statistics: the reference's cudaEvent phase timers
+ * (FluidSolver3D.cuh:112-119) plus solver diagnostics.  Times in ms. */
+typedef struct fp_step_stats {
+    int64_t step;              /* steps taken so far                              */
+    int64_t num_particles;
+    int32_t num_fluid_cells;   /* fluidCellsAmount                                */
+    int32_t pcg_iters;         /* inner PCG iterations of the last solve          */
+    int32_t outer_iters;       /* refinement loops of the last solve              */
+    int32_t fallback;          /* 1 if the learned preconditioner fell back       */
+    int32_t solve_status;      /* FP_OK or the failure of the last solve          */
+    int32_t pad_;
+    double  residual;          /* final true relative residual ||b-Ax||/||b||    */
+    float   t_label, t_p2g, t_forces, t_pressure, t_project, t_body, t_g2p, t_advect;
+    float   t_total;
+    float   pad2_;
+    double  body_pos[3], body_vel[3], body_omega[3], body_angles[3];
+    double  body_force[3], body_torque[3];
+    int64_t kernel_launches;   /* kernels this library launched, cumulative     */
+    float   t_pcg;             /* device time of the PCG kernel(s), last solve  */
+    float   pad3_;
+} fp_step_stats;
+
+typedef struct fp_solver fp_solver;
+
+/* Fill *cfg with the reference defaults. */
+int fp_config_default(fp_config* cfg);
+
+/* Parse a reference config.json (keys of main.cpp:17-52 plus the additions)
+ * into *cfg; missing keys keep their current values.  label_path receives
+ * "inputLabelData" and frames "frameAmount" when non-null. */
+int fp_config_load_json(const char* path, fp_config* cfg, char* label_path, size_t label_path_len, int* frames);
+
+/* FluidSolver3D::FluidSolver3D (FluidSolver3D.cu:4-35).  Grid dimensions come
+ * from fp_load_labels / fp_set_labels, as in the reference's init(). */
+int fp_create(const fp_config* cfg, fp_solver** out);
+int fp_destroy(fp_solver* s);
+const char* fp_last_error(const fp_solver* s);
+
+/* Labels: the reference file format (init, FluidSolver3D.cu:81-153; 2D reader
+ * FluidSolver2D.cu:52-104) or a caller array (n = W*H*D uint8).  Sizes the
+ * grids; SOLID cells stay fixed for the whole run. */
+int fp_load_labels(fp_solver* s, const char* path);
+int fp_set_labels(fp_solver* s, const uint8_t* labels, int W, int H, int D);
+int fp_get_dims(const fp_solver* s, int* W, int* H, int* D);
+
+/* Body SDF (RigidBody::loadSDF, utility.cuh:231-338) from a text file, or the
+ * analytic sphere of fp_config.body_radius when path is NULL. */
+int fp_load_sdf(fp_solver* s, const char* path);
+
+/* Particles: seeding of FLUID cells (seedParticles, FluidSolver3D.cu:213-297)
+ * with a deterministic mt19937(seed); caller arrays; PLY files. */
+int fp_seed_particles(fp_solver* s, int ppc, uint32_t seed);
+int fp_set_particles(fp_solver* s, const float* pos, const float* vel, int64_t n);
+int fp_load_ply(fp_solver* s, const char* path);
+int fp_save_ply(fp_solver* s, const char* path, int format);
+int64_t fp_num_particles(const fp_solver* s);
+int fp_get_particles(fp_solver* s, float* pos, float* vel, int64_t n);
+
+/* One full step (frameStep, FluidSolver3D.cu:3030-3098), n times. */
+int fp_step(fp_solver* s, int n);
+
+/* run() (FluidSolver3D.cu:3100-3163): frames*iter_per_frame + 1 steps with
+ * frame output every iter_per_frame steps (particles PLY/OFF, body PLY and
+ * the body CSV when a body is active). */
+int fp_run(fp_solver* s, int frames);
+
+/* One phase of the step on the current state (diagnostics and parity tests). */
+int fp_run_phase(fp_solver* s, int phase);
+
+/* Grid and label copies (n must equal the grid's element count). */
+int fp_get_grid(fp_solver* s, int which, float* out, int64_t n);
+int fp_set_grid(fp_solver* s, int which, const float* in, int64_t n);
+int fp_get_labels(fp_solver* s, uint8_t* out, int64_t n);
+
+/* Rigid-body kinematic state used by the RHS and projection; setting it
+ * overrides the integrated state (FluidSolver3D.cu:1368-1370). */
+int fp_set_body_state(fp_solver* s, const float* pos, const float* vel, const float* omega);
+
+int fp_stats(const fp_solver* s, fp_step_stats* out);
+
+/* The solver's CUDA stream (a cudaStream_t), for callers that record their
+ * own events or order their own work after the solver's. */
+void* fp_cuda_stream(const fp_solver* s);
+
+/* Pressure solve of the current labels for a caller right-hand side (dense,
+ * W*H*D, zero off FLUID cells); x receives the dense solution.  Uses the
+ * configured solver.  Reports iterations and the true relative residual. */
+int fp_pressure_solve(fp_solver* s, const float* rhs, float* x, int64_t n, int* iters, double* relres);
+
+/* Stand-alone SPD solve of an upper-triangle CSR matrix (the storage passed to
+ * cuDSS with CUDSS_MVIEW_UPPER, FluidSolver3D.cu:1932-1945) by GPU CG with
+ * FP64 vectors: the known-answer path of test.cu:223-395.  Host arrays. */
+int fp_solve_csr_upper(int n, const int* offsets, const int* cols, const double* vals, const double* b, double* x,
+                       double tol, int max_iters, int* iters, double* relres);
+
+/* Host-only readers (no GPU needed).  fp_read_label_file parses a reference
+ * label file (dim 3: FluidSolver3D.cu:81-153, dim 2: FluidSolver2D.cu:52-104);
+ * call with out = NULL to get dims[0..2] = W, H, D (D = 1 in 2D) first.
+ * fp_read_ply_file reads ascii or binary_little_endian PLY vertices; call with
+ * pos = NULL to get *n; vel may be NULL; *has_vel reports vx vy vz. */
+int fp_read_label_file(const char* path, int dim, int* dims, uint8_t* out);
+int fp_read_ply_file(const char* path, int64_t* n, float* pos, float* vel, int* has_vel);
+
+/* Library version string. */
+const char* fp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLUIDPRJCT_H */

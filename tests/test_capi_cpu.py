@@ -1,0 +1,150 @@
+"""The C ABI without a GPU: symbols, defaults, host-side parsers, scenes."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+HEADER = os.path.join(ROOT, "include", "fluidprjct.h")
+
+
+def header_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fp_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from fluidprjct_b200 import capi
+    lib = capi.lib()
+    syms = header_symbols()
+    assert len(syms) >= 25
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+    # and the binding declares a signature for each of them
+    assert sorted(capi.declared_symbols()) == syms
+    out = subprocess.run(["nm", "-D", "--defined-only", capi.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (fp_\w+)", out))
+    assert set(syms) <= exported
+
+
+def test_config_defaults_match_reference():
+    from fluidprjct_b200 import capi
+    c = capi.default_config()
+    # main.cpp:18-48 and FluidSolver3D.cuh:72, FluidSolver3D.cu:3092
+    assert (c.dim, c.iter_per_frame, c.ppc) == (3, 1, 4)
+    f32 = lambda x: float(np.float32(x))
+    assert (c.dt, c.dx, c.pic_weight, c.cfl, c.body_mass) == (f32(0.02), f32(0.1), f32(0.01), f32(0.1), 50.0)
+    assert list(c.body_pos) == pytest.approx([0.5, 0.5, 0.5])
+    assert c.output_template == b"InputData/particles_"
+    assert c.solver == capi.SOLVER_PCG and c.advection == capi.ADVECT_RK3REF
+
+
+def test_config_json(tmp_path):
+    from fluidprjct_b200 import capi
+    p = tmp_path / "config.json"
+    # the keys of the reference's InputData/config.json:1-14 plus additions
+    p.write_text('{"dt": 0.005, "dx": 0.02, "PIC_WEIGHT": 0.001, "iterPerFrame": 1, "outputFormat": "PLY",\n'
+                 ' "inputLabelData": "InputData/labels_gaussian.txt", "frameAmount": 280,\n'
+                 ' "outputTemplate": "OutputData/particles_", "body_x": 0.5, "body_y": 0.2, "body_z": 0.5,\n'
+                 ' "body_mass": 0.03, "activeBody": true, "solver": "pcg_mixed", "advection": "rk2",'
+                 ' "seed": 7, "nested": {"a": [1, 2, {"b": null}]}}')
+    cfg = capi.default_config()
+    lab = C.create_string_buffer(256)
+    frames = C.c_int(0)
+    rc = capi.lib().fp_config_load_json(str(p).encode(), C.byref(cfg), lab, 256, C.byref(frames))
+    assert rc == capi.FP_OK
+    f32 = lambda x: float(np.float32(x))
+    assert (cfg.dt, cfg.dx, cfg.pic_weight, cfg.body_mass) == (f32(0.005), f32(0.02), f32(0.001), f32(0.03))
+    assert cfg.active_body == 1
+    assert list(cfg.body_pos) == pytest.approx([0.5, 0.2, 0.5])
+    assert cfg.output_template == b"OutputData/particles_" and cfg.output_format == capi.OUT_PLY
+    assert lab.value == b"InputData/labels_gaussian.txt" and frames.value == 280
+    assert cfg.solver == capi.SOLVER_PCG_MIXED and cfg.advection == capi.ADVECT_RK2 and cfg.seed == 7
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"dt": 0.1, "solver": "magic"}')
+    assert capi.lib().fp_config_load_json(str(bad).encode(), C.byref(cfg), None, 0, None) == capi.FP_ERR_IO
+
+
+@pytest.mark.parametrize("name,dim", [("labels_simple3d", 3), ("labels_3d_sphere", 3), ("labels_bathymetry", 3),
+                                      ("labels_simple", 2), ("labels_colimn", 2)])
+def test_host_label_reader(golden_labels, name, dim, tmp_path):
+    from fluidprjct_b200 import capi, scenes
+    exp = golden_labels[name]
+    path = os.path.join("/root/reference/InputData", name + ".txt")
+    if not os.path.exists(path):
+        path = str(tmp_path / "l.txt")
+        (scenes.write_labels3d if dim == 3 else scenes.write_labels2d)(path, exp)
+    assert np.array_equal(capi.read_label_file(path, dim), exp)
+
+
+def test_label_reader_rejects_corrupt_files(tmp_path):
+    from fluidprjct_b200 import capi
+    p = tmp_path / "bad.txt"
+    p.write_text("3 3 1\nSSS\nSXS\nSSS\n")
+    with pytest.raises(capi.FluidError):
+        capi.read_label_file(p, 3)
+    p.write_text("3 3 2\nSSS\nSFS\nSSS\n")  # truncated
+    with pytest.raises(capi.FluidError):
+        capi.read_label_file(p, 3)
+    with pytest.raises(capi.FluidError):
+        capi.read_label_file(tmp_path / "missing.txt", 3)
+
+
+def test_ply_reader_ascii_and_binary(golden_particles, tmp_path):
+    from fluidprjct_b200 import capi
+    pos = golden_particles
+    # ascii, positions only (the reference's writer, utility.cu:91-109)
+    a = tmp_path / "a.ply"
+    with open(a, "w") as f:
+        f.write(f"ply\nformat ascii 1.0\nelement vertex {len(pos)}\nproperty float x\nproperty float y\n"
+                "property float z\nend_header\n")
+        np.savetxt(f, pos, fmt="%.9g")
+    p2, v2 = capi.read_ply_file(a)
+    assert v2 is None and np.array_equal(p2, pos)
+    if os.path.exists("/root/reference/InputData/particles_-1.ply"):
+        p3, _ = capi.read_ply_file("/root/reference/InputData/particles_-1.ply")
+        assert np.array_equal(p3, pos)
+    # binary little endian with velocities and an extra double property
+    rng = np.random.default_rng(1)
+    vel = rng.standard_normal(pos.shape).astype(np.float32)
+    b = tmp_path / "b.ply"
+    rec = np.zeros(len(pos), dtype=[("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("q", "<f8"), ("vx", "<f4"),
+                                    ("vy", "<f4"), ("vz", "<f4")])
+    rec["x"], rec["y"], rec["z"] = pos.T
+    rec["vx"], rec["vy"], rec["vz"] = vel.T
+    with open(b, "wb") as f:
+        f.write((f"ply\nformat binary_little_endian 1.0\nelement vertex {len(pos)}\nproperty float x\n"
+                 "property float y\nproperty float z\nproperty double q\nproperty float vx\nproperty float vy\n"
+                 "property float vz\nend_header\n").encode())
+        f.write(rec.tobytes())
+    p4, v4 = capi.read_ply_file(b)
+    assert np.array_equal(p4, pos) and np.array_equal(v4, vel)
+    # truncated files fail loudly
+    t = tmp_path / "t.ply"
+    t.write_bytes(open(b, "rb").read()[:-10])
+    with pytest.raises(capi.FluidError):
+        capi.read_ply_file(t)
+
+
+def test_scene_cell_counts():
+    from fluidprjct_b200 import scenes
+    lab = scenes.dam_break_3d(128)
+    assert int((lab == 1).sum()) == 50 * 76 * 126 == 478800   # x<0.4, y<0.6, z<1 inside the walls
+    lab2 = scenes.dam_break_2d(64)
+    assert int((lab2 == 1).sum()) == 25 * 31 == 775
+    pool = scenes.pool_3d(160)
+    assert int((pool == 1).sum()) == 158 * 55 * 158
+    assert (lab[0] == 0).all() and (lab[:, -1] == 0).all() and (lab[:, :, 0] == 0).all()
+
+
+def test_scene_file_round_trip(tmp_path):
+    from fluidprjct_b200 import capi, scenes
+    lab = scenes.random_boxes(5, n=20)
+    p = tmp_path / "s.txt"
+    scenes.write_labels3d(p, lab)
+    assert np.array_equal(capi.read_label_file(p, 3), lab)

@@ -1,0 +1,141 @@
+"""The CPU oracle checked against the reference's own fixtures and KATs.
+
+Pins (all from the reference checkout, see tests/golden/make_golden.py):
+  * InputData/particles_-1.ply binned at dx = 0.02: 11,036 cells, 4 particles
+    each, cells i in [4,45], j in [1,8], k in [4,45];
+  * InputData/labels_*.txt cell counts through the oracle's readers;
+  * labels_simple3d.txt: the upper-CSR Poisson operator of MatrixBuilder3D /
+    MatrixFiller3D (FluidSolver3D.cu:1598-1777), checked by hand;
+  * src/FluidSim/test.cu's 5x5 SPD system, x = 1..5 to 2e-15.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, rel_l2
+
+REF = "/root/reference/InputData"
+
+
+def test_particles_m1_binning(O, golden, golden_particles):
+    pos = golden_particles
+    meta = golden["particles_m1"]
+    assert len(pos) == meta["n"] == 44144
+    keys, counts = O.bin3d(pos, (50, 50, 50), meta["dx"])
+    occupied = np.nonzero(counts)[0]
+    assert len(occupied) == meta["cells"] == 11036
+    assert set(np.unique(counts[occupied])) == {4}
+    i, j, k = occupied % 50, (occupied // 50) % 50, occupied // 2500
+    assert (i.min(), i.max(), j.min(), j.max(), k.min(), k.max()) == (4, 45, 1, 8, 4, 45)
+    # keys are consistent with counts
+    assert np.array_equal(np.bincount(keys, minlength=50 ** 3), counts)
+
+
+@pytest.mark.parametrize("name", ["labels_simple3d", "labels_3d_sphere", "labels_bathymetry"])
+def test_label_reader_3d(O, golden, golden_labels, name, tmp_path):
+    exp = golden_labels[name]
+    path = os.path.join(REF, name + ".txt")
+    if not os.path.exists(path):  # away from the reference checkout: rebuild the file in its format
+        from fluidprjct_b200.scenes import write_labels3d
+        path = str(tmp_path / (name + ".txt"))
+        write_labels3d(path, exp)
+    lab = O.read_labels3d(path)
+    assert np.array_equal(lab, exp)
+    c = golden["labels"][name]
+    assert int((lab == 1).sum()) == c["F"] and int((lab == 0).sum()) == c["S"]
+
+
+@pytest.mark.parametrize("name", ["labels_simple", "labels_colimn"])
+def test_label_reader_2d(O, golden, golden_labels, name, tmp_path):
+    exp = golden_labels[name]
+    path = os.path.join(REF, name + ".txt")
+    if not os.path.exists(path):
+        from fluidprjct_b200.scenes import write_labels2d
+        path = str(tmp_path / (name + ".txt"))
+        write_labels2d(path, exp)
+    lab = O.read_labels2d(path)
+    assert np.array_equal(lab, exp)
+    assert int((lab == 1).sum()) == golden["labels"][name]["F"]
+
+
+def test_simple3d_poisson_operator(O):
+    lab = O.read_labels3d(os.path.join(GOLDEN, "labels_simple3d.txt"))
+    off, cols, vals = O.build_csr_upper(lab)
+    # 6 FLUID cells (1..3, 1..2) of a 5x4x1 grid; fluid numbering i-fastest.
+    # Diagonal = in-domain FLUID/AIR neighbours; -1 to higher-numbered FLUID.
+    assert off.tolist() == [0, 3, 6, 8, 10, 12, 13]
+    assert cols.tolist() == [0, 1, 3, 1, 2, 4, 2, 5, 3, 4, 4, 5, 5]
+    assert vals.tolist() == [2, -1, -1, 3, -1, -1, 2, -1, 2, -1, 3, -1, 2]
+
+
+def test_cudss_kat_5x5(O, golden):
+    kat = golden["kat"]
+    x, it, rr = O.cg_csr_upper(kat["offsets"], kat["cols"], kat["vals"], kat["b"], tol=1e-15)
+    assert np.max(np.abs(x - np.array(kat["x"]))) <= 1e-14
+    assert it <= 5
+
+
+def test_dense_solver_matches_csr(O):
+    """The oracle's matrix-free FP64 operator equals its CSR form."""
+    from fluidprjct_b200.scenes import box_3d
+    lab = box_3d(9, 8, 7, 0.1, 0.55, 0.45, 0.5)
+    lab[3, 2, 2] = 0  # an interior obstacle cell
+    sim = O.Sim3(9, 8, 7, 0.1, 0.01, fp64=True)
+    sim.set_labels(lab)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(lab.size) * (lab.ravel() == 1)
+    ax = sim.apply(x)
+    off, cols, vals = O.build_csr_upper(lab)
+    fl = np.nonzero(lab.ravel() == 1)[0]
+    xs = x[fl]
+    y = np.zeros(len(fl))
+    for r in range(len(fl)):
+        for e in range(off[r], off[r + 1]):
+            c = cols[e]
+            y[r] += vals[e] * xs[c]
+            if c != r:
+                y[c] += vals[e] * xs[r]
+    assert np.allclose(ax[fl], y, rtol=0, atol=1e-12)
+    b = rng.standard_normal(lab.size) * (lab.ravel() == 1)
+    sol, it = sim.solve(b)
+    assert rel_l2(sim.apply(sol)[fl], b[fl]) < 1e-10
+
+
+def _dam_scene(O, fp64, W=14, H=12, D=10, dx=0.08, dt=0.01, seed=3):
+    from fluidprjct_b200.scenes import box_3d
+    lab = box_3d(W, H, D, dx, 0.5, 0.55, 0.6)
+    pos = O.seed3d(lab, dx, 8, seed)
+    rng = np.random.default_rng(seed)
+    vel = rng.uniform(-0.5, 0.5, pos.shape).astype(np.float32)
+    sim = O.Sim3(W, H, D, dx, dt, fp64=fp64, pic_weight=0.05, tol=1e-12)
+    sim.set_labels(lab)
+    sim.set_particles(pos, vel)
+    return sim, lab, pos, vel
+
+
+def test_oracle_fp32_vs_fp64_one_step(O):
+    s32, *_ = _dam_scene(O, False)
+    s64, *_ = _dam_scene(O, True)
+    s32.step(1)
+    s64.step(1)
+    for g in (O.GRID_U, O.GRID_V, O.GRID_W, O.GRID_P):
+        assert rel_l2(s32.grid(g), s64.grid(g)) < 1e-5
+    p32, v32 = s32.particles()
+    p64, v64 = s64.particles()
+    assert rel_l2(v32, v64) < 1e-5
+    assert np.max(np.abs(p32 - p64)) < 1e-5
+
+
+def test_oracle_projection_is_divergence_free(O):
+    """After pressure + projection (FP64), the discrete divergence at FLUID
+    cells vanishes -- the defining property of the reference's projection."""
+    sim, lab, _, _ = _dam_scene(O, True)
+    for ph in (O.PH_LABEL, O.PH_P2G, O.PH_SAVE, O.PH_FORCES):
+        sim.phase(ph)
+    b_before = sim.rhs()
+    sim.phase(O.PH_PRESSURE)
+    sim.phase(O.PH_PROJECT)
+    b_after = sim.rhs()
+    fl = sim.labels().ravel() == 1
+    assert np.linalg.norm(b_after[fl]) < 1e-8 * np.linalg.norm(b_before[fl])
