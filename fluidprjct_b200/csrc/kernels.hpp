@@ -22,19 +22,25 @@ struct PcgOut {
     double rz;
 };
 
-// Device buffers of the pressure system (compact over FLUID cells, except dd).
+// Device buffers of the pressure system.  Compact arrays are indexed by the
+// fluid number n (i-fastest order of FLUID cells); padded dense grids have a
+// one-cell zero halo, (W+2)*(H+2)*(D+2) entries.  Vector storage is sized for
+// FP64 and reinterpreted as FP32 by the mixed-precision solves.
 struct PressureBufs {
     int* nf;              // [1] number of FLUID cells
-    int* fidx;            // [nc] cell index of the n-th FLUID cell
+    int* fidx;            // [nc] padded index of the n-th FLUID cell
     uint8_t* diag;        // [nc] diagonal of the unit operator (compact)
     float* b;             // [nc] right-hand side (compact)
     float* bin;           // [nc] right-hand side of an inner refinement solve
-    float* x;             // [nc] solution (compact)
-    float* r;             // [nc] residual (compact)
-    float* q;             // [nc] A*d (compact)
-    float* dd;            // [nc] search direction (dense, zero off FLUID)
+    void* R[2];           // padded dense residual (double-buffered)
+    void* Wv[2];          // padded dense w = A M^-1 r
+    void* S[2];           // padded dense s = A p
+    void* invd;           // padded dense 1/diag
+    void* P;              // [nc] compact search direction
+    void* X;              // [nc] compact solution
     double* x64;          // [nc] refinement accumulator (compact)
-    double* part;         // [3 * max_blocks] per-block partial sums
+    double* xd;           // padded dense FP64 copy of x64
+    double* part;         // [6 * max_blocks] per-block partial sums
     GridBar* bar;         // [1]
     PcgOut* out;          // [1]
     int* tile_sums;       // scan scratch
@@ -63,18 +69,22 @@ void launch_copy(const float* src, float* dst, int64_t n, cudaStream_t st);
 // computed rhs (caller-provided system).
 void launch_pressure_setup(const uint8_t* labels, const float* u, const float* v, const float* w, Dims g, float dt,
                            BodyKin body, const float* rhs_dense, float* p, PressureBufs& pb, cudaStream_t st);
-// Persistent cooperative PCG (Jacobi).  x starts at zero; solves A x = b to
-// ||r||/||b|| <= tol.  Results in pb.out.
-int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, double tol, int maxit, int max_blocks, cudaStream_t st);
+// Persistent cooperative Jacobi PCG (Chronopoulos-Gear form, one grid barrier
+// per iteration) from x0 = 0 for A x = rhs to ||r||/||rhs|| <= tol; vectors in
+// FP64 (fp64 = 1) or FP32 (0), reductions always FP64.  Solution in pb.X,
+// diagnostics in pb.out.  The padded work grids must be zero on entry;
+// launch_pcg_clear restores that after a solve.
+int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, int fp64, double tol, int maxit, cudaStream_t st);
+void launch_pcg_clear(PressureBufs& pb, int fp64, int with_invd, cudaStream_t st);
 int pcg_max_blocks();
-// p[fidx[n]] = x[n] (x64 when use64).
-void launch_scatter_p(const PressureBufs& pb, float* p, int use64, Dims g, cudaStream_t st);
-// ||b - A p||^2 and ||b||^2 in FP64 into pb.red[0..1] (p dense float).
-void launch_true_residual(const PressureBufs& pb, const float* p, Dims g, cudaStream_t st);
-// Iterative refinement helpers: r = b - A x64 (FP64, via the dense double
-// scratch xd), and x64 += x.
-void launch_ir_residual(PressureBufs& pb, double* xd, Dims g, cudaStream_t st);
-void launch_ir_update(PressureBufs& pb, double* xd, Dims g, cudaStream_t st);
+// p[cell] = X[n] (src 0: FP32 X, 1: FP64 X, 2: x64).
+void launch_scatter_p(const PressureBufs& pb, float* p, int src, Dims g, cudaStream_t st);
+// ||b - A X||^2 and ||b||^2 in FP64 into pb.red[0..1] (uses R[0] as scratch).
+void launch_true_residual(PressureBufs& pb, int fp64, Dims g, cudaStream_t st);
+// Iterative refinement: bin = float(b - A x64) with the FP64 residual norms in
+// pb.red; x64 += X (FP32) and its padded copy xd.
+void launch_ir_residual(PressureBufs& pb, Dims g, cudaStream_t st);
+void launch_ir_update(PressureBufs& pb, Dims g, cudaStream_t st);
 
 // -------- projection (kernels_pressure.cu) --------
 void launch_project(float* u, float* v, float* w, const float* p, const uint8_t* labels, Dims g, float dt, BodyKin b,

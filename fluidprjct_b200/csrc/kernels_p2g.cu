@@ -8,16 +8,98 @@
 // (:700-761, gravity on every face with the x > (float)INT_MIN test).
 //
 // B200 design: particles are sorted by cell, so each CTA owns a brick of
-// BX x BY x BZ cells and the faces of those cells.  It reads the particles of
-// the brick plus a one-cell halo (contiguous runs per (j,k) row of cells),
-// splats them into shared-memory accumulators, and writes each owned face
-// once: no global atomics, no accumulator arrays in HBM, coalesced particle
-// loads.  Halo particles are read by up to 8 CTAs (from L2).
+// BX x BY x BZ cells and the faces of those cells.  One thread per cell of
+// the brick plus a one-cell halo walks that cell's (contiguous) particles and
+// sums their contributions to the 2x3x3 faces the cell can reach in
+// registers; it then adds the faces owned by the brick into shared-memory
+// accumulators (one atomic per face and cell instead of one per particle and
+// corner), and the CTA writes each owned face once: no global atomics and no
+// accumulator arrays in HBM.  Halo cells are read by up to 8 CTAs (from L2).
 #include "kernels.hpp"
 
 namespace fp {
 
 namespace {
+
+// Slot weights along one axis: slot m is face s0 + m; the particle's two
+// corners are faces base (weight 1 - f) and base + 1 (weight f).
+template <int NS>
+__device__ __forceinline__ void axis_weights(int s0, int base, float f, float (&w)[NS]) {
+#pragma unroll
+    for (int m = 0; m < NS; ++m) {
+        const int face = s0 + m;
+        w[m] = face == base ? 1.0f - f : (face == base + 1 ? f : 0.0f);
+    }
+}
+
+// Accumulates one velocity component of the particles [q0, q1) of cell
+// (ci, cj, ck) over the faces that cell can reach -- NX x NY x NZ slots whose
+// first face is (sx0, sy0, sz0) -- and adds the owned ones into shared memory.
+// COMP selects the component and its base-index rules (AccumulateVelocities,
+// FluidSolver3D.cu:465-574); weights are (wx*wy)*wz and contributions
+// vel*wgt, rounded as in the reference.
+template <int COMP, int NX, int NY, int NZ>
+__device__ __forceinline__ void splat_cell(const float4* __restrict__ pos, const float4* __restrict__ vel, int q0,
+                                           int q1, int ci, int cj, int ck, const Dims& g, float* s_num, float* s_den,
+                                           int fx0, int fx1, int fy0, int fy1, int fz0, int fz1, int lsx, int lsy) {
+    const int W = g.W, H = g.H, D = g.D;
+    const int sx0 = COMP == 0 ? ci : ci - 1, sy0 = COMP == 1 ? cj : cj - 1, sz0 = COMP == 2 ? ck : ck - 1;
+    float an[NX * NY * NZ], ad[NX * NY * NZ];
+#pragma unroll
+    for (int m = 0; m < NX * NY * NZ; ++m) { an[m] = 0.0f; ad[m] = 0.0f; }
+    const float dx = g.dx;
+    for (int q = q0; q < q1; ++q) {
+        const float4 P = pos[q];
+        const float4 V = vel[q];
+        const float rx = P.x / dx, ry = P.y / dx, rz = P.z / dx;
+        int bi, bj, bk;
+        float fx, fy, fz, vc;
+        if (COMP == 0) {
+            bi = clampi(int(floorf(rx)), 0, W); bj = clampi(int(floorf(ry - 0.5f)), 0, H - 1);
+            bk = clampi(int(floorf(rz - 0.5f)), 0, D - 1);
+            fx = clamp01(rx - float(bi)); fy = clamp01((ry - 0.5f) - float(bj)); fz = clamp01((rz - 0.5f) - float(bk));
+            vc = V.x;
+        } else if (COMP == 1) {
+            bi = clampi(int(floorf(rx - 0.5f)), 0, W - 1); bj = clampi(int(floorf(ry)), 0, H);
+            bk = clampi(int(floorf(rz - 0.5f)), 0, D - 1);
+            fx = clamp01((rx - 0.5f) - float(bi)); fy = clamp01(ry - float(bj)); fz = clamp01((rz - 0.5f) - float(bk));
+            vc = V.y;
+        } else {
+            bi = clampi(int(floorf(rx - 0.5f)), 0, W - 1); bj = clampi(int(floorf(ry - 0.5f)), 0, H - 1);
+            bk = clampi(int(floorf(rz)), 0, D);
+            fx = clamp01((rx - 0.5f) - float(bi)); fy = clamp01((ry - 0.5f) - float(bj)); fz = clamp01(rz - float(bk));
+            vc = V.z;
+        }
+        float wx[NX], wy[NY], wz[NZ];
+        axis_weights<NX>(sx0, bi, fx, wx);
+        axis_weights<NY>(sy0, bj, fy, wy);
+        axis_weights<NZ>(sz0, bk, fz, wz);
+#pragma unroll
+        for (int c = 0; c < NZ; ++c)
+#pragma unroll
+            for (int b = 0; b < NY; ++b)
+#pragma unroll
+                for (int a = 0; a < NX; ++a) {
+                    const float wgt = wx[a] * wy[b] * wz[c];
+                    const int m = a + NX * (b + NY * c);
+                    an[m] += __fmul_rn(vc, wgt);
+                    ad[m] += wgt;
+                }
+    }
+#pragma unroll
+    for (int c = 0; c < NZ; ++c)
+#pragma unroll
+        for (int b = 0; b < NY; ++b)
+#pragma unroll
+            for (int a = 0; a < NX; ++a) {
+                const int m = a + NX * (b + NY * c);
+                const int fi = sx0 + a, fj = sy0 + b, fk = sz0 + c;
+                if (ad[m] == 0.0f || fi < fx0 || fi > fx1 || fj < fy0 || fj > fy1 || fk < fz0 || fk > fz1) continue;
+                const int sidx = (fi - fx0) + lsx * ((fj - fy0) + lsy * (fk - fz0));
+                atomicAdd(&s_num[sidx], an[m]);
+                atomicAdd(&s_den[sidx], ad[m]);
+            }
+}
 
 template <int BX, int BY, int BZ, int NT>
 __global__ void __launch_bounds__(NT) k_p2g(const float4* __restrict__ pos, const float4* __restrict__ vel,
@@ -26,11 +108,8 @@ __global__ void __launch_bounds__(NT) k_p2g(const float4* __restrict__ pos, cons
                                             float* __restrict__ us, float* __restrict__ vs, float* __restrict__ ws,
                                             int fused) {
     constexpr int NU = (BX + 1) * BY * BZ, NV = BX * (BY + 1) * BZ, NW = BX * BY * (BZ + 1);
-    constexpr int MAXROWS = (BY + 2) * (BZ + 2);
     __shared__ float s_num[NU + NV + NW];
     __shared__ float s_den[NU + NV + NW];
-    __shared__ int s_row_begin[MAXROWS];
-    __shared__ int s_row_pref[MAXROWS + 1];
 
     const int W = g.W, H = g.H, D = g.D;
     const int nbx = (W + BX - 1) / BX, nby = (H + BY - 1) / BY;
@@ -39,133 +118,29 @@ __global__ void __launch_bounds__(NT) k_p2g(const float4* __restrict__ pos, cons
 
     for (int t = threadIdx.x; t < NU + NV + NW; t += NT) { s_num[t] = 0.0f; s_den[t] = 0.0f; }
 
-    // Particle rows of the halo region [i0-1, i0+BX] x [j0-1, j0+BY] x [k0-1, k0+BZ].
-    const int ilo = max(i0 - 1, 0), ihi = min(i0 + BX, W - 1);
-    const int jlo = max(j0 - 1, 0), jhi = min(j0 + BY, H - 1);
-    const int klo = max(k0 - 1, 0), khi = min(k0 + BZ, D - 1);
-    const int nrj = jhi - jlo + 1, nrows = nrj * (khi - klo + 1);
-    for (int r = threadIdx.x; r < nrows; r += NT) {
-        int rj = jlo + r % nrj, rk = klo + r / nrj;
-        int c0 = ilo + rj * W + rk * W * H, c1 = ihi + rj * W + rk * W * H;
-        int b0 = start[c0];
-        s_row_begin[r] = b0;
-        s_row_pref[r + 1] = start[c1 + 1] - b0;
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {  // inclusive scan of the row lengths by one warp
-        int carry = 0;
-        for (int base = 0; base < nrows; base += 32) {
-            int r = base + threadIdx.x;
-            int x = r < nrows ? s_row_pref[r + 1] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, x, o);
-                if ((threadIdx.x & 31) >= o) x += y;
-            }
-            if (r < nrows) s_row_pref[r + 1] = carry + x;
-            carry += __shfl_sync(0xffffffffu, x, 31);
-        }
-        if (threadIdx.x == 0) s_row_pref[0] = 0;
-    }
-    __syncthreads();
-
-    // Owned face ranges (inclusive upper bounds); the last brick on an axis
-    // also owns the far boundary face of that axis' component.
+    // Owned face ranges (inclusive); the last brick on an axis also owns the
+    // far boundary face of that axis' component.
     const int ie = min(i0 + BX, W) - 1, je = min(j0 + BY, H) - 1, ke = min(k0 + BZ, D) - 1;
     const int iue = (i0 + BX >= W) ? W : ie;
     const int jve = (j0 + BY >= H) ? H : je;
     const int kwe = (k0 + BZ >= D) ? D : ke;
+    __syncthreads();
 
-    const int total = s_row_pref[nrows];
-    const float dx = g.dx;
-    for (int t = threadIdx.x; t < total; t += NT) {
-        int lo = 0, hi = nrows - 1;  // last row with pref <= t
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (s_row_pref[mid] <= t) lo = mid; else hi = mid - 1;
-        }
-        const int q = s_row_begin[lo] + (t - s_row_pref[lo]);
-        const float4 P = pos[q];
-        const float4 V = vel[q];
-        const float rx = P.x / dx, ry = P.y / dx, rz = P.z / dx;
-        // U component (AccumulateVelocities, FluidSolver3D.cu:465-498)
-        {
-            int iU = clampi(int(floorf(rx)), 0, W), jU = clampi(int(floorf(ry - 0.5f)), 0, H - 1),
-                kU = clampi(int(floorf(rz - 0.5f)), 0, D - 1);
-            float fx = clamp01(rx - float(iU)), fy = clamp01((ry - 0.5f) - float(jU)), fz = clamp01((rz - 0.5f) - float(kU));
-#pragma unroll
-            for (int dz = 0; dz < 2; ++dz) {
-                int k = kU + dz;
-                if (k >= D || k < k0 || k > ke) continue;
-#pragma unroll
-                for (int dy = 0; dy < 2; ++dy) {
-                    int j = jU + dy;
-                    if (j >= H || j < j0 || j > je) continue;
-#pragma unroll
-                    for (int dxx = 0; dxx < 2; ++dxx) {
-                        int i = iU + dxx;
-                        if (i > W || i < i0 || i > iue) continue;
-                        float wx = dxx == 0 ? 1.0f - fx : fx, wy = dy == 0 ? 1.0f - fy : fy, wz = dz == 0 ? 1.0f - fz : fz;
-                        float wgt = wx * wy * wz;
-                        int s = (i - i0) + (BX + 1) * ((j - j0) + BY * (k - k0));
-                        atomicAdd(&s_num[s], __fmul_rn(V.x, wgt));
-                        atomicAdd(&s_den[s], wgt);
-                    }
-                }
-            }
-        }
-        // V component (:503-536)
-        {
-            int iV = clampi(int(floorf(rx - 0.5f)), 0, W - 1), jV = clampi(int(floorf(ry)), 0, H),
-                kV = clampi(int(floorf(rz - 0.5f)), 0, D - 1);
-            float fx = clamp01((rx - 0.5f) - float(iV)), fy = clamp01(ry - float(jV)), fz = clamp01((rz - 0.5f) - float(kV));
-#pragma unroll
-            for (int dz = 0; dz < 2; ++dz) {
-                int k = kV + dz;
-                if (k >= D || k < k0 || k > ke) continue;
-#pragma unroll
-                for (int dy = 0; dy < 2; ++dy) {
-                    int j = jV + dy;
-                    if (j > H || j < j0 || j > jve) continue;
-#pragma unroll
-                    for (int dxx = 0; dxx < 2; ++dxx) {
-                        int i = iV + dxx;
-                        if (i >= W || i < i0 || i > ie) continue;
-                        float wx = dxx == 0 ? 1.0f - fx : fx, wy = dy == 0 ? 1.0f - fy : fy, wz = dz == 0 ? 1.0f - fz : fz;
-                        float wgt = wx * wy * wz;
-                        int s = NU + (i - i0) + BX * ((j - j0) + (BY + 1) * (k - k0));
-                        atomicAdd(&s_num[s], __fmul_rn(V.y, wgt));
-                        atomicAdd(&s_den[s], wgt);
-                    }
-                }
-            }
-        }
-        // W component (:541-574)
-        {
-            int iW = clampi(int(floorf(rx - 0.5f)), 0, W - 1), jW = clampi(int(floorf(ry - 0.5f)), 0, H - 1),
-                kW = clampi(int(floorf(rz)), 0, D);
-            float fx = clamp01((rx - 0.5f) - float(iW)), fy = clamp01((ry - 0.5f) - float(jW)), fz = clamp01(rz - float(kW));
-#pragma unroll
-            for (int dz = 0; dz < 2; ++dz) {
-                int k = kW + dz;
-                if (k > D || k < k0 || k > kwe) continue;
-#pragma unroll
-                for (int dy = 0; dy < 2; ++dy) {
-                    int j = jW + dy;
-                    if (j >= H || j < j0 || j > je) continue;
-#pragma unroll
-                    for (int dxx = 0; dxx < 2; ++dxx) {
-                        int i = iW + dxx;
-                        if (i >= W || i < i0 || i > ie) continue;
-                        float wx = dxx == 0 ? 1.0f - fx : fx, wy = dy == 0 ? 1.0f - fy : fy, wz = dz == 0 ? 1.0f - fz : fz;
-                        float wgt = wx * wy * wz;
-                        int s = NU + NV + (i - i0) + BX * ((j - j0) + BY * (k - k0));
-                        atomicAdd(&s_num[s], __fmul_rn(V.z, wgt));
-                        atomicAdd(&s_den[s], wgt);
-                    }
-                }
-            }
-        }
+    // Cells whose particles reach an owned face: the brick plus one halo cell.
+    const int ilo = max(i0 - 1, 0), ihi = min(i0 + BX, W - 1);
+    const int jlo = max(j0 - 1, 0), jhi = min(j0 + BY, H - 1);
+    const int klo = max(k0 - 1, 0), khi = min(k0 + BZ, D - 1);
+    const int ni = ihi - ilo + 1, nj = jhi - jlo + 1, ncell = ni * nj * (khi - klo + 1);
+    for (int t = threadIdx.x; t < ncell; t += NT) {
+        const int ci = ilo + t % ni, cj = jlo + (t / ni) % nj, ck = klo + t / (ni * nj);
+        const int c = ci + cj * W + ck * W * H;
+        const int q0 = start[c], q1 = start[c + 1];
+        if (q0 == q1) continue;
+        splat_cell<0, 2, 3, 3>(pos, vel, q0, q1, ci, cj, ck, g, s_num, s_den, i0, iue, j0, je, k0, ke, BX + 1, BY);
+        splat_cell<1, 3, 2, 3>(pos, vel, q0, q1, ci, cj, ck, g, s_num + NU, s_den + NU, i0, ie, j0, jve, k0, ke, BX,
+                               BY + 1);
+        splat_cell<2, 3, 3, 2>(pos, vel, q0, q1, ci, cj, ck, g, s_num + NU + NV, s_den + NU + NV, i0, ie, j0, je, k0,
+                               kwe, BX, BY);
     }
     __syncthreads();
 
@@ -181,30 +156,30 @@ __global__ void __launch_bounds__(NT) k_p2g(const float4* __restrict__ pos, cons
         }
     };
     {
-        const int ni = iue - i0 + 1, nj = je - j0 + 1, nk = ke - k0 + 1;
-        for (int t = threadIdx.x; t < ni * nj * nk; t += NT) {
-            int li = t % ni, lj = (t / ni) % nj, lk = t / (ni * nj);
-            int s = li + (BX + 1) * (lj + BY * lk);
+        const int ni2 = iue - i0 + 1, nj2 = je - j0 + 1, nk2 = ke - k0 + 1;
+        for (int t = threadIdx.x; t < ni2 * nj2 * nk2; t += NT) {
+            int li = t % ni2, lj = (t / ni2) % nj2, lk = t / (ni2 * nj2);
+            int sidx = li + (BX + 1) * (lj + BY * lk);
             int64_t idx = int64_t(i0 + li) + int64_t(j0 + lj) * (W + 1) + int64_t(k0 + lk) * (W + 1) * H;
-            finish(s_num[s], s_den[s], grav.x, u, us, idx);
+            finish(s_num[sidx], s_den[sidx], grav.x, u, us, idx);
         }
     }
     {
-        const int ni = ie - i0 + 1, nj = jve - j0 + 1, nk = ke - k0 + 1;
-        for (int t = threadIdx.x; t < ni * nj * nk; t += NT) {
-            int li = t % ni, lj = (t / ni) % nj, lk = t / (ni * nj);
-            int s = NU + li + BX * (lj + (BY + 1) * lk);
+        const int ni2 = ie - i0 + 1, nj2 = jve - j0 + 1, nk2 = ke - k0 + 1;
+        for (int t = threadIdx.x; t < ni2 * nj2 * nk2; t += NT) {
+            int li = t % ni2, lj = (t / ni2) % nj2, lk = t / (ni2 * nj2);
+            int sidx = NU + li + BX * (lj + (BY + 1) * lk);
             int64_t idx = int64_t(i0 + li) + int64_t(j0 + lj) * W + int64_t(k0 + lk) * W * (H + 1);
-            finish(s_num[s], s_den[s], grav.y, v, vs, idx);
+            finish(s_num[sidx], s_den[sidx], grav.y, v, vs, idx);
         }
     }
     {
-        const int ni = ie - i0 + 1, nj = je - j0 + 1, nk = kwe - k0 + 1;
-        for (int t = threadIdx.x; t < ni * nj * nk; t += NT) {
-            int li = t % ni, lj = (t / ni) % nj, lk = t / (ni * nj);
-            int s = NU + NV + li + BX * (lj + BY * lk);
+        const int ni2 = ie - i0 + 1, nj2 = je - j0 + 1, nk2 = kwe - k0 + 1;
+        for (int t = threadIdx.x; t < ni2 * nj2 * nk2; t += NT) {
+            int li = t % ni2, lj = (t / ni2) % nj2, lk = t / (ni2 * nj2);
+            int sidx = NU + NV + li + BX * (lj + BY * lk);
             int64_t idx = int64_t(i0 + li) + int64_t(j0 + lj) * W + int64_t(k0 + lk) * W * H;
-            finish(s_num[s], s_den[s], grav.z, w, ws, idx);
+            finish(s_num[sidx], s_den[sidx], grav.z, w, ws, idx);
         }
     }
 }
@@ -224,7 +199,7 @@ __global__ void k_copy(const float* __restrict__ s, float* __restrict__ d, int64
 
 }  // namespace
 
-constexpr int P2G_BX = 16, P2G_BY = 8, P2G_BZ = 8, P2G_NT = 512;
+constexpr int P2G_BX = 16, P2G_BY = 8, P2G_BZ = 8, P2G_NT = 256;
 
 void launch_p2g(const float4* pos, const float4* vel, const int* start, Dims g, float dt, float3 gravity, float* u,
                 float* v, float* w, float* us, float* vs, float* ws, int fused_forces, cudaStream_t st) {

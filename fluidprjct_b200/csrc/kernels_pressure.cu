@@ -140,28 +140,26 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_fluid_build(const uint8_t* __res
 }
 
 // ---------------------------------------------------------------- grid barrier
-// Sense-free generation barrier for a cooperative launch.  The wait is bounded:
-// after ~2^26 polls the block records DEV_TIMEOUT and leaves; every caller
-// checks the status after the barrier and returns, so no block waits forever.
+// Grid barrier for a cooperative launch on one 32-bit word: every block adds
+// 1 except block 0, which adds 2^31 - (nblocks - 1), so the word's top bit
+// flips exactly when the last block arrives and no reset is needed between
+// barriers.  The wait is bounded: after ~2^28 polls the block records
+// DEV_TIMEOUT and leaves; callers check the status after every barrier and
+// return, so no block waits forever.  The fences around the arrival give the
+// barrier release/acquire semantics, so plain (L1-cached) loads after it see
+// every write made before it by any block.
 __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* status) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* vgen = &bar->gen;
-        unsigned gen0 = *vgen;
+        const unsigned inc = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
         __threadfence();
-        unsigned arrived = atomicAdd(&bar->count, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(&bar->count, 0u);
-            __threadfence();
-            atomicAdd(&bar->gen, 1u);
-        } else {
-            long long polls = 0;
-            while (*vgen == gen0) {
-                if (++polls > (1ll << 26)) {
-                    atomicExch(status, DEV_TIMEOUT);
-                    break;
-                }
-                __nanosleep(32);
+        const unsigned old = atomicAdd(&bar->count, inc);
+        volatile unsigned* vc = &bar->count;
+        long long polls = 0;
+        while (((old ^ *vc) & 0x80000000u) == 0u) {
+            if (++polls > (1ll << 28)) {
+                atomicExch(status, DEV_TIMEOUT);
+                break;
             }
         }
         __threadfence();
@@ -218,17 +216,87 @@ __device__ __forceinline__ double2 grid_sum2(const double2* part, int nb) {
     return r;
 }
 
+// Sum of three per-block partial arrays part[0..nb), part[nb..2nb),
+// part[2nb..3nb), returned to every thread of every block.  All threads load
+// (one L2 round trip when nb <= blockDim) and reduce with a fixed tree, so
+// every block obtains the same bits.
+__device__ __forceinline__ double3 grid_sum3(const double* part, int nb) {
+    __shared__ double3 red3[32];
+    __shared__ double3 res3;
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+        a += __ldcg(part + t);
+        b += __ldcg(part + nb + t);
+        c += __ldcg(part + 2 * nb + t);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red3[wid] = make_double3(a, b, c);
+    __syncthreads();
+    if (wid == 0) {
+        double3 r = lane < int(blockDim.x >> 5) ? red3[lane] : make_double3(0.0, 0.0, 0.0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            r.x += __shfl_down_sync(0xffffffffu, r.x, o);
+            r.y += __shfl_down_sync(0xffffffffu, r.y, o);
+            r.z += __shfl_down_sync(0xffffffffu, r.z, o);
+        }
+        if (lane == 0) res3 = r;
+    }
+    __syncthreads();
+    double3 r = res3;
+    __syncthreads();
+    return r;
+}
+
+// Block sum of three doubles; result valid in thread 0.
+__device__ __forceinline__ double3 block_sum3(double a, double b, double c) {
+    __shared__ double3 sh3[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh3[wid] = make_double3(a, b, c);
+    __syncthreads();
+    double3 r = make_double3(0.0, 0.0, 0.0);
+    if (wid == 0) {
+        r = lane < int(blockDim.x >> 5) ? sh3[lane] : make_double3(0.0, 0.0, 0.0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            r.x += __shfl_down_sync(0xffffffffu, r.x, o);
+            r.y += __shfl_down_sync(0xffffffffu, r.y, o);
+            r.z += __shfl_down_sync(0xffffffffu, r.z, o);
+        }
+    }
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+template <class T>
 struct PcgArgs {
     Dims g;
     const int* nf;
-    const int* fidx;
-    const uint8_t* diag;
-    const float* b;
-    float* x;
-    float* r;
-    float* q;
-    float* dd;
-    double2* part;  // [3 * nblocks]
+    const int* fidx;     // padded dense index of the n-th FLUID cell
+    const uint8_t* diag; // compact diagonal
+    const float* b;      // compact right-hand side
+    T* R[2];             // padded dense residual r (double-buffered)
+    T* Wv[2];            // padded dense w = A M^-1 r
+    T* S[2];             // padded dense s = A p
+    T* invd;             // padded dense 1/diag (0 off the fluid)
+    T* P;                // compact search direction
+    T* X;                // compact solution
+    double* part;        // [2 parities][3][nblocks]
     GridBar* bar;
     int* status;
     PcgOut* out;
@@ -236,96 +304,129 @@ struct PcgArgs {
     int maxit;
 };
 
-__global__ void __launch_bounds__(PCG_THREADS) k_pcg(PcgArgs a) {
+// Jacobi-preconditioned conjugate gradients in the Chronopoulos-Gear form
+// (one reduction phase per iteration):
+//   s_i = w_i + b_i s_{i-1}; p_i = u_i + b_i p_{i-1}; x += a_i p_i;
+//   r_{i+1} = r_i - a_i s_i; u = M^-1 r; w_{i+1} = A u_{i+1};
+//   g = (r,u), d = (w,u); b = g_new/g; a = g_new/(d - b g_new/a_old).
+// The stencil of w_{i+1} needs u_{i+1} at the six neighbours; each thread
+// recomputes those from the neighbours' r_i, w_i, s_{i-1} of the previous
+// iteration (double-buffered, fused multiply-adds pinned with __fma_rn so the
+// owner and its neighbours produce the same bits), so a single grid barrier
+// per iteration both publishes the vectors and completes the reductions.
+template <class T>
+__global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
     const int nf = *a.nf;
-    const unsigned nb = gridDim.x;
-    const int stride = int(nb) * PCG_THREADS;
-    const int t0 = blockIdx.x * PCG_THREADS + threadIdx.x;
-    const int sx = 1, sy = a.g.W + 2, sz = (a.g.W + 2) * (a.g.H + 2);
-    double2* partA = a.part;
-    double2* partB = a.part + nb;
-    double2* partI = a.part + 2 * nb;
+    const int nb = int(gridDim.x);
+    // Blocked distribution: block b owns the contiguous fluid range
+    // [n0, n1), so the x and y neighbours of its cells mostly lie in the
+    // same block (L1 hits); threads stride by blockDim (coalesced).
+    const int chunk = (nf + nb - 1) / nb;
+    const int n0 = min(nf, int(blockIdx.x) * chunk), n1 = min(nf, n0 + chunk);
+    const int sy = a.g.W + 2, sz = (a.g.W + 2) * (a.g.H + 2);
+    const int offs[6] = {1, -1, sy, -sy, sz, -sz};
 
-    // x0 = 0, r0 = b, z0 = r0/diag, d0 = z0.
-    double rz_l = 0.0, rr_l = 0.0;
-    for (int n = t0; n < nf; n += stride) {
-        float rv = a.b[n];
-        float dg = float(a.diag[n]);
-        float z = dg > 0.0f ? rv / dg : 0.0f;
-        a.x[n] = 0.0f;
-        a.r[n] = rv;
-        a.dd[a.fidx[n]] = z;
-        rz_l += double(rv) * double(z);
-        rr_l += double(rv) * double(rv);
+    // Init 1: r0 = b, 1/diag, s_{-1} = p_{-1} = x0 = 0.
+    for (int n = n0 + threadIdx.x; n < n1; n += PCG_THREADS) {
+        const int c = a.fidx[n];
+        const uint8_t d = a.diag[n];
+        a.invd[c] = d > 0 ? T(1) / T(d) : T(0);
+        a.R[0][c] = T(a.b[n]);
+        a.S[0][c] = T(0);
+        a.P[n] = T(0);
+        a.X[n] = T(0);
     }
-    double2 bs = block_sum2(rz_l, rr_l);
-    if (threadIdx.x == 0) partI[blockIdx.x] = bs;
-    if (!grid_barrier(a.bar, nb, a.status)) return;
-    double2 tot = grid_sum2(partI, nb);
-    double rz = tot.x, rr = tot.y;
-    const double bb = tot.y;
+    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+    // Init 2: u0 = M^-1 r0, w0 = A u0; partials (r,u), (w,u), (r,r).
+    {
+        double g_l = 0.0, d_l = 0.0, rr_l = 0.0;
+        const T* __restrict__ R0 = a.R[0];
+        const T* __restrict__ iv = a.invd;
+        for (int n = n0 + threadIdx.x; n < n1; n += PCG_THREADS) {
+            const int c = a.fidx[n];
+            const T r = R0[c];
+            const T u = r * iv[c];
+            T nbs = T(0);
+#pragma unroll
+            for (int o = 0; o < 6; ++o) nbs += R0[c + offs[o]] * iv[c + offs[o]];
+            const T w = T(a.diag[n]) * u - nbs;
+            a.Wv[0][c] = w;
+            g_l += double(r) * double(u);
+            d_l += double(w) * double(u);
+            rr_l += double(r) * double(r);
+        }
+        double3 bs = block_sum3(g_l, d_l, rr_l);
+        double* pp = a.part + 3 * nb;  // parity 1
+        if (threadIdx.x == 0) { pp[blockIdx.x] = bs.x; pp[nb + blockIdx.x] = bs.y; pp[2 * nb + blockIdx.x] = bs.z; }
+    }
+    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+    double3 tot = grid_sum3(a.part + 3 * nb, nb);
+    double gam = tot.x, del = tot.y, rr = tot.z;
+    const double bb = tot.z;
     const double thr = a.tol * a.tol * bb;
+    double alpha = del > 0.0 ? gam / del : 0.0, beta = 0.0;
     int it = 0;
     int st = DEV_OK;
-    while (rr > thr && bb > 0.0) {
+    if (bb > 0.0 && !(del > 0.0)) st = isnan(del) ? DEV_NAN : DEV_BREAKDOWN;
+    while (st == DEV_OK && rr > thr && bb > 0.0) {
         if (it >= a.maxit) { st = DEV_MAXIT; break; }
-        // Phase A: q = A d, partial d.q
-        double dq_l = 0.0;
-        for (int n = t0; n < nf; n += stride) {
+        const int cur = it & 1, nxt = cur ^ 1;
+        const T al = T(alpha), be = T(beta);
+        const T* __restrict__ Rc = a.R[cur];
+        const T* __restrict__ Wc = a.Wv[cur];
+        const T* __restrict__ Sc = a.S[cur];
+        const T* __restrict__ iv = a.invd;
+        T* __restrict__ Rn = a.R[nxt];
+        T* __restrict__ Wn = a.Wv[nxt];
+        T* __restrict__ Sn = a.S[nxt];
+        double g_l = 0.0, d_l = 0.0, rr_l = 0.0;
+        for (int n = n0 + threadIdx.x; n < n1; n += PCG_THREADS) {
             const int c = a.fidx[n];
-            const float* d = a.dd + c;
-            // Neighbours were written by other CTAs in this launch: read through L2.
-            float dc = __ldcg(d);
-            float nbs = (__ldcg(d + sx) + __ldcg(d - sx)) + (__ldcg(d + sy) + __ldcg(d - sy)) +
-                        (__ldcg(d + sz) + __ldcg(d - sz));
-            float qv = float(a.diag[n]) * dc - nbs;
-            a.q[n] = qv;
-            dq_l += double(dc) * double(qv);
+            const T id = iv[c];
+            const T r = Rc[c];
+            const T s = fmaT(be, Sc[c], Wc[c]);        // s_i
+            const T p = fmaT(be, a.P[n], r * id);      // p_i
+            a.X[n] = fmaT(al, p, a.X[n]);
+            const T rn = fmaT(-al, s, r);              // r_{i+1}
+            const T un = rn * id;
+            T nbs = T(0);
+#pragma unroll
+            for (int o = 0; o < 6; ++o) {
+                const int q = c + offs[o];
+                const T sq = fmaT(be, Sc[q], Wc[q]);
+                nbs += fmaT(-al, sq, Rc[q]) * iv[q];
+            }
+            const T wn = T(a.diag[n]) * un - nbs;
+            Rn[c] = rn;
+            Wn[c] = wn;
+            Sn[c] = s;
+            a.P[n] = p;
+            g_l += double(rn) * double(un);
+            d_l += double(wn) * double(un);
+            rr_l += double(rn) * double(rn);
         }
-        bs = block_sum2(dq_l, 0.0);
-        if (threadIdx.x == 0) partA[blockIdx.x] = bs;
-        if (!grid_barrier(a.bar, nb, a.status)) return;
-        const double dq = grid_sum2(partA, nb).x;
-        if (!(dq > 0.0) || isnan(dq)) { st = isnan(dq) ? DEV_NAN : DEV_BREAKDOWN; break; }
-        const float alpha = float(rz / dq);
-        // Phase B: x += alpha d, r -= alpha q, z = r/diag; partial r.z, r.r
-        double rz_n = 0.0, rr_n = 0.0;
-        for (int n = t0; n < nf; n += stride) {
-            const int c = a.fidx[n];
-            float dc = a.dd[c];
-            a.x[n] += alpha * dc;
-            float rv = a.r[n] - alpha * a.q[n];
-            a.r[n] = rv;
-            float dg = float(a.diag[n]);
-            float z = dg > 0.0f ? rv / dg : 0.0f;
-            rz_n += double(rv) * double(z);
-            rr_n += double(rv) * double(rv);
-        }
-        bs = block_sum2(rz_n, rr_n);
-        if (threadIdx.x == 0) partB[blockIdx.x] = bs;
-        if (!grid_barrier(a.bar, nb, a.status)) return;
-        tot = grid_sum2(partB, nb);
+        double3 bs = block_sum3(g_l, d_l, rr_l);
+        double* pp = a.part + (it & 1) * 3 * nb;
+        if (threadIdx.x == 0) { pp[blockIdx.x] = bs.x; pp[nb + blockIdx.x] = bs.y; pp[2 * nb + blockIdx.x] = bs.z; }
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+        tot = grid_sum3(pp, nb);
         ++it;
-        if (isnan(tot.x) || isnan(tot.y)) { st = DEV_NAN; rr = tot.y; break; }
-        const float beta = float(tot.x / rz);
-        rz = tot.x;
-        rr = tot.y;
+        if (isnan(tot.x) || isnan(tot.y) || isnan(tot.z)) { st = DEV_NAN; rr = tot.z; break; }
+        const double gn = tot.x, dn = tot.y;
+        rr = tot.z;
         if (rr <= thr) break;
-        // Phase C: d = z + beta d
-        for (int n = t0; n < nf; n += stride) {
-            const int c = a.fidx[n];
-            float dg = float(a.diag[n]);
-            float z = dg > 0.0f ? a.r[n] / dg : 0.0f;
-            a.dd[c] = z + beta * a.dd[c];
-        }
-        if (!grid_barrier(a.bar, nb, a.status)) return;
+        beta = gn / gam;
+        const double den = dn - beta * gn / alpha;
+        if (!(den > 0.0) || !(gn > 0.0)) { st = DEV_BREAKDOWN; break; }
+        alpha = gn / den;
+        gam = gn;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.out->iters = it;
         atomicCAS(a.status, DEV_OK, st);  // never masks a timeout recorded by another CTA
         a.out->rr = rr;
         a.out->bb = bb;
-        a.out->rz = rz;
+        a.out->rz = gam;
     }
 }
 
@@ -335,21 +436,36 @@ __global__ void k_reset_pcg(GridBar* bar, int* status) {
     *status = DEV_OK;
 }
 
-__global__ void k_scatter_p(const int* __restrict__ nf_p, const int* __restrict__ fidx, const float* __restrict__ x,
-                            const double* __restrict__ x64, int use64, Dims g, float* __restrict__ p) {
+// Zero the FLUID entries of the padded work grids after a solve, so that every
+// solve starts from all-zero grids whatever cells were fluid before.
+template <class T>
+__global__ void k_clear_padded(const int* __restrict__ nf_p, const int* __restrict__ fidx, T* r0, T* r1, T* w0, T* w1,
+                               T* s0, T* s1, T* invd) {
+    const int nf = *nf_p;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) {
+        const int c = fidx[n];
+        r0[c] = T(0); r1[c] = T(0); w0[c] = T(0); w1[c] = T(0); s0[c] = T(0); s1[c] = T(0);
+        if (invd) invd[c] = T(0);
+    }
+}
+
+// Compact T vector -> padded dense grid.
+template <class T>
+__global__ void k_to_dense(const int* __restrict__ nf_p, const int* __restrict__ fidx, const T* __restrict__ x,
+                           T* __restrict__ dst) {
+    const int nf = *nf_p;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) dst[fidx[n]] = x[n];
+}
+
+template <class T>
+__global__ void k_scatter_p(const int* __restrict__ nf_p, const int* __restrict__ fidx, const T* __restrict__ x, Dims g,
+                            float* __restrict__ p) {
     const int nf = *nf_p;
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) {
         int cp = fidx[n];
         int i = cp % (g.W + 2) - 1, j = (cp / (g.W + 2)) % (g.H + 2) - 1, k = cp / ((g.W + 2) * (g.H + 2)) - 1;
-        p[int64_t(i) + int64_t(j) * g.W + int64_t(k) * g.W * g.H] = use64 ? float(x64[n]) : x[n];
+        p[int64_t(i) + int64_t(j) * g.W + int64_t(k) * g.W * g.H] = float(x[n]);
     }
-}
-
-// Fill the padded dense grid dd (float) or xd (double) from a compact vector.
-__global__ void k_to_dense_f(const int* __restrict__ nf_p, const int* __restrict__ fidx, const float* __restrict__ x,
-                             float* __restrict__ dd) {
-    const int nf = *nf_p;
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) dd[fidx[n]] = x[n];
 }
 
 // Partials of ||b - A x||^2 and ||b||^2 over the padded dense x (float or double).
@@ -498,53 +614,86 @@ void launch_pressure_setup(const uint8_t* labels, const float* u, const float* v
 int pcg_max_blocks() {
     static int cached = 0;
     if (cached) return cached;
-    int dev = 0, sms = 0, per_sm = 0;
+    int dev = 0, sms = 0, pf = 0, pd = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, PCG_THREADS, 0);
-    cached = sms * (per_sm > 0 ? per_sm : 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, k_pcg_cg<float>, PCG_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd, k_pcg_cg<double>, PCG_THREADS, 0);
+    int per_sm = std::max(1, std::min(pf, pd));
+    cached = sms * per_sm;
     return cached;
 }
 
-int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, double tol, int maxit, int max_blocks, cudaStream_t st) {
-    int nb = pcg_max_blocks();
-    if (max_blocks > 0 && max_blocks < nb) nb = max_blocks;
+template <class T>
+static int launch_pcg_t(Dims g, PressureBufs& pb, const float* rhs, double tol, int maxit, cudaStream_t st) {
+    const int nb = pcg_max_blocks();
     int* status = &pb.out->status;
     k_reset_pcg<<<1, 1, 0, st>>>(pb.bar, status);
-    PcgArgs a;
+    PcgArgs<T> a;
     a.g = g; a.nf = pb.nf; a.fidx = pb.fidx; a.diag = pb.diag; a.b = rhs;
-    a.x = pb.x; a.r = pb.r; a.q = pb.q; a.dd = pb.dd;
-    a.part = reinterpret_cast<double2*>(pb.part); a.bar = pb.bar; a.status = status; a.out = pb.out;
+    for (int i = 0; i < 2; ++i) {
+        a.R[i] = static_cast<T*>(pb.R[i]);
+        a.Wv[i] = static_cast<T*>(pb.Wv[i]);
+        a.S[i] = static_cast<T*>(pb.S[i]);
+    }
+    a.invd = static_cast<T*>(pb.invd);
+    a.P = static_cast<T*>(pb.P);
+    a.X = static_cast<T*>(pb.X);
+    a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;
     a.tol = tol; a.maxit = maxit;
     void* args[] = {&a};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(nb), dim3(PCG_THREADS), args, 0, st);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_cg<T>, dim3(nb), dim3(PCG_THREADS), args, 0, st);
     return e == cudaSuccess ? 0 : int(e);
 }
 
-void launch_scatter_p(const PressureBufs& pb, float* p, int use64, Dims g, cudaStream_t st) {
-    k_scatter_p<<<592, 256, 0, st>>>(pb.nf, pb.fidx, pb.x, pb.x64, use64, g, p);
+int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, int fp64, double tol, int maxit, cudaStream_t st) {
+    return fp64 ? launch_pcg_t<double>(g, pb, rhs, tol, maxit, st) : launch_pcg_t<float>(g, pb, rhs, tol, maxit, st);
 }
 
-void launch_true_residual(const PressureBufs& pb, const float* p, Dims g, cudaStream_t st) {
-    // Rebuild the padded dense x from the compact solution, then reduce.
-    k_to_dense_f<<<592, 256, 0, st>>>(pb.nf, pb.fidx, pb.x, pb.dd);
+void launch_pcg_clear(PressureBufs& pb, int fp64, int with_invd, cudaStream_t st) {
+    if (fp64) {
+        auto c = [&](void* p) { return static_cast<double*>(p); };
+        k_clear_padded<double><<<592, 256, 0, st>>>(pb.nf, pb.fidx, c(pb.R[0]), c(pb.R[1]), c(pb.Wv[0]), c(pb.Wv[1]),
+                                                    c(pb.S[0]), c(pb.S[1]), with_invd ? c(pb.invd) : nullptr);
+    } else {
+        auto c = [&](void* p) { return static_cast<float*>(p); };
+        k_clear_padded<float><<<592, 256, 0, st>>>(pb.nf, pb.fidx, c(pb.R[0]), c(pb.R[1]), c(pb.Wv[0]), c(pb.Wv[1]),
+                                                   c(pb.S[0]), c(pb.S[1]), with_invd ? c(pb.invd) : nullptr);
+    }
+}
+
+void launch_scatter_p(const PressureBufs& pb, float* p, int src, Dims g, cudaStream_t st) {
+    if (src == 0) k_scatter_p<float><<<592, 256, 0, st>>>(pb.nf, pb.fidx, static_cast<const float*>(pb.X), g, p);
+    else if (src == 1) k_scatter_p<double><<<592, 256, 0, st>>>(pb.nf, pb.fidx, static_cast<const double*>(pb.X), g, p);
+    else k_scatter_p<double><<<592, 256, 0, st>>>(pb.nf, pb.fidx, pb.x64, g, p);
+}
+
+void launch_true_residual(PressureBufs& pb, int fp64, Dims g, cudaStream_t st) {
+    // The compact solution goes to the padded R[0] grid (free after a solve).
     const int nb = 592;
-    k_residual<float><<<nb, 256, 0, st>>>(pb.nf, pb.fidx, pb.diag, pb.b, pb.dd, g,
-                                          reinterpret_cast<double2*>(pb.part), nullptr, nullptr);
-    k_sum_partials<<<1, 32, 0, st>>>(reinterpret_cast<double2*>(pb.part), nb, pb.red);
-    (void)p;
+    auto* part = reinterpret_cast<double2*>(pb.part);
+    if (fp64) {
+        k_to_dense<double><<<592, 256, 0, st>>>(pb.nf, pb.fidx, static_cast<const double*>(pb.X), static_cast<double*>(pb.R[0]));
+        k_residual<double><<<nb, 256, 0, st>>>(pb.nf, pb.fidx, pb.diag, pb.b, static_cast<const double*>(pb.R[0]), g, part,
+                                               nullptr, nullptr);
+    } else {
+        k_to_dense<float><<<592, 256, 0, st>>>(pb.nf, pb.fidx, static_cast<const float*>(pb.X), static_cast<float*>(pb.R[0]));
+        k_residual<float><<<nb, 256, 0, st>>>(pb.nf, pb.fidx, pb.diag, pb.b, static_cast<const float*>(pb.R[0]), g, part,
+                                              nullptr, nullptr);
+    }
+    k_sum_partials<<<1, 32, 0, st>>>(part, nb, pb.red);
 }
 
-void launch_ir_residual(PressureBufs& pb, double* xd, Dims g, cudaStream_t st) {
-    // r = b - A x64 in FP64; the inner right-hand side is r rounded to FP32.
+void launch_ir_residual(PressureBufs& pb, Dims g, cudaStream_t st) {
+    // r = b - A x64 in FP64 over the padded x64 grid xd; bin = r rounded to FP32.
     const int nb = 592;
-    k_residual<double><<<nb, 256, 0, st>>>(pb.nf, pb.fidx, pb.diag, pb.b, xd, g, reinterpret_cast<double2*>(pb.part),
-                                           pb.bin, nullptr);
-    k_sum_partials<<<1, 32, 0, st>>>(reinterpret_cast<double2*>(pb.part), nb, pb.red);
+    auto* part = reinterpret_cast<double2*>(pb.part);
+    k_residual<double><<<nb, 256, 0, st>>>(pb.nf, pb.fidx, pb.diag, pb.b, pb.xd, g, part, pb.bin, nullptr);
+    k_sum_partials<<<1, 32, 0, st>>>(part, nb, pb.red);
 }
 
-void launch_ir_update(PressureBufs& pb, double* xd, Dims g, cudaStream_t st) {
-    k_ir_update<<<592, 256, 0, st>>>(pb.nf, pb.fidx, pb.x, pb.x64, xd);
+void launch_ir_update(PressureBufs& pb, Dims g, cudaStream_t st) {
+    k_ir_update<<<592, 256, 0, st>>>(pb.nf, pb.fidx, static_cast<const float*>(pb.X), pb.x64, pb.xd);
     (void)g;
 }
 

@@ -38,6 +38,10 @@ void dfree(T*& p) {
     if (p) cudaFree(p);
     p = nullptr;
 }
+cudaError_t dalloc_bytes(void** p, size_t bytes) {
+    *p = nullptr;
+    return cudaMalloc(p, bytes ? bytes : 1);
+}
 
 }  // namespace
 
@@ -56,7 +60,7 @@ struct fp_solver {
     // grids
     uint8_t *d_base = nullptr, *d_labels = nullptr, *d_bodymark = nullptr;
     float *d_u = nullptr, *d_v = nullptr, *d_w = nullptr, *d_us = nullptr, *d_vs = nullptr, *d_ws = nullptr,
-          *d_p = nullptr, *d_scratch = nullptr;
+          *d_p = nullptr, *d_scratch = nullptr, *d_scratch2 = nullptr;
     int *d_counts = nullptr, *d_start = nullptr, *d_tiles = nullptr;
     // particles (cell order; pid in pos.w)
     float4 *d_pos = nullptr, *d_vel = nullptr, *d_pos2 = nullptr, *d_vel2 = nullptr;
@@ -66,7 +70,6 @@ struct fp_solver {
     bool sorted = false;
     // pressure
     PressureBufs pb{};
-    double* d_xd = nullptr;
     int64_t padded = 0;
     // pinned result mirrors
     PcgOut* h_out = nullptr;
@@ -93,12 +96,13 @@ namespace {
 void free_grid(fp_solver* s) {
     dfree(s->d_base); dfree(s->d_labels); dfree(s->d_bodymark);
     dfree(s->d_u); dfree(s->d_v); dfree(s->d_w); dfree(s->d_us); dfree(s->d_vs); dfree(s->d_ws);
-    dfree(s->d_p); dfree(s->d_scratch);
+    dfree(s->d_p); dfree(s->d_scratch); dfree(s->d_scratch2);
     dfree(s->d_counts); dfree(s->d_start); dfree(s->d_tiles);
     PressureBufs& pb = s->pb;
-    dfree(pb.nf); dfree(pb.fidx); dfree(pb.diag); dfree(pb.b); dfree(pb.bin); dfree(pb.x); dfree(pb.r); dfree(pb.q);
-    dfree(pb.dd); dfree(pb.x64); dfree(pb.part); dfree(pb.bar); dfree(pb.out); dfree(pb.red);
-    dfree(s->d_xd);
+    dfree(pb.nf); dfree(pb.fidx); dfree(pb.diag); dfree(pb.b); dfree(pb.bin);
+    for (int i = 0; i < 2; ++i) { dfree(pb.R[i]); dfree(pb.Wv[i]); dfree(pb.S[i]); }
+    dfree(pb.invd); dfree(pb.P); dfree(pb.X);
+    dfree(pb.x64); dfree(pb.xd); dfree(pb.part); dfree(pb.bar); dfree(pb.out); dfree(pb.red);
     s->have_grid = false;
 }
 
@@ -122,15 +126,19 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     ck(dalloc(&s->d_u, s->g.nu())); ck(dalloc(&s->d_us, s->g.nu()));
     ck(dalloc(&s->d_v, s->g.nv())); ck(dalloc(&s->d_vs, s->g.nv()));
     ck(dalloc(&s->d_w, s->g.nw())); ck(dalloc(&s->d_ws, s->g.nw()));
-    ck(dalloc(&s->d_p, nc)); ck(dalloc(&s->d_scratch, nc));
+    ck(dalloc(&s->d_p, nc)); ck(dalloc(&s->d_scratch, nc)); ck(dalloc(&s->d_scratch2, nc));
     ck(dalloc(&s->d_counts, nc + 1)); ck(dalloc(&s->d_start, nc + 1)); ck(dalloc(&s->d_tiles, ntiles));
     PressureBufs& pb = s->pb;
     ck(dalloc(&pb.nf, 1)); ck(dalloc(&pb.fidx, nc)); ck(dalloc(&pb.diag, nc)); ck(dalloc(&pb.b, nc));
-    ck(dalloc(&pb.bin, nc)); ck(dalloc(&pb.x, nc)); ck(dalloc(&pb.r, nc)); ck(dalloc(&pb.q, nc));
-    ck(dalloc(&pb.dd, s->padded)); ck(dalloc(&pb.x64, nc));
+    ck(dalloc(&pb.bin, nc));
+    const size_t pbytes = sizeof(double) * size_t(s->padded), cbytes = sizeof(double) * size_t(nc);
+    for (int i = 0; i < 2; ++i) {
+        ck(dalloc_bytes(&pb.R[i], pbytes)); ck(dalloc_bytes(&pb.Wv[i], pbytes)); ck(dalloc_bytes(&pb.S[i], pbytes));
+    }
+    ck(dalloc_bytes(&pb.invd, pbytes)); ck(dalloc_bytes(&pb.P, cbytes)); ck(dalloc_bytes(&pb.X, cbytes));
+    ck(dalloc(&pb.x64, nc)); ck(dalloc(&pb.xd, s->padded));
     ck(dalloc(&pb.part, size_t(6) * std::max(maxb, 1024)));
     ck(dalloc(&pb.bar, 1)); ck(dalloc(&pb.out, 1)); ck(dalloc(&pb.red, 2));
-    ck(dalloc(&s->d_xd, s->padded));
     pb.tile_sums = s->d_tiles;
     if (e != cudaSuccess) { free_grid(s); return s->cuda_fail(e, "device allocation of the grid"); }
     for (float* a : {s->d_u, s->d_us}) ck(cudaMemsetAsync(a, 0, sizeof(float) * s->g.nu(), s->st));
@@ -138,7 +146,12 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     for (float* a : {s->d_w, s->d_ws}) ck(cudaMemsetAsync(a, 0, sizeof(float) * s->g.nw(), s->st));
     ck(cudaMemsetAsync(s->d_p, 0, sizeof(float) * nc, s->st));
     ck(cudaMemsetAsync(s->d_bodymark, 0, nc, s->st));
-    ck(cudaMemsetAsync(pb.dd, 0, sizeof(float) * s->padded, s->st));
+    for (int i = 0; i < 2; ++i) {
+        ck(cudaMemsetAsync(pb.R[i], 0, pbytes, s->st)); ck(cudaMemsetAsync(pb.Wv[i], 0, pbytes, s->st));
+        ck(cudaMemsetAsync(pb.S[i], 0, pbytes, s->st));
+    }
+    ck(cudaMemsetAsync(pb.invd, 0, pbytes, s->st));
+    ck(cudaMemsetAsync(pb.xd, 0, sizeof(double) * size_t(s->padded), s->st));
     ck(cudaMemsetAsync(pb.bar, 0, sizeof(GridBar), s->st));
     if (e != cudaSuccess) { free_grid(s); return s->cuda_fail(e, "grid initialisation"); }
     s->have_grid = true;
@@ -188,54 +201,59 @@ void phase_save(fp_solver* s) {
     launch_copy(s->d_w, s->d_ws, s->g.nw(), s->st);
 }
 
-// Pressure solve of the system already set up in s->pb; leaves the solution in
-// p and the diagnostics in the pinned mirrors.  Returns FP_OK or an error.
+// Pressure solve of the system already set up in s->pb (fidx, diag, b); writes
+// the dense solution to p_out and the diagnostics to s->stats.
+//   FP_SOLVER_PCG       one FP64-vector PCG to tol (the FP64 path);
+//   FP_SOLVER_PCG_MIXED FP64 iterative refinement: r = b - A x in FP64, an
+//                       FP32-vector PCG solves A c = r loosely, x += c.
 int solve_system(fp_solver* s, float* p_out) {
     PressureBufs& pb = s->pb;
     const double tol = s->cfg.tol;
     const int maxit = s->cfg.max_iters;
     int outer = 0, inner_total = 0;
     int dev_status = DEV_OK;
-    const int solver = s->cfg.solver;
     float pcg_ms = 0.0f;
-    if (solver == FP_SOLVER_PCG) {
+    cudaError_t ce;
+    if (s->cfg.solver == FP_SOLVER_PCG) {
         cudaEventRecord(s->ev_pcg[0], s->st);
-        int e = launch_pcg(s->g, pb, pb.b, tol, maxit, 0, s->st);
+        int e = launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st);
         cudaEventRecord(s->ev_pcg[1], s->st);
         if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
-        s->launches += 2 + 1 + 3;  // reset + pcg, scatter, residual (3)
-        launch_scatter_p(pb, p_out, 0, s->g, s->st);
-        launch_true_residual(pb, p_out, s->g, s->st);
+        launch_scatter_p(pb, p_out, 1, s->g, s->st);
+        launch_true_residual(pb, 1, s->g, s->st);
+        launch_pcg_clear(pb, 1, 1, s->st);
+        s->launches += 2 + 1 + 3 + 1;  // reset + pcg, scatter, residual (3), clear
         cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
         cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
         cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
-        cudaError_t ce = cudaStreamSynchronize(s->st);
+        ce = cudaStreamSynchronize(s->st);
         if (ce != cudaSuccess) return s->cuda_fail(ce, "pressure solve");
         inner_total = s->h_out->iters;
         dev_status = s->h_out->status;
         outer = 1;
         cudaEventElapsedTime(&pcg_ms, s->ev_pcg[0], s->ev_pcg[1]);
     } else {
-        // FP64 iterative refinement around FP32-vector PCG (FP64 reductions).
         cudaMemsetAsync(pb.x64, 0, sizeof(double) * s->g.nc(), s->st);
-        cudaMemsetAsync(s->d_xd, 0, sizeof(double) * s->padded, s->st);
-        launch_ir_residual(pb, s->d_xd, s->g, s->st);
-        s->launches += 2;
+        launch_ir_residual(pb, s->g, s->st);  // x64 = 0: bin = b
+        s->launches += 3;
         cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
         cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
-        cudaError_t ce = cudaStreamSynchronize(s->st);
+        ce = cudaStreamSynchronize(s->st);
         if (ce != cudaSuccess) return s->cuda_fail(ce, "refinement residual");
         const double bb = s->h_red[1];
         double relres = bb > 0 ? std::sqrt(s->h_red[0] / bb) : 0.0;
         while (relres > tol && outer < 12 && inner_total < maxit) {
-            double inner_tol = std::min(0.1, std::max(1e-4, 0.5 * tol / relres));
+            // Inner accuracy: enough to land below tol after this update, but
+            // not below what FP32 vectors can resolve.
+            const double inner_tol = std::min(0.1, std::max(2e-4, 0.5 * tol / relres));
             cudaEventRecord(s->ev_pcg[0], s->st);
-            int e = launch_pcg(s->g, pb, pb.bin, inner_tol, maxit - inner_total, 0, s->st);
+            int e = launch_pcg(s->g, pb, pb.bin, 0, inner_tol, maxit - inner_total, s->st);
             cudaEventRecord(s->ev_pcg[1], s->st);
             if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
-            s->launches += 2 + 1 + 2;  // reset + pcg, update, residual (2)
-            launch_ir_update(pb, s->d_xd, s->g, s->st);
-            launch_ir_residual(pb, s->d_xd, s->g, s->st);
+            launch_ir_update(pb, s->g, s->st);
+            launch_pcg_clear(pb, 0, 0, s->st);
+            launch_ir_residual(pb, s->g, s->st);
+            s->launches += 2 + 1 + 1 + 2;  // reset + pcg, update, clear, residual (2)
             cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
             cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
             ce = cudaStreamSynchronize(s->st);
@@ -246,15 +264,18 @@ int solve_system(fp_solver* s, float* p_out) {
             cudaEventElapsedTime(&ms, s->ev_pcg[0], s->ev_pcg[1]);
             pcg_ms += ms;
             if (s->h_out->status == DEV_TIMEOUT || s->h_out->status == DEV_NAN) { dev_status = s->h_out->status; break; }
-            double nr = bb > 0 ? std::sqrt(s->h_red[0] / bb) : 0.0;
-            if (!(nr < relres)) { relres = nr; dev_status = DEV_BREAKDOWN; break; }  // stalled refinement
+            const double nr = bb > 0 ? std::sqrt(s->h_red[0] / bb) : 0.0;
+            if (!(nr < relres)) { relres = nr; dev_status = DEV_BREAKDOWN; break; }  // refinement stalled
             relres = nr;
         }
-        launch_scatter_p(pb, p_out, 1, s->g, s->st);
-        s->launches += 1;
+        launch_pcg_clear(pb, 0, 1, s->st);  // 1/diag grid
+        launch_scatter_p(pb, p_out, 2, s->g, s->st);
+        s->launches += 2;
         s->h_red[0] = relres * relres * bb;
         s->h_red[1] = bb;
         if (relres > tol && dev_status == DEV_OK) dev_status = DEV_MAXIT;
+        // xd must be zero at the start of the next solve
+        cudaMemsetAsync(pb.xd, 0, sizeof(double) * size_t(s->padded), s->st);
     }
     s->pcg_ms = pcg_ms;
     s->stats.t_pcg = pcg_ms;
@@ -266,17 +287,15 @@ int solve_system(fp_solver* s, float* p_out) {
     int status = FP_OK;
     if (*s->h_nf == 0) status = FP_ERR_NO_FLUID;
     else if (dev_status == DEV_TIMEOUT) status = FP_ERR_TIMEOUT;
-    else if (dev_status == DEV_NAN || dev_status == DEV_BREAKDOWN) status = FP_ERR_SOLVER;
-    else if (dev_status == DEV_MAXIT) status = FP_ERR_SOLVER;
+    else if (dev_status != DEV_OK) status = FP_ERR_SOLVER;
     s->stats.solve_status = status;
     if (status == FP_ERR_TIMEOUT) return s->fail(status, "PCG grid barrier timed out");
     if (dev_status == DEV_NAN) return s->fail(status, "PCG produced NaN");
-    return FP_OK;  // no-fluid, breakdown and iteration cap are reported in stats, as the step continues
+    return FP_OK;  // no-fluid, breakdown and iteration cap are reported in stats; the step continues
 }
 
 int phase_pressure(fp_solver* s) {
     s->launches += 3;  // fluid tiles, tile scan, fluid build
-    cudaMemsetAsync(s->pb.dd, 0, sizeof(float) * s->padded, s->st);
     BodyKin b = s->body;
     b.active = s->cfg.active_body;
     launch_pressure_setup(s->d_labels, s->d_u, s->d_v, s->d_w, s->g, s->cfg.dt, b, nullptr, s->d_p, s->pb, s->st);
@@ -707,15 +726,14 @@ int fp_pressure_solve(fp_solver* s, const float* rhs, float* x, int64_t n, int* 
     if (n != s->g.nc()) return s->fail(FP_ERR_ARG, "rhs size mismatch");
     cudaError_t e = cudaMemcpyAsync(s->d_scratch, rhs, sizeof(float) * n, cudaMemcpyHostToDevice, s->st);
     if (e != cudaSuccess) return s->cuda_fail(e, "rhs upload");
-    cudaMemsetAsync(s->pb.dd, 0, sizeof(float) * s->padded, s->st);
     BodyKin b{};
-    // The solution goes to pb.q reused as a dense float scratch of nc entries.
-    launch_pressure_setup(s->d_labels, s->d_u, s->d_v, s->d_w, s->g, s->cfg.dt, b, s->d_scratch, s->pb.q, s->pb, s->st);
-    int rc = solve_system(s, s->d_scratch);
+    // rhs in d_scratch; the dense solution goes to d_scratch2 (zeroed by the
+    // setup), leaving the solver's own pressure grid untouched.
+    float* xdense = s->d_scratch2;
+    launch_pressure_setup(s->d_labels, s->d_u, s->d_v, s->d_w, s->g, s->cfg.dt, b, s->d_scratch, xdense, s->pb, s->st);
+    int rc = solve_system(s, xdense);
     if (rc) return rc;
-    e = cudaMemsetAsync(s->d_scratch, 0, sizeof(float) * n, s->st);
-    launch_scatter_p(s->pb, s->d_scratch, s->cfg.solver != FP_SOLVER_PCG, s->g, s->st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(x, s->d_scratch, sizeof(float) * n, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(x, xdense, sizeof(float) * n, cudaMemcpyDeviceToHost, s->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
     if (e != cudaSuccess) return s->cuda_fail(e, "solution download");
     if (iters) *iters = s->stats.pcg_iters;

@@ -159,14 +159,18 @@ def test_projection_matches_oracle(O):
     s, o = _prepare_pressure(O, "pcg_mixed", tol=1e-9)
     s.phase(capi.PHASE_PRESSURE)
     o.set_grid(O.GRID_P, s.grid(capi.GRID_P).astype(np.float64))  # same p on both sides
+    fl = o.labels().ravel() == 1
+    b_before = o.rhs()
     s.phase(capi.PHASE_PROJECT)
     o.phase(O.PH_PROJECT)
     for g in (capi.GRID_U, capi.GRID_V, capi.GRID_W):
         assert rel_l2(s.grid(g), o.grid(g)) <= 1e-5
-    # projected field is discretely divergence-free at FLUID cells
-    b = o.rhs()
-    fl = o.labels().ravel() == 1
-    assert np.linalg.norm(b[fl]) <= 1e-3 * max(1.0, np.abs(b).max())
+    # the projected field is discretely divergence-free at FLUID cells, to
+    # the accuracy of the 1e-9 solve and FP32 face velocities
+    for g, go in ((capi.GRID_U, O.GRID_U), (capi.GRID_V, O.GRID_V), (capi.GRID_W, O.GRID_W)):
+        o.set_grid(go, s.grid(g).astype(np.float64))
+    b_after = o.rhs()
+    assert np.linalg.norm(b_after[fl]) <= 1e-5 * np.linalg.norm(b_before[fl])
 
 
 def test_g2p_and_advection_match_oracle(O):
@@ -211,8 +215,10 @@ def test_full_steps_match_oracle(O):
 
 
 def test_simple3d_poisson_on_gpu(O):
-    """labels_simple3d.txt (5x4x1): the GPU pressure solve of a caller rhs
-    equals the oracle's FP64 solution."""
+    """labels_simple3d.txt (5x4x1): six FLUID cells walled in by SOLID, a
+    pure-Neumann (singular) system whose null space is the constants.  For a
+    consistent rhs (zero sum) the GPU solve equals the oracle's FP64 solution
+    up to that constant."""
     from fluidprjct_b200 import capi
     lab = capi.read_label_file(os.path.join(GOLDEN, "labels_simple3d.txt"), 3)
     s = _solver(dx=0.1, dt=0.01, solver="pcg_mixed", tol=1e-10)
@@ -220,12 +226,14 @@ def test_simple3d_poisson_on_gpu(O):
     assert s.dims == (5, 4, 1)
     b = np.zeros(lab.size, np.float32)
     fl = lab.ravel() == 1
-    b[fl] = [1.0, -2.0, 0.5, 3.0, -1.0, 0.25]
+    b[fl] = [1.0, -2.0, 0.5, 3.0, -1.0, -1.5]
     x, it, rr, rc = s.pressure_solve(b)
     o = O.Sim3(5, 4, 1, 0.1, 0.01, fp64=True)
     o.set_labels(lab)
     xo, _ = o.solve(b.astype(np.float64))
-    assert rr <= 1e-10 and rel_l2(x.ravel()[fl], xo[fl]) <= 1e-6
+    xg, xr = x.ravel()[fl].astype(np.float64), xo[fl]
+    assert rr <= 1e-10 and rel_l2(xg - xg.mean(), xr - xr.mean()) <= 1e-6
+    assert rel_l2(o.apply(x.ravel().astype(np.float64))[fl], b[fl]) <= 1e-6
 
 
 def test_cudss_kat_on_gpu(golden):
