@@ -23,6 +23,7 @@ SOURCES = [
     "kernels_p2g.cu",
     "kernels_pressure.cu",
     "kernels_advect.cu",
+    "kernels_body.cu",
     "solver.cu",
     "io.cpp",
 ]

@@ -189,6 +189,11 @@ class Solver:
         lib().fp_get_dims(self._h, C.byref(W), C.byref(H), C.byref(D))
         return W.value, H.value, D.value
 
+    def load_sdf(self, path=None):
+        """Body SDF from a reference SDF file, or the analytic sphere of the
+        config (body_radius, body_density) when path is None."""
+        return self._check(lib().fp_load_sdf(self._h, None if path is None else str(path).encode()))
+
     def seed_particles(self, ppc, seed):
         return self._check(lib().fp_seed_particles(self._h, ppc, seed))
 

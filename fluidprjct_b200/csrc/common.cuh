@@ -118,6 +118,22 @@ __device__ __forceinline__ float3 interp_vel(const float* __restrict__ u, const 
                        sample(w, stencil_w(rx, ry, rz, g), g.W, g.W * g.H));
 }
 
+// Rigid-body geometry for marking and the force integral: an analytic
+// sphere, or the reference's voxel SDF (RigidBody, utility.cuh:195-491) with
+// its rotation (row-major, world = R * local) and local centre of mass.
+enum : int { BODY_SPHERE = 0, BODY_SDF = 1 };
+struct BodyShape {
+    int kind;
+    float3 com;          // body position (centre of mass) in world space
+    float radius;        // sphere radius
+    float rot[9];        // rotation matrix, row-major
+    float3 local_com;    // centre of mass in SDF-file coordinates
+    float3 origin;       // SDF file origin
+    float cell;          // SDF voxel size
+    int nx, ny, nz;      // SDF dimensions
+    const float* sdf;    // device SDF values, i fastest
+};
+
 // Labels with out-of-domain cells reading as SOLID.
 __device__ __forceinline__ uint8_t label_at(const uint8_t* __restrict__ lab, const Dims& g, int i, int j, int k) {
     if (i < 0 || i >= g.W || j < 0 || j >= g.H || k < 0 || k >= g.D) return SOLID;

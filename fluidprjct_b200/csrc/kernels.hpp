@@ -95,6 +95,17 @@ void launch_g2p_advect(float4* pos, float4* vel, int64_t np, const float* u, con
                        const float* us, const float* vs, const float* ws, const uint8_t* labels, Dims g, float alpha,
                        float dt, float cfl, int do_g2p, int do_advect, int rk2, cudaStream_t st);
 
+// -------- rigid body (kernels_body.cu) --------
+// mark[c] = 1 where the cell centre is inside the body (SDF <= 0).
+void launch_mark_body(uint8_t* mark, Dims g, const BodyShape& b, cudaStream_t st);
+// labels[c] = BODY where mark[c] and labels[c] != SOLID (init-time marking).
+void launch_apply_mark(uint8_t* labels, const uint8_t* mark, Dims g, cudaStream_t st);
+// Fluid force and torque on the body (FP64): out[0..2] force, out[3..5]
+// torque about b.com; part holds body_force_partials() doubles.
+void launch_body_force(const float* p, const uint8_t* labels, Dims g, const BodyShape& b, double* part, double* out,
+                       cudaStream_t st);
+int body_force_partials();
+
 // -------- particle order helpers --------
 // out[pid] = in[slot] for the xyz part of float4 arrays (pid in pos.w bits).
 void launch_unsort(const float4* pos, const float4* vel, int64_t np, float* pos_out, float* vel_out, cudaStream_t st);

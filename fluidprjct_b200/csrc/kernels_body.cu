@@ -1,0 +1,156 @@
+// kernels_body.cu -- SDF rigid body: cell marking and fluid force/torque.
+//
+// Marking restates MarkBodyCellsFunctor + Utility::contains
+// (FluidSolver3D.cu:45-78, utility.cu:163-206): a cell whose centre lies
+// inside the body (SDF <= 0) and is not SOLID becomes BODY.  The SDF is either
+// the reference's voxel grid (nearest-lower voxel in body coordinates, rotated
+// about the centre of mass) or an analytic sphere |x - c| - r.
+//
+// The fluid force replaces the reference's panel drag/lift plus host
+// buoyancy loop (DragLiftForceCalculator :2674-2791, applyBuoyancy
+// :2917-3026) by the pressure integral over the body written with SDF face
+// fractions:  F = - sum_faces theta_f (p_R - p_L) dx^2 e_axis,
+// tau = sum_faces (x_f - c) x dF, where theta_f = clamp(1/2 - phi(x_f)/dx, 0, 1)
+// is the body fraction of face f and p is extended one cell into the body
+// (BODY cells take the mean of their FLUID/AIR neighbours).  Along every grid
+// line through the body the sum telescopes to the pressure difference across
+// the body surface, so buoyancy and dynamic pressure forces both follow, and
+// the force varies smoothly as the body moves by sub-cell amounts.  Each block
+// reduces its faces in FP64 in a fixed order; a second kernel sums the block
+// partials in a fixed order.
+#include "kernels.hpp"
+
+namespace fp {
+
+namespace {
+
+__device__ __forceinline__ float sdf_at(const BodyShape& b, float3 x) {
+    const float3 d = make_float3(x.x - b.com.x, x.y - b.com.y, x.z - b.com.z);
+    // Explicitly rounded (no contraction) so BODY marks match a CPU evaluation bit for bit.
+    if (b.kind == BODY_SPHERE)
+        return sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(d.x, d.x), __fmul_rn(d.y, d.y)), __fmul_rn(d.z, d.z))) - b.radius;
+    // Voxel SDF: local = R^T (x - pos) + local_com; coordinate (local - origin)/cell.
+    const float lx = b.rot[0] * d.x + b.rot[3] * d.y + b.rot[6] * d.z + b.local_com.x;
+    const float ly = b.rot[1] * d.x + b.rot[4] * d.y + b.rot[7] * d.z + b.local_com.y;
+    const float lz = b.rot[2] * d.x + b.rot[5] * d.y + b.rot[8] * d.z + b.local_com.z;
+    const float sx = (lx - b.origin.x) / b.cell, sy = (ly - b.origin.y) / b.cell, sz = (lz - b.origin.z) / b.cell;
+    if (sx < 0.0f || sx >= float(b.nx) || sy < 0.0f || sy >= float(b.ny) || sz < 0.0f || sz >= float(b.nz)) return 1e30f;
+    const int i = min(int(sx), b.nx - 1), j = min(int(sy), b.ny - 1), k = min(int(sz), b.nz - 1);
+    return __ldg(b.sdf + i + j * b.nx + k * b.nx * b.ny);
+}
+
+__global__ void k_mark_body(uint8_t* __restrict__ mark, Dims g, BodyShape b) {
+    const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= g.nc()) return;
+    const int i = int(c % g.W), j = int((c / g.W) % g.H), k = int(c / (int64_t(g.W) * g.H));
+    const float3 x = make_float3((float(i) + 0.5f) * g.dx, (float(j) + 0.5f) * g.dx, (float(k) + 0.5f) * g.dx);
+    mark[c] = sdf_at(b, x) <= 0.0f ? 1 : 0;
+}
+
+// Pressure with BODY cells extended by the mean of their FLUID/AIR neighbours
+// (0 when they have none); SOLID and out-of-domain cells are invalid.
+__device__ __forceinline__ bool p_ext(const float* __restrict__ p, const uint8_t* __restrict__ lab, const Dims& g,
+                                      int i, int j, int k, float& out) {
+    const uint8_t l = label_at(lab, g, i, j, k);
+    if (l == SOLID) return false;
+    if (l != BODY) { out = p[i + j * g.W + k * g.W * g.H]; return true; }
+    const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    float s = 0.0f;
+    int n = 0;
+#pragma unroll
+    for (int o = 0; o < 6; ++o) {
+        const int a = i + off[o][0], b = j + off[o][1], e = k + off[o][2];
+        const uint8_t ln = label_at(lab, g, a, b, e);
+        if (ln == FLUID || ln == AIR) { s += p[a + b * g.W + e * g.W * g.H]; ++n; }
+    }
+    out = n ? s / float(n) : 0.0f;
+    return true;
+}
+
+constexpr int FORCE_THREADS = 256;
+
+__global__ void __launch_bounds__(FORCE_THREADS) k_body_force(const float* __restrict__ p,
+                                                              const uint8_t* __restrict__ lab, Dims g, BodyShape b,
+                                                              double* __restrict__ part) {
+    const int64_t nc1 = int64_t(g.W + 1) * (g.H + 1) * (g.D + 1);
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const float dx = g.dx;
+    const double area = double(dx) * double(dx);
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < nc1; t += int64_t(gridDim.x) * blockDim.x) {
+        const int i = int(t % (g.W + 1)), j = int((t / (g.W + 1)) % (g.H + 1)), k = int(t / (int64_t(g.W + 1) * (g.H + 1)));
+        for (int ax = 0; ax < 3; ++ax) {
+            // face of axis ax at the low side of cell (i,j,k)
+            if (ax == 0 && (j >= g.H || k >= g.D)) continue;
+            if (ax == 1 && (i >= g.W || k >= g.D)) continue;
+            if (ax == 2 && (i >= g.W || j >= g.H)) continue;
+            const float3 xf = make_float3(ax == 0 ? float(i) * dx : (float(i) + 0.5f) * dx,
+                                          ax == 1 ? float(j) * dx : (float(j) + 0.5f) * dx,
+                                          ax == 2 ? float(k) * dx : (float(k) + 0.5f) * dx);
+            const float theta = clamp01(0.5f - sdf_at(b, xf) / dx);
+            if (theta <= 0.0f) continue;
+            float pl, pr;
+            const int li = i - (ax == 0), lj = j - (ax == 1), lk = k - (ax == 2);
+            if (!p_ext(p, lab, g, li, lj, lk, pl) || !p_ext(p, lab, g, i, j, k, pr)) continue;
+            const double dF = -double(theta) * (double(pr) - double(pl)) * area;
+            const double rx = double(xf.x) - double(b.com.x), ry = double(xf.y) - double(b.com.y),
+                         rz = double(xf.z) - double(b.com.z);
+            const double fx = ax == 0 ? dF : 0.0, fy = ax == 1 ? dF : 0.0, fz = ax == 2 ? dF : 0.0;
+            acc[0] += fx; acc[1] += fy; acc[2] += fz;
+            acc[3] += ry * fz - rz * fy;
+            acc[4] += rz * fx - rx * fz;
+            acc[5] += rx * fy - ry * fx;
+        }
+    }
+    __shared__ double sh[6][FORCE_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        double v = acc[m];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[m][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double v = 0.0;
+        for (int w = 0; w < FORCE_THREADS / 32; ++w) v += sh[threadIdx.x][w];
+        part[blockIdx.x * 6 + threadIdx.x] = v;
+    }
+}
+
+__global__ void k_body_force_sum(const double* __restrict__ part, int nb, double* __restrict__ out) {
+    if (threadIdx.x < 6) {
+        double v = 0.0;
+        for (int b = 0; b < nb; ++b) v += part[b * 6 + threadIdx.x];
+        out[threadIdx.x] = v;
+    }
+}
+
+}  // namespace
+
+namespace {
+__global__ void k_apply_mark(uint8_t* __restrict__ labels, const uint8_t* __restrict__ mark, int64_t nc) {
+    const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c < nc && mark[c] && labels[c] != SOLID) labels[c] = BODY;
+}
+}  // namespace
+
+void launch_apply_mark(uint8_t* labels, const uint8_t* mark, Dims g, cudaStream_t st) {
+    k_apply_mark<<<unsigned((g.nc() + 255) / 256), 256, 0, st>>>(labels, mark, g.nc());
+}
+
+void launch_mark_body(uint8_t* mark, Dims g, const BodyShape& b, cudaStream_t st) {
+    k_mark_body<<<unsigned((g.nc() + 255) / 256), 256, 0, st>>>(mark, g, b);
+}
+
+constexpr int FORCE_BLOCKS = 592;
+
+void launch_body_force(const float* p, const uint8_t* labels, Dims g, const BodyShape& b, double* part, double* out,
+                       cudaStream_t st) {
+    k_body_force<<<FORCE_BLOCKS, FORCE_THREADS, 0, st>>>(p, labels, g, b, part);
+    k_body_force_sum<<<1, 32, 0, st>>>(part, FORCE_BLOCKS, out);
+}
+
+int body_force_partials() { return FORCE_BLOCKS * 6; }
+
+}  // namespace fp

@@ -45,6 +45,47 @@ cudaError_t dalloc_bytes(void** p, size_t bytes) {
 
 }  // namespace
 
+// Rigid body state on the host (RigidBody, utility.cuh:195-491): position,
+// velocity, Euler angles (theta, psi, phi) with their rotation matrix, scalar
+// inertia 0.4*m*r^2 (FluidSolver3D.cu:165-169).
+struct HostBody {
+    bool loaded = false;
+    int kind = BODY_SPHERE;
+    double pos[3] = {0, 0, 0}, vel[3] = {0, 0, 0}, omega[3] = {0, 0, 0};
+    double theta = 0, psi = 0, phi = 0;
+    double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    double mass = 1, inertia = 1, radius = 0;
+    double force[3] = {0, 0, 0}, torque[3] = {0, 0, 0};
+    // voxel SDF
+    int nx = 0, ny = 0, nz = 0;
+    float origin[3] = {0, 0, 0}, cell = 1, local_com[3] = {0, 0, 0};
+
+    // update_rotation_matrix (utility.cuh:470-484)
+    void update_rotation() {
+        const double ct = std::cos(theta), st = std::sin(theta), cp = std::cos(psi), sp = std::sin(psi),
+                     cf = std::cos(phi), sf = std::sin(phi);
+        R[0] = ct * cp; R[1] = st * sf - ct * cf * sp; R[2] = cf * st + ct * sf * sp;
+        R[3] = sp;      R[4] = cf * cp;                R[5] = -cp * sf;
+        R[6] = -cp * st; R[7] = ct * sf + cf * st * sp; R[8] = ct * cf - st * sf * sp;
+    }
+    // integrate (utility.cuh:408-467): semi-implicit Euler for the centre of
+    // mass; body-frame angular acceleration tau/I; Euler-angle kinematics.
+    void integrate(double dt) {
+        for (int a = 0; a < 3; ++a) { vel[a] += force[a] / mass * dt; pos[a] += vel[a] * dt; }
+        const double pi = 3.14159265358979323846;
+        theta = std::min(std::max(theta, -pi), pi);
+        update_rotation();
+        const double tl[3] = {R[0] * torque[0] + R[3] * torque[1] + R[6] * torque[2],
+                              R[1] * torque[0] + R[4] * torque[1] + R[7] * torque[2],
+                              R[2] * torque[0] + R[5] * torque[1] + R[8] * torque[2]};
+        for (int a = 0; a < 3; ++a) omega[a] += tl[a] / inertia * dt;
+        const double dth = omega[1] * std::cos(phi) - omega[2] * std::sin(phi);
+        const double dps = (omega[1] * std::sin(phi) + omega[2] * std::cos(phi)) / std::cos(theta);
+        const double dph = omega[0] + dps * std::sin(theta);
+        theta += dth * dt; psi += dps * dt; phi += dph * dt;
+    }
+};
+
 struct fp_solver {
     fp_config cfg{};
     std::string err;
@@ -77,6 +118,9 @@ struct fp_solver {
     int* h_nf = nullptr;
     // body
     BodyKin body{};
+    HostBody hb;
+    float* d_sdf = nullptr;
+    double *d_bpart = nullptr, *d_bforce = nullptr, *h_bforce = nullptr;
     // stats
     fp_step_stats stats{};
     int64_t steps = 0;
@@ -104,6 +148,11 @@ void free_grid(fp_solver* s) {
     dfree(pb.invd); dfree(pb.P); dfree(pb.X);
     dfree(pb.x64); dfree(pb.xd); dfree(pb.part); dfree(pb.bar); dfree(pb.out); dfree(pb.red);
     s->have_grid = false;
+}
+
+void free_body(fp_solver* s) {
+    dfree(s->d_sdf); dfree(s->d_bpart); dfree(s->d_bforce);
+    s->hb.loaded = false;
 }
 
 void free_particles(fp_solver* s) {
@@ -174,12 +223,54 @@ int alloc_particles(fp_solver* s, int64_t n) {
 
 float3 gravity3() { return make_float3(kGravity[0], kGravity[1], kGravity[2]); }
 
+bool body_on(const fp_solver* s) { return s->cfg.active_body && s->hb.loaded; }
+
+BodyShape body_shape(const fp_solver* s) {
+    const HostBody& h = s->hb;
+    BodyShape b{};
+    b.kind = h.kind;
+    b.com = make_float3(float(h.pos[0]), float(h.pos[1]), float(h.pos[2]));
+    b.radius = float(h.radius);
+    for (int i = 0; i < 9; ++i) b.rot[i] = float(h.R[i]);
+    b.local_com = make_float3(h.local_com[0], h.local_com[1], h.local_com[2]);
+    b.origin = make_float3(h.origin[0], h.origin[1], h.origin[2]);
+    b.cell = h.cell;
+    b.nx = h.nx; b.ny = h.ny; b.nz = h.nz;
+    b.sdf = s->d_sdf;
+    return b;
+}
+
+// The rigid-body velocity field seen by the RHS and the projection.
+BodyKin body_kin(const fp_solver* s) {
+    BodyKin b{};
+    b.active = 1;  // zero velocities unless a body is loaded or its state was set
+    const HostBody& h = s->hb;
+    b.vel = make_float3(float(h.vel[0]), float(h.vel[1]), float(h.vel[2]));
+    b.omega = make_float3(float(h.omega[0]), float(h.omega[1]), float(h.omega[2]));
+    b.com = make_float3(float(h.pos[0]), float(h.pos[1]), float(h.pos[2]));
+    return b;
+}
+
+void fill_body_stats(fp_solver* s) {
+    const HostBody& h = s->hb;
+    for (int a = 0; a < 3; ++a) {
+        s->stats.body_pos[a] = h.pos[a];
+        s->stats.body_vel[a] = h.vel[a];
+        s->stats.body_omega[a] = h.omega[a];
+    }
+    s->stats.body_angles[0] = h.theta; s->stats.body_angles[1] = h.psi; s->stats.body_angles[2] = h.phi;
+}
+
 // ---------------------------------------------------------------- phases
 void phase_label(fp_solver* s) {
     s->launches += 5;  // bin, label tiles, tile scan, start tiles, scatter
     cudaMemsetAsync(s->d_counts, 0, sizeof(int) * (s->g.nc() + 1), s->st);
+    if (body_on(s)) {
+        launch_mark_body(s->d_bodymark, s->g, body_shape(s), s->st);  // MarkBodyCellsFunctor at the body's pose
+        s->launches += 1;
+    }
     launch_bin(s->d_pos, s->np, s->g, s->d_counts, s->d_key, s->d_rank, s->st);
-    launch_label_scan(s->d_base, s->cfg.active_body ? s->d_bodymark : nullptr, s->d_counts, s->d_labels, s->d_start,
+    launch_label_scan(s->d_base, body_on(s) ? s->d_bodymark : nullptr, s->d_counts, s->d_labels, s->d_start,
                       s->d_tiles, s->g, s->st);
     launch_scatter(s->d_pos, s->d_vel, s->d_key, s->d_rank, s->d_start, s->np, s->d_pos2, s->d_vel2, s->st);
     std::swap(s->d_pos, s->d_pos2);
@@ -296,17 +387,36 @@ int solve_system(fp_solver* s, float* p_out) {
 
 int phase_pressure(fp_solver* s) {
     s->launches += 3;  // fluid tiles, tile scan, fluid build
-    BodyKin b = s->body;
-    b.active = s->cfg.active_body;
+    BodyKin b = body_kin(s);
     launch_pressure_setup(s->d_labels, s->d_u, s->d_v, s->d_w, s->g, s->cfg.dt, b, nullptr, s->d_p, s->pb, s->st);
     return solve_system(s, s->d_p);
 }
 
 void phase_project(fp_solver* s) {
-    BodyKin b = s->body;
-    b.active = s->cfg.active_body;
+    BodyKin b = body_kin(s);
     s->launches += 1;
     launch_project(s->d_u, s->d_v, s->d_w, s->d_p, s->d_labels, s->g, s->cfg.dt, b, s->st);
+}
+
+// updateBody (FluidSolver3D.cu:2793-2846): fluid force and torque from the
+// pressure (FP64 reduction on the GPU), gravity m*g, then integrate.
+int phase_body(fp_solver* s) {
+    if (!body_on(s)) return FP_OK;
+    launch_body_force(s->d_p, s->d_labels, s->g, body_shape(s), s->d_bpart, s->d_bforce, s->st);
+    s->launches += 2;
+    cudaMemcpyAsync(s->h_bforce, s->d_bforce, sizeof(double) * 6, cudaMemcpyDeviceToHost, s->st);
+    cudaError_t e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "body force");
+    HostBody& h = s->hb;
+    for (int a = 0; a < 3; ++a) {
+        h.force[a] = h.mass * double(kGravity[a]) + s->h_bforce[a];
+        h.torque[a] = s->h_bforce[3 + a];
+        s->stats.body_force[a] = h.force[a];
+        s->stats.body_torque[a] = h.torque[a];
+    }
+    h.integrate(double(s->cfg.dt));
+    fill_body_stats(s);
+    return FP_OK;
 }
 
 void phase_g2p_advect(fp_solver* s, int do_g2p, int do_adv) {
@@ -337,7 +447,9 @@ int one_step(fp_solver* s) {
     if (rc != FP_OK) return rc;
     phase_project(s);
     cudaEventRecord(s->ev[5], s->st);
-    cudaEventRecord(s->ev[6], s->st);  // body coupling slot
+    rc = phase_body(s);
+    if (rc != FP_OK) return rc;
+    cudaEventRecord(s->ev[6], s->st);
     cudaEventRecord(s->ev[7], s->st);
     phase_g2p_advect(s, 1, 1);
     cudaEventRecord(s->ev[8], s->st);
@@ -350,7 +462,7 @@ int one_step(fp_solver* s) {
     s->stats.t_forces = t[2];
     s->stats.t_pressure = t[3];
     s->stats.t_project = t[4];
-    s->stats.t_body = t[5];
+    s->stats.t_body = t[5] + t[6];
     s->stats.t_g2p = 0.0f;
     s->stats.t_advect = t[7];
     cudaEventElapsedTime(&s->stats.t_total, s->ev[0], s->ev[8]);
@@ -461,12 +573,12 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_out, sizeof(PcgOut));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_red, sizeof(double) * 2);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_nf, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_bforce, sizeof(double) * 6);
     if (e != cudaSuccess) {
         std::fprintf(stderr, "fp_create: %s\n", cudaGetErrorString(e));
         fp_destroy(s);
         return FP_ERR_CUDA;
     }
-    s->body.com = make_float3(s->cfg.body_pos[0], s->cfg.body_pos[1], s->cfg.body_pos[2]);
     *out = s;
     return FP_OK;
 }
@@ -476,6 +588,8 @@ int fp_destroy(fp_solver* s) {
     if (s->st) cudaStreamSynchronize(s->st);
     free_grid(s);
     free_particles(s);
+    free_body(s);
+    if (s->h_bforce) cudaFreeHost(s->h_bforce);
     for (auto& ev : s->ev) if (ev) cudaEventDestroy(ev);
     for (auto& ev : s->ev_pcg) if (ev) cudaEventDestroy(ev);
     if (s->h_out) cudaFreeHost(s->h_out);
@@ -525,8 +639,52 @@ int fp_get_dims(const fp_solver* s, int* W, int* H, int* D) {
 
 int fp_load_sdf(fp_solver* s, const char* path) {
     if (!s) return FP_ERR_ARG;
-    (void)path;
-    return s->fail(FP_ERR_STATE, "rigid-body coupling is not enabled in this build");
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "labels must be loaded before the body");
+    free_body(s);
+    HostBody& h = s->hb;
+    h = HostBody();
+    const double pi = 3.14159265358979323846;
+    std::vector<float> data;
+    if (!path) {
+        if (!(s->cfg.body_radius > 0.0f)) return s->fail(FP_ERR_ARG, "analytic body needs body_radius > 0");
+        h.kind = BODY_SPHERE;
+        h.radius = s->cfg.body_radius;
+        const double vol = 4.0 / 3.0 * pi * h.radius * h.radius * h.radius;
+        h.mass = s->cfg.body_density > 0.0f ? double(s->cfg.body_density) * 1000.0 * vol : double(s->cfg.body_mass);
+    } else {
+        // RigidBody::loadSDF (utility.cuh:231-338): the SDF box is centred on
+        // the initial position; local centre of mass = box centre.
+        int w, hh, d;
+        float org[3], cell;
+        if (!io::read_sdf(path, w, hh, d, org, cell, data, s->err)) return FP_ERR_IO;
+        h.kind = BODY_SDF;
+        h.nx = w; h.ny = hh; h.nz = d; h.cell = cell;
+        for (int a = 0; a < 3; ++a) h.origin[a] = org[a];
+        const float size[3] = {w * cell, hh * cell, d * cell};
+        for (int a = 0; a < 3; ++a) h.local_com[a] = org[a] + size[a] * 0.5f;
+        h.radius = size[0] / 2.0;  // FluidSolver3D.cu:167
+        h.mass = s->cfg.body_mass;
+    }
+    for (int a = 0; a < 3; ++a) h.pos[a] = s->cfg.body_pos[a];
+    h.inertia = 0.4 * h.mass * h.radius * h.radius;  // FluidSolver3D.cu:168
+    h.update_rotation();
+    cudaError_t e = cudaSuccess;
+    if (!data.empty()) {
+        e = dalloc(&s->d_sdf, data.size());
+        if (e == cudaSuccess) e = cudaMemcpy(s->d_sdf, data.data(), sizeof(float) * data.size(), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = dalloc(&s->d_bpart, size_t(body_force_partials()));
+    if (e == cudaSuccess) e = dalloc(&s->d_bforce, 6);
+    if (e != cudaSuccess) { free_body(s); return s->cuda_fail(e, "body upload"); }
+    h.loaded = true;
+    s->cfg.active_body = 1;
+    // init's marking before seeding (FluidSolver3D.cu:177-193)
+    launch_mark_body(s->d_bodymark, s->g, body_shape(s), s->st);
+    launch_apply_mark(s->d_labels, s->d_bodymark, s->g, s->st);
+    e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "body marking");
+    fill_body_stats(s);
+    return FP_OK;
 }
 
 int fp_set_particles(fp_solver* s, const float* pos, const float* vel, int64_t n) {
@@ -652,7 +810,7 @@ int fp_run_phase(fp_solver* s, int phase) {
         case FP_PHASE_FORCES: launch_forces(s->d_u, s->d_v, s->d_w, s->g, s->cfg.dt, gravity3(), s->st); break;
         case FP_PHASE_PRESSURE: rc = phase_pressure(s); break;
         case FP_PHASE_PROJECT: phase_project(s); break;
-        case FP_PHASE_BODY: break;
+        case FP_PHASE_BODY: rc = phase_body(s); break;
         case FP_PHASE_G2P: phase_g2p_advect(s, 1, 0); break;
         case FP_PHASE_ADVECT: phase_g2p_advect(s, 0, 1); break;
         default: return s->fail(FP_ERR_ARG, "unknown phase");
@@ -705,9 +863,12 @@ int fp_get_labels(fp_solver* s, uint8_t* out, int64_t n) {
 
 int fp_set_body_state(fp_solver* s, const float* pos, const float* vel, const float* omega) {
     if (!s) return FP_ERR_ARG;
-    if (pos) s->body.com = make_float3(pos[0], pos[1], pos[2]);
-    if (vel) s->body.vel = make_float3(vel[0], vel[1], vel[2]);
-    if (omega) s->body.omega = make_float3(omega[0], omega[1], omega[2]);
+    for (int a = 0; a < 3; ++a) {
+        if (pos) s->hb.pos[a] = pos[a];
+        if (vel) s->hb.vel[a] = vel[a];
+        if (omega) s->hb.omega[a] = omega[a];
+    }
+    fill_body_stats(s);
     return FP_OK;
 }
 

@@ -70,6 +70,36 @@ inline R trilin(R xd, R yd, R zd, R c000, R c100, R c001, R c101, R c010, R c110
 
 template <class R> inline R clamp01(R f) { return std::min(std::max(f, R(0)), R(1)); }
 
+// Rigid body (RigidBody, utility.cuh:195-491) with an analytic sphere SDF.
+struct OBody {
+    bool loaded = false;
+    double pos[3] = {0, 0, 0}, vel[3] = {0, 0, 0}, omega[3] = {0, 0, 0};
+    double theta = 0, psi = 0, phi = 0, Rm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    double mass = 1, inertia = 1, radius = 0;
+    double force[3] = {0, 0, 0}, torque[3] = {0, 0, 0};
+    void update_rotation() {  // utility.cuh:470-484
+        const double ct = std::cos(theta), st = std::sin(theta), cp = std::cos(psi), sp = std::sin(psi),
+                     cf = std::cos(phi), sf = std::sin(phi);
+        Rm[0] = ct * cp; Rm[1] = st * sf - ct * cf * sp; Rm[2] = cf * st + ct * sf * sp;
+        Rm[3] = sp;      Rm[4] = cf * cp;                Rm[5] = -cp * sf;
+        Rm[6] = -cp * st; Rm[7] = ct * sf + cf * st * sp; Rm[8] = ct * cf - st * sf * sp;
+    }
+    void integrate(double dt) {  // utility.cuh:408-467
+        for (int a = 0; a < 3; ++a) { vel[a] += force[a] / mass * dt; pos[a] += vel[a] * dt; }
+        const double pi = 3.14159265358979323846;
+        theta = std::min(std::max(theta, -pi), pi);
+        update_rotation();
+        const double tl[3] = {Rm[0] * torque[0] + Rm[3] * torque[1] + Rm[6] * torque[2],
+                              Rm[1] * torque[0] + Rm[4] * torque[1] + Rm[7] * torque[2],
+                              Rm[2] * torque[0] + Rm[5] * torque[1] + Rm[8] * torque[2]};
+        for (int a = 0; a < 3; ++a) omega[a] += tl[a] / inertia * dt;
+        const double dth = omega[1] * std::cos(phi) - omega[2] * std::sin(phi);
+        const double dps = (omega[1] * std::sin(phi) + omega[2] * std::cos(phi)) / std::cos(theta);
+        const double dph = omega[0] + dps * std::sin(theta);
+        theta += dth * dt; psi += dps * dt; phi += dph * dt;
+    }
+};
+
 template <class R> struct Sim3 {
     int W = 0, H = 0, D = 0;
     R dx = 0, dt = 0;
@@ -79,6 +109,7 @@ template <class R> struct Sim3 {
     double tol = 1e-12;     // relative residual of the FP64 solve
     int maxit = 100000;
     BodyKin<R> body;
+    OBody ob;
     std::vector<uint8_t> labels;
     std::vector<R> u, v, w, us, vs, ws, p;
     std::vector<R> px, py, pz, vx, vy, vz;
@@ -116,8 +147,23 @@ template <class R> struct Sim3 {
         j = std::min(std::max(j, 0), H - 1);
         k = std::min(std::max(k, 0), D - 1);
     }
+    // Sphere SDF in FP32 (the GPU's explicitly rounded float evaluation).
+    float sphere_sdf(float x, float y, float z) const {
+        const float cx = float(ob.pos[0]), cy = float(ob.pos[1]), cz = float(ob.pos[2]);
+        const float dxp = x - cx, dyp = y - cy, dzp = z - cz;
+        const float s2 = (dxp * dxp + dyp * dyp) + dzp * dzp;
+        return std::sqrt(s2) - float(ob.radius);
+    }
     void label_grid() {
-        for (auto& l : labels) l = (l == SOLID) ? SOLID : AIR;  // ClearNonSolidFunctor; BODY is re-marked below
+        for (auto& l : labels) l = (l == SOLID) ? SOLID : AIR;  // ClearNonSolidFunctor
+        if (ob.loaded) {  // MarkBodyCellsFunctor (:45-78) with the analytic sphere
+            const float fdx = float(dx);
+            for (int k = 0; k < D; ++k) for (int j = 0; j < H; ++j) for (int i = 0; i < W; ++i) {
+                uint8_t& l = labels[cidx(i, j, k)];
+                if (l != SOLID && sphere_sdf((float(i) + 0.5f) * fdx, (float(j) + 0.5f) * fdx, (float(k) + 0.5f) * fdx) <= 0.0f)
+                    l = BODY;
+            }
+        }
         for (size_t q = 0; q < np(); ++q) {
             int i, j, k;
             cell_of(px[q], py[q], pz[q], i, j, k);
@@ -489,7 +535,65 @@ template <class R> struct Sim3 {
         for (long long q = 0; q < (long long)np(); ++q) advect_one(px[q], py[q], pz[q]);
     }
 
-    // frameStep (:3030-3098) without the body phase.
+    // Fluid force and torque on the body: -sum_f theta_f (p_R - p_L) dx^2 e_axis
+    // over faces with body fraction theta_f = clamp(1/2 - phi(x_f)/dx, 0, 1);
+    // BODY cells take the mean pressure of their FLUID/AIR neighbours; faces
+    // touching SOLID or the outside are skipped.  FP64 accumulation.
+    bool p_ext(int i, int j, int k, double& out) const {
+        const uint8_t l = lab(i, j, k);
+        if (l == SOLID) return false;
+        if (l != BODY) { out = double(p[cidx(i, j, k)]); return true; }
+        const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+        float acc = 0.0f;
+        int n = 0;
+        for (auto& o : off) {
+            const uint8_t ln = lab(i + o[0], j + o[1], k + o[2]);
+            if (ln == FLUID || ln == AIR) { acc += float(p[cidx(i + o[0], j + o[1], k + o[2])]); ++n; }
+        }
+        out = n ? double(acc / float(n)) : 0.0;
+        return true;
+    }
+    void body_force(double out[6]) const {
+        for (int m = 0; m < 6; ++m) out[m] = 0.0;
+        const float fdx = float(dx);
+        const double area = double(fdx) * double(fdx);
+        for (int k = 0; k <= D; ++k) for (int j = 0; j <= H; ++j) for (int i = 0; i <= W; ++i)
+            for (int ax = 0; ax < 3; ++ax) {
+                if (ax == 0 && (j >= H || k >= D)) continue;
+                if (ax == 1 && (i >= W || k >= D)) continue;
+                if (ax == 2 && (i >= W || j >= H)) continue;
+                const float xf = ax == 0 ? float(i) * fdx : (float(i) + 0.5f) * fdx;
+                const float yf = ax == 1 ? float(j) * fdx : (float(j) + 0.5f) * fdx;
+                const float zf = ax == 2 ? float(k) * fdx : (float(k) + 0.5f) * fdx;
+                const float th = std::min(std::max(0.5f - sphere_sdf(xf, yf, zf) / fdx, 0.0f), 1.0f);
+                if (th <= 0.0f) continue;
+                double pl, pr;
+                if (!p_ext(i - (ax == 0), j - (ax == 1), k - (ax == 2), pl) || !p_ext(i, j, k, pr)) continue;
+                const double dF = -double(th) * (pr - pl) * area;
+                const double rx = double(xf) - double(float(ob.pos[0])), ry = double(yf) - double(float(ob.pos[1])),
+                             rz = double(zf) - double(float(ob.pos[2]));
+                const double fx = ax == 0 ? dF : 0.0, fy = ax == 1 ? dF : 0.0, fz = ax == 2 ? dF : 0.0;
+                out[0] += fx; out[1] += fy; out[2] += fz;
+                out[3] += ry * fz - rz * fy; out[4] += rz * fx - rx * fz; out[5] += rx * fy - ry * fx;
+            }
+    }
+    // updateBody (:2793-2846) with the pressure-integral force.
+    void body_phase() {
+        if (!ob.loaded) return;
+        double f[6];
+        body_force(f);
+        const double g[3] = {0.0, double(-9.81f), 0.0};
+        for (int a = 0; a < 3; ++a) { ob.force[a] = ob.mass * g[a] + f[a]; ob.torque[a] = f[3 + a]; }
+        ob.integrate(double(float(dt)));
+        sync_body_kin();
+    }
+    void sync_body_kin() {
+        body.vel = {R(float(ob.vel[0])), R(float(ob.vel[1])), R(float(ob.vel[2]))};
+        body.omega = {R(float(ob.omega[0])), R(float(ob.omega[1])), R(float(ob.omega[2]))};
+        body.com = {R(float(ob.pos[0])), R(float(ob.pos[1])), R(float(ob.pos[2]))};
+    }
+
+    // frameStep (:3030-3098).
     int phase(int ph) {
         switch (ph) {
             case 0: label_grid(); return 0;
@@ -498,7 +602,7 @@ template <class R> struct Sim3 {
             case 3: forces(); return 0;
             case 4: return pressure();
             case 5: project(); return 0;
-            case 6: return 0;  // body update: no body in the oracle's core step
+            case 6: body_phase(); return 0;
             case 7: g2p(); return 0;
             case 8: advect(); return 0;
         }
@@ -763,6 +867,34 @@ int or3_grid_io(void* p, int which, double* buf, int set) {
         return 0;
     });
 }
+// Analytic sphere body (radius r, mass m) at pos, at rest.
+void or3_set_sphere(void* p, const double* pos, double r, double m) {
+    with(static_cast<Handle*>(p), [&](auto& s) {
+        s.ob = OBody();
+        s.ob.loaded = true;
+        for (int a = 0; a < 3; ++a) s.ob.pos[a] = pos[a];
+        s.ob.radius = r; s.ob.mass = m; s.ob.inertia = 0.4 * m * r * r;
+        s.ob.update_rotation();
+        s.sync_body_kin();
+        return 0;
+    });
+}
+// out: pos[3] vel[3] omega[3] angles[3] force[3] torque[3]
+void or3_body_state(void* p, double* out) {
+    with(static_cast<Handle*>(p), [&](auto& s) {
+        const OBody& b = s.ob;
+        for (int a = 0; a < 3; ++a) {
+            out[a] = b.pos[a]; out[3 + a] = b.vel[a]; out[6 + a] = b.omega[a];
+            out[12 + a] = b.force[a]; out[15 + a] = b.torque[a];
+        }
+        out[9] = b.theta; out[10] = b.psi; out[11] = b.phi;
+        return 0;
+    });
+}
+void or3_body_force(void* p, double* out) {
+    with(static_cast<Handle*>(p), [&](auto& s) { s.body_force(out); return 0; });
+}
+
 int or3_phase(void* p, int ph) { return with(static_cast<Handle*>(p), [&](auto& s) { return s.phase(ph); }); }
 int or3_step(void* p, int n) {
     return with(static_cast<Handle*>(p), [&](auto& s) { int rc = 0; for (int i = 0; i < n; ++i) rc = s.step(); return rc; });

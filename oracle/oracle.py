@@ -49,6 +49,9 @@ def lib():
         L.or3_set_params.argtypes = [P, D, D, D, I]
         L.or3_set_body.argtypes = [P, P, P, P]
         L.or3_set_rk2.argtypes = [P, I]
+        L.or3_set_sphere.argtypes = [P, P, D, D]
+        L.or3_body_state.argtypes = [P, P]
+        L.or3_body_force.argtypes = [P, P]
         L.or3_set_labels.argtypes = [P, P]
         L.or3_get_labels.argtypes = [P, P]
         L.or3_set_particles.argtypes = [P, I64, P, P]
@@ -163,6 +166,21 @@ class Sim3:
     def set_body(self, vel, omega, com):
         a = [np.ascontiguousarray(x, np.float64) for x in (vel, omega, com)]
         lib().or3_set_body(self.h, *[_p(x) for x in a])
+
+    def set_sphere(self, pos, radius, mass):
+        a = np.ascontiguousarray(pos, np.float64)
+        lib().or3_set_sphere(self.h, _p(a), radius, mass)
+
+    def body_state(self):
+        out = np.zeros(18, np.float64)
+        lib().or3_body_state(self.h, _p(out))
+        return {"pos": out[0:3], "vel": out[3:6], "omega": out[6:9], "angles": out[9:12], "force": out[12:15],
+                "torque": out[15:18]}
+
+    def body_force(self):
+        out = np.zeros(6, np.float64)
+        lib().or3_body_force(self.h, _p(out))
+        return out
 
     def set_labels(self, labels):
         lab = np.ascontiguousarray(labels, np.uint8).reshape(-1)

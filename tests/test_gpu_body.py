@@ -1,0 +1,100 @@
+"""Rigid-body coupling on the GPU against the oracle and against physics.
+
+The body is an analytic sphere (the rigid-body drop configuration).  Marking
+of BODY cells is bit-exact; the face-fraction pressure force equals the
+oracle's FP64 evaluation on the same pressure; the force on a submerged body
+in still water is its buoyancy.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _pool(O, n=40, level=0.7, c=(0.5, 0.35, 0.5), r=0.12, density=0.5, seed=3, dt=0.002):
+    from fluidprjct_b200 import capi, scenes
+    dx = 1.0 / n
+    lab = scenes.box_3d(n, n, n, dx, 2.0, level, 2.0)
+    s = capi.Solver(dx=dx, dt=dt, pic_weight=0.05, solver="pcg_mixed", tol=1e-9, body_radius=r,
+                    body_density=density, body_pos=c, active_body=1)
+    s.set_labels(lab)
+    s.load_sdf(None)
+    marked = s.labels()
+    lab2 = lab.copy()
+    lab2[marked == 3] = 3
+    pos = O.seed3d(lab2, dx, 8, seed)
+    s.set_particles(pos)
+    r32 = float(np.float32(r))  # the library holds the radius as float32
+    mass = float(np.float32(density)) * 1000.0 * 4.0 / 3.0 * np.pi * r32 ** 3
+    o = O.Sim3(n, n, n, dx, dt, fp64=False, pic_weight=0.05, tol=1e-12)
+    o.set_labels(lab)
+    o.set_sphere(np.array(c, np.float64), r, mass)
+    o.set_particles(pos)
+    return s, o, lab, pos, mass
+
+
+def test_body_marking_bit_exact(O):
+    from fluidprjct_b200 import capi
+    s, o, lab, pos, _ = _pool(O, n=48, c=(0.47, 0.41, 0.53), r=0.13)
+    s.phase(capi.PHASE_LABEL)
+    o.phase(O.PH_LABEL)
+    assert np.array_equal(s.labels(), o.labels())
+    assert int((s.labels() == 3).sum()) > 1000
+
+
+def test_body_force_matches_oracle_and_buoyancy(O):
+    from fluidprjct_b200 import capi
+    s, o, lab, pos, mass = _pool(O, n=48)
+    for ph_s, ph_o in ((capi.PHASE_LABEL, O.PH_LABEL), (capi.PHASE_P2G, O.PH_P2G), (capi.PHASE_SAVE, O.PH_SAVE),
+                       (capi.PHASE_FORCES, O.PH_FORCES), (capi.PHASE_PRESSURE, O.PH_PRESSURE)):
+        s.phase(ph_s)
+        o.phase(ph_o)
+    # same pressure on both sides -> the FP64 force reductions must agree
+    o.set_grid(O.GRID_P, s.grid(capi.GRID_P).astype(np.float64))
+    f_ref = o.body_force()
+    s.phase(capi.PHASE_BODY)
+    st = s.stats()
+    f_gpu = np.array(st["body_force"]) - mass * np.array([0.0, -9.81, 0.0])
+    assert np.allclose(f_gpu, f_ref[:3], rtol=1e-9, atol=1e-9 * abs(f_ref[1]))
+    assert np.allclose(np.array(st["body_torque"]), f_ref[3:], atol=1e-9 * abs(f_ref[1]))
+    # buoyancy of the fully submerged sphere in still water (staircase error O(dx/r))
+    V = 4.0 / 3.0 * np.pi * 0.12 ** 3
+    assert 0.97 < f_gpu[1] / (1000 * 9.81 * V) < 1.12
+    # integration: v = (F + m g)/m * dt from rest
+    assert np.allclose(st["body_vel"][1], (f_gpu[1] - mass * 9.81) / mass * 0.002, rtol=1e-6)
+
+
+def test_body_steps_match_oracle(O):
+    from fluidprjct_b200 import capi
+    s, o, lab, pos, mass = _pool(O, n=40, c=(0.5, 0.62, 0.5), r=0.1)
+    s.step(3)
+    o.step(3)
+    st = s.stats()
+    ob = o.body_state()
+    assert np.allclose(st["body_pos"], ob["pos"], atol=1e-6)
+    assert np.allclose(st["body_vel"], ob["vel"], rtol=1e-3, atol=1e-5)
+    assert np.array_equal(s.labels(), o.labels())
+    for g, go in ((capi.GRID_U, O.GRID_U), (capi.GRID_V, O.GRID_V), (capi.GRID_P, O.GRID_P)):
+        assert rel_l2(s.grid(g), o.grid(go)) < 1e-4
+
+
+def test_rigid_body_drop_160(O):
+    """Rigid-body drop at full size: 160^3, water y < 0.35 (8 ppc), sphere
+    r = 0.12, density 0.5, released at (0.5, 0.7, 0.5) at rest."""
+    from fluidprjct_b200 import capi, scenes
+    n = 160
+    lab = scenes.pool_3d(n, 0.35)
+    s = capi.Solver(dx=1.0 / n, dt=0.002, pic_weight=0.05, solver="pcg_mixed", tol=1e-6, body_radius=0.12,
+                    body_density=0.5, body_pos=(0.5, 0.7, 0.5), active_body=1, advection="rk2")
+    s.set_labels(lab)
+    s.load_sdf(None)
+    s.seed_particles(8, 2)
+    assert s.num_particles == 158 * 55 * 158 * 8
+    s.step(5)
+    st = s.stats()
+    assert st["solve_status"] == 0 and st["residual"] <= 1e-6
+    # in the air the body falls freely: v_y = -g t after 5 steps
+    assert abs(st["body_vel"][1] - (-9.81 * 0.002 * 5)) < 1e-3
+    assert abs(st["body_pos"][0] - 0.5) < 1e-6 and abs(st["body_pos"][2] - 0.5) < 1e-6
