@@ -65,14 +65,17 @@ __device__ __forceinline__ float trilin(float xd, float yd, float zd, float c000
 // MAC sample stencil: base corner index and fractions.  Base indices are
 // clamped so that base+1 stays inside the face grid; for positions inside
 // [0, (N-1)*dx] (where advection keeps particles) these are the reference's
-// clamps of interpVelDevice3D (FluidSolver3D.cu:1059-1140).
+// clamps of interpVelDevice3D (FluidSolver3D.cu:1059-1140).  A 2D grid is a
+// grid with D = 1: its z corner pairs collapse onto one slice (slice stride 0
+// in sample()) with weight 0 on the duplicate, which is exact bilinear
+// interpolation.
 struct Stencil {
     int base;
     float fx, fy, fz;
 };
 __device__ __forceinline__ Stencil stencil_u(float rx, float ry, float rz, const Dims& g) {
     int i = int(floorf(rx)), j = int(floorf(ry - 0.5f)), k = int(floorf(rz - 0.5f));
-    i = clampi(i, 0, g.W - 1); j = clampi(j, 0, g.H - 2); k = clampi(k, 0, g.D - 2);
+    i = clampi(i, 0, g.W - 1); j = clampi(j, 0, g.H - 2); k = clampi(k, 0, max(g.D - 2, 0));
     Stencil s;
     s.fx = clamp01(rx - float(i)); s.fy = clamp01((ry - 0.5f) - float(j)); s.fz = clamp01((rz - 0.5f) - float(k));
     s.base = i + j * (g.W + 1) + k * (g.W + 1) * g.H;
@@ -80,7 +83,7 @@ __device__ __forceinline__ Stencil stencil_u(float rx, float ry, float rz, const
 }
 __device__ __forceinline__ Stencil stencil_v(float rx, float ry, float rz, const Dims& g) {
     int i = int(floorf(rx - 0.5f)), j = int(floorf(ry)), k = int(floorf(rz - 0.5f));
-    i = clampi(i, 0, g.W - 2); j = clampi(j, 0, g.H - 1); k = clampi(k, 0, g.D - 2);
+    i = clampi(i, 0, g.W - 2); j = clampi(j, 0, g.H - 1); k = clampi(k, 0, max(g.D - 2, 0));
     Stencil s;
     s.fx = clamp01((rx - 0.5f) - float(i)); s.fy = clamp01(ry - float(j)); s.fz = clamp01((rz - 0.5f) - float(k));
     s.base = i + j * g.W + k * g.W * (g.H + 1);
@@ -110,11 +113,15 @@ __device__ __forceinline__ float sample_delta(const float* __restrict__ f, const
     return trilin(s.fx, s.fy, s.fz, d(0), d(1), d(sxy), d(1 + sxy), d(sx), d(1 + sx), d(sx + sxy), d(1 + sx + sxy));
 }
 
+// Slice strides of the u and v face grids for sample() (0 on a 2D grid).
+__device__ __forceinline__ int sxy_u(const Dims& g) { return g.D > 1 ? (g.W + 1) * g.H : 0; }
+__device__ __forceinline__ int sxy_v(const Dims& g) { return g.D > 1 ? g.W * (g.H + 1) : 0; }
+
 __device__ __forceinline__ float3 interp_vel(const float* __restrict__ u, const float* __restrict__ v,
                                              const float* __restrict__ w, const Dims& g, float3 pos) {
     float rx = pos.x / g.dx, ry = pos.y / g.dx, rz = pos.z / g.dx;
-    return make_float3(sample(u, stencil_u(rx, ry, rz, g), g.W + 1, (g.W + 1) * g.H),
-                       sample(v, stencil_v(rx, ry, rz, g), g.W, g.W * (g.H + 1)),
+    return make_float3(sample(u, stencil_u(rx, ry, rz, g), g.W + 1, sxy_u(g)),
+                       sample(v, stencil_v(rx, ry, rz, g), g.W, sxy_v(g)),
                        sample(w, stencil_w(rx, ry, rz, g), g.W, g.W * g.H));
 }
 

@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256) k_g2p_advect(float4* __restrict__ pos, fl
         const float4 V = vel[q];
         const float rx = p.x / dx, ry = p.y / dx, rz = p.z / dx;
         const Stencil su = stencil_u(rx, ry, rz, g), sv = stencil_v(rx, ry, rz, g), sw = stencil_w(rx, ry, rz, g);
-        const int sxu = g.W + 1, sxyu = (g.W + 1) * g.H, sxv = g.W, sxyv = g.W * (g.H + 1), sxw = g.W, sxyw = g.W * g.H;
+        const int sxu = g.W + 1, sxyu = sxy_u(g), sxv = g.W, sxyv = sxy_v(g), sxw = g.W, sxyw = g.W * g.H;
         const float uP = sample(u, su, sxu, sxyu), dU = sample_delta(u, us, su, sxu, sxyu);
         const float vP = sample(v, sv, sxv, sxyv), dV = sample_delta(v, vs, sv, sxv, sxyv);
         const float wP = sample(w, sw, sxw, sxyw), dW = sample_delta(w, ws, sw, sxw, sxyw);

@@ -430,8 +430,9 @@ void phase_g2p_advect(fp_solver* s, int do_g2p, int do_adv) {
 int check_ready(fp_solver* s) {
     if (!s) return FP_ERR_ARG;
     if (!s->have_grid) return s->fail(FP_ERR_STATE, "labels not loaded");
-    if (s->cfg.dim != 3) return s->fail(FP_ERR_ARG, "only dim = 3 is supported by this entry point");
-    if (s->W < 2 || s->H < 2 || s->D < 2) return s->fail(FP_ERR_ARG, "grid must be at least 2 cells on every axis");
+    if (s->W < 2 || s->H < 2) return s->fail(FP_ERR_ARG, "grid must be at least 2 cells wide and high");
+    if (s->cfg.dim == 3 && s->D < 2) return s->fail(FP_ERR_ARG, "a 3D grid needs at least 2 cells in depth");
+    if (s->cfg.dim == 2 && s->D != 1) return s->fail(FP_ERR_ARG, "a 2D grid has depth 1");
     return FP_OK;
 }
 

@@ -417,13 +417,13 @@ template <class R> struct Sim3 {
     inline Stencil st_u(R rx, R ry, R rz) const {
         const R h = R(0.5f);
         int i = int(std::floor(rx)), j = int(std::floor(ry - h)), k = int(std::floor(rz - h));
-        i = std::min(std::max(i, 0), W - 1); j = std::min(std::max(j, 0), H - 2); k = std::min(std::max(k, 0), D - 2);
+        i = std::min(std::max(i, 0), W - 1); j = std::min(std::max(j, 0), H - 2); k = std::min(std::max(k, 0), std::max(D - 2, 0));
         return {i, j, k, clamp01(rx - R(i)), clamp01((ry - h) - R(j)), clamp01((rz - h) - R(k))};
     }
     inline Stencil st_v(R rx, R ry, R rz) const {
         const R h = R(0.5f);
         int i = int(std::floor(rx - h)), j = int(std::floor(ry)), k = int(std::floor(rz - h));
-        i = std::min(std::max(i, 0), W - 2); j = std::min(std::max(j, 0), H - 1); k = std::min(std::max(k, 0), D - 2);
+        i = std::min(std::max(i, 0), W - 2); j = std::min(std::max(j, 0), H - 1); k = std::min(std::max(k, 0), std::max(D - 2, 0));
         return {i, j, k, clamp01((rx - h) - R(i)), clamp01(ry - R(j)), clamp01((rz - h) - R(k))};
     }
     inline Stencil st_w(R rx, R ry, R rz) const {
@@ -438,10 +438,14 @@ template <class R> struct Sim3 {
         auto val = [&](size_t o) { return g ? f[b + o] - (*g)[b + o] : f[b + o]; };
         return trilin(s.fx, s.fy, s.fz, val(0), val(1), val(sxy), val(1 + sxy), val(sx), val(1 + sx), val(sx + sxy), val(1 + sx + sxy));
     }
+    // Slice strides of u and v for sample(); a 2D grid (D = 1) uses 0, so the
+    // duplicate z corners carry weight 0 (exact bilinear interpolation).
+    size_t sxy_u() const { return D > 1 ? size_t(W + 1) * H : 0; }
+    size_t sxy_v() const { return D > 1 ? size_t(W) * (H + 1) : 0; }
     inline V3<R> interp_vel(V3<R> pos) const {
         R rx = pos.x / dx, ry = pos.y / dx, rz = pos.z / dx;
-        return {sample(u, nullptr, st_u(rx, ry, rz), size_t(W + 1), size_t(W + 1) * H),
-                sample(v, nullptr, st_v(rx, ry, rz), size_t(W), size_t(W) * (H + 1)),
+        return {sample(u, nullptr, st_u(rx, ry, rz), size_t(W + 1), sxy_u()),
+                sample(v, nullptr, st_v(rx, ry, rz), size_t(W), sxy_v()),
                 sample(w, nullptr, st_w(rx, ry, rz), size_t(W), size_t(W) * H)};
     }
 
@@ -451,7 +455,7 @@ template <class R> struct Sim3 {
         for (long long q = 0; q < (long long)np(); ++q) {
             R rx = px[q] / dx, ry = py[q] / dx, rz = pz[q] / dx;
             Stencil su = st_u(rx, ry, rz), sv = st_v(rx, ry, rz), sw = st_w(rx, ry, rz);
-            size_t sxu = W + 1, sxyu = size_t(W + 1) * H, sxv = W, sxyv = size_t(W) * (H + 1), sxw = W, sxyw = size_t(W) * H;
+            size_t sxu = W + 1, sxyu = sxy_u(), sxv = W, sxyv = sxy_v(), sxw = W, sxyw = size_t(W) * H;
             R uP = sample(u, nullptr, su, sxu, sxyu), dU = sample(u, &us, su, sxu, sxyu);
             R vP = sample(v, nullptr, sv, sxv, sxyv), dV = sample(v, &vs, sv, sxv, sxyv);
             R wP = sample(w, nullptr, sw, sxw, sxyw), dW = sample(w, &ws, sw, sxw, sxyw);
@@ -688,6 +692,34 @@ int64_t or_seed3d(const uint8_t* labels, int W, int H, int D, float dx, int ppc,
             y = std::clamp(y, j * dx, (j + 1) * dx);
             z = std::clamp(z, k * dx, (k + 1) * dx);
             if (pos) { pos[3 * n] = x; pos[3 * n + 1] = y; pos[3 * n + 2] = z; }
+            ++n;
+        }
+    }
+    return n;
+}
+
+// 2D seeding (FluidSolver2D.cu:114-158): quadrant centres (top-left,
+// top-right, bottom-right, bottom-left), jitter U(-0.24, 0.24)*dx, clamped to
+// the cell; z = 0.  pos (n x 3) may be null.
+int64_t or_seed2d(const uint8_t* labels, int W, int H, float dx, int ppc, uint32_t seed, float* pos) {
+    std::mt19937 gen(seed);
+    std::uniform_int_distribution<> sub(0, 3);
+    std::uniform_real_distribution<> jit(-0.24f, 0.24f);
+    int64_t n = 0;
+    for (int j = 0; j < H; ++j) for (int i = 0; i < W; ++i) {
+        if (labels[size_t(i) + size_t(j) * W] != FLUID) continue;
+        const float cx = (i + 0.5f) * dx, cy = (j + 0.5f) * dx;
+        const float sc[4][2] = {{cx - 0.25f * dx, cy + 0.25f * dx}, {cx + 0.25f * dx, cy + 0.25f * dx},
+                                {cx + 0.25f * dx, cy - 0.25f * dx}, {cx - 0.25f * dx, cy - 0.25f * dx}};
+        for (int q = 0; q < ppc; ++q) {
+            const int s = sub(gen);
+            const float jx = float(jit(gen) * dx), jy = float(jit(gen) * dx);
+            float x = sc[s][0] + jx, y = sc[s][1] + jy;
+            if (pos) {
+                pos[3 * n] = std::clamp(x, cx - 0.5f * dx, cx + 0.5f * dx);
+                pos[3 * n + 1] = std::clamp(y, cy - 0.5f * dx, cy + 0.5f * dx);
+                pos[3 * n + 2] = 0.0f;
+            }
             ++n;
         }
     }

@@ -41,6 +41,8 @@ def lib():
         L.or_seed3d.argtypes = [P, I, I, I, C.c_float, I, U32, P]
         L.or_seed3d.restype = I64
         L.or_bin3d.argtypes = [P, I64, I, I, I, C.c_float, P, P]
+        L.or_seed2d.argtypes = [P, I, I, C.c_float, I, U32, P]
+        L.or_seed2d.restype = I64
         L.or_build_csr_upper.argtypes = [P, I, I, I, P, P, P, P, P]
         L.or_cg_csr_upper.argtypes = [I, P, P, P, P, P, D, I, P]
         L.or3_create.argtypes = [I, I, I, D, D, I]
@@ -108,6 +110,15 @@ def seed3d(labels: np.ndarray, dx: float, ppc: int, seed: int) -> np.ndarray:
     n = lib().or_seed3d(_p(lab), W, H, D, dx, ppc, seed, None)
     pos = np.zeros((n, 3), np.float32)
     lib().or_seed3d(_p(lab), W, H, D, dx, ppc, seed, _p(pos))
+    return pos
+
+
+def seed2d(labels: np.ndarray, dx: float, ppc: int, seed: int) -> np.ndarray:
+    lab = np.ascontiguousarray(labels, np.uint8)
+    H, W = lab.shape
+    n = lib().or_seed2d(_p(lab), W, H, dx, ppc, seed, None)
+    pos = np.zeros((n, 3), np.float32)
+    lib().or_seed2d(_p(lab), W, H, dx, ppc, seed, _p(pos))
     return pos
 
 

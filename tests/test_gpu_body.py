@@ -56,14 +56,15 @@ def test_body_force_matches_oracle_and_buoyancy(O):
     f_ref = o.body_force()
     s.phase(capi.PHASE_BODY)
     st = s.stats()
-    f_gpu = np.array(st["body_force"]) - mass * np.array([0.0, -9.81, 0.0])
+    g = float(np.float32(-9.81))  # the library's gravity constant is the float -9.81f
+    f_gpu = np.array(st["body_force"]) - mass * np.array([0.0, g, 0.0])
     assert np.allclose(f_gpu, f_ref[:3], rtol=1e-9, atol=1e-9 * abs(f_ref[1]))
     assert np.allclose(np.array(st["body_torque"]), f_ref[3:], atol=1e-9 * abs(f_ref[1]))
     # buoyancy of the fully submerged sphere in still water (staircase error O(dx/r))
     V = 4.0 / 3.0 * np.pi * 0.12 ** 3
     assert 0.97 < f_gpu[1] / (1000 * 9.81 * V) < 1.12
     # integration: v = (F + m g)/m * dt from rest
-    assert np.allclose(st["body_vel"][1], (f_gpu[1] - mass * 9.81) / mass * 0.002, rtol=1e-6)
+    assert np.allclose(st["body_vel"][1], (f_gpu[1] + mass * g) / mass * float(np.float32(0.002)), rtol=1e-6)
 
 
 def test_body_steps_match_oracle(O):

@@ -139,3 +139,22 @@ def test_oracle_projection_is_divergence_free(O):
     b_after = sim.rhs()
     fl = sim.labels().ravel() == 1
     assert np.linalg.norm(b_after[fl]) < 1e-8 * np.linalg.norm(b_before[fl])
+
+
+def test_oracle_2d_dam_break_behaviour(O):
+    """2D dam break (64^2, 4 ppc): particles are conserved, stay in the
+    domain and the column collapses (its front advances)."""
+    from fluidprjct_b200.scenes import dam_break_2d
+    lab = dam_break_2d(64)
+    dx = 1 / 64
+    pos = O.seed2d(lab, dx, 4, 0)
+    assert len(pos) == 775 * 4 and np.all(pos[:, 2] == 0)
+    s = O.Sim3(64, 64, 1, dx, 0.005, fp64=False, pic_weight=0.05, tol=1e-8)
+    s.set_labels(lab[None])
+    s.set_particles(pos)
+    s.step(40)
+    p, v = s.particles()
+    assert p.shape[0] == len(pos) and np.isfinite(p).all()
+    assert p[:, :2].min() >= 0 and p[:, :2].max() <= 63 * dx + 1e-6 and np.all(p[:, 2] == 0)
+    assert p[:, 0].max() > pos[:, 0].max() + 0.1   # the front moved right
+    assert s.stats()["relres"] <= 1e-8
