@@ -24,6 +24,7 @@ SOURCES = [
     "kernels_pressure.cu",
     "kernels_advect.cu",
     "kernels_body.cu",
+    "kernels_mg.cu",
     "solver.cu",
     "io.cpp",
 ]

@@ -47,6 +47,29 @@ struct PressureBufs {
     double* red;          // [2] FP64 reduction results (true residual)
 };
 
+// -------- multigrid-preconditioned PCG (kernels_mg.cu) --------
+constexpr int MG_MAX_LEVELS = 8;
+constexpr int MG_BLOCK_CELLS = 512;  // levels at most this big are swept by one block
+// One multigrid level: padded dense grids with a SOLID / zero halo.
+struct MgLevel {
+    int W, H, D;    // interior cells
+    int sy, sz;     // padded strides: W+2 and (W+2)*(H+2)
+    uint8_t* lab;   // labels (BODY folded into SOLID)
+    float* x;       // correction (level 0: the preconditioned residual z)
+    float* b;       // right-hand side (level 0: the residual r)
+};
+// Fills lv[].W/H/D/sy/sz of the level hierarchy for a W x H x D grid; returns L.
+int mg_levels_for(int W, int H, int D, MgLevel* lv);
+int mg_max_blocks();
+// Level labels from the cell labels (per solve).
+void launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStream_t st);
+// MG-preconditioned PCG (FP32 V-cycle, FP64 Krylov vectors and reductions) for
+// A x = rhs (compact) to ||r||/||rhs|| <= tol; solution in pb.X (FP64
+// compact).  p, q, xs, r are level-0 padded dense FP64 work grids, zero at
+// entry and on exit.
+int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
+                  const float* rhs, double tol, int maxit, cudaStream_t st);
+
 // -------- labelling and the particle sort (kernels_sort.cu) --------
 // counts[nc] must be zero on entry.  Writes key/rank per particle.
 void launch_bin(const float4* pos, int64_t np, Dims g, int* counts, int* key, int* rank, cudaStream_t st);

@@ -1,0 +1,463 @@
+// kernels_mg.cu -- multigrid-preconditioned conjugate gradients for the
+// pressure Poisson system (FP_SOLVER_PCG_MG).
+//
+// Same system as the reference's cuDSS solve (FluidSolver3D.cu:1815-2062):
+// unit 7-point operator over FLUID cells, AIR = Dirichlet 0, SOLID/BODY and
+// out-of-domain = Neumann.  Preconditioner: one geometric multigrid V-cycle.
+//   * Levels coarsen by 2 per axis; a coarse cell is AIR if any child is AIR,
+//     else FLUID if any child is FLUID, else SOLID (Dirichlet priority), and
+//     carries the rediscretised unit operator of its labels.
+//   * Restriction sums the FLUID children's residuals and scales by 1/4 (3D)
+//     or 1/2 (2D); prolongation adds the coarse value to every FLUID child.
+//     With these transfers R*A*P equals the coarse unit operator, and P is a
+//     multiple of R^T.
+//   * Smoother: red-black Gauss-Seidel, red then black going down, black then
+//     red coming up; the coarsest level does the same symmetric sweeps.  The
+//     V-cycle is therefore a symmetric positive definite preconditioner.
+//     After the black sweep only red cells carry a residual, so restriction
+//     sums the red children.  Level 0 works on the compact FLUID list.
+// Levels with more than MG_BLOCK_CELLS cells are swept by the whole grid with a
+// grid barrier between sweeps; the remaining coarse levels are done by block 0
+// alone with __syncthreads.  The whole PCG runs in one persistent cooperative
+// launch with the bounded grid barrier.  Precision split: the V-cycle works in
+// FP32; the Krylov vectors (x, r, p, q) and all dot products are FP64, so the
+// recurrence residual tracks the true residual down to the 1e-6 target
+// without restarts.  Loops over the FLUID list take four cells per thread per
+// trip with all loads issued before use (the solve is latency bound: the
+// 128^3 working set lives in L2).
+#include "kernels.hpp"
+#include "pcg_common.cuh"
+
+namespace fp {
+
+namespace {
+
+constexpr int MG_THREADS = 512;
+
+struct MgArgs {
+    int L, G;                    // levels; levels [0, G) are grid-wide
+    float rscale;                // restriction scale (1/4 in 3D, 1/2 in 2D)
+    int nu_coarse;               // symmetric sweep pairs on the coarsest level
+    MgLevel lv[MG_MAX_LEVELS];
+    double* p;                   // level-0 padded dense Krylov vectors (FP64)
+    double* q;
+    double* xs;
+    double* r;
+    const float* rhs;            // compact right-hand side
+    const int* fidx;             // compact FLUID list (level-0 padded index)
+    const uint8_t* diag;         // compact diagonal, bit 7 = red/black colour
+    const int* nf;
+    double* X;                   // compact solution out (FP64)
+    double* part;
+    GridBar* bar;
+    int* status;
+    PcgOut* out;
+    double tol;
+    int maxit;
+};
+
+__device__ __forceinline__ int lv_diag(const MgLevel& L, int c) {
+    const uint8_t* l = L.lab;
+    const int o[6] = {1, -1, L.sy, -L.sy, L.sz, -L.sz};
+    int d = 0;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) { const uint8_t v = l[c + o[m]]; d += (v == FLUID || v == AIR); }
+    return d;
+}
+__device__ __forceinline__ float lv_nbsum(const MgLevel& L, int c) {
+    const float* x = L.x;
+    return (x[c + 1] + x[c - 1]) + (x[c + L.sy] + x[c - L.sy]) + (x[c + L.sz] + x[c - L.sz]);
+}
+__device__ __forceinline__ int lv_cell(const MgLevel& L, int t, int& i, int& j, int& k) {
+    i = t % L.W; j = (t / L.W) % L.H; k = t / (L.W * L.H);
+    return (i + 1) + (j + 1) * L.sy + (k + 1) * L.sz;
+}
+
+// ---- level-0 operations over the compact FLUID list (colour and diagonal
+// precomputed in the diag byte), four cells per thread per trip ----
+constexpr int UNR = 4;
+template <int N = UNR>
+struct Cells {
+    int c[N];
+    uint8_t db[N];
+    bool ok[N];
+};
+// Lanes past the end of the list get `safe`, the padded index of interior cell
+// (0,0,0): it and its six stencil neighbours lie inside every level-0 grid, so
+// the unconditional loads of an idle lane stay in bounds (its result is dropped).
+template <int N>
+__device__ __forceinline__ void load_cells(Cells<N>& k, const int* fidx, const uint8_t* dg, int nf, int base, int stride,
+                                           int safe) {
+#pragma unroll
+    for (int u = 0; u < N; ++u) {
+        const int n = base + u * stride;
+        k.ok[u] = n < nf;
+        k.c[u] = k.ok[u] ? fidx[n] : safe;
+        k.db[u] = k.ok[u] ? dg[n] : 0;
+    }
+}
+__device__ void op0_first_red(const MgLevel& L, const int* fidx, const uint8_t* dg, int nf, int t0, int stride) {
+    for (int base = t0; base < nf; base += UNR * stride) {
+        Cells<> k;
+        load_cells(k, fidx, dg, nf, base, stride, 1 + L.sy + L.sz);
+        float b[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) b[u] = L.b[k.c[u]];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int d = k.db[u] & 0x7F;
+            if (k.ok[u]) L.x[k.c[u]] = ((k.db[u] >> 7) == 0 && d > 0) ? b[u] / float(d) : 0.0f;
+        }
+    }
+}
+__device__ void op0_sweep(const MgLevel& L, const int* fidx, const uint8_t* dg, int nf, int color, int t0, int stride) {
+    for (int base = t0; base < nf; base += UNR * stride) {
+        Cells<> k;
+        load_cells(k, fidx, dg, nf, base, stride, 1 + L.sy + L.sz);
+        float b[UNR], nb[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) { b[u] = L.b[k.c[u]]; nb[u] = lv_nbsum(L, k.c[u]); }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int d = k.db[u] & 0x7F;
+            if (k.ok[u] && (k.db[u] >> 7) == color) L.x[k.c[u]] = d > 0 ? (b[u] + nb[u]) / float(d) : 0.0f;
+        }
+    }
+}
+__device__ void op0_prolong(const MgLevel& F, const MgLevel& Cl, const int* fidx, int nf, int t0, int stride) {
+    for (int n = t0; n < nf; n += stride) {
+        const int c = fidx[n];
+        const int i = c % F.sy - 1, j = (c / F.sy) % (F.H + 2) - 1, k = c / F.sz - 1;
+        const int cc = (i / 2 + 1) + (j / 2 + 1) * Cl.sy + (k / 2 + 1) * Cl.sz;
+        if (Cl.lab[cc] == FLUID) F.x[c] += Cl.x[cc];
+    }
+}
+
+// ---- level operations over a (t0, stride) share of the work ----
+// First sweep of a cycle: x = b/d on red FLUID cells, 0 everywhere else.
+__device__ void op_first_red(const MgLevel& L, int t0, int stride) {
+    const int n = L.W * L.H * L.D;
+    for (int t = t0; t < n; t += stride) {
+        int i, j, k;
+        const int c = lv_cell(L, t, i, j, k);
+        float v = 0.0f;
+        if (L.lab[c] == FLUID && ((i + j + k) & 1) == 0) {
+            const int d = lv_diag(L, c);
+            v = d > 0 ? L.b[c] / float(d) : 0.0f;
+        }
+        L.x[c] = v;
+    }
+}
+// Gauss-Seidel update of the FLUID cells of one colour.
+__device__ void op_sweep(const MgLevel& L, int color, int t0, int stride) {
+    const int n = L.W * L.H * L.D;
+    for (int t = t0; t < n; t += stride) {
+        int i, j, k;
+        const int c = lv_cell(L, t, i, j, k);
+        if (((i + j + k) & 1) != color || L.lab[c] != FLUID) continue;
+        const int d = lv_diag(L, c);
+        L.x[c] = d > 0 ? (L.b[c] + lv_nbsum(L, c)) / float(d) : 0.0f;
+    }
+}
+// b_coarse = scale * sum over FLUID children of (b - A x).
+__device__ void op_restrict(const MgLevel& F, const MgLevel& Cl, float scale, int t0, int stride) {
+    const int n = Cl.W * Cl.H * Cl.D;
+    for (int t = t0; t < n; t += stride) {
+        int I, J, K;
+        const int cc = lv_cell(Cl, t, I, J, K);
+        float s = 0.0f;
+        if (Cl.lab[cc] == FLUID) {
+            for (int c3 = 0; c3 < 2; ++c3)
+                for (int b3 = 0; b3 < 2; ++b3)
+                    for (int a3 = 0; a3 < 2; ++a3) {
+                        const int i = 2 * I + a3, j = 2 * J + b3, k = 2 * K + c3;
+                        if (i >= F.W || j >= F.H || k >= F.D) continue;
+                        // after the black sweep the black residuals vanish: sum red children only
+                        if (((i + j + k) & 1) != 0) continue;
+                        const int c = (i + 1) + (j + 1) * F.sy + (k + 1) * F.sz;
+                        if (F.lab[c] != FLUID) continue;
+                        s += F.b[c] - (float(lv_diag(F, c)) * F.x[c] - lv_nbsum(F, c));
+                    }
+            s *= scale;
+        }
+        Cl.b[cc] = s;
+    }
+}
+// x_fine += x_coarse(parent) on FLUID cells with a FLUID parent.
+__device__ void op_prolong(const MgLevel& F, const MgLevel& Cl, int t0, int stride) {
+    const int n = F.W * F.H * F.D;
+    for (int t = t0; t < n; t += stride) {
+        int i, j, k;
+        const int c = lv_cell(F, t, i, j, k);
+        if (F.lab[c] != FLUID) continue;
+        const int cc = (i / 2 + 1) + (j / 2 + 1) * Cl.sy + (k / 2 + 1) * Cl.sz;
+        if (Cl.lab[cc] == FLUID) F.x[c] += Cl.x[cc];
+    }
+}
+
+// V-cycle over levels [l0, L) by block 0 alone.
+__device__ void block_vcycle(const MgArgs& a, int l0) {
+    const int t0 = threadIdx.x, st = blockDim.x;
+    for (int l = l0; l < a.L - 1; ++l) {
+        op_first_red(a.lv[l], t0, st); __syncthreads();
+        op_sweep(a.lv[l], 1, t0, st); __syncthreads();
+        op_restrict(a.lv[l], a.lv[l + 1], a.rscale, t0, st); __syncthreads();
+    }
+    const MgLevel& C = a.lv[a.L - 1];
+    op_first_red(C, t0, st); __syncthreads();
+    op_sweep(C, 1, t0, st); __syncthreads();
+    for (int it = 1; it < a.nu_coarse; ++it) {
+        op_sweep(C, 0, t0, st); __syncthreads();
+        op_sweep(C, 1, t0, st); __syncthreads();
+    }
+    for (int it = 0; it < a.nu_coarse; ++it) {
+        op_sweep(C, 1, t0, st); __syncthreads();
+        op_sweep(C, 0, t0, st); __syncthreads();
+    }
+    for (int l = a.L - 2; l >= l0; --l) {
+        op_prolong(a.lv[l], a.lv[l + 1], t0, st); __syncthreads();
+        op_sweep(a.lv[l], 1, t0, st); __syncthreads();
+        op_sweep(a.lv[l], 0, t0, st); __syncthreads();
+    }
+}
+
+// z = V-cycle(r) with r = lv[0].b, z = lv[0].x.  Starts and ends with a grid
+// barrier; returns false if a barrier timed out.
+__device__ bool vcycle(const MgArgs& a) {
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
+    const unsigned nb = gridDim.x;
+    if (!grid_barrier(a.bar, nb, a.status)) return false;
+    const int G = min(a.G, a.L - 1);
+    const int nf = *a.nf;
+    for (int l = 0; l < G; ++l) {
+        if (l == 0) op0_first_red(a.lv[0], a.fidx, a.diag, nf, t0, st);
+        else op_first_red(a.lv[l], t0, st);
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
+        if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 1, t0, st);
+        else op_sweep(a.lv[l], 1, t0, st);
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
+        op_restrict(a.lv[l], a.lv[l + 1], a.rscale, t0, st);
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
+    }
+    if (blockIdx.x == 0) block_vcycle(a, G);
+    if (!grid_barrier(a.bar, nb, a.status)) return false;
+    for (int l = G - 1; l >= 0; --l) {
+        if (l == 0) op0_prolong(a.lv[0], a.lv[1], a.fidx, nf, t0, st);
+        else op_prolong(a.lv[l], a.lv[l + 1], t0, st);
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
+        if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 1, t0, st);
+        else op_sweep(a.lv[l], 1, t0, st);
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
+        if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 0, t0, st);
+        else op_sweep(a.lv[l], 0, t0, st);
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
+    const int nf = *a.nf;
+    const int nb = int(gridDim.x);
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, st = nb * blockDim.x;
+    const MgLevel& F = a.lv[0];
+    float* b0 = F.b;  // FP32 copy of r: the V-cycle's right-hand side
+    float* z = F.x;   // FP32 preconditioned residual
+    double* r = a.r;
+    int red = 0;      // reduction counter (partial buffers double-buffered by parity)
+    auto partial = [&](double v0, double v1, double v2) {
+        double3 bs = block_sum3(v0, v1, v2);
+        double* pp = a.part + (red & 1) * 3 * nb;
+        if (threadIdx.x == 0) { pp[blockIdx.x] = bs.x; pp[nb + blockIdx.x] = bs.y; pp[2 * nb + blockIdx.x] = bs.z; }
+    };
+    auto total = [&]() { double3 t = grid_sum3(a.part + (red & 1) * 3 * nb, nb); ++red; return t; };
+    const int sy = F.sy, sz = F.sz;
+
+    for (int n = t0; n < nf; n += st) {
+        const int c = a.fidx[n];
+        const double rv = double(a.rhs[n]);
+        r[c] = rv;
+        b0[c] = float(rv);
+        a.xs[c] = 0.0;
+    }
+    if (!vcycle(a)) return;
+    {
+        double rz = 0.0, rr = 0.0;
+        for (int n = t0; n < nf; n += st) {
+            const int c = a.fidx[n];
+            const double zv = double(z[c]);
+            rz += r[c] * zv;
+            rr += r[c] * r[c];
+            a.p[c] = zv;
+        }
+        partial(rz, rr, 0.0);
+    }
+    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+    double3 tot = total();
+    double rz = tot.x, rr = tot.y;
+    const double bb = tot.y;
+    const double thr = a.tol * a.tol * bb;
+    int it = 0, stt = DEV_OK;
+    while (rr > thr && bb > 0.0) {
+        if (it >= a.maxit) { stt = DEV_MAXIT; break; }
+        // q = A p, (p, q)
+        double pq = 0.0;
+        constexpr int U2 = 2;  // FP64: two cells in flight fit the register budget
+        for (int base = t0; base < nf; base += U2 * st) {
+            Cells<U2> k;
+            load_cells(k, a.fidx, a.diag, nf, base, st, 1 + sy + sz);
+            double pc[U2], ns[U2];
+#pragma unroll
+            for (int u = 0; u < U2; ++u) {
+                const double* pp = a.p + k.c[u];
+                pc[u] = pp[0];
+                ns[u] = (pp[1] + pp[-1]) + (pp[sy] + pp[-sy]) + (pp[sz] + pp[-sz]);
+            }
+#pragma unroll
+            for (int u = 0; u < U2; ++u) {
+                if (!k.ok[u]) continue;
+                const double qv = double(k.db[u] & 0x7F) * pc[u] - ns[u];
+                a.q[k.c[u]] = qv;
+                pq += pc[u] * qv;
+            }
+        }
+        partial(pq, 0.0, 0.0);
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+        const double pqs = total().x;
+        if (!(pqs > 0.0) || isnan(pqs)) { stt = isnan(pqs) ? DEV_NAN : DEV_BREAKDOWN; break; }
+        const double alpha = rz / pqs;
+        double rrl = 0.0;
+        for (int n = t0; n < nf; n += st) {
+            const int c = a.fidx[n];
+            a.xs[c] += alpha * a.p[c];
+            const double rv = r[c] - alpha * a.q[c];
+            r[c] = rv;
+            b0[c] = float(rv);
+            rrl += rv * rv;
+        }
+        if (!vcycle(a)) return;  // z = M^-1 r (begins with a barrier)
+        double rzl = 0.0;
+        for (int n = t0; n < nf; n += st) {
+            const int c = a.fidx[n];
+            rzl += r[c] * double(z[c]);
+        }
+        partial(rzl, rrl, 0.0);
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+        tot = total();
+        ++it;
+        if (isnan(tot.x) || isnan(tot.y)) { stt = DEV_NAN; break; }
+        rr = tot.y;
+        if (rr <= thr) break;
+        const double beta = tot.x / rz;
+        rz = tot.x;
+        for (int n = t0; n < nf; n += st) {
+            const int c = a.fidx[n];
+            a.p[c] = double(z[c]) + beta * a.p[c];
+        }
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+    }
+    // compact solution; zero the level-0 work grids at the FLUID cells so the
+    // next solve starts from zero whatever cells are fluid then
+    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+    for (int n = t0; n < nf; n += st) {
+        const int c = a.fidx[n];
+        a.X[n] = a.xs[c];
+        a.xs[c] = 0.0; a.p[c] = 0.0; a.q[c] = 0.0; r[c] = 0.0; b0[c] = 0.0f; z[c] = 0.0f;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.out->iters = it;
+        atomicCAS(a.status, DEV_OK, stt);
+        a.out->rr = rr;
+        a.out->bb = bb;
+        a.out->rz = rz;
+    }
+}
+
+// Level-0 labels with a SOLID halo; BODY counts as SOLID (Neumann).
+__global__ void k_pad_labels(const uint8_t* __restrict__ lab, Dims g, MgLevel L) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= g.nc()) return;
+    int i, j, k;
+    const int c = lv_cell(L, int(t), i, j, k);
+    const uint8_t l = lab[t];
+    L.lab[c] = l == BODY ? SOLID : l;
+}
+
+// Coarse labels with Dirichlet priority: AIR if any child AIR, else FLUID if
+// any child FLUID, else SOLID.
+__global__ void k_coarsen(MgLevel F, MgLevel Cl) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= Cl.W * Cl.H * Cl.D) return;
+    int I, J, K;
+    const int cc = lv_cell(Cl, t, I, J, K);
+    bool air = false, fluid = false;
+    for (int c3 = 0; c3 < 2; ++c3)
+        for (int b3 = 0; b3 < 2; ++b3)
+            for (int a3 = 0; a3 < 2; ++a3) {
+                const int i = 2 * I + a3, j = 2 * J + b3, k = 2 * K + c3;
+                if (i >= F.W || j >= F.H || k >= F.D) continue;
+                const uint8_t l = F.lab[(i + 1) + (j + 1) * F.sy + (k + 1) * F.sz];
+                air |= l == AIR;
+                fluid |= l == FLUID;
+            }
+    Cl.lab[cc] = air ? AIR : (fluid ? FLUID : SOLID);
+}
+
+}  // namespace
+
+int mg_levels_for(int W, int H, int D, MgLevel* lv) {
+    int L = 0;
+    int w = W, h = H, d = D;
+    while (L < MG_MAX_LEVELS) {
+        lv[L].W = w; lv[L].H = h; lv[L].D = d;
+        lv[L].sy = w + 2; lv[L].sz = (w + 2) * (h + 2);
+        ++L;
+        if (int64_t(w) * h * d <= 512 || (w <= 2 && h <= 2 && d <= 2)) break;
+        w = (w + 1) / 2; h = (h + 1) / 2; d = (d + 1) / 2;
+    }
+    return L;
+}
+
+int mg_max_blocks() {
+    static int cached = 0;
+    if (cached) return cached;
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_mg, MG_THREADS, 0);
+    cached = sms * std::max(1, per);
+    return cached;
+}
+
+void launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStream_t st) {
+    k_pad_labels<<<unsigned((g.nc() + 255) / 256), 256, 0, st>>>(labels, g, lv[0]);
+    for (int l = 1; l < L; ++l) {
+        const int n = lv[l].W * lv[l].H * lv[l].D;
+        k_coarsen<<<(n + 255) / 256, 256, 0, st>>>(lv[l - 1], lv[l]);
+    }
+}
+
+int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
+                  const float* rhs, double tol, int maxit, cudaStream_t st) {
+    const int nb = mg_max_blocks();
+    int* status = &pb.out->status;
+    cudaMemsetAsync(pb.bar, 0, sizeof(GridBar), st);
+    cudaMemsetAsync(status, 0, sizeof(int), st);
+    MgArgs a;
+    a.L = L;
+    a.G = 0;
+    for (int l = 0; l < L; ++l) {
+        a.lv[l] = lv[l];
+        if (int64_t(lv[l].W) * lv[l].H * lv[l].D > MG_BLOCK_CELLS) a.G = l + 1;
+    }
+    a.rscale = g.D > 1 ? 0.25f : 0.5f;
+    a.nu_coarse = 2;
+    a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
+    a.X = static_cast<double*>(pb.X);
+    a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;
+    a.tol = tol; a.maxit = maxit;
+    void* args[] = {&a};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_mg, dim3(nb), dim3(MG_THREADS), args, 0, st);
+    return e == cudaSuccess ? 0 : int(e);
+}
+
+}  // namespace fp

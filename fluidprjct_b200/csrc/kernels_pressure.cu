@@ -20,6 +20,7 @@
 #include <cstdio>
 
 #include "kernels.hpp"
+#include "pcg_common.cuh"
 #include "scan.cuh"
 
 namespace fp {
@@ -133,151 +134,10 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_fluid_build(const uint8_t* __res
             uint8_t l = label_at(labels, g, i + off[o][0], j + off[o][1], k + off[o][2]);
             d += (l == FLUID || l == AIR);
         }
-        diag[n] = uint8_t(d);
+        diag[n] = uint8_t(d | (((i + j + k) & 1) << 7));  // bit 7: red/black colour
         b[n] = rhs_dense ? rhs_dense[e] : rhs_at(labels, u, v, w, g, i, j, k, scale, body);
         ++n;
     }
-}
-
-// ---------------------------------------------------------------- grid barrier
-// Grid barrier for a cooperative launch on one 32-bit word: every block adds
-// 1 except block 0, which adds 2^31 - (nblocks - 1), so the word's top bit
-// flips exactly when the last block arrives and no reset is needed between
-// barriers.  The wait is bounded: after ~2^28 polls the block records
-// DEV_TIMEOUT and leaves; callers check the status after every barrier and
-// return, so no block waits forever.  The fences around the arrival give the
-// barrier release/acquire semantics, so plain (L1-cached) loads after it see
-// every write made before it by any block.
-__device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* status) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned inc = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
-        __threadfence();
-        const unsigned old = atomicAdd(&bar->count, inc);
-        volatile unsigned* vc = &bar->count;
-        long long polls = 0;
-        while (((old ^ *vc) & 0x80000000u) == 0u) {
-            if (++polls > (1ll << 28)) {
-                atomicExch(status, DEV_TIMEOUT);
-                break;
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return *(volatile int*)status == DEV_OK;
-}
-
-// Block sum of two doubles (fixed tree, deterministic); result valid in thread 0.
-__device__ __forceinline__ double2 block_sum2(double a, double b) {
-    __shared__ double2 sh[32];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xffffffffu, a, o);
-        b += __shfl_down_sync(0xffffffffu, b, o);
-    }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) sh[wid] = make_double2(a, b);
-    __syncthreads();
-    double2 r = make_double2(0.0, 0.0);
-    if (wid == 0) {
-        r = lane < int(blockDim.x >> 5) ? sh[lane] : make_double2(0.0, 0.0);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            r.x += __shfl_down_sync(0xffffffffu, r.x, o);
-            r.y += __shfl_down_sync(0xffffffffu, r.y, o);
-        }
-    }
-    __syncthreads();
-    return r;
-}
-
-// Sum of per-block partials part[0..nb) (pairs), identical in every block.
-__device__ __forceinline__ double2 grid_sum2(const double2* part, int nb) {
-    __shared__ double2 res;
-    if (threadIdx.x < 32) {
-        double2 s = make_double2(0.0, 0.0);
-        for (int t = threadIdx.x; t < nb; t += 32) {
-            // Written by other CTAs in this launch: read through L2.
-            double2 v = __ldcg(part + t);
-            s.x += v.x;
-            s.y += v.y;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            s.x += __shfl_down_sync(0xffffffffu, s.x, o);
-            s.y += __shfl_down_sync(0xffffffffu, s.y, o);
-        }
-        if (threadIdx.x == 0) res = s;
-    }
-    __syncthreads();
-    double2 r = res;
-    __syncthreads();
-    return r;
-}
-
-// Sum of three per-block partial arrays part[0..nb), part[nb..2nb),
-// part[2nb..3nb), returned to every thread of every block.  All threads load
-// (one L2 round trip when nb <= blockDim) and reduce with a fixed tree, so
-// every block obtains the same bits.
-__device__ __forceinline__ double3 grid_sum3(const double* part, int nb) {
-    __shared__ double3 red3[32];
-    __shared__ double3 res3;
-    double a = 0.0, b = 0.0, c = 0.0;
-    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
-        a += __ldcg(part + t);
-        b += __ldcg(part + nb + t);
-        c += __ldcg(part + 2 * nb + t);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xffffffffu, a, o);
-        b += __shfl_down_sync(0xffffffffu, b, o);
-        c += __shfl_down_sync(0xffffffffu, c, o);
-    }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) red3[wid] = make_double3(a, b, c);
-    __syncthreads();
-    if (wid == 0) {
-        double3 r = lane < int(blockDim.x >> 5) ? red3[lane] : make_double3(0.0, 0.0, 0.0);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            r.x += __shfl_down_sync(0xffffffffu, r.x, o);
-            r.y += __shfl_down_sync(0xffffffffu, r.y, o);
-            r.z += __shfl_down_sync(0xffffffffu, r.z, o);
-        }
-        if (lane == 0) res3 = r;
-    }
-    __syncthreads();
-    double3 r = res3;
-    __syncthreads();
-    return r;
-}
-
-// Block sum of three doubles; result valid in thread 0.
-__device__ __forceinline__ double3 block_sum3(double a, double b, double c) {
-    __shared__ double3 sh3[32];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xffffffffu, a, o);
-        b += __shfl_down_sync(0xffffffffu, b, o);
-        c += __shfl_down_sync(0xffffffffu, c, o);
-    }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) sh3[wid] = make_double3(a, b, c);
-    __syncthreads();
-    double3 r = make_double3(0.0, 0.0, 0.0);
-    if (wid == 0) {
-        r = lane < int(blockDim.x >> 5) ? sh3[lane] : make_double3(0.0, 0.0, 0.0);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            r.x += __shfl_down_sync(0xffffffffu, r.x, o);
-            r.y += __shfl_down_sync(0xffffffffu, r.y, o);
-            r.z += __shfl_down_sync(0xffffffffu, r.z, o);
-        }
-    }
-    __syncthreads();
-    return r;
 }
 
 __device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
@@ -329,7 +189,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
     // Init 1: r0 = b, 1/diag, s_{-1} = p_{-1} = x0 = 0.
     for (int n = n0 + threadIdx.x; n < n1; n += PCG_THREADS) {
         const int c = a.fidx[n];
-        const uint8_t d = a.diag[n];
+        const uint8_t d = a.diag[n] & 0x7F;
         a.invd[c] = d > 0 ? T(1) / T(d) : T(0);
         a.R[0][c] = T(a.b[n]);
         a.S[0][c] = T(0);
@@ -349,7 +209,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
             T nbs = T(0);
 #pragma unroll
             for (int o = 0; o < 6; ++o) nbs += R0[c + offs[o]] * iv[c + offs[o]];
-            const T w = T(a.diag[n]) * u - nbs;
+            const T w = T(a.diag[n] & 0x7F) * u - nbs;
             a.Wv[0][c] = w;
             g_l += double(r) * double(u);
             d_l += double(w) * double(u);
@@ -396,7 +256,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
                 const T sq = fmaT(be, Sc[q], Wc[q]);
                 nbs += fmaT(-al, sq, Rc[q]) * iv[q];
             }
-            const T wn = T(a.diag[n]) * un - nbs;
+            const T wn = T(a.diag[n] & 0x7F) * un - nbs;
             Rn[c] = rn;
             Wn[c] = wn;
             Sn[c] = s;
@@ -479,7 +339,7 @@ __global__ void __launch_bounds__(256) k_residual(const int* __restrict__ nf_p, 
     double e2 = 0.0, b2 = 0.0;
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) {
         const T* x = xd + fidx[n];
-        double ax = double(diag[n]) * double(x[0]) -
+        double ax = double(diag[n] & 0x7F) * double(x[0]) -
                     (double(x[sx]) + double(x[-sx]) + double(x[sy]) + double(x[-sy]) + double(x[sz]) + double(x[-sz]));
         double e = double(b[n]) - ax;
         if (r_out) r_out[n] = float(e);

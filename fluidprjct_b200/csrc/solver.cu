@@ -112,6 +112,10 @@ struct fp_solver {
     // pressure
     PressureBufs pb{};
     int64_t padded = 0;
+    // multigrid hierarchy (level 0 shares the padded layout of pb)
+    MgLevel mg[MG_MAX_LEVELS]{};
+    int mgL = 0;
+    double *d_mgp = nullptr, *d_mgq = nullptr, *d_mgx = nullptr, *d_mgr = nullptr;
     // pinned result mirrors
     PcgOut* h_out = nullptr;
     double* h_red = nullptr;
@@ -147,6 +151,9 @@ void free_grid(fp_solver* s) {
     for (int i = 0; i < 2; ++i) { dfree(pb.R[i]); dfree(pb.Wv[i]); dfree(pb.S[i]); }
     dfree(pb.invd); dfree(pb.P); dfree(pb.X);
     dfree(pb.x64); dfree(pb.xd); dfree(pb.part); dfree(pb.bar); dfree(pb.out); dfree(pb.red);
+    for (int l = 0; l < s->mgL; ++l) { dfree(s->mg[l].lab); dfree(s->mg[l].x); dfree(s->mg[l].b); }
+    s->mgL = 0;
+    dfree(s->d_mgp); dfree(s->d_mgq); dfree(s->d_mgx); dfree(s->d_mgr);
     s->have_grid = false;
 }
 
@@ -189,6 +196,23 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     ck(dalloc(&pb.part, size_t(6) * std::max(maxb, 1024)));
     ck(dalloc(&pb.bar, 1)); ck(dalloc(&pb.out, 1)); ck(dalloc(&pb.red, 2));
     pb.tile_sums = s->d_tiles;
+    if (s->cfg.solver == FP_SOLVER_PCG_MG) {
+        s->mgL = mg_levels_for(W, H, D, s->mg);
+        for (int l = 0; l < s->mgL && e == cudaSuccess; ++l) {
+            MgLevel& L = s->mg[l];
+            const size_t np_ = size_t(L.W + 2) * (L.H + 2) * (L.D + 2);
+            ck(dalloc(&L.lab, np_)); ck(dalloc(&L.x, np_)); ck(dalloc(&L.b, np_));
+            if (e == cudaSuccess) {
+                ck(cudaMemsetAsync(L.lab, 0, np_, s->st));  // SOLID halo
+                ck(cudaMemsetAsync(L.x, 0, np_ * sizeof(float), s->st));
+                ck(cudaMemsetAsync(L.b, 0, np_ * sizeof(float), s->st));
+            }
+        }
+        ck(dalloc(&s->d_mgp, size_t(s->padded))); ck(dalloc(&s->d_mgq, size_t(s->padded)));
+        ck(dalloc(&s->d_mgx, size_t(s->padded))); ck(dalloc(&s->d_mgr, size_t(s->padded)));
+        for (double* a : {s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr})
+            if (e == cudaSuccess) ck(cudaMemsetAsync(a, 0, sizeof(double) * size_t(s->padded), s->st));
+    }
     if (e != cudaSuccess) { free_grid(s); return s->cuda_fail(e, "device allocation of the grid"); }
     for (float* a : {s->d_u, s->d_us}) ck(cudaMemsetAsync(a, 0, sizeof(float) * s->g.nu(), s->st));
     for (float* a : {s->d_v, s->d_vs}) ck(cudaMemsetAsync(a, 0, sizeof(float) * s->g.nv(), s->st));
@@ -305,15 +329,24 @@ int solve_system(fp_solver* s, float* p_out) {
     int dev_status = DEV_OK;
     float pcg_ms = 0.0f;
     cudaError_t ce;
-    if (s->cfg.solver == FP_SOLVER_PCG) {
+    if (s->cfg.solver == FP_SOLVER_PCG || s->cfg.solver == FP_SOLVER_PCG_MG) {
+        const bool mg = s->cfg.solver == FP_SOLVER_PCG_MG;
+        if (mg) {
+            launch_mg_setup(s->d_labels, s->g, s->mg, s->mgL, s->st);
+            s->launches += s->mgL;
+        }
         cudaEventRecord(s->ev_pcg[0], s->st);
-        int e = launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st);
+        int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr, pb.b, tol, maxit,
+                                   s->st)
+                   : launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st);
         cudaEventRecord(s->ev_pcg[1], s->st);
         if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
         launch_scatter_p(pb, p_out, 1, s->g, s->st);
         launch_true_residual(pb, 1, s->g, s->st);
-        launch_pcg_clear(pb, 1, 1, s->st);
-        s->launches += 2 + 1 + 3 + 1;  // reset + pcg, scatter, residual (3), clear
+        // the residual check leaves the solution in the padded R[0] grid: clear
+        // it (and the Jacobi work grids) at this solve's FLUID cells
+        launch_pcg_clear(pb, 1, mg ? 0 : 1, s->st);
+        s->launches += (mg ? 1 : 2) + 1 + 3 + 1;  // [reset +] pcg, scatter, residual (3), clear
         cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
         cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
         cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
@@ -561,7 +594,7 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     if (!s) return FP_ERR_ARG;
     if (cfg) s->cfg = *cfg; else fp_config_default(&s->cfg);
     if (!(s->cfg.dx > 0) || !(s->cfg.dt > 0) || (s->cfg.dim != 2 && s->cfg.dim != 3)) { delete s; return FP_ERR_ARG; }
-    if (s->cfg.solver != FP_SOLVER_PCG && s->cfg.solver != FP_SOLVER_PCG_MIXED) {
+    if (s->cfg.solver != FP_SOLVER_PCG && s->cfg.solver != FP_SOLVER_PCG_MIXED && s->cfg.solver != FP_SOLVER_PCG_MG) {
         std::fprintf(stderr, "fp_create: solver %d is not available in this build\n", s->cfg.solver);
         delete s;
         return FP_ERR_ARG;

@@ -62,12 +62,13 @@ def test_2d_phases_match_oracle(O):
     assert np.all(pg[:, 2] == 0)
 
 
-def test_2d_dam_break_config(O):
+@pytest.mark.parametrize("solver", ["pcg_mixed", "pcg_mg"])
+def test_2d_dam_break_config(O, solver):
     """The plain 2D dam break: 64^2, dx = 1/64, 4 ppc (seed 0), dt = 0.005,
     FLIP 0.95, 100 steps, PCG to 1e-6."""
     from fluidprjct_b200 import capi, scenes
     lab = scenes.dam_break_2d(64)
-    s = capi.Solver(dim=2, dx=1 / 64, dt=0.005, pic_weight=0.05, solver="pcg_mixed", tol=1e-6)
+    s = capi.Solver(dim=2, dx=1 / 64, dt=0.005, pic_weight=0.05, solver=solver, tol=1e-6)
     s.set_labels(lab)
     s.seed_particles(4, 0)
     p0, _ = s.particles()

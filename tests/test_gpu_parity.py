@@ -128,7 +128,7 @@ def _prepare_pressure(O, solver="pcg", tol=1e-6):
     return s, o
 
 
-@pytest.mark.parametrize("solver", ["pcg", "pcg_mixed"])
+@pytest.mark.parametrize("solver", ["pcg", "pcg_mixed", "pcg_mg"])
 def test_pressure_residual_and_solution(O, solver):
     from fluidprjct_b200 import capi
     s, o = _prepare_pressure(O, solver, tol=1e-6)
@@ -144,9 +144,10 @@ def test_pressure_residual_and_solution(O, solver):
     assert np.all(p_gpu.ravel()[~fl] == 0.0)
 
 
-def test_pressure_tight_refinement_matches_fp64(O):
+@pytest.mark.parametrize("solver", ["pcg_mixed", "pcg_mg"])
+def test_pressure_tight_refinement_matches_fp64(O, solver):
     from fluidprjct_b200 import capi
-    s, o = _prepare_pressure(O, "pcg_mixed", tol=1e-9)
+    s, o = _prepare_pressure(O, solver, tol=1e-9)
     s.phase(capi.PHASE_PRESSURE)
     st = s.stats()
     assert st["residual"] <= 1e-9, st
@@ -243,11 +244,12 @@ def test_cudss_kat_on_gpu(golden):
     assert np.max(np.abs(x - np.array(kat["x"]))) <= 1e-12
 
 
-def test_dam_break_128_properties(O):
+@pytest.mark.parametrize("solver", ["pcg", "pcg_mg"])
+def test_dam_break_128_properties(O, solver):
     """Config 2 at full size: one step; size-independent properties."""
     from fluidprjct_b200 import capi, scenes
     lab = scenes.dam_break_3d(128)
-    s = _solver(dx=1 / 128, dt=0.002, pic_weight=0.05, tol=1e-6)
+    s = _solver(dx=1 / 128, dt=0.002, pic_weight=0.05, tol=1e-6, solver=solver)
     s.set_labels(lab)
     s.seed_particles(8, 1)
     n0 = s.num_particles
