@@ -26,6 +26,7 @@ SOURCES = [
     "kernels_body.cu",
     "kernels_mg.cu",
     "solver.cu",
+    "noalloc.cu",
     "io.cpp",
 ]
 

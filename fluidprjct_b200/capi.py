@@ -98,6 +98,7 @@ _SIGS = {
     "fp_cuda_stream": (C.c_void_p, [_P]),
     "fp_pressure_solve": (C.c_int, [_P, _P, _P, C.c_int64, _P, _P]),
     "fp_solve_csr_upper": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, C.c_double, C.c_int, _P, _P]),
+    "fp_solve_csr_upper_noalloc": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, C.c_double, C.c_int, _P, _P, _P]),
     "fp_read_label_file": (C.c_int, [C.c_char_p, C.c_int, _P, _P]),
     "fp_read_ply_file": (C.c_int, [C.c_char_p, _P, _P, _P, _P]),
     "fp_version": (C.c_char_p, []),
@@ -288,6 +289,22 @@ def solve_csr_upper(offsets, cols, vals, b, tol=1e-14, max_iters=10000):
     if rc != FP_OK:
         raise FluidError(rc, "fp_solve_csr_upper failed")
     return x, it.value, rr.value
+
+
+FP_NOALLOC_MAX_N = 1 << 18
+
+
+def solve_csr_upper_noalloc(n, d_offsets, d_cols, d_vals, d_b, d_x, tol=1e-14, max_iters=10000, stream=None):
+    """fp_solve_csr_upper_noalloc on caller-owned device buffers (raw device
+    addresses as ints); the solution is written to d_x.  Returns (iters,
+    relres); raises FluidError on a non-zero status."""
+    it, rr = C.c_int(), C.c_double()
+    rc = lib().fp_solve_csr_upper_noalloc(int(n), C.c_void_p(d_offsets), C.c_void_p(d_cols), C.c_void_p(d_vals),
+                                          C.c_void_p(d_b), C.c_void_p(d_x), tol, max_iters, C.byref(it),
+                                          C.byref(rr), C.c_void_p(stream))
+    if rc != FP_OK:
+        raise FluidError(rc, "fp_solve_csr_upper_noalloc failed")
+    return it.value, rr.value
 
 
 def read_label_file(path, dim=3) -> np.ndarray:

@@ -195,6 +195,22 @@ int fp_pressure_solve(fp_solver* s, const float* rhs, float* x, int64_t n, int* 
 int fp_solve_csr_upper(int n, const int* offsets, const int* cols, const double* vals, const double* b, double* x,
                        double tol, int max_iters, int* iters, double* relres);
 
+/* Allocation-free variant of fp_solve_csr_upper; it has no counterpart in the
+ * reference.  Same system, algorithm and status codes, but every pointer is a
+ * DEVICE buffer owned by the caller (offsets n+1, cols/vals offsets[n], b and
+ * x n doubles) and the work vectors live in one fixed device array, so the
+ * call never allocates.  For hosts whose own pool allocator owns the GPU, and
+ * for loops that cannot pay cudaMalloc's latency and device-wide sync.
+ *   - n above FP_NOALLOC_MAX_N is rejected with FP_ERR_ARG;
+ *   - all calls on a device share the array: overlapping calls race;
+ *   - the first call on a device, with that device current, looks up the
+ *     array's address; make it before any stream capture on that device.
+ * stream may be NULL (the legacy default stream). */
+#define FP_NOALLOC_MAX_N (1 << 18)
+int fp_solve_csr_upper_noalloc(int n, const int* d_offsets, const int* d_cols, const double* d_vals,
+                               const double* d_b, double* d_x, double tol, int max_iters, int* iters,
+                               double* relres, void* stream);
+
 /* Host-only readers (no GPU needed).  fp_read_label_file parses a reference
  * label file (dim 3: FluidSolver3D.cu:81-153, dim 2: FluidSolver2D.cu:52-104);
  * call with out = NULL to get dims[0..2] = W, H, D (D = 1 in 2D) first.
