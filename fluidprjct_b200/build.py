@@ -25,6 +25,8 @@ SOURCES = [
     "kernels_advect.cu",
     "kernels_body.cu",
     "kernels_mg.cu",
+    "kernels_unet.cu",
+    "unet.cu",
     "solver.cu",
     "noalloc.cu",
     "io.cpp",

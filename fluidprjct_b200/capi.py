@@ -19,7 +19,7 @@ SOLID, FLUID, AIR, BODY = 0, 1, 2, 3
 OUT_PLY, OUT_OFF, OUT_PLY_BINARY, OUT_NONE = 0, 1, 2, 3
 SOLVER_PCG, SOLVER_PCG_MIXED, SOLVER_PCG_MG, SOLVER_PCG_LEARNED = 0, 1, 2, 3
 ADVECT_RK3REF, ADVECT_RK2 = 0, 1
-GRID_U, GRID_V, GRID_W, GRID_U_SAVED, GRID_V_SAVED, GRID_W_SAVED, GRID_P = range(7)
+GRID_U, GRID_V, GRID_W, GRID_U_SAVED, GRID_V_SAVED, GRID_W_SAVED, GRID_P, GRID_RHS = range(8)
 (PHASE_LABEL, PHASE_P2G, PHASE_SAVE, PHASE_FORCES, PHASE_PRESSURE, PHASE_PROJECT, PHASE_BODY, PHASE_G2P,
  PHASE_ADVECT) = range(9)
 
@@ -45,10 +45,10 @@ class FpStepStats(C.Structure):
         ("residual", C.c_double),
         ("t_label", C.c_float), ("t_p2g", C.c_float), ("t_forces", C.c_float), ("t_pressure", C.c_float),
         ("t_project", C.c_float), ("t_body", C.c_float), ("t_g2p", C.c_float), ("t_advect", C.c_float),
-        ("t_total", C.c_float), ("pad2_", C.c_float),
+        ("t_total", C.c_float), ("guess_relres", C.c_float),
         ("body_pos", C.c_double * 3), ("body_vel", C.c_double * 3), ("body_omega", C.c_double * 3),
         ("body_angles", C.c_double * 3), ("body_force", C.c_double * 3), ("body_torque", C.c_double * 3),
-        ("kernel_launches", C.c_int64), ("t_pcg", C.c_float), ("pad3_", C.c_float),
+        ("kernel_launches", C.c_int64), ("t_pcg", C.c_float), ("t_learned", C.c_float),
     ]
 
     def as_dict(self):
@@ -93,6 +93,21 @@ _SIGS = {
     "fp_get_grid": (C.c_int, [_P, C.c_int, _P, C.c_int64]),
     "fp_set_grid": (C.c_int, [_P, C.c_int, _P, C.c_int64]),
     "fp_get_labels": (C.c_int, [_P, _P, C.c_int64]),
+    "fp_get_grid_device": (C.c_int, [_P, C.c_int, _P, C.c_int64]),
+    "fp_get_labels_device": (C.c_int, [_P, _P, C.c_int64]),
+    "fp_load_learned": (C.c_int, [_P, C.c_char_p]),
+    "fp_unet_num_params": (C.c_int64, []),
+    "fp_unet_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, _P]),
+    "fp_unet_destroy": (None, [_P]),
+    "fp_unet_last_error": (C.c_char_p, [_P]),
+    "fp_unet_cuda_stream": (C.c_void_p, [_P]),
+    "fp_unet_get_params": (C.c_int, [_P, _P, C.c_int64]),
+    "fp_unet_set_params": (C.c_int, [_P, _P, C.c_int64]),
+    "fp_unet_save": (C.c_int, [_P, C.c_char_p]),
+    "fp_unet_load": (C.c_int, [_P, C.c_char_p]),
+    "fp_unet_forward": (C.c_int, [_P, _P, _P, _P]),
+    "fp_unet_loss_grad": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    "fp_unet_train_step": (C.c_int, [_P, _P, _P, _P, C.c_float, _P]),
     "fp_set_body_state": (C.c_int, [_P, _P, _P, _P]),
     "fp_stats": (C.c_int, [_P, _P]),
     "fp_cuda_stream": (C.c_void_p, [_P]),
@@ -234,7 +249,7 @@ class Solver:
     def grid_shape(self, which):
         W, H, D = self.dims
         return {GRID_U: (D, H, W + 1), GRID_U_SAVED: (D, H, W + 1), GRID_V: (D, H + 1, W), GRID_V_SAVED: (D, H + 1, W),
-                GRID_W: (D + 1, H, W), GRID_W_SAVED: (D + 1, H, W), GRID_P: (D, H, W)}[which]
+                GRID_W: (D + 1, H, W), GRID_W_SAVED: (D + 1, H, W), GRID_P: (D, H, W), GRID_RHS: (D, H, W)}[which]
 
     def grid(self, which):
         shp = self.grid_shape(which)
@@ -245,6 +260,17 @@ class Solver:
     def set_grid(self, which, data):
         a = np.ascontiguousarray(data, np.float32).reshape(-1)
         return self._check(lib().fp_set_grid(self._h, which, ptr(a), a.size))
+
+    def grid_to_device(self, which, d_out: int, n: int):
+        """Copy a grid into caller device memory at address d_out (n floats)."""
+        return self._check(lib().fp_get_grid_device(self._h, which, C.c_void_p(d_out), n))
+
+    def labels_to_device(self, d_out: int, n: int):
+        return self._check(lib().fp_get_labels_device(self._h, C.c_void_p(d_out), n))
+
+    def load_learned(self, path):
+        """Weights of the learned initial guess (FP_SOLVER_PCG_LEARNED)."""
+        return self._check(lib().fp_load_learned(self._h, str(path).encode()))
 
     def labels(self):
         W, H, D = self.dims
@@ -330,3 +356,72 @@ def read_ply_file(path):
     vel = np.zeros((n.value, 3), np.float32) if hv.value else None
     lib().fp_read_ply_file(str(path).encode(), C.byref(n), ptr(pos), None if vel is None else ptr(vel), C.byref(hv))
     return pos, vel
+
+
+class UNet:
+    """The learned preconditioner's network (fp_unet_*).  Array arguments of
+    forward / loss_grad / train_step are raw DEVICE addresses (ints) of the
+    real-grid arrays: labels uint8, rhs / p / x float32, W*H*D each."""
+
+    def __init__(self, W, H, D, train=False, seed=0):
+        h = C.c_void_p()
+        rc = lib().fp_unet_create(W, H, D, int(bool(train)), seed, C.byref(h))
+        if rc != FP_OK:
+            raise FluidError(rc, "fp_unet_create failed")
+        self._h = h
+        self.dims = (W, H, D)
+
+    def _check(self, rc):
+        if rc != FP_OK:
+            raise FluidError(rc, (lib().fp_unet_last_error(self._h) or b"").decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fp_unet_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def num_params() -> int:
+        return int(lib().fp_unet_num_params())
+
+    @property
+    def stream(self) -> int:
+        return lib().fp_unet_cuda_stream(self._h) or 0
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.num_params(), np.float32)
+        self._check(lib().fp_unet_get_params(self._h, ptr(out), out.size))
+        return out
+
+    def set_params(self, w):
+        a = np.ascontiguousarray(w, np.float32)
+        return self._check(lib().fp_unet_set_params(self._h, ptr(a), a.size))
+
+    def save(self, path):
+        return self._check(lib().fp_unet_save(self._h, str(path).encode()))
+
+    def load(self, path):
+        return self._check(lib().fp_unet_load(self._h, str(path).encode()))
+
+    def forward(self, d_labels: int, d_rhs: int, d_x: int):
+        return self._check(lib().fp_unet_forward(self._h, C.c_void_p(d_labels), C.c_void_p(d_rhs), C.c_void_p(d_x)))
+
+    def loss_grad(self, d_labels: int, d_rhs: int, d_p: int):
+        loss = C.c_double()
+        g = np.zeros(self.num_params(), np.float32)
+        self._check(lib().fp_unet_loss_grad(self._h, C.c_void_p(d_labels), C.c_void_p(d_rhs), C.c_void_p(d_p),
+                                            C.byref(loss), ptr(g)))
+        return loss.value, g
+
+    def train_step(self, d_labels: int, d_rhs: int, d_p: int, lr: float, want_loss=False):
+        loss = C.c_double()
+        self._check(lib().fp_unet_train_step(self._h, C.c_void_p(d_labels), C.c_void_p(d_rhs), C.c_void_p(d_p),
+                                             lr, C.byref(loss) if want_loss else None))
+        return loss.value if want_loss else None

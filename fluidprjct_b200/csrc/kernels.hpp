@@ -20,6 +20,7 @@ struct PcgOut {
     double rr;      // ||r||^2 of the recurrence at exit
     double bb;      // ||b||^2
     double rz;
+    double rr0;     // ||b - A x0||^2 of the initial iterate (MG kernel)
 };
 
 // Device buffers of the pressure system.  Compact arrays are indexed by the
@@ -67,8 +68,10 @@ void launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStre
 // A x = rhs (compact) to ||r||/||rhs|| <= tol; solution in pb.X (FP64
 // compact).  p, q, xs, r are level-0 padded dense FP64 work grids, zero at
 // entry and on exit.
+// x0: compact initial guess (scaled on the device by its energy-optimal
+// factor), or null to start from x = 0.
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
-                  const float* rhs, double tol, int maxit, cudaStream_t st);
+                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0 = nullptr);
 
 // -------- labelling and the particle sort (kernels_sort.cu) --------
 // counts[nc] must be zero on entry.  Writes key/rank per particle.

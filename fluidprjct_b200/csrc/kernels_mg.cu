@@ -44,6 +44,7 @@ struct MgArgs {
     double* xs;
     double* r;
     const float* rhs;            // compact right-hand side
+    const float* x0;             // compact initial guess, or null for x = 0
     const int* fidx;             // compact FLUID list (level-0 padded index)
     const uint8_t* diag;         // compact diagonal, bit 7 = red/black colour
     const int* nf;
@@ -277,7 +278,36 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         const double rv = double(a.rhs[n]);
         r[c] = rv;
         b0[c] = float(rv);
-        a.xs[c] = 0.0;
+        a.xs[c] = a.x0 ? double(a.x0[n]) : 0.0;
+    }
+    double bb_warm = 0.0;  // ||b||^2 when started from a guess
+    if (a.x0) {
+        // Scale the guess by its energy-optimal factor alpha = (x0, b) / (x0, A x0):
+        // the A-norm error of alpha x0 is never above that of x = 0.  Then r = b - A x.
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+        double xb = 0.0, xq = 0.0, bbl = 0.0;
+        for (int n = t0; n < nf; n += st) {
+            const int c = a.fidx[n];
+            const double* xp = a.xs + c;
+            const double qv = double(a.diag[n] & 0x7F) * xp[0] -
+                              ((xp[1] + xp[-1]) + (xp[sy] + xp[-sy]) + (xp[sz] + xp[-sz]));
+            a.q[c] = qv;
+            xb += xp[0] * r[c];
+            xq += xp[0] * qv;
+            bbl += r[c] * r[c];
+        }
+        partial(xb, xq, bbl);
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+        const double3 t = total();
+        const double alpha = (t.y > 0.0 && isfinite(t.x / t.y)) ? t.x / t.y : 0.0;
+        bb_warm = t.z;  // all reads of x ended before the barrier above
+        for (int n = t0; n < nf; n += st) {
+            const int c = a.fidx[n];
+            a.xs[c] *= alpha;
+            const double rv = r[c] - alpha * a.q[c];
+            r[c] = rv;
+            b0[c] = float(rv);
+        }
     }
     if (!vcycle(a)) return;
     {
@@ -294,7 +324,8 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
     double3 tot = total();
     double rz = tot.x, rr = tot.y;
-    const double bb = tot.y;
+    const double bb = a.x0 ? bb_warm : tot.y;
+    const double rr0 = tot.y;
     const double thr = a.tol * a.tol * bb;
     int it = 0, stt = DEV_OK;
     while (rr > thr && bb > 0.0) {
@@ -369,6 +400,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         a.out->rr = rr;
         a.out->bb = bb;
         a.out->rz = rz;
+        a.out->rr0 = rr0;
     }
 }
 
@@ -437,7 +469,7 @@ void launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStre
 }
 
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
-                  const float* rhs, double tol, int maxit, cudaStream_t st) {
+                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0) {
     const int nb = mg_max_blocks();
     int* status = &pb.out->status;
     cudaMemsetAsync(pb.bar, 0, sizeof(GridBar), st);
@@ -451,7 +483,7 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     }
     a.rscale = g.D > 1 ? 0.25f : 0.5f;
     a.nu_coarse = 2;
-    a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
+    a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
     a.X = static_cast<double*>(pb.X);
     a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;
     a.tol = tol; a.maxit = maxit;

@@ -20,6 +20,7 @@
 #include "../../include/fluidprjct.h"
 #include "io.hpp"
 #include "kernels.hpp"
+#include "unet.hpp"
 
 using namespace fp;
 
@@ -116,6 +117,12 @@ struct fp_solver {
     MgLevel mg[MG_MAX_LEVELS]{};
     int mgL = 0;
     double *d_mgp = nullptr, *d_mgq = nullptr, *d_mgx = nullptr, *d_mgr = nullptr;
+    // learned initial guess
+    fp_unet* net = nullptr;
+    std::string learned_path;
+    float* d_rhs_dense = nullptr;  // dense right-hand side (network input, FP_GRID_RHS)
+    float* d_x0c = nullptr;        // compact initial guess
+    cudaEvent_t ev_net = nullptr;
     // pinned result mirrors
     PcgOut* h_out = nullptr;
     double* h_red = nullptr;
@@ -154,6 +161,8 @@ void free_grid(fp_solver* s) {
     for (int l = 0; l < s->mgL; ++l) { dfree(s->mg[l].lab); dfree(s->mg[l].x); dfree(s->mg[l].b); }
     s->mgL = 0;
     dfree(s->d_mgp); dfree(s->d_mgq); dfree(s->d_mgx); dfree(s->d_mgr);
+    dfree(s->d_rhs_dense); dfree(s->d_x0c);
+    if (s->net) { fp_unet_destroy(s->net); s->net = nullptr; }
     s->have_grid = false;
 }
 
@@ -166,6 +175,23 @@ void free_particles(fp_solver* s) {
     dfree(s->d_pos); dfree(s->d_vel); dfree(s->d_pos2); dfree(s->d_vel2);
     dfree(s->d_key); dfree(s->d_rank); dfree(s->d_io);
     s->np = s->cap = 0;
+}
+
+// (Re)create the inference network for the current grid from learned_path.
+int load_net(fp_solver* s) {
+    if (s->net) { fp_unet_destroy(s->net); s->net = nullptr; }
+    if (s->cfg.dim != 3 || s->W < 4 || s->H < 4 || s->D < 4)
+        return s->fail(FP_ERR_ARG, "the learned preconditioner needs a 3D grid of at least 4 cells per axis");
+    int rc = fp_unet_create(s->W, s->H, s->D, 0, 0, &s->net);
+    if (rc) return s->fail(rc, "network allocation failed");
+    rc = fp_unet_load(s->net, s->learned_path.c_str());
+    if (rc) {
+        s->err = fp_unet_last_error(s->net);
+        fp_unet_destroy(s->net);
+        s->net = nullptr;
+        return rc;
+    }
+    return FP_OK;
 }
 
 int alloc_grid(fp_solver* s, int W, int H, int D) {
@@ -196,7 +222,9 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     ck(dalloc(&pb.part, size_t(6) * std::max(maxb, 1024)));
     ck(dalloc(&pb.bar, 1)); ck(dalloc(&pb.out, 1)); ck(dalloc(&pb.red, 2));
     pb.tile_sums = s->d_tiles;
-    if (s->cfg.solver == FP_SOLVER_PCG_MG) {
+    ck(dalloc(&s->d_rhs_dense, nc));
+    if (s->cfg.solver == FP_SOLVER_PCG_LEARNED) ck(dalloc(&s->d_x0c, nc));
+    if (s->cfg.solver == FP_SOLVER_PCG_MG || s->cfg.solver == FP_SOLVER_PCG_LEARNED) {
         s->mgL = mg_levels_for(W, H, D, s->mg);
         for (int l = 0; l < s->mgL && e == cudaSuccess; ++l) {
             MgLevel& L = s->mg[l];
@@ -229,6 +257,7 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     if (e != cudaSuccess) { free_grid(s); return s->cuda_fail(e, "grid initialisation"); }
     s->have_grid = true;
     s->sorted = false;
+    if (!s->learned_path.empty()) return load_net(s);
     return FP_OK;
 }
 
@@ -329,33 +358,77 @@ int solve_system(fp_solver* s, float* p_out) {
     int dev_status = DEV_OK;
     float pcg_ms = 0.0f;
     cudaError_t ce;
-    if (s->cfg.solver == FP_SOLVER_PCG || s->cfg.solver == FP_SOLVER_PCG_MG) {
-        const bool mg = s->cfg.solver == FP_SOLVER_PCG_MG;
+    float learned_ms = 0.0f, guess_relres = 1.0f;
+    int fallback = 0;
+    if (s->cfg.solver == FP_SOLVER_PCG || s->cfg.solver == FP_SOLVER_PCG_MG ||
+        s->cfg.solver == FP_SOLVER_PCG_LEARNED) {
+        const bool learned = s->cfg.solver == FP_SOLVER_PCG_LEARNED;
+        const bool mg = s->cfg.solver != FP_SOLVER_PCG;
+        if (learned && !s->net) return s->fail(FP_ERR_STATE, "learned solver: no weights loaded (fp_load_learned)");
         if (mg) {
             launch_mg_setup(s->d_labels, s->g, s->mg, s->mgL, s->st);
             s->launches += s->mgL;
         }
         cudaEventRecord(s->ev_pcg[0], s->st);
-        int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr, pb.b, tol, maxit,
-                                   s->st)
+        const float* x0 = nullptr;
+        if (learned) {
+            const unet::Lvl real{s->W, s->H, s->D};
+            unet::launch_rhs_dense(pb.nf, pb.fidx, real, pb.b, s->d_rhs_dense, s->st);
+            if (unet::forward_on(s->net, s->d_labels, s->d_rhs_dense, s->st))
+                return s->cuda_fail(cudaGetLastError(), "U-Net forward");
+            unet::launch_output_compact(pb.nf, pb.fidx, real, unet::net_level0(s->net), unet::net_out(s->net),
+                                        unet::net_scal(s->net), s->d_x0c, s->st);
+            s->launches += 1 + 14 + 1;  // rhs scatter, network (2 scale/input + 10 conv + 2 pool), guess
+            cudaEventRecord(s->ev_net, s->st);
+            x0 = s->d_x0c;
+        }
+        // A learned solve that has not converged after kLearnedMaxit iterations
+        // counts as stalled and hands over to the plain PCG.
+        constexpr int kLearnedMaxit = 300;
+        int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr, pb.b, tol,
+                                   learned ? std::min(maxit, kLearnedMaxit) : maxit, s->st, x0)
                    : launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st);
         cudaEventRecord(s->ev_pcg[1], s->st);
         if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
-        launch_scatter_p(pb, p_out, 1, s->g, s->st);
-        launch_true_residual(pb, 1, s->g, s->st);
-        // the residual check leaves the solution in the padded R[0] grid: clear
-        // it (and the Jacobi work grids) at this solve's FLUID cells
-        launch_pcg_clear(pb, 1, mg ? 0 : 1, s->st);
-        s->launches += (mg ? 1 : 2) + 1 + 3 + 1;  // [reset +] pcg, scatter, residual (3), clear
-        cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
-        cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
-        cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
-        ce = cudaStreamSynchronize(s->st);
+        // FP64 solution to p, its true residual, then clear the work grids at
+        // this solve's FLUID cells (the residual check leaves x in R[0])
+        auto finish = [&](bool jacobi) -> cudaError_t {
+            launch_scatter_p(pb, p_out, 1, s->g, s->st);
+            launch_true_residual(pb, 1, s->g, s->st);
+            launch_pcg_clear(pb, 1, jacobi ? 1 : 0, s->st);
+            s->launches += (jacobi ? 1 : 0) + 1 + 1 + 3 + 1;  // [reset +] pcg, scatter, residual (3), clear
+            cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
+            cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+            cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+            return cudaStreamSynchronize(s->st);
+        };
+        ce = finish(!mg);
         if (ce != cudaSuccess) return s->cuda_fail(ce, "pressure solve");
         inner_total = s->h_out->iters;
         dev_status = s->h_out->status;
         outer = 1;
         cudaEventElapsedTime(&pcg_ms, s->ev_pcg[0], s->ev_pcg[1]);
+        if (learned) {
+            cudaEventElapsedTime(&learned_ms, s->ev_pcg[0], s->ev_net);
+            guess_relres = s->h_out->bb > 0 ? float(std::sqrt(s->h_out->rr0 / s->h_out->bb)) : 0.0f;
+            const double rel = s->h_red[1] > 0 ? std::sqrt(s->h_red[0] / s->h_red[1]) : 0.0;
+            if (*s->h_nf > 0 && dev_status != DEV_TIMEOUT && (dev_status != DEV_OK || !(rel <= tol))) {
+                // fallback: the plain FP64 PCG from x = 0
+                fallback = 1;
+                cudaEventRecord(s->ev_pcg[0], s->st);
+                e = launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st);
+                cudaEventRecord(s->ev_pcg[1], s->st);
+                if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
+                ce = finish(true);
+                if (ce != cudaSuccess) return s->cuda_fail(ce, "pressure solve (fallback)");
+                inner_total += s->h_out->iters;
+                dev_status = s->h_out->status;
+                outer = 2;
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, s->ev_pcg[0], s->ev_pcg[1]);
+                pcg_ms += ms;
+            }
+        }
     } else {
         cudaMemsetAsync(pb.x64, 0, sizeof(double) * s->g.nc(), s->st);
         launch_ir_residual(pb, s->g, s->st);  // x64 = 0: bin = b
@@ -406,7 +479,9 @@ int solve_system(fp_solver* s, float* p_out) {
     s->stats.num_fluid_cells = *s->h_nf;
     s->stats.pcg_iters = inner_total;
     s->stats.outer_iters = outer;
-    s->stats.fallback = 0;
+    s->stats.fallback = fallback;
+    s->stats.t_learned = learned_ms;
+    s->stats.guess_relres = guess_relres;
     s->stats.residual = s->h_red[1] > 0 ? std::sqrt(s->h_red[0] / s->h_red[1]) : 0.0;
     int status = FP_OK;
     if (*s->h_nf == 0) status = FP_ERR_NO_FLUID;
@@ -594,7 +669,7 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     if (!s) return FP_ERR_ARG;
     if (cfg) s->cfg = *cfg; else fp_config_default(&s->cfg);
     if (!(s->cfg.dx > 0) || !(s->cfg.dt > 0) || (s->cfg.dim != 2 && s->cfg.dim != 3)) { delete s; return FP_ERR_ARG; }
-    if (s->cfg.solver != FP_SOLVER_PCG && s->cfg.solver != FP_SOLVER_PCG_MIXED && s->cfg.solver != FP_SOLVER_PCG_MG) {
+    if (s->cfg.solver < FP_SOLVER_PCG || s->cfg.solver > FP_SOLVER_PCG_LEARNED) {
         std::fprintf(stderr, "fp_create: solver %d is not available in this build\n", s->cfg.solver);
         delete s;
         return FP_ERR_ARG;
@@ -604,6 +679,7 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
     for (auto& ev : s->ev) if (e == cudaSuccess) e = cudaEventCreate(&ev);
     for (auto& ev : s->ev_pcg) if (e == cudaSuccess) e = cudaEventCreate(&ev);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_net);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_out, sizeof(PcgOut));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_red, sizeof(double) * 2);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_nf, sizeof(int));
@@ -626,6 +702,7 @@ int fp_destroy(fp_solver* s) {
     if (s->h_bforce) cudaFreeHost(s->h_bforce);
     for (auto& ev : s->ev) if (ev) cudaEventDestroy(ev);
     for (auto& ev : s->ev_pcg) if (ev) cudaEventDestroy(ev);
+    if (s->ev_net) cudaEventDestroy(s->ev_net);
     if (s->h_out) cudaFreeHost(s->h_out);
     if (s->h_red) cudaFreeHost(s->h_red);
     if (s->h_nf) cudaFreeHost(s->h_nf);
@@ -859,11 +936,16 @@ static int64_t grid_len(const fp_solver* s, int which) {
         case FP_GRID_U: case FP_GRID_U_SAVED: return s->g.nu();
         case FP_GRID_V: case FP_GRID_V_SAVED: return s->g.nv();
         case FP_GRID_W: case FP_GRID_W_SAVED: return s->g.nw();
-        case FP_GRID_P: return s->g.nc();
+        case FP_GRID_P: case FP_GRID_RHS: return s->g.nc();
     }
     return -1;
 }
 static float* grid_ptr(fp_solver* s, int which) {
+    if (which == FP_GRID_RHS) {  // densify the last solve's compact right-hand side
+        unet::launch_rhs_dense(s->pb.nf, s->pb.fidx, unet::Lvl{s->W, s->H, s->D}, s->pb.b, s->d_rhs_dense, s->st);
+        s->launches += 1;
+        return s->d_rhs_dense;
+    }
     float* a[7] = {s->d_u, s->d_v, s->d_w, s->d_us, s->d_vs, s->d_ws, s->d_p};
     return (which >= 0 && which < 7) ? a[which] : nullptr;
 }
@@ -877,8 +959,36 @@ int fp_get_grid(fp_solver* s, int which, float* out, int64_t n) {
     return e == cudaSuccess ? FP_OK : s->cuda_fail(e, "grid download");
 }
 
+int fp_get_grid_device(fp_solver* s, int which, float* d_out, int64_t n) {
+    if (!s || !d_out) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "no grid");
+    if (grid_len(s, which) != n) return s->fail(FP_ERR_ARG, "grid size mismatch");
+    cudaError_t e = cudaMemcpyAsync(d_out, grid_ptr(s, which), sizeof(float) * n, cudaMemcpyDeviceToDevice, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    return e == cudaSuccess ? FP_OK : s->cuda_fail(e, "grid copy");
+}
+
+int fp_get_labels_device(fp_solver* s, uint8_t* d_out, int64_t n) {
+    if (!s || !d_out) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "no grid");
+    if (n != s->g.nc()) return s->fail(FP_ERR_ARG, "label size mismatch");
+    cudaError_t e = cudaMemcpyAsync(d_out, s->d_labels, size_t(n), cudaMemcpyDeviceToDevice, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    return e == cudaSuccess ? FP_OK : s->cuda_fail(e, "label copy");
+}
+
+int fp_load_learned(fp_solver* s, const char* weights_path) {
+    if (!s || !weights_path) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "labels must be loaded before the learned weights");
+    s->learned_path = weights_path;
+    const int rc = load_net(s);
+    if (rc) s->learned_path.clear();
+    return rc;
+}
+
 int fp_set_grid(fp_solver* s, int which, const float* in, int64_t n) {
     if (!s || !in) return FP_ERR_ARG;
+    if (which == FP_GRID_RHS) return s->fail(FP_ERR_ARG, "the right-hand side grid is read only");
     if (!s->have_grid) return s->fail(FP_ERR_STATE, "no grid");
     if (grid_len(s, which) != n) return s->fail(FP_ERR_ARG, "grid size mismatch");
     cudaError_t e = cudaMemcpyAsync(grid_ptr(s, which), in, sizeof(float) * n, cudaMemcpyHostToDevice, s->st);

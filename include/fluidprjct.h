@@ -65,9 +65,11 @@ enum { FP_SOLVER_PCG = 0, FP_SOLVER_PCG_MIXED = 1, FP_SOLVER_PCG_MG = 2, FP_SOLV
  * FluidSolver3D.cu:1241-1330) or midpoint RK2 with the same substepping. */
 enum { FP_ADVECT_RK3REF = 0, FP_ADVECT_RK2 = 1 };
 
-/* Grid selectors for fp_get_grid / fp_set_grid. */
+/* Grid selectors for fp_get_grid / fp_set_grid.  FP_GRID_RHS (read only) is
+ * the dense right-hand side of the last pressure solve, zero off FLUID cells
+ * (the reference's RHS, FluidSolver3D.cu:1518-1596, before compaction). */
 enum { FP_GRID_U = 0, FP_GRID_V = 1, FP_GRID_W = 2, FP_GRID_U_SAVED = 3, FP_GRID_V_SAVED = 4,
-       FP_GRID_W_SAVED = 5, FP_GRID_P = 6 };
+       FP_GRID_W_SAVED = 5, FP_GRID_P = 6, FP_GRID_RHS = 7 };
 
 /* Step phases for fp_run_phase, in frameStep order (FluidSolver3D.cu:3030-3098). */
 enum { FP_PHASE_LABEL = 0, FP_PHASE_P2G = 1, FP_PHASE_SAVE = 2, FP_PHASE_FORCES = 3, FP_PHASE_PRESSURE = 4,
@@ -114,12 +116,13 @@ typedef struct fp_step_stats {
     double  residual;          /* final true relative residual ||b-Ax||/||b||    */
     float   t_label, t_p2g, t_forces, t_pressure, t_project, t_body, t_g2p, t_advect;
     float   t_total;
-    float   pad2_;
+    float   guess_relres;      /* ||b - A x0|| / ||b|| of the learned initial guess
+                                  (1 for solves that start from x = 0)           */
     double  body_pos[3], body_vel[3], body_omega[3], body_angles[3];
     double  body_force[3], body_torque[3];
     int64_t kernel_launches;   /* kernels this library launched, cumulative     */
-    float   t_pcg;             /* device time of the PCG kernel(s), last solve  */
-    float   pad3_;
+    float   t_pcg;             /* device time of the pressure solve, last step  */
+    float   t_learned;         /* of which the learned initial guess            */
 } fp_step_stats;
 
 typedef struct fp_solver fp_solver;
@@ -173,6 +176,10 @@ int fp_run_phase(fp_solver* s, int phase);
 int fp_get_grid(fp_solver* s, int which, float* out, int64_t n);
 int fp_set_grid(fp_solver* s, int which, const float* in, int64_t n);
 int fp_get_labels(fp_solver* s, uint8_t* out, int64_t n);
+/* The same copies into caller DEVICE memory, ordered on the solver's stream
+ * and complete on return (no host staging; used to build training sets). */
+int fp_get_grid_device(fp_solver* s, int which, float* d_out, int64_t n);
+int fp_get_labels_device(fp_solver* s, uint8_t* d_out, int64_t n);
 
 /* Rigid-body kinematic state used by the RHS and projection; setting it
  * overrides the integrated state (FluidSolver3D.cu:1368-1370). */
@@ -210,6 +217,42 @@ int fp_solve_csr_upper(int n, const int* offsets, const int* cols, const double*
 int fp_solve_csr_upper_noalloc(int n, const int* d_offsets, const int* d_cols, const double* d_vals,
                                const double* d_b, double* d_x, double tol, int max_iters, int* iters,
                                double* relres, void* stream);
+
+/* Learned preconditioner (no counterpart in the reference).  A 3D U-Net with
+ * three levels (16/32/64 channels, 3x3x3 convolutions, BF16 weights and
+ * activations, FP32 accumulation) maps the cell labels and the divergence to
+ * a pressure guess.  FP_SOLVER_PCG_LEARNED scales that guess by its
+ * energy-optimal factor and uses it as the initial iterate of the
+ * multigrid-preconditioned PCG.  If that solve stalls or misses tol, the plain
+ * FP64 PCG solves again from zero (fp_step_stats.fallback = 1).
+ * fp_load_learned loads a weight file written by fp_unet_save (labels must be
+ * loaded first; 3D only). */
+int fp_load_learned(fp_solver* s, const char* weights_path);
+
+/* The network itself, for training and tests.  All array arguments are DEVICE
+ * pointers on the real grid (labels uint8, rhs/p/x float, W*H*D each); grids
+ * are padded to multiples of 4 inside, the padding counting as SOLID.  Calls
+ * are complete on return, except fp_unet_train_step with loss == NULL, which
+ * returns once the step is queued on the network's stream.  Weights are the
+ * flat FP32 vector of fp_unet_num_params() entries: layers L0..L9 as
+ * [27][COUT][CIN] (tap = (dz+1)*9 + (dy+1)*3 + (dx+1)), then 16 head
+ * weights.  The loss is sum_F (out - p/s)^2 / sum_F (p/s)^2 over FLUID cells,
+ * s = the RMS of rhs over FLUID cells. */
+typedef struct fp_unet fp_unet;
+int64_t fp_unet_num_params(void);
+int fp_unet_create(int W, int H, int D, int train, uint64_t seed, fp_unet** out);
+void fp_unet_destroy(fp_unet* u);
+const char* fp_unet_last_error(const fp_unet* u);
+void* fp_unet_cuda_stream(const fp_unet* u);
+int fp_unet_get_params(fp_unet* u, float* out, int64_t n);
+int fp_unet_set_params(fp_unet* u, const float* in, int64_t n);
+int fp_unet_save(fp_unet* u, const char* path);
+int fp_unet_load(fp_unet* u, const char* path);
+int fp_unet_forward(fp_unet* u, const uint8_t* d_labels, const float* d_rhs, float* d_x);
+int fp_unet_loss_grad(fp_unet* u, const uint8_t* d_labels, const float* d_rhs, const float* d_p, double* loss,
+                      float* grad);
+int fp_unet_train_step(fp_unet* u, const uint8_t* d_labels, const float* d_rhs, const float* d_p, float lr,
+                       double* loss);
 
 /* Host-only readers (no GPU needed).  fp_read_label_file parses a reference
  * label file (dim 3: FluidSolver3D.cu:81-153, dim 2: FluidSolver2D.cu:52-104);

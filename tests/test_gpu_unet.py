@@ -1,0 +1,166 @@
+"""The learned preconditioner's network on the GPU against the CPU oracle.
+
+The CUDA forward output and every weight gradient are compared with
+oracle/unet_oracle.py in its bf16 mode. That mode rounds to bf16 at the same
+points as the kernels, so only FP32 accumulation order separates the two.
+The tolerances below allow for that and for the rare bf16 rounding flips it
+causes. Then a short training run must lower the loss, the trained guess
+must cut the MG-PCG iteration count on a held-out system, and the
+plain-PCG fallback must engage when the learned solve cannot converge.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(seed=0, D=13, H=17, W=22):
+    rng = np.random.default_rng(seed)
+    lab = np.full((D, H, W), 1, np.uint8)
+    lab[0] = lab[-1] = 0
+    lab[:, 0] = lab[:, -1] = 0
+    lab[:, :, 0] = lab[:, :, -1] = 0
+    lab[1:-1, H - 6:-1, 1:-1] = 2
+    lab[5, 4, 7] = 3
+    lab[8, 6, 3:6] = 0
+    rhs = np.where(lab == 1, rng.standard_normal(lab.shape), 0).astype(np.float32)
+    p = np.where(lab == 1, rng.standard_normal(lab.shape), 0).astype(np.float32)
+    return lab, rhs, p
+
+
+def _dev(*arrs):
+    import torch
+    return [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in arrs]
+
+
+def test_unet_forward_matches_oracle():
+    from fluidprjct_b200 import capi
+    from oracle import unet_oracle as U
+    lab, rhs, _ = _scene()
+    D, H, W = lab.shape
+    th = U.init_params(11)
+    net = capi.UNet(W, H, D, train=False)
+    net.set_params(th)
+    assert np.array_equal(net.params(), th)
+    tl, tr = _dev(lab, rhs)
+    import torch
+    x = torch.zeros_like(tr)
+    torch.cuda.synchronize()
+    net.forward(tl.data_ptr(), tr.data_ptr(), x.data_ptr())
+    out_ref, xd_ref, _ = U.forward(th, lab, rhs, bf=True)
+    xg = x.cpu().numpy()
+    err = rel_l2(xg, xd_ref)
+    assert err <= 1e-2, err
+    assert np.all(xg[lab != 1] == 0)
+
+
+def test_unet_loss_grad_matches_oracle():
+    from fluidprjct_b200 import capi
+    from oracle import unet_oracle as U
+    lab, rhs, p = _scene(1)
+    D, H, W = lab.shape
+    th = U.init_params(12)
+    net = capi.UNet(W, H, D, train=True)
+    net.set_params(th)
+    tl, tr, tp = _dev(lab, rhs, p)
+    import torch
+    torch.cuda.synchronize()
+    loss, g = net.loss_grad(tl.data_ptr(), tr.data_ptr(), tp.data_ptr())
+    loss_ref, g_ref = U.loss_grad(th, lab, rhs, p, bf=True)
+    assert abs(loss - loss_ref) <= 1e-3 * loss_ref, (loss, loss_ref)
+    sizes = np.cumsum([0] + U.layer_sizes() + [U.HEAD])
+    for l in range(len(sizes) - 1):
+        a, b = g[sizes[l]:sizes[l + 1]], g_ref[sizes[l]:sizes[l + 1]]
+        err = rel_l2(a, b)
+        cos = float(a @ b) / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30)
+        assert err <= 3e-2 and cos >= 0.999, (l, err, cos)
+    # deterministic: the same call gives the same bits
+    loss2, g2 = net.loss_grad(tl.data_ptr(), tr.data_ptr(), tp.data_ptr())
+    assert loss2 == loss and np.array_equal(g2, g)
+
+
+def test_unet_weight_file_roundtrip(tmp_path):
+    from fluidprjct_b200 import capi
+    net = capi.UNet(8, 8, 8, seed=3)
+    w = net.params()
+    assert w.size == capi.UNet.num_params() == 359440 and np.isfinite(w).all()
+    path = tmp_path / "w.bin"
+    net.save(path)
+    net2 = capi.UNet(12, 8, 16, seed=4)
+    assert not np.array_equal(net2.params(), w)
+    net2.load(path)
+    assert np.array_equal(net2.params(), w)
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(b"not a weight file")
+    with pytest.raises(capi.FluidError) as e:
+        net2.load(bad)
+    assert e.value.code == capi.FP_ERR_IO
+    with pytest.raises(capi.FluidError) as e:
+        net2.set_params(np.full(w.size, np.nan, np.float32))
+    assert e.value.code == capi.FP_ERR_ARG
+
+
+@pytest.fixture(scope="module")
+def trained(tmp_path_factory):
+    """A network trained briefly on 32^3 FLIP scenes, its data and weight file."""
+    from fluidprjct_b200 import learned
+    data = learned.generate(n=32, scenes=6, steps_per_scene=12, seed=5)
+    held = learned.generate(n=32, scenes=2, steps_per_scene=6, seed=77)
+    net0_loss = None
+    from fluidprjct_b200 import capi
+    net = capi.UNet(32, 32, 32, train=True, seed=1)
+    net0_loss = learned.eval_loss(net, held, range(12))
+    net, hist = learned.train(data, adam_steps=400, lr=2e-3, seed=1, net=net, log_every=50)
+    path = tmp_path_factory.mktemp("w") / "unet32.bin"
+    net.save(path)
+    return {"data": data, "held": held, "net": net, "hist": hist, "path": str(path), "loss0": net0_loss}
+
+
+def test_unet_training_lowers_the_heldout_loss(trained):
+    from fluidprjct_b200 import learned
+    after = learned.eval_loss(trained["net"], trained["held"], range(12))
+    print("held-out loss", trained["loss0"], "->", after, "history", trained["hist"])
+    assert np.isfinite(after) and after < 0.5 * trained["loss0"] and after < 0.6
+
+
+def test_learned_guess_keeps_mg_iterations(trained):
+    """At 32^3 after 400 Adam steps the guess is not accurate enough to save
+    MG iterations; it must not cost any either, nor need the fallback."""
+    from fluidprjct_b200 import learned
+    held = trained["held"]
+    for k in (5, 11):
+        lab = held[0][k].cpu().numpy()
+        rhs = held[1][k].cpu().numpy()
+        r = learned.compare_solvers(lab, rhs, trained["path"], tol=1e-6, repeats=1)
+        print(k, r)
+        for v in r.values():
+            assert v["status"] == 0 and v["residual"] <= 1e-6
+        assert r["pcg_learned"]["fallback"] == 0
+        assert r["pcg_learned"]["iters"] <= r["pcg_mg"]["iters"]
+
+
+def test_learned_solver_falls_back_to_plain_pcg(trained):
+    """With an iteration cap too small for the learned solve, the plain PCG
+    runs next and the step reports the fallback."""
+    from fluidprjct_b200 import capi
+    held = trained["held"]
+    lab = held[0][3].cpu().numpy()
+    rhs = held[1][3].cpu().numpy()
+    s = capi.Solver(dim=3, dx=1 / 32, dt=0.008, solver="pcg_learned", tol=1e-6, max_iters=2,
+                    output_format=capi.OUT_NONE)
+    s.set_labels(lab)
+    s.load_learned(trained["path"])
+    _, it, rr, rc = s.pressure_solve(rhs)
+    st = s.stats()
+    assert st["fallback"] == 1 and st["outer_iters"] == 2 and rc == capi.FP_ERR_SOLVER
+    # a missing weight file is an I/O error, and the solver needs weights
+    s2 = capi.Solver(dim=3, dx=1 / 32, dt=0.008, solver="pcg_learned", output_format=capi.OUT_NONE)
+    s2.set_labels(lab)
+    with pytest.raises(capi.FluidError) as e:
+        s2.load_learned("/nonexistent/weights.bin")
+    assert e.value.code == capi.FP_ERR_IO
+    with pytest.raises(capi.FluidError) as e:
+        s2.pressure_solve(rhs)
+    assert e.value.code == capi.FP_ERR_STATE
