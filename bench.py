@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--solver", default="pcg_mg", choices=["pcg", "pcg_mixed", "pcg_mg", "pcg_learned"],
+                    help="pressure solver of the timed steps")
     return ap.parse_args()
 
 
@@ -130,6 +132,9 @@ def new_solver(lab, device, solver="pcg", n=N_GRID, ppc=PPC):
     s = capi.Solver(dx=1.0 / n, dt=DT, pic_weight=PIC, advection="rk2", solver=solver, tol=1e-6, max_iters=20000,
                     device=device, output_format=capi.OUT_NONE)
     s.set_labels(lab)
+    if solver == "pcg_learned":
+        from fluidprjct_b200.learned import DEFAULT_WEIGHTS
+        s.load_learned(DEFAULT_WEIGHTS)
     s.seed_particles(ppc, SEED)
     return s
 
@@ -160,7 +165,7 @@ def run_ours(args, rank, local, world):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     lab = make_scene(args.n, args.ppc)
-    s = new_solver(lab, local, "pcg_mixed", args.n, args.ppc)
+    s = new_solver(lab, local, args.solver, args.n, args.ppc)
     np_ = s.num_particles
     nc = args.n ** 3
     stream, Ev = event_timer(s.stream)
@@ -199,14 +204,25 @@ def run_ours(args, rank, local, world):
     ms_step = ms / args.steps
     value = world * args.steps / (ms / 1000.0)
 
-    # ---- roofline of the dominant kernel (the persistent PCG) ----
+    # ---- roofline of the dominant kernel (the persistent pressure solver) ----
     nf = statistics.mean(p["num_fluid_cells"] for p in per)
     iters = [p["pcg_iters"] for p in per]
-    pcg_ms = [p["t_pcg"] for p in per]
-    pcg_bytes = [41.0 * p["num_fluid_cells"] * p["pcg_iters"] + 17.0 * p["num_fluid_cells"] * p["outer_iters"]
-                 for p in per]
+    solve_ms = [p["t_pcg"] - p["t_learned"] for p in per]  # the network's share is timed apart
+    if args.solver in ("pcg_mg", "pcg_learned"):
+        kernel = "k_pcg_mg"
+        # per MG-PCG iteration: Krylov loops 117 B per FLUID cell (FP64 p, q, x, r;
+        # FP32 z; index and diagonal), level-0 V-cycle 75 B per FLUID cell plus
+        # 5 B per cell for the restriction, coarser levels 7 B per fine cell
+        solve_bytes = [(192.0 * p["num_fluid_cells"] + 12.0 * nc) * p["pcg_iters"] for p in per]
+        note = ("192 B per fluid cell + 12 B per cell per MG-PCG iteration; the kernel is bound by its "
+                "~26 grid barriers per V-cycle, not by HBM")
+    else:
+        kernel = "k_pcg_cg"
+        solve_bytes = [41.0 * p["num_fluid_cells"] * p["pcg_iters"] + 17.0 * p["num_fluid_cells"] * p["outer_iters"]
+                       for p in per]
+        note = "41 B per fluid cell per iteration + 17 B per fluid cell; working set is L2-resident at 128^3"
     peak, peak_kind = load_peaks()
-    pcg_gbs = sum(pcg_bytes) / (sum(pcg_ms) / 1000.0) / 1e9
+    solve_gbs = sum(solve_bytes) / (sum(solve_ms) / 1000.0) / 1e9
     traffic = load_traffic()
     phase_ms = {k: statistics.mean(p[k] for p in per) for k in ("t_label", "t_p2g", "t_pressure", "t_project",
                                                                  "t_advect", "t_total")}
@@ -214,22 +230,28 @@ def run_ours(args, rank, local, world):
     phases = {
         "label": {"ms": phase_ms["t_label"], "gbs": ab["label"] / phase_ms["t_label"] / 1e6},
         "p2g+save+forces": {"ms": phase_ms["t_p2g"], "gbs": ab["p2g"] / phase_ms["t_p2g"] / 1e6},
-        "pressure": {"ms": phase_ms["t_pressure"], "pcg_ms": statistics.mean(pcg_ms), "pcg_iters": statistics.mean(iters)},
+        "pressure": {"ms": phase_ms["t_pressure"], "solve_ms": statistics.mean(solve_ms),
+                     "learned_ms": statistics.mean(p["t_learned"] for p in per), "iters": statistics.mean(iters)},
         "project": {"ms": phase_ms["t_project"], "gbs": ab["project"] / phase_ms["t_project"] / 1e6},
         "g2p+advect": {"ms": phase_ms["t_advect"], "gbs": ab["g2p_advect"] / phase_ms["t_advect"] / 1e6},
     }
-    roofline = {"kernel": "k_pcg (persistent cooperative PCG)", "bound": "hbm", "achieved": round(pcg_gbs, 1),
-                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(pcg_gbs / peak, 4),
-                "traffic": (traffic or {}).get("k_pcg_bytes_per_launch"),
-                "algorithmic_bytes_per_launch": statistics.mean(pcg_bytes),
-                "note": "41 B per fluid cell per iteration + 17 B per fluid cell; working set is L2-resident at 128^3"}
+    roofline = {"kernel": kernel + " (persistent cooperative solver)", "bound": "hbm", "achieved": round(solve_gbs, 1),
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(solve_gbs / peak, 4),
+                "traffic": (traffic or {}).get(kernel + "_bytes_per_launch"),
+                "algorithmic_bytes_per_launch": statistics.mean(solve_bytes), "note": note}
+    solver_desc = {
+        "pcg": "plain PCG (Jacobi, FP64 vectors)",
+        "pcg_mixed": "pcg_mixed (Jacobi PCG, FP32 stencil/vectors, FP64 reductions, FP64 refinement)",
+        "pcg_mg": "pcg_mg (FP32 multigrid V-cycle preconditioner, FP64 Krylov vectors and reductions)",
+        "pcg_learned": "pcg_learned (U-Net initial guess + pcg_mg, plain PCG fallback)",
+    }[args.solver]
 
     out = {"metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32 (FP64 reductions)", "data": "synthetic",
            "config": {"workload": f"3D dam break {args.n}^3, dx=1/{args.n}, fluid x<0.4 y<0.6 z<1, {args.ppc} ppc",
                       "particles": int(np_), "fluid_cells_mean": nf, "dt": DT, "flip": 1 - PIC, "advection": "rk2",
-                      "solver": "pcg_mixed (Jacobi PCG, FP32 stencil/vectors, FP64 reductions, FP64 refinement)",
+                      "solver": solver_desc,
                       "tol": 1e-6,
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                       "l2": "inputs larger than L2 (particle arrays 2 x 61 MB + grids 58 MB per step)"},
@@ -257,7 +279,9 @@ def run_ours(args, rank, local, world):
                              "iters": statistics.mean(x["pcg_iters"] for x in st),
                              "outer": statistics.mean(x["outer_iters"] for x in st),
                              "residual_max": max(x["residual"] for x in st),
-                             "fallback": sum(x["fallback"] for x in st)}
+                             "fallback": sum(x["fallback"] for x in st),
+                             "learned_ms": round(statistics.mean(x["t_learned"] for x in st), 4),
+                             "guess_relres": round(statistics.mean(x["guess_relres"] for x in st), 4)}
             except Exception as e:
                 var[name] = {"error": str(e)}
             v.close()

@@ -37,6 +37,7 @@ constexpr int MG_THREADS = 512;
 struct MgArgs {
     int L, G;                    // levels; levels [0, G) are grid-wide
     float rscale;                // restriction scale (1/4 in 3D, 1/2 in 2D)
+    float omega;                 // over-relaxation of the coarse-grid correction
     int nu_coarse;               // symmetric sweep pairs on the coarsest level
     MgLevel lv[MG_MAX_LEVELS];
     double* p;                   // level-0 padded dense Krylov vectors (FP64)
@@ -125,12 +126,13 @@ __device__ void op0_sweep(const MgLevel& L, const int* fidx, const uint8_t* dg, 
         }
     }
 }
-__device__ void op0_prolong(const MgLevel& F, const MgLevel& Cl, const int* fidx, int nf, int t0, int stride) {
+__device__ void op0_prolong(const MgLevel& F, const MgLevel& Cl, float omega, const int* fidx, int nf, int t0,
+                            int stride) {
     for (int n = t0; n < nf; n += stride) {
         const int c = fidx[n];
         const int i = c % F.sy - 1, j = (c / F.sy) % (F.H + 2) - 1, k = c / F.sz - 1;
         const int cc = (i / 2 + 1) + (j / 2 + 1) * Cl.sy + (k / 2 + 1) * Cl.sz;
-        if (Cl.lab[cc] == FLUID) F.x[c] += Cl.x[cc];
+        if (Cl.lab[cc] == FLUID) F.x[c] += omega * Cl.x[cc];
     }
 }
 
@@ -184,15 +186,15 @@ __device__ void op_restrict(const MgLevel& F, const MgLevel& Cl, float scale, in
         Cl.b[cc] = s;
     }
 }
-// x_fine += x_coarse(parent) on FLUID cells with a FLUID parent.
-__device__ void op_prolong(const MgLevel& F, const MgLevel& Cl, int t0, int stride) {
+// x_fine += omega * x_coarse(parent) on FLUID cells with a FLUID parent.
+__device__ void op_prolong(const MgLevel& F, const MgLevel& Cl, float omega, int t0, int stride) {
     const int n = F.W * F.H * F.D;
     for (int t = t0; t < n; t += stride) {
         int i, j, k;
         const int c = lv_cell(F, t, i, j, k);
         if (F.lab[c] != FLUID) continue;
         const int cc = (i / 2 + 1) + (j / 2 + 1) * Cl.sy + (k / 2 + 1) * Cl.sz;
-        if (Cl.lab[cc] == FLUID) F.x[c] += Cl.x[cc];
+        if (Cl.lab[cc] == FLUID) F.x[c] += omega * Cl.x[cc];
     }
 }
 
@@ -216,7 +218,7 @@ __device__ void block_vcycle(const MgArgs& a, int l0) {
         op_sweep(C, 0, t0, st); __syncthreads();
     }
     for (int l = a.L - 2; l >= l0; --l) {
-        op_prolong(a.lv[l], a.lv[l + 1], t0, st); __syncthreads();
+        op_prolong(a.lv[l], a.lv[l + 1], a.omega, t0, st); __syncthreads();
         op_sweep(a.lv[l], 1, t0, st); __syncthreads();
         op_sweep(a.lv[l], 0, t0, st); __syncthreads();
     }
@@ -243,8 +245,8 @@ __device__ bool vcycle(const MgArgs& a) {
     if (blockIdx.x == 0) block_vcycle(a, G);
     if (!grid_barrier(a.bar, nb, a.status)) return false;
     for (int l = G - 1; l >= 0; --l) {
-        if (l == 0) op0_prolong(a.lv[0], a.lv[1], a.fidx, nf, t0, st);
-        else op_prolong(a.lv[l], a.lv[l + 1], t0, st);
+        if (l == 0) op0_prolong(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
+        else op_prolong(a.lv[l], a.lv[l + 1], a.omega, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 1, t0, st);
         else op_sweep(a.lv[l], 1, t0, st);
@@ -482,6 +484,12 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
         if (int64_t(lv[l].W) * lv[l].H * lv[l].D > MG_BLOCK_CELLS) a.G = l + 1;
     }
     a.rscale = g.D > 1 ? 0.25f : 0.5f;
+    // The piecewise-constant prolongation underestimates the coarse correction;
+    // scaling it by 1.7 roughly halves the PCG iterations (29 -> 15 at 128^3,
+    // 31 -> 14 at 256^2 in a float64 model of this V-cycle).  Any omega > 0
+    // keeps the preconditioner symmetric; in that model PCG converged for
+    // every omega up to 2 on dam-break, pool and random-box scenes.
+    a.omega = 1.7f;
     a.nu_coarse = 2;
     a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
     a.X = static_cast<double*>(pb.X);

@@ -539,12 +539,32 @@ __global__ void k_rhs_dense(const int* __restrict__ nf_p, const int* __restrict_
     }
 }
 
+// Global gradient norm (fixed-order, FP64) and the clipping factor
+// min(1, clip / norm) in scal[3]; the norm itself goes to red[2 * RED_BLOCKS + 1].
+__global__ void __launch_bounds__(THREADS) k_gnorm_part(const float* __restrict__ g, int64_t n,
+                                                         double* __restrict__ red) {
+    __shared__ double sh[THREADS / 32];
+    double v[1] = {0.0};
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        v[0] += double(g[i]) * double(g[i]);
+    block_sum_d<1>(v, sh);
+    if (threadIdx.x == 0) red[blockIdx.x] = v[0];
+}
+__global__ void k_gnorm_final(double* __restrict__ red, float clip, float* __restrict__ scal) {
+    if (threadIdx.x != 0) return;
+    double ss = 0.0;
+    for (int b = 0; b < RED_BLOCKS; ++b) ss += red[b];
+    const double nrm = sqrt(ss);
+    red[2 * RED_BLOCKS + 1] = nrm;
+    scal[3] = (nrm > double(clip) && isfinite(nrm)) ? float(double(clip) / nrm) : (isfinite(nrm) ? 1.0f : 0.0f);
+}
+
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
-                       const float* __restrict__ g, int64_t n, float lr, float b1, float b2, float eps, float bc1,
-                       float bc2) {
+                       const float* __restrict__ g, const float* __restrict__ scal, int64_t n, float lr, float b1,
+                       float b2, float eps, float bc1, float bc2) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float gi = g[i];
+    const float gi = g[i] * scal[3];
     const float mi = b1 * m[i] + (1.0f - b1) * gi;
     const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
     m[i] = mi;
@@ -730,8 +750,10 @@ void launch_rhs_dense(const int* nf, const int* fidx, Lvl real, const float* b, 
 }
 
 void launch_adam(float* w, float* m, float* v, const float* g, int64_t n, float lr, float b1, float b2, float eps,
-                 float bc1, float bc2, cudaStream_t st) {
-    k_adam<<<unsigned((n + 255) / 256), 256, 0, st>>>(w, m, v, g, n, lr, b1, b2, eps, bc1, bc2);
+                 float bc1, float bc2, float clip, double* red, float* scal, cudaStream_t st) {
+    k_gnorm_part<<<RED_BLOCKS, THREADS, 0, st>>>(g, n, red);
+    k_gnorm_final<<<1, 32, 0, st>>>(red, clip, scal);
+    k_adam<<<unsigned((n + 255) / 256), 256, 0, st>>>(w, m, v, g, scal, n, lr, b1, b2, eps, bc1, bc2);
 }
 
 void launch_weights_bf16(const float* w32, bf16* wf, bf16* wt, cudaStream_t st) {

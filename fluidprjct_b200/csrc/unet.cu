@@ -20,7 +20,8 @@
 using namespace fp::unet;
 
 namespace {
-constexpr int kRedLoss = 2 * 256;  // index of the loss in the reduction buffer
+constexpr int kRedLoss = 2 * 256;  // index of the loss in the reduction buffer (the gradient norm follows)
+constexpr float kClip = 1.0f;      // global gradient-norm clip of the training step
 constexpr char kMagic[8] = {'F', 'P', 'U', 'N', 'E', 'T', '0', '1'};
 }  // namespace
 
@@ -364,7 +365,7 @@ int fp_unet_train_step(fp_unet* u, const uint8_t* d_labels, const float* d_rhs, 
     const float b1 = 0.9f, b2 = 0.999f;
     const float bc1 = float(1.0 - std::pow(double(b1), double(u->step)));
     const float bc2 = float(1.0 - std::pow(double(b2), double(u->step)));
-    launch_adam(u->w32, u->m, u->v, u->grad, kParams, lr, b1, b2, 1e-8f, bc1, bc2, u->st);
+    launch_adam(u->w32, u->m, u->v, u->grad, kParams, lr, b1, b2, 1e-8f, bc1, bc2, kClip, u->red, u->scal, u->st);
     launch_weights_bf16(u->w32, u->wf, u->wt, u->st);
     if (loss) {
         cudaMemcpyAsync(u->h_loss, u->red + kRedLoss, sizeof(double), cudaMemcpyDeviceToHost, u->st);

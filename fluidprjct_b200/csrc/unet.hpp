@@ -96,8 +96,10 @@ void launch_output_compact(const int* nf, const int* fidx, Lvl real, Lvl net, co
                            float* x0, cudaStream_t st);
 // Dense right-hand side from the solver's compact one (zero off FLUID cells).
 void launch_rhs_dense(const int* nf, const int* fidx, Lvl real, const float* b, float* dense, cudaStream_t st);
+// Adam on the gradient scaled by min(1, clip / ||g||) (global norm, computed
+// on the device; scal[3] receives the factor, red the norm).
 void launch_adam(float* w, float* m, float* v, const float* g, int64_t n, float lr, float b1, float b2, float eps,
-                 float bc1, float bc2, cudaStream_t st);
+                 float bc1, float bc2, float clip, double* red, float* scal, cudaStream_t st);
 void launch_weights_bf16(const float* w32, bf16* wf, bf16* wt, cudaStream_t st);
 
 // Forward pass of a network made by fp_unet_create on the stream st; leaves

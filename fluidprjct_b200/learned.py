@@ -71,7 +71,7 @@ def generate(n=128, scenes=64, steps_per_scene=64, seed=0, ppc=4, dt=None, tol=1
     return lab, rhs, p
 
 
-def train(data, adam_steps=2000, lr=1e-3, lr_min=1e-5, seed=0, net=None, log=None, log_every=100):
+def train(data, adam_steps=2000, lr=5e-4, lr_min=1e-5, seed=0, net=None, log=None, log_every=100):
     """Adam on the relative pressure loss; returns (net, [(step, loss), ...]).
     The learning rate follows a cosine from lr to lr_min."""
     lab, rhs, p = data
@@ -102,14 +102,14 @@ def eval_loss(net, data, idx):
     return float(np.mean(out))
 
 
-def compare_solvers(labels, rhs, weights, tol=1e-6, dx=None, repeats=3):
+def compare_solvers(labels, rhs, weights, tol=1e-6, dx=None, repeats=3, names=("pcg", "pcg_mg", "pcg_learned")):
     """Solve the same system with the MG-preconditioned PCG from x = 0, with
     the learned initial guess, and with the plain PCG; returns iterations,
     times and residuals of each (device times from fp_step_stats)."""
     D, H, W = labels.shape
     dx = dx if dx is not None else 1.0 / W
     res = {}
-    for name in ("pcg", "pcg_mg", "pcg_learned"):
+    for name in names:
         s = capi.Solver(dim=3, dx=dx, dt=0.002, solver=name, tol=tol, output_format=capi.OUT_NONE)
         s.set_labels(labels)
         if name == "pcg_learned":
@@ -133,7 +133,7 @@ def main(argv=None):
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--steps-per-scene", type=int, default=64)
     ap.add_argument("--adam-steps", type=int, default=2000)
-    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr", type=float, default=5e-4)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--report", default=None, help="JSON summary of the run")

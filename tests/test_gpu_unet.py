@@ -164,3 +164,26 @@ def test_learned_solver_falls_back_to_plain_pcg(trained):
     with pytest.raises(capi.FluidError) as e:
         s2.pressure_solve(rhs)
     assert e.value.code == capi.FP_ERR_STATE
+
+
+def test_committed_weights_gain_on_a_heldout_128_scene(tmp_path):
+    """The committed 128^3 network (fluidprjct_b200/weights) on a FLIP scene
+    outside its training set. Its scaled guess starts the MG-PCG well below
+    the zero-start residual and saves iterations. The same network untrained
+    starts near the zero-start residual."""
+    import os
+    from fluidprjct_b200 import capi, learned
+    assert os.path.exists(learned.DEFAULT_WEIGHTS)
+    held = learned.generate(n=128, scenes=1, steps_per_scene=16, seed=4242)
+    lab = held[0][15].cpu().numpy()
+    rhs = held[1][15].cpu().numpy()
+    r = learned.compare_solvers(lab, rhs, learned.DEFAULT_WEIGHTS, repeats=1)
+    untrained = tmp_path / "untrained.bin"
+    capi.UNet(8, 8, 8, seed=9).save(untrained)
+    r0 = learned.compare_solvers(lab, rhs, str(untrained), repeats=1, names=("pcg_learned",))
+    print(r, r0)
+    for v in list(r.values()) + list(r0.values()):
+        assert v["status"] == 0 and v["residual"] <= 1e-6 and v["fallback"] == 0
+    assert r["pcg_learned"]["guess_relres"] < 0.6
+    assert r0["pcg_learned"]["guess_relres"] > 0.8
+    assert r["pcg_learned"]["iters"] < r["pcg_mg"]["iters"]
