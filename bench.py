@@ -300,9 +300,7 @@ def run_ours(args, rank, local, world):
         for _ in range(k):
             s.set_particles(hpn, hvn)                      # H2D of the step's input state
             s.step(1)
-            p2, v2 = s.particles()                         # D2H of the step's result
-            hpn[:] = p2
-            hvn[:] = v2
+            s.particles(out=(hpn, hvn))                    # D2H of the step's result, the next input
         a1.record(stream)
         a1.synchronize()
         ems = a0.elapsed_time(a1)

@@ -228,10 +228,18 @@ class Solver:
     def num_particles(self):
         return lib().fp_num_particles(self._h)
 
-    def particles(self):
+    def particles(self, out=None):
+        """(pos, vel) as n x 3 float32 in the order given.  out = (pos, vel)
+        reuses caller arrays (pinned host memory makes the copy direct)."""
         n = self.num_particles
-        pos = np.zeros((n, 3), np.float32)
-        vel = np.zeros((n, 3), np.float32)
+        if out is None:
+            pos = np.empty((n, 3), np.float32)
+            vel = np.empty((n, 3), np.float32)
+        else:
+            pos, vel = out
+            for a in (pos, vel):
+                if a.dtype != np.float32 or a.shape != (n, 3) or not a.flags.c_contiguous:
+                    raise ValueError("out arrays must be C-contiguous float32 of shape (n, 3)")
         self._check(lib().fp_get_particles(self._h, ptr(pos), ptr(vel), n))
         return pos, vel
 

@@ -135,7 +135,10 @@ int body_force_partials();
 // -------- particle order helpers --------
 // out[pid] = in[slot] for the xyz part of float4 arrays (pid in pos.w bits).
 void launch_unsort(const float4* pos, const float4* vel, int64_t np, float* pos_out, float* vel_out, cudaStream_t st);
-void launch_pack(const float* pos, const float* vel, int64_t np, float4* pos4, float4* vel4, cudaStream_t st);
+// AoS to float4 (w = original index); the lowest index holding a non-finite
+// value goes to *bad (set to INT_MAX before the call), if bad is not null.
+void launch_pack(const float* pos, const float* vel, int64_t np, float4* pos4, float4* vel4, int* bad,
+                 cudaStream_t st);
 
 // -------- generic CSR CG with FP64 vectors (kernels_pressure.cu) --------
 int csr_cg_solve(int n, const int* offsets, const int* cols, const double* vals, const double* b, double* x, double tol,

@@ -129,12 +129,19 @@ __global__ void k_unsort(const float4* __restrict__ pos, const float4* __restric
     if (vel_out) { const float4 V = vel[q]; vel_out[3 * id] = V.x; vel_out[3 * id + 1] = V.y; vel_out[3 * id + 2] = V.z; }
 }
 
+// AoS (x y z) arrays to float4 pos (w = original index) and vel.  The
+// lowest index of a particle with a non-finite value goes to *bad (the
+// caller sets it to INT_MAX first).
 __global__ void k_pack(const float* __restrict__ pos, const float* __restrict__ vel, int64_t np, float4* __restrict__ p4,
-                       float4* __restrict__ v4) {
+                       float4* __restrict__ v4, int* __restrict__ bad) {
     const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (q >= np) return;
-    p4[q] = make_float4(pos[3 * q], pos[3 * q + 1], pos[3 * q + 2], __int_as_float(int(q)));
-    v4[q] = vel ? make_float4(vel[3 * q], vel[3 * q + 1], vel[3 * q + 2], 0.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 p = make_float4(pos[3 * q], pos[3 * q + 1], pos[3 * q + 2], __int_as_float(int(q)));
+    const float4 v = vel ? make_float4(vel[3 * q], vel[3 * q + 1], vel[3 * q + 2], 0.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    p4[q] = p;
+    v4[q] = v;
+    if (bad && !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z)))
+        atomicMin(bad, int(q));
 }
 
 }  // namespace
@@ -152,9 +159,10 @@ void launch_unsort(const float4* pos, const float4* vel, int64_t np, float* pos_
     k_unsort<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, pos_out, vel_out);
 }
 
-void launch_pack(const float* pos, const float* vel, int64_t np, float4* pos4, float4* vel4, cudaStream_t st) {
+void launch_pack(const float* pos, const float* vel, int64_t np, float4* pos4, float4* vel4, int* bad,
+                 cudaStream_t st) {
     if (np == 0) return;
-    k_pack<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, pos4, vel4);
+    k_pack<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, pos4, vel4, bad);
 }
 
 }  // namespace fp

@@ -127,6 +127,8 @@ struct fp_solver {
     PcgOut* h_out = nullptr;
     double* h_red = nullptr;
     int* h_nf = nullptr;
+    int* d_bad = nullptr;   // first non-finite particle of an upload
+    int* h_bad = nullptr;
     // body
     BodyKin body{};
     HostBody hb;
@@ -683,6 +685,8 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_out, sizeof(PcgOut));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_red, sizeof(double) * 2);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_nf, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_bad, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_bad, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_bforce, sizeof(double) * 6);
     if (e != cudaSuccess) {
         std::fprintf(stderr, "fp_create: %s\n", cudaGetErrorString(e));
@@ -706,6 +710,8 @@ int fp_destroy(fp_solver* s) {
     if (s->h_out) cudaFreeHost(s->h_out);
     if (s->h_red) cudaFreeHost(s->h_red);
     if (s->h_nf) cudaFreeHost(s->h_nf);
+    if (s->h_bad) cudaFreeHost(s->h_bad);
+    if (s->d_bad) cudaFree(s->d_bad);
     if (s->st) cudaStreamDestroy(s->st);
     delete s;
     return FP_OK;
@@ -802,21 +808,28 @@ int fp_set_particles(fp_solver* s, const float* pos, const float* vel, int64_t n
     if (!s || n < 0 || (n > 0 && !pos)) return s ? s->fail(FP_ERR_ARG, "bad particle arrays") : FP_ERR_ARG;
     if (!s->have_grid) return s->fail(FP_ERR_STATE, "labels must be set before particles");
     if (n >= (int64_t(1) << 31)) return s->fail(FP_ERR_ARG, "too many particles");
-    for (int64_t q = 0; q < 3 * n; ++q)
-        if (!std::isfinite(pos[q]) || (vel && !std::isfinite(vel[q])))
-            return s->fail(FP_ERR_ARG, "non-finite particle value at index " + std::to_string(q / 3));
     int rc = alloc_particles(s, n);
     if (rc) return rc;
+    s->sorted = false;
     if (n == 0) return FP_OK;
     float* dpos = s->d_io;
     float* dvel = s->d_io + 3 * n;
     cudaError_t e = cudaMemcpyAsync(dpos, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->st);
     if (e == cudaSuccess && vel) e = cudaMemcpyAsync(dvel, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_bad, 0x7F, sizeof(int), s->st);  // 0x7F7F7F7F > any index
     if (e != cudaSuccess) return s->cuda_fail(e, "particle upload");
-    launch_pack(dpos, vel ? dvel : nullptr, n, s->d_pos, s->d_vel, s->st);
-    e = cudaStreamSynchronize(s->st);
+    // pack into the second buffer and check every value on the device
+    launch_pack(dpos, vel ? dvel : nullptr, n, s->d_pos2, s->d_vel2, s->d_bad, s->st);
+    s->launches += 1;
+    e = cudaMemcpyAsync(s->h_bad, s->d_bad, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
     if (e != cudaSuccess) return s->cuda_fail(e, "particle upload");
-    s->sorted = false;
+    if (*s->h_bad < n) {
+        s->np = 0;
+        return s->fail(FP_ERR_ARG, "non-finite particle value at index " + std::to_string(*s->h_bad));
+    }
+    std::swap(s->d_pos, s->d_pos2);
+    std::swap(s->d_vel, s->d_vel2);
     return FP_OK;
 }
 

@@ -127,6 +127,39 @@ def compare_solvers(labels, rhs, weights, tol=1e-6, dx=None, repeats=3, names=("
     return res
 
 
+def time_network(n=128, reps=10):
+    """Device time (ms) of one forward pass and one training step of the
+    network on an n^3 dam-break-like input, from CUDA events on its stream."""
+    torch = _torch()
+    net = capi.UNet(n, n, n, train=True, seed=0)
+    dev = torch.device("cuda")
+    lab = torch.ones((n, n, n), dtype=torch.uint8, device=dev)
+    lab[0] = 0
+    lab[:, :2] = 0
+    lab[:, -max(2, n // 12):] = 2
+    gen = torch.Generator(device=dev).manual_seed(0)
+    rhs = torch.randn((n, n, n), device=dev, generator=gen) * (lab == 1)
+    p = torch.randn((n, n, n), device=dev, generator=gen) * (lab == 1)
+    x = torch.zeros_like(rhs)
+    torch.cuda.synchronize()
+    st = torch.cuda.ExternalStream(net.stream)
+    out = {}
+    for name, fn in (("forward_ms", lambda: net.forward(lab.data_ptr(), rhs.data_ptr(), x.data_ptr())),
+                     ("train_step_ms", lambda: net.train_step(lab.data_ptr(), rhs.data_ptr(), p.data_ptr(), 1e-4))):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps
+    net.close()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--n", type=int, default=128)
@@ -137,7 +170,12 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--report", default=None, help="JSON summary of the run")
+    ap.add_argument("--time", action="store_true", help="only time the network's forward pass and training step")
+    ap.add_argument("--reps", type=int, default=10)
     a = ap.parse_args(argv)
+    if a.time:
+        print(json.dumps({"n": a.n, **time_network(a.n, a.reps)}))
+        return
     log = lambda m: print(m, flush=True)
     t0 = time.time()
     data = generate(a.n, a.scenes, a.steps_per_scene, a.seed, log=log)

@@ -153,7 +153,9 @@ int fp_get_dims(const fp_solver* s, int* W, int* H, int* D);
 int fp_load_sdf(fp_solver* s, const char* path);
 
 /* Particles: seeding of FLUID cells (seedParticles, FluidSolver3D.cu:213-297)
- * with a deterministic mt19937(seed); caller arrays; PLY files. */
+ * with a deterministic mt19937(seed); caller arrays; PLY files.  A
+ * non-finite position or velocity is rejected with FP_ERR_ARG (checked on
+ * the device); the solver then holds no particles. */
 int fp_seed_particles(fp_solver* s, int ppc, uint32_t seed);
 int fp_set_particles(fp_solver* s, const float* pos, const float* vel, int64_t n);
 int fp_load_ply(fp_solver* s, const char* path);
