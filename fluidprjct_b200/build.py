@@ -26,6 +26,7 @@ SOURCES = [
     "kernels_body.cu",
     "kernels_mg.cu",
     "kernels_unet.cu",
+    "kernels_unet_tc.cu",
     "unet.cu",
     "solver.cu",
     "noalloc.cu",

@@ -616,6 +616,7 @@ int run_conv(const ConvArgs& a, cudaStream_t st) {
     auto kern = k_conv3<CA, CB, COUT, NCO, EPI>;
     if (per_sm < 0) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
         if (per_sm < 1) per_sm = 1;
     }
@@ -634,6 +635,7 @@ int run_corr(const CorrArgs& a, int nblk, cudaStream_t st) {
     auto kern = k_corr3<CA, CB, COUT, TPC>;
     if (!init) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         init = true;
     }
     kern<<<dim3(nblk, 27 / TPC), THREADS, smem, st>>>(a);

@@ -404,8 +404,11 @@ int solve_system(fp_solver* s, float* p_out) {
             cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
             return cudaStreamSynchronize(s->st);
         };
+        if (learned)
+            cudaMemcpyAsync(s->h_bad, unet::net_status(s->net), sizeof(int), cudaMemcpyDeviceToHost, s->st);
         ce = finish(!mg);
         if (ce != cudaSuccess) return s->cuda_fail(ce, "pressure solve");
+        if (learned && *s->h_bad) return s->fail(FP_ERR_TIMEOUT, "U-Net forward: a bounded tensor-core wait gave up");
         inner_total = s->h_out->iters;
         dev_status = s->h_out->status;
         outer = 1;

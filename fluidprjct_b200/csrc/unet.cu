@@ -35,6 +35,8 @@ struct fp_unet {
     bf16 *wf = nullptr, *wt = nullptr;
     double* red = nullptr;
     float* scal = nullptr;  // s, 1/s, 2/sum(t^2)
+    int* d_status = nullptr;  // nonzero once a bounded wait in a convolution gave up
+    int* h_status = nullptr;
     double* h_loss = nullptr;
     // forward
     bf16 *X0, *a0, *e0, *q0, *a1, *e1, *q1, *a2, *e2, *d1a, *d1, *d0a, *d0;
@@ -72,6 +74,7 @@ namespace unet {
 Lvl net_level0(const fp_unet* u) { return u->L[0]; }
 const float* net_out(const fp_unet* u) { return u->out; }
 const float* net_scal(const fp_unet* u) { return u->scal; }
+const int* net_status(const fp_unet* u) { return u->d_status; }
 
 static int conv_fwd(fp_unet* u, int l, const bf16* xa, const bf16* xb, bf16* y, cudaStream_t st) {
     ConvArgs a{};
@@ -83,7 +86,8 @@ static int conv_fwd(fp_unet* u, int l, const bf16* xa, const bf16* xb, bf16* y, 
     a.lc = kSpec[l].level < 2 ? u->L[kSpec[l].level + 1] : a.lv;
     a.head_w = u->w32 + layer_offset(kLayers);
     a.head_out = u->out;
-    return conv_forward_layer(l, a, st);
+    a.status = u->d_status;
+    return conv_forward_layer_tc(l, a, st);
 }
 
 // Forward pass: u->out (net level 0) and u->scal (s, 1/s).
@@ -113,6 +117,14 @@ int forward_kernel_count() { return 2 + 10 + 2; }
 
 namespace {
 
+// Reads the device status after the stream is synchronised.
+int device_status(fp_unet* u, const char* what) {
+    if (cudaMemcpy(u->h_status, u->d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return u->cuda_check(what);
+    if (*u->h_status) return u->fail(FP_ERR_TIMEOUT, std::string(what) + ": a bounded tensor-core wait gave up");
+    return FP_OK;
+}
+
 int conv_bwd(fp_unet* u, int l, const bf16* g, const bf16* mask, bf16* y, cudaStream_t st) {
     ConvArgs a{};
     a.xb = g;
@@ -121,7 +133,8 @@ int conv_bwd(fp_unet* u, int l, const bf16* g, const bf16* mask, bf16* y, cudaSt
     a.mask = mask;
     a.lv = u->L[kSpec[l].level];
     a.lc = a.lv;
-    return conv_backward_layer(l, a, st);
+    a.status = u->d_status;
+    return conv_backward_layer_tc(l, a, st);
 }
 
 int wgrad(fp_unet* u, int l, const bf16* xa, const bf16* xb, const bf16* g, cudaStream_t st) {
@@ -221,6 +234,7 @@ int fp_unet_create(int W, int H, int D, int train, uint64_t seed, fp_unet** out)
     u->wt = u->alloc<bf16>(kParams);
     u->red = u->alloc<double>(1024);
     u->scal = u->alloc<float>(4);
+    u->d_status = u->alloc<int>(1);
     u->X0 = u->alloc<bf16>(n0 * 16);
     u->a0 = u->alloc<bf16>(n0 * 16);
     u->e0 = u->alloc<bf16>(n0 * 16);
@@ -261,6 +275,8 @@ int fp_unet_create(int W, int H, int D, int train, uint64_t seed, fp_unet** out)
         u->hpart = u->alloc<float>(int64_t(u->hblk) * kHead);
     }
     if (cudaMallocHost(&u->h_loss, sizeof(double)) != cudaSuccess) u->alloc_failed = true;
+    if (cudaMallocHost(&u->h_status, sizeof(int)) != cudaSuccess) u->alloc_failed = true;
+    if (!u->alloc_failed && cudaMemsetAsync(u->d_status, 0, sizeof(int), u->st) != cudaSuccess) u->alloc_failed = true;
     if (u->alloc_failed) {
         fp_unet_destroy(u);
         return FP_ERR_CUDA;
@@ -280,6 +296,7 @@ void fp_unet_destroy(fp_unet* u) {
     if (u->st) cudaStreamSynchronize(u->st);
     for (void* p : u->allocs) cudaFree(p);
     if (u->h_loss) cudaFreeHost(u->h_loss);
+    if (u->h_status) cudaFreeHost(u->h_status);
     if (u->st) cudaStreamDestroy(u->st);
     delete u;
 }
@@ -337,7 +354,8 @@ int fp_unet_forward(fp_unet* u, const uint8_t* d_labels, const float* d_rhs, flo
     if (forward_on(u, d_labels, d_rhs, u->st)) return u->cuda_check("U-Net forward");
     launch_output_dense(d_labels, u->real, u->L[0], u->out, u->scal, d_x, u->st);
     if (cudaStreamSynchronize(u->st) != cudaSuccess) return u->cuda_check("U-Net forward");
-    return u->cuda_check("U-Net forward");
+    if (int rc = u->cuda_check("U-Net forward")) return rc;
+    return device_status(u, "U-Net forward");
 }
 
 int fp_unet_loss_grad(fp_unet* u, const uint8_t* d_labels, const float* d_rhs, const float* d_p, double* loss,
@@ -351,7 +369,8 @@ int fp_unet_loss_grad(fp_unet* u, const uint8_t* d_labels, const float* d_rhs, c
     if (grad) cudaMemcpyAsync(grad, u->grad, sizeof(float) * size_t(kParams), cudaMemcpyDeviceToHost, u->st);
     if (cudaStreamSynchronize(u->st) != cudaSuccess) return u->cuda_check("U-Net backward");
     if (loss) *loss = *u->h_loss;
-    return u->cuda_check("U-Net backward");
+    if (int rc = u->cuda_check("U-Net backward")) return rc;
+    return device_status(u, "U-Net backward");
 }
 
 int fp_unet_train_step(fp_unet* u, const uint8_t* d_labels, const float* d_rhs, const float* d_p, float lr,
@@ -371,6 +390,7 @@ int fp_unet_train_step(fp_unet* u, const uint8_t* d_labels, const float* d_rhs, 
         cudaMemcpyAsync(u->h_loss, u->red + kRedLoss, sizeof(double), cudaMemcpyDeviceToHost, u->st);
         if (cudaStreamSynchronize(u->st) != cudaSuccess) return u->cuda_check("U-Net training step");
         *loss = *u->h_loss;
+        if (int rc = device_status(u, "U-Net training step")) return rc;
     }
     return u->cuda_check("U-Net training step");
 }

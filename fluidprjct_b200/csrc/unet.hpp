@@ -55,6 +55,7 @@ struct ConvArgs {
     const float* head_w;   // EPI_HEAD: 16 head weights
     float* head_out;       // EPI_HEAD: one FP32 value per voxel
     Lvl lv, lc;            // this level, the coarse level of xa
+    int* status;           // set to nonzero if a bounded device wait gave up
 };
 
 // Arguments of the weight-gradient kernel: dw[t][co][ci] = sum_v g[v][co] x[v + off(t)][ci].
@@ -71,6 +72,9 @@ enum { EPI_RELU = 0, EPI_MASK = 1, EPI_RAW = 2, EPI_HEAD = 3 };
 // Launchers (kernels_unet.cu).  Each returns 0 or a cudaError_t value.
 int conv_forward_layer(int layer, const ConvArgs& a, cudaStream_t st);   // EPI_RELU, or EPI_HEAD for L9
 int conv_backward_layer(int layer, const ConvArgs& a, cudaStream_t st);  // data gradient of layer (1..9)
+// The same convolutions on tcgen05 (kernels_unet_tc.cu).
+int conv_forward_layer_tc(int layer, const ConvArgs& a, cudaStream_t st);
+int conv_backward_layer_tc(int layer, const ConvArgs& a, cudaStream_t st);
 int corr_layer(int layer, const CorrArgs& a, int nblk, cudaStream_t st);
 int corr_blocks(int layer, const Lvl& lv);                               // gridDim.x for corr_layer
 void reduce_partials(const float* part, int nblk, int64_t n, float* out, cudaStream_t st);
@@ -108,6 +112,7 @@ int forward_on(fp_unet* u, const uint8_t* labels, const float* rhs, cudaStream_t
 Lvl net_level0(const fp_unet* u);
 const float* net_out(const fp_unet* u);
 const float* net_scal(const fp_unet* u);
+const int* net_status(const fp_unet* u);  // device word, nonzero after a timed-out wait
 
 }  // namespace unet
 }  // namespace fp
