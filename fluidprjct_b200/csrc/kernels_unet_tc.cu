@@ -4,21 +4,22 @@
 //
 // One persistent CTA of 128 threads walks output bricks of 8x16x2 voxels.
 // A brick is two M = 128 tiles, one per z slice: row m of a tile is the voxel
-// (x = m % 8, y = m / 8).  Per brick:
-//   1. all threads stage the zero-padded input halo (10x18x4 voxels, every
-//      input channel) in shared memory with cp.async.  The layout is
+// (x = m % 8, y = m / 8).  Per brick and 16-channel input group:
+//   1. all threads stage that group of the zero-padded input halo (10x18x4
+//      voxels) in one of two shared-memory stages with cp.async.  The layout is
 //      chunk-major ([8-channel chunk][halo voxel][8 channels]), the K-major
 //      no-swizzle UMMA layout: any 8 consecutive voxels of a halo row form one
 //      8x16-byte core matrix.  The operand of tap (dz, dy, dx) is then the
 //      same layout shifted by that tap's halo offset: core matrices of
 //      successive y rows lie 160 bytes apart (SBO), the two K halves of a
 //      16-channel step one chunk plane apart (LBO).
-//   2. one thread issues 27 taps x CIN/16 MMAs per tile (M = 128, N = NCO,
-//      K = 16) into the tile's TMEM columns, then commits them to an
-//      mbarrier.
-//   3. after the mbarrier completes, each warp reads its 32 TMEM lanes
+//   2. one thread issues the group's 27 tap MMAs per tile (M = 128, N = NCO,
+//      K = 16) into the brick's TMEM accumulator set, then commits them to
+//      the stage's mbarrier; loading the next group overlaps these MMAs.
+//   3. once the brick's last commit has arrived, each warp reads its 32 TMEM lanes
 //      (tcgen05.ld 32x32b): every thread then holds one voxel's NCO outputs
-//      and writes them as contiguous 16-byte vectors.
+//      and writes them as contiguous 16-byte vectors.  Two accumulator sets
+//      let this epilogue overlap the next brick's MMAs.
 // The CTA's output-channel group of the weights ([tap][chunk][co][8], the
 // K-major layout of B) is loaded once and stays resident.  The waits are
 // bounded: a wait that gives up sets *status, waits again (bounded) for the
@@ -84,6 +85,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity
     return false;
 }
 
+// Thread 0 alone polls the barrier (bounded); the other warps wait at the
+// block barrier, which costs them no issue slots.  Every thread returns the
+// same verdict.
+__device__ __forceinline__ bool block_wait(uint32_t mbar, uint32_t parity) {
+    int got = 1;
+    if (threadIdx.x == 0) got = mbar_wait_bounded(mbar, parity) ? 1 : 0;
+    return __syncthreads_and(got) != 0;
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     uint32_t r[16];
     asm volatile(
@@ -95,35 +105,46 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Two accumulator sets (one per brick in flight), each two tiles of NCO columns.
 template <int NCO>
 constexpr int tmem_cols() {
-    return (2 * NCO <= 32) ? 32 : (2 * NCO <= 64) ? 64 : (2 * NCO <= 128) ? 128 : 256;
+    return (4 * NCO <= 32) ? 32 : (4 * NCO <= 64) ? 64 : (4 * NCO <= 128) ? 128 : 256;
 }
 
-template <int CA, int CB, int COUT, int NCO>
+constexpr int STAGE_BYTES = HVOX * 2 * 16;  // one 16-channel K group of the halo: 23,040 bytes
+
+template <int CA, int CB, int COUT, int NCO, int NST>
 constexpr size_t tc_smem_bytes() {
-    // halo + weights + mbarrier/TMEM slot + alignment slack
-    return size_t(HVOX) * (CA + CB) * 2 + size_t(27) * (CA + CB) * NCO * 2 + 16 + 128;
+    // NST halo stages + resident weights + five mbarriers and the TMEM slot + alignment slack
+    return size_t(NST) * STAGE_BYTES + size_t(27) * (CA + CB) * NCO * 2 + 48 + 128;
 }
 
-template <int CA, int CB, int COUT, int NCO, int EPI>
+// Pipeline of one CTA: the steps are (brick i, 16-channel group g) in order.
+// Step s loads its group's halo into stage s % NST; with two stages that load
+// overlaps the MMAs of step s - 1.  A stage is reused once the MMAs that read
+// it have completed (commit to that stage's mbarrier).  One stage keeps the
+// footprint small, so that more CTAs share an SM and overlap each other.  Brick i accumulates into TMEM set i & 1; its
+// epilogue runs after the first MMAs of brick i + 1 are issued, once the
+// commit after its last group has arrived on that set's mbarrier.
+template <int CA, int CB, int COUT, int NCO, int EPI, int NST>
 __global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(ConvArgs a) {
     constexpr int CIN = CA + CB;
-    constexpr int CH = CIN / 8;
+    constexpr int G = CIN / 16;  // K groups per brick
     constexpr int NCOLS = tmem_cols<NCO>();
     constexpr uint32_t IDESC = umma_idesc_bf16(NCO);
     static_assert(CIN % 16 == 0 && NCO % 16 == 0 && NCO <= 48 && COUT % NCO == 0, "channel tiling");
     static_assert(EPI != EPI_HEAD || (NCO == 16 && COUT == 16), "the head needs all 16 channels");
+    static_assert(NST == 1 || NST == 2, "one or two halo stages");
     extern __shared__ unsigned char smem_raw[];
-    // 128-byte aligned operand area: halo, then weights, then the barrier word
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 127u) & ~127u;
     unsigned char* sbase = smem_raw + (base - raw);
-    const uint32_t sA = base;
-    const uint32_t sB = sA + uint32_t(HVOX * CH * 16);
-    unsigned long long* mbar_p = reinterpret_cast<unsigned long long*>(sbase + HVOX * CH * 16 + 27 * CH * NCO * 16);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar_p + 1);
-    const uint32_t mbar = smem_u32(mbar_p);
+    const uint32_t sStage = base;                            // NST x [2 chunks][HVOX][8 channels]
+    const uint32_t sB = base + uint32_t(NST * STAGE_BYTES);  // [tap][chunk][co][8]
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(sbase + NST * STAGE_BYTES + 27 * CIN * NCO * 2);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 5);
+    // barriers (8 bytes apart): stage 0, stage 1, accumulator set 0, set 1, spare
+    const uint32_t bar_stage0 = smem_u32(bars), bar_acc0 = smem_u32(bars + 2), bar_spare = smem_u32(bars + 4);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int cog = blockIdx.y;
 
@@ -133,13 +154,12 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(ConvArgs a) {
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar));
+        for (int b = 0; b < 5; ++b) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_stage0 + 8u * b));
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    // weights of this output-channel group: [tap][chunk][co][8]
-    for (int i = tid; i < 27 * NCO * CH; i += TC_THREADS) {
-        const int co = i % NCO, c = (i / NCO) % CH, tap = i / (NCO * CH);
-        cp_async16(sB + uint32_t(((tap * CH + c) * NCO + co) * 16),
+    for (int i = tid; i < 27 * NCO * (CIN / 8); i += TC_THREADS) {
+        const int co = i % NCO, c = (i / NCO) % (CIN / 8), tap = i / (NCO * (CIN / 8));
+        cp_async16(sB + uint32_t(((tap * (CIN / 8) + c) * NCO + co) * 16),
                    a.w + (int64_t(tap) * COUT + cog * NCO + co) * CIN + c * 8, true);
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -149,65 +169,19 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(ConvArgs a) {
 
     const int nbx = (a.lv.W + TX - 1) / TX, nby = (a.lv.H + TY - 1) / TY, nbz = (a.lv.D + TZ - 1) / TZ;
     const int nbricks = nbx * nby * nbz;
-    uint32_t phase = 0;
-    bool ok = true;
-    for (int brick = blockIdx.x; brick < nbricks && ok; brick += gridDim.x) {
+    const int mine = int(blockIdx.x) < nbricks ? (nbricks - 1 - int(blockIdx.x)) / int(gridDim.x) + 1 : 0;
+
+    // epilogue of this CTA's brick i (TMEM set i & 1)
+    auto epilogue = [&](int i) {
+        const int brick = int(blockIdx.x) + i * int(gridDim.x);
         const int bx = brick % nbx, by = (brick / nbx) % nby, bz = brick / (nbx * nby);
-        const int x0 = bx * TX - 1, y0 = by * TY - 1, z0 = bz * TZ - 1;
-        // 1. halo, voxel-fastest so the shared-memory writes are contiguous
-        for (int i = tid; i < HVOX * CH; i += TC_THREADS) {
-            const int hv = i % HVOX, c = i / HVOX;
-            const int gx = x0 + hv % HX, gy = y0 + (hv / HX) % HY, gz = z0 + hv / (HX * HY);
-            const bool in = gx >= 0 && gx < a.lv.W && gy >= 0 && gy < a.lv.H && gz >= 0 && gz < a.lv.D;
-            const bf16* src;
-            if (CA > 0 && c * 8 < CA)
-                src = in ? a.xa + ((int64_t(gz >> 1) * a.lc.H + (gy >> 1)) * a.lc.W + (gx >> 1)) * CA + c * 8 : a.xa;
-            else
-                src = in ? a.xb + ((int64_t(gz) * a.lv.H + gy) * a.lv.W + gx) * CB + (c * 8 - CA) : a.xb;
-            cp_async16(sA + uint32_t((c * HVOX + hv) * 16), src, in);
-        }
-        asm volatile("cp.async.wait_all;\n" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // generic-proxy writes -> tensor core
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        // 2. one thread issues the MMAs of both tiles
-        if (tid == 0) {
-#pragma unroll 1
-            for (int zo = 0; zo < TZ; ++zo) {
-#pragma unroll 1
-                for (int tap = 0; tap < 27; ++tap) {
-                    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-                    const int hv0 = ((zo + 1 + dz) * HY + (1 + dy)) * HX + (1 + dx);
-#pragma unroll
-                    for (int kc = 0; kc < CIN / 16; ++kc) {
-                        const uint64_t ad = umma_desc(sA + uint32_t((2 * kc * HVOX + hv0) * 16), HVOX * 16, HX * 16);
-                        const uint64_t bd = umma_desc(sB + uint32_t((tap * CH + 2 * kc) * NCO * 16), NCO * 16, 128);
-                        umma_bf16(tmem + uint32_t(zo * NCO), ad, bd, IDESC, (tap | kc) != 0 ? 1u : 0u);
-                    }
-                }
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar)
-                         : "memory");
-        }
-        // 3. wait for the MMAs (every thread observes the barrier; the block
-        // agrees on the outcome), then the epilogue from TMEM
-        const bool got = mbar_wait_bounded(mbar, phase);
-        if (!__syncthreads_and(got ? 1 : 0)) {
-            if (tid == 0) {
-                if (a.status) atomicExch(a.status, DEV_TIMEOUT_CODE);
-                mbar_wait_bounded(mbar, phase);  // one more bounded wait for this CTA's own MMAs
-            }
-            ok = false;
-            break;
-        }
-        phase ^= 1u;
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t set = uint32_t(i & 1) * uint32_t(2 * NCO);
 #pragma unroll 1
         for (int zo = 0; zo < TZ; ++zo) {
             float v[NCO];
 #pragma unroll
             for (int j = 0; j < NCO / 16; ++j)
-                tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(zo * NCO + 16 * j), v + 16 * j);
+                tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + set + uint32_t(zo * NCO + 16 * j), v + 16 * j);
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
             const int m = warp * 32 + lane;
             const int gx = bx * TX + (m & 7), gy = by * TY + (m >> 3), gz = bz * TZ + zo;
@@ -215,7 +189,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(ConvArgs a) {
             const int64_t vox = (int64_t(gz) * a.lv.H + gy) * a.lv.W + gx;
             if (EPI == EPI_RELU || EPI == EPI_HEAD) {
 #pragma unroll
-                for (int i = 0; i < NCO; ++i) v[i] = fmaxf(v[i], 0.0f);
+                for (int q = 0; q < NCO; ++q) v[q] = fmaxf(v[q], 0.0f);
             }
             if (EPI == EPI_MASK) {
 #pragma unroll
@@ -247,9 +221,87 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(ConvArgs a) {
             }
             if (EPI == EPI_HEAD) a.head_out[vox] = hsum;
         }
-        // every thread's TMEM reads and shared-memory use end before the next brick
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    };
+
+    bool ok = true;
+    const int steps = mine * G;
+    for (int s = 0; s < steps && ok; ++s) {
+        const int i = s / G, g = s % G;
+        const int brick = int(blockIdx.x) + i * int(gridDim.x);
+        const int bx = brick % nbx, by = (brick / nbx) % nby, bz = brick / (nbx * nby);
+        const int sl = s % NST, use = s / NST;  // stage slot, and how often it has been filled before
+        const uint32_t stage = sStage + uint32_t(sl * STAGE_BYTES);
+        // the stage's previous MMAs (step s - NST) must be done before it is overwritten
+        if (use >= 1 && !block_wait(bar_stage0 + 8u * uint32_t(sl), uint32_t((use - 1) & 1))) {
+            ok = false;
+            break;
+        }
+        // channels [16 g, 16 g + 16) of the halo, voxel-fastest
+        const int x0 = bx * TX - 1, y0 = by * TY - 1, z0 = bz * TZ - 1;
+        for (int t = tid; t < HVOX * 2; t += TC_THREADS) {
+            const int hv = t % HVOX, cl = t / HVOX;
+            const int c = 2 * g + cl;  // 8-channel chunk of the full input
+            const int gx = x0 + hv % HX, gy = y0 + (hv / HX) % HY, gz = z0 + hv / (HX * HY);
+            const bool in = gx >= 0 && gx < a.lv.W && gy >= 0 && gy < a.lv.H && gz >= 0 && gz < a.lv.D;
+            const bf16* src;
+            if (CA > 0 && c * 8 < CA)
+                src = in ? a.xa + ((int64_t(gz >> 1) * a.lc.H + (gy >> 1)) * a.lc.W + (gx >> 1)) * CA + c * 8 : a.xa;
+            else
+                src = in ? a.xb + ((int64_t(gz) * a.lv.H + gy) * a.lv.W + gx) * CB + (c * 8 - CA) : a.xb;
+            cp_async16(stage + uint32_t((cl * HVOX + hv) * 16), src, in);
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // generic-proxy writes -> tensor core
         __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        if (tid == 0) {
+            const uint32_t set = uint32_t(i & 1) * uint32_t(2 * NCO);
+#pragma unroll 1
+            for (int zo = 0; zo < TZ; ++zo) {
+#pragma unroll 1
+                for (int tap = 0; tap < 27; ++tap) {
+                    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+                    const int hv0 = ((zo + 1 + dz) * HY + (1 + dy)) * HX + (1 + dx);
+                    const uint64_t ad = umma_desc(stage + uint32_t(hv0 * 16), HVOX * 16, HX * 16);
+                    const uint64_t bd = umma_desc(sB + uint32_t((tap * (CIN / 8) + 2 * g) * NCO * 16), NCO * 16, 128);
+                    umma_bf16(tmem + set + uint32_t(zo * NCO), ad, bd, IDESC, (g | tap) != 0 ? 1u : 0u);
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             bar_stage0 + 8u * uint32_t(sl))
+                         : "memory");
+            if (g == G - 1)
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                                 bar_acc0 + 8u * uint32_t(i & 1))
+                             : "memory");
+        }
+        // the previous brick's epilogue overlaps this brick's first MMAs
+        if (g == 0 && i >= 1) {
+            if (!block_wait(bar_acc0 + 8u * uint32_t((i - 1) & 1), uint32_t(((i - 1) >> 1) & 1))) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            epilogue(i - 1);
+        }
+    }
+    if (ok && mine > 0) {
+        const int i = mine - 1;
+        if (block_wait(bar_acc0 + 8u * uint32_t(i & 1), uint32_t((i >> 1) & 1))) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            epilogue(i);
+        } else {
+            ok = false;
+        }
+    }
+    if (!ok && tid == 0) {
+        if (a.status) atomicExch(a.status, DEV_TIMEOUT_CODE);
+        // one more bounded wait for this CTA's own MMAs: a final commit arrives
+        // on the spare barrier once every MMA issued so far has completed
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar_spare)
+                     : "memory");
+        mbar_wait_bounded(bar_spare, 0u);
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
@@ -259,12 +311,12 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(ConvArgs a) {
 
 int g_tc_sms = 0;
 
-template <int CA, int CB, int COUT, int NCO, int EPI>
+template <int CA, int CB, int COUT, int NCO, int EPI, int NST = 1>
 int run_conv_tc(const ConvArgs& a, cudaStream_t st) {
-    constexpr size_t smem = tc_smem_bytes<CA, CB, COUT, NCO>();
+    constexpr size_t smem = tc_smem_bytes<CA, CB, COUT, NCO, NST>();
     static_assert(smem <= 232448, "shared memory of one CTA");
     static int per_sm = -1;
-    auto kern = k_conv3_tc<CA, CB, COUT, NCO, EPI>;
+    auto kern = k_conv3_tc<CA, CB, COUT, NCO, EPI, NST>;
     if (per_sm < 0) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         // all of the SM's unified memory as shared memory, so that several
