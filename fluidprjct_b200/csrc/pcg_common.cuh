@@ -12,11 +12,11 @@ namespace {
 // Grid barrier for a cooperative launch on one 32-bit word: every block adds
 // 1 except block 0, which adds 2^31 - (nblocks - 1), so the word's top bit
 // flips exactly when the last block arrives and no reset is needed between
-// barriers.  The wait is bounded: after ~2^28 polls the block records
+// barriers.  The wait is bounded: after 2^27 polls the block records
 // DEV_TIMEOUT and leaves; callers check the status after every barrier and
-// return, so no block waits forever.  The fences around the arrival give the
-// barrier release/acquire semantics, so plain (L1-cached) loads after it see
-// every write made before it by any block.
+// return, so no block waits forever.  The arrival is a release atomic and the
+// poll an acquire load (the pattern of a release-acquire grid barrier), so
+// plain loads after it see every write made before it by any block.
 __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* status) {
     __shared__ int s_ok;
     __syncthreads();
@@ -26,19 +26,27 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int
         // this or the next barrier, and every wait below is bounded.
         const int st0 = *(volatile int*)status;
         const unsigned inc = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
-        __threadfence();
-        const unsigned old = atomicAdd(&bar->count, inc);
-        volatile unsigned* vc = &bar->count;
+        // arrival with release semantics: after the block barrier above it
+        // publishes every write this block made before the grid barrier
+        unsigned old;
+        asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;\n"
+                     : "=r"(old)
+                     : "l"(&bar->count), "r"(inc)
+                     : "memory");
         long long polls = 0;
         bool ok = st0 == DEV_OK;
-        while (((old ^ *vc) & 0x80000000u) == 0u) {
+        for (;;) {
+            // acquire load: writes published by the other blocks' arrivals are
+            // visible to this block once the top bit has flipped
+            unsigned cur;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(cur) : "l"(&bar->count) : "memory");
+            if (((old ^ cur) & 0x80000000u) != 0u) break;
             if (++polls > (1ll << 27)) {
                 atomicExch(status, DEV_TIMEOUT);
                 ok = false;
                 break;
             }
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
