@@ -98,20 +98,6 @@ __device__ __forceinline__ void load_cells(Cells<N>& k, const int* fidx, const u
         k.db[u] = k.ok[u] ? dg[n] : 0;
     }
 }
-__device__ void op0_first_red(const MgLevel& L, const int* fidx, const uint8_t* dg, int nf, int t0, int stride) {
-    for (int base = t0; base < nf; base += UNR * stride) {
-        Cells<> k;
-        load_cells(k, fidx, dg, nf, base, stride, 1 + L.sy + L.sz);
-        float b[UNR];
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) b[u] = L.b[k.c[u]];
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            const int d = k.db[u] & 0x7F;
-            if (k.ok[u]) L.x[k.c[u]] = ((k.db[u] >> 7) == 0 && d > 0) ? b[u] / float(d) : 0.0f;
-        }
-    }
-}
 __device__ void op0_sweep(const MgLevel& L, const int* fidx, const uint8_t* dg, int nf, int color, int t0, int stride) {
     for (int base = t0; base < nf; base += UNR * stride) {
         Cells<> k;
@@ -126,31 +112,7 @@ __device__ void op0_sweep(const MgLevel& L, const int* fidx, const uint8_t* dg, 
         }
     }
 }
-__device__ void op0_prolong(const MgLevel& F, const MgLevel& Cl, float omega, const int* fidx, int nf, int t0,
-                            int stride) {
-    for (int n = t0; n < nf; n += stride) {
-        const int c = fidx[n];
-        const int i = c % F.sy - 1, j = (c / F.sy) % (F.H + 2) - 1, k = c / F.sz - 1;
-        const int cc = (i / 2 + 1) + (j / 2 + 1) * Cl.sy + (k / 2 + 1) * Cl.sz;
-        if (Cl.lab[cc] == FLUID) F.x[c] += omega * Cl.x[cc];
-    }
-}
-
 // ---- level operations over a (t0, stride) share of the work ----
-// First sweep of a cycle: x = b/d on red FLUID cells, 0 everywhere else.
-__device__ void op_first_red(const MgLevel& L, int t0, int stride) {
-    const int n = L.W * L.H * L.D;
-    for (int t = t0; t < n; t += stride) {
-        int i, j, k;
-        const int c = lv_cell(L, t, i, j, k);
-        float v = 0.0f;
-        if (L.lab[c] == FLUID && ((i + j + k) & 1) == 0) {
-            const int d = lv_diag(L, c);
-            v = d > 0 ? L.b[c] / float(d) : 0.0f;
-        }
-        L.x[c] = v;
-    }
-}
 // Gauss-Seidel update of the FLUID cells of one colour.
 __device__ void op_sweep(const MgLevel& L, int color, int t0, int stride) {
     const int n = L.W * L.H * L.D;
@@ -162,13 +124,15 @@ __device__ void op_sweep(const MgLevel& L, int color, int t0, int stride) {
         L.x[c] = d > 0 ? (L.b[c] + lv_nbsum(L, c)) / float(d) : 0.0f;
     }
 }
-// b_coarse = scale * sum over FLUID children of (b - A x).
-__device__ void op_restrict(const MgLevel& F, const MgLevel& Cl, float scale, int t0, int stride) {
+// Restriction to the next level fused with that level's first sweep:
+// b_coarse = scale * sum over the red FLUID children of (b - A x), then
+// x_coarse = b/d on red FLUID cells, 0 elsewhere.
+__device__ void op_restrict_first(const MgLevel& F, const MgLevel& Cl, float scale, int t0, int stride) {
     const int n = Cl.W * Cl.H * Cl.D;
     for (int t = t0; t < n; t += stride) {
         int I, J, K;
         const int cc = lv_cell(Cl, t, I, J, K);
-        float s = 0.0f;
+        float s = 0.0f, xv = 0.0f;
         if (Cl.lab[cc] == FLUID) {
             for (int c3 = 0; c3 < 2; ++c3)
                 for (int b3 = 0; b3 < 2; ++b3)
@@ -182,32 +146,54 @@ __device__ void op_restrict(const MgLevel& F, const MgLevel& Cl, float scale, in
                         s += F.b[c] - (float(lv_diag(F, c)) * F.x[c] - lv_nbsum(F, c));
                     }
             s *= scale;
+            if (((I + J + K) & 1) == 0) {
+                const int d = lv_diag(Cl, cc);
+                xv = d > 0 ? s / float(d) : 0.0f;
+            }
         }
         Cl.b[cc] = s;
+        Cl.x[cc] = xv;
     }
 }
-// x_fine += omega * x_coarse(parent) on FLUID cells with a FLUID parent.
-__device__ void op_prolong(const MgLevel& F, const MgLevel& Cl, float omega, int t0, int stride) {
-    const int n = F.W * F.H * F.D;
+// Red Gauss-Seidel sweep of a level fused with the prolongation of its result
+// to the finer level F: every FLUID cell (the black ones are final already)
+// adds omega * x to its FLUID children.  Each fine cell has one parent, so no
+// two threads write the same fine cell.
+__device__ void op_sweep_red_prolong(const MgLevel& L, const MgLevel& F, float omega, int t0, int stride) {
+    const int n = L.W * L.H * L.D;
     for (int t = t0; t < n; t += stride) {
-        int i, j, k;
-        const int c = lv_cell(F, t, i, j, k);
-        if (F.lab[c] != FLUID) continue;
-        const int cc = (i / 2 + 1) + (j / 2 + 1) * Cl.sy + (k / 2 + 1) * Cl.sz;
-        if (Cl.lab[cc] == FLUID) F.x[c] += omega * Cl.x[cc];
+        int I, J, K;
+        const int c = lv_cell(L, t, I, J, K);
+        if (L.lab[c] != FLUID) continue;
+        float v = L.x[c];
+        if (((I + J + K) & 1) == 0) {
+            const int d = lv_diag(L, c);
+            v = d > 0 ? (L.b[c] + lv_nbsum(L, c)) / float(d) : 0.0f;
+            L.x[c] = v;
+        }
+        const float corr = omega * v;
+        for (int c3 = 0; c3 < 2; ++c3)
+            for (int b3 = 0; b3 < 2; ++b3)
+                for (int a3 = 0; a3 < 2; ++a3) {
+                    const int i = 2 * I + a3, j = 2 * J + b3, k = 2 * K + c3;
+                    if (i >= F.W || j >= F.H || k >= F.D) continue;
+                    const int cf = (i + 1) + (j + 1) * F.sy + (k + 1) * F.sz;
+                    if (F.lab[cf] == FLUID) F.x[cf] += corr;
+                }
     }
 }
 
-// V-cycle over levels [l0, L) by block 0 alone.
+// V-cycle over levels [l0, L) by block 0 alone.  Level l0's first sweep is
+// already done (fused into the step that wrote its right-hand side); the last
+// red sweep of level l0 also prolongs into level l0 - 1 when l0 > 0.
 __device__ void block_vcycle(const MgArgs& a, int l0) {
     const int t0 = threadIdx.x, st = blockDim.x;
     for (int l = l0; l < a.L - 1; ++l) {
-        op_first_red(a.lv[l], t0, st); __syncthreads();
         op_sweep(a.lv[l], 1, t0, st); __syncthreads();
-        op_restrict(a.lv[l], a.lv[l + 1], a.rscale, t0, st); __syncthreads();
+        op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st); __syncthreads();
     }
-    const MgLevel& C = a.lv[a.L - 1];
-    op_first_red(C, t0, st); __syncthreads();
+    const int lc = a.L - 1;
+    const MgLevel& C = a.lv[lc];
     op_sweep(C, 1, t0, st); __syncthreads();
     for (int it = 1; it < a.nu_coarse; ++it) {
         op_sweep(C, 0, t0, st); __syncthreads();
@@ -215,17 +201,26 @@ __device__ void block_vcycle(const MgArgs& a, int l0) {
     }
     for (int it = 0; it < a.nu_coarse; ++it) {
         op_sweep(C, 1, t0, st); __syncthreads();
-        op_sweep(C, 0, t0, st); __syncthreads();
+        if (it + 1 < a.nu_coarse || lc == 0) {
+            op_sweep(C, 0, t0, st); __syncthreads();
+        } else {
+            op_sweep_red_prolong(C, a.lv[lc - 1], a.omega, t0, st); __syncthreads();
+        }
     }
-    for (int l = a.L - 2; l >= l0; --l) {
-        op_prolong(a.lv[l], a.lv[l + 1], a.omega, t0, st); __syncthreads();
+    for (int l = lc - 1; l >= l0; --l) {
         op_sweep(a.lv[l], 1, t0, st); __syncthreads();
-        op_sweep(a.lv[l], 0, t0, st); __syncthreads();
+        if (l > 0) op_sweep_red_prolong(a.lv[l], a.lv[l - 1], a.omega, t0, st);
+        else op_sweep(a.lv[l], 0, t0, st);
+        __syncthreads();
     }
 }
 
-// z = V-cycle(r) with r = lv[0].b, z = lv[0].x.  Starts and ends with a grid
-// barrier; returns false if a barrier timed out.
+// z = V-cycle(r) with r = lv[0].b, z = lv[0].x.  The caller has already done
+// the first (red) sweep of level 0: z = b/d on red FLUID cells, 0 on black
+// ones.  Starts and ends with a grid barrier; returns false if a barrier
+// timed out.  Grid-wide levels take four barriers each: black sweep,
+// restriction (with the next level's first sweep), black sweep, red sweep
+// (with the prolongation into the finer level).
 __device__ bool vcycle(const MgArgs& a) {
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
     const unsigned nb = gridDim.x;
@@ -233,29 +228,29 @@ __device__ bool vcycle(const MgArgs& a) {
     const int G = min(a.G, a.L - 1);
     const int nf = *a.nf;
     for (int l = 0; l < G; ++l) {
-        if (l == 0) op0_first_red(a.lv[0], a.fidx, a.diag, nf, t0, st);
-        else op_first_red(a.lv[l], t0, st);
-        if (!grid_barrier(a.bar, nb, a.status)) return false;
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 1, t0, st);
         else op_sweep(a.lv[l], 1, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
-        op_restrict(a.lv[l], a.lv[l + 1], a.rscale, t0, st);
+        op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
     if (blockIdx.x == 0) block_vcycle(a, G);
     if (!grid_barrier(a.bar, nb, a.status)) return false;
     for (int l = G - 1; l >= 0; --l) {
-        if (l == 0) op0_prolong(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
-        else op_prolong(a.lv[l], a.lv[l + 1], a.omega, t0, st);
-        if (!grid_barrier(a.bar, nb, a.status)) return false;
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 1, t0, st);
         else op_sweep(a.lv[l], 1, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 0, t0, st);
-        else op_sweep(a.lv[l], 0, t0, st);
+        else op_sweep_red_prolong(a.lv[l], a.lv[l - 1], a.omega, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
     return true;
+}
+
+// Level-0 first sweep value of one FLUID cell: b/d on red cells, 0 on black.
+__device__ __forceinline__ float first_red0(float b, uint8_t db) {
+    const int d = db & 0x7F;
+    return ((db >> 7) == 0 && d > 0) ? b / float(d) : 0.0f;
 }
 
 __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
@@ -280,6 +275,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         const double rv = double(a.rhs[n]);
         r[c] = rv;
         b0[c] = float(rv);
+        z[c] = first_red0(float(rv), a.diag[n]);  // the V-cycle's first sweep
         a.xs[c] = a.x0 ? double(a.x0[n]) : 0.0;
     }
     double bb_warm = 0.0;  // ||b||^2 when started from a guess
@@ -309,6 +305,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
             const double rv = r[c] - alpha * a.q[c];
             r[c] = rv;
             b0[c] = float(rv);
+            z[c] = first_red0(float(rv), a.diag[n]);
         }
     }
     if (!vcycle(a)) return;
@@ -365,6 +362,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
             const double rv = r[c] - alpha * a.q[c];
             r[c] = rv;
             b0[c] = float(rv);
+            z[c] = first_red0(float(rv), a.diag[n]);
             rrl += rv * rv;
         }
         if (!vcycle(a)) return;  // z = M^-1 r (begins with a barrier)
