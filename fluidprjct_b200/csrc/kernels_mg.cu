@@ -33,6 +33,7 @@ namespace fp {
 namespace {
 
 constexpr int MG_THREADS = 512;
+constexpr int MG_SMEM_CELLS = 1024;  // padded coarsest level held in shared memory
 
 struct MgArgs {
     int L, G;                    // levels; levels [0, G) are grid-wide
@@ -155,31 +156,39 @@ __device__ void op_restrict_first(const MgLevel& F, const MgLevel& Cl, float sca
         Cl.x[cc] = xv;
     }
 }
-// Red Gauss-Seidel sweep of a level fused with the prolongation of its result
-// to the finer level F: every FLUID cell (the black ones are final already)
-// adds omega * x to its FLUID children.  Each fine cell has one parent, so no
-// two threads write the same fine cell.
-__device__ void op_sweep_red_prolong(const MgLevel& L, const MgLevel& F, float omega, int t0, int stride) {
-    const int n = L.W * L.H * L.D;
+// The last (red) sweep of a coarse level fused with the prolongation of its
+// result: every FLUID fine cell with a FLUID parent adds omega * (parent's
+// value), where a red parent's value is its Gauss-Seidel update (recomputed
+// by each of its children from the final black neighbours, with the same
+// arithmetic, so all eight see the same bits) and a black parent's is final.
+// The coarse x is not needed after this, so it is not written back.
+__device__ __forceinline__ float parent_value(const MgLevel& Cl, int cc, int I, int J, int K) {
+    if (((I + J + K) & 1) != 0) return Cl.x[cc];
+    const int d = lv_diag(Cl, cc);
+    return d > 0 ? (Cl.b[cc] + lv_nbsum(Cl, cc)) / float(d) : 0.0f;
+}
+// ... over every cell of the fine level F (dense levels)
+__device__ void op_prolong_red(const MgLevel& F, const MgLevel& Cl, float omega, int t0, int stride) {
+    const int n = F.W * F.H * F.D;
     for (int t = t0; t < n; t += stride) {
-        int I, J, K;
-        const int c = lv_cell(L, t, I, J, K);
-        if (L.lab[c] != FLUID) continue;
-        float v = L.x[c];
-        if (((I + J + K) & 1) == 0) {
-            const int d = lv_diag(L, c);
-            v = d > 0 ? (L.b[c] + lv_nbsum(L, c)) / float(d) : 0.0f;
-            L.x[c] = v;
-        }
-        const float corr = omega * v;
-        for (int c3 = 0; c3 < 2; ++c3)
-            for (int b3 = 0; b3 < 2; ++b3)
-                for (int a3 = 0; a3 < 2; ++a3) {
-                    const int i = 2 * I + a3, j = 2 * J + b3, k = 2 * K + c3;
-                    if (i >= F.W || j >= F.H || k >= F.D) continue;
-                    const int cf = (i + 1) + (j + 1) * F.sy + (k + 1) * F.sz;
-                    if (F.lab[cf] == FLUID) F.x[cf] += corr;
-                }
+        int i, j, k;
+        const int c = lv_cell(F, t, i, j, k);
+        if (F.lab[c] != FLUID) continue;
+        const int I = i >> 1, J = j >> 1, K = k >> 1;
+        const int cc = (I + 1) + (J + 1) * Cl.sy + (K + 1) * Cl.sz;
+        if (Cl.lab[cc] != FLUID) continue;
+        F.x[c] += omega * parent_value(Cl, cc, I, J, K);
+    }
+}
+// ... over the level-0 FLUID list
+__device__ void op0_prolong_red(const MgLevel& F, const MgLevel& Cl, float omega, const int* fidx, int nf, int t0,
+                                int stride) {
+    for (int n = t0; n < nf; n += stride) {
+        const int c = fidx[n];
+        const int i = c % F.sy - 1, j = (c / F.sy) % (F.H + 2) - 1, k = c / F.sz - 1;
+        const int I = i >> 1, J = j >> 1, K = k >> 1;
+        const int cc = (I + 1) + (J + 1) * Cl.sy + (K + 1) * Cl.sz;
+        if (Cl.lab[cc] == FLUID) F.x[c] += omega * parent_value(Cl, cc, I, J, K);
     }
 }
 
@@ -193,7 +202,24 @@ __device__ void block_vcycle(const MgArgs& a, int l0) {
         op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st); __syncthreads();
     }
     const int lc = a.L - 1;
-    const MgLevel& C = a.lv[lc];
+    // The coarsest level lives in shared memory when it fits: its sweeps then
+    // cost no global-memory latency (level-op pointers are generic, so the
+    // same operations run on the shared copy).
+    __shared__ float s_x[MG_SMEM_CELLS], s_b[MG_SMEM_CELLS];
+    __shared__ uint8_t s_lab[MG_SMEM_CELLS];
+    MgLevel C = a.lv[lc];
+    const int npad = (C.W + 2) * (C.H + 2) * (C.D + 2);
+    if (lc > 0 && npad <= MG_SMEM_CELLS) {  // (a single-level hierarchy's x is the output: keep it global)
+        for (int c = t0; c < npad; c += st) {
+            s_lab[c] = C.lab[c];
+            s_b[c] = C.b[c];
+            s_x[c] = C.x[c];
+        }
+        C.lab = s_lab;
+        C.b = s_b;
+        C.x = s_x;
+        __syncthreads();
+    }
     op_sweep(C, 1, t0, st); __syncthreads();
     for (int it = 1; it < a.nu_coarse; ++it) {
         op_sweep(C, 0, t0, st); __syncthreads();
@@ -204,12 +230,12 @@ __device__ void block_vcycle(const MgArgs& a, int l0) {
         if (it + 1 < a.nu_coarse || lc == 0) {
             op_sweep(C, 0, t0, st); __syncthreads();
         } else {
-            op_sweep_red_prolong(C, a.lv[lc - 1], a.omega, t0, st); __syncthreads();
+            op_prolong_red(a.lv[lc - 1], C, a.omega, t0, st); __syncthreads();
         }
     }
     for (int l = lc - 1; l >= l0; --l) {
         op_sweep(a.lv[l], 1, t0, st); __syncthreads();
-        if (l > 0) op_sweep_red_prolong(a.lv[l], a.lv[l - 1], a.omega, t0, st);
+        if (l > 0) op_prolong_red(a.lv[l - 1], a.lv[l], a.omega, t0, st);
         else op_sweep(a.lv[l], 0, t0, st);
         __syncthreads();
     }
@@ -241,7 +267,8 @@ __device__ bool vcycle(const MgArgs& a) {
         else op_sweep(a.lv[l], 1, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 0, t0, st);
-        else op_sweep_red_prolong(a.lv[l], a.lv[l - 1], a.omega, t0, st);
+        else if (l == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
+        else op_prolong_red(a.lv[l - 1], a.lv[l], a.omega, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
     return true;
