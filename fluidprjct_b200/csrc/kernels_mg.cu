@@ -193,8 +193,10 @@ __device__ void op0_prolong_red(const MgLevel& F, const MgLevel& Cl, float omega
 }
 
 // V-cycle over levels [l0, L) by block 0 alone.  Level l0's first sweep is
-// already done (fused into the step that wrote its right-hand side); the last
-// red sweep of level l0 also prolongs into level l0 - 1 when l0 > 0.
+// already done (fused into the step that wrote its right-hand side).  With
+// l0 > 0 the stage stops after level l0's last black sweep: the final red
+// sweep of level l0 is the grid-wide prolongation into level l0 - 1, which
+// recomputes it.  With l0 == 0 it finishes level 0 itself.
 __device__ void block_vcycle(const MgArgs& a, int l0) {
     const int t0 = threadIdx.x, st = blockDim.x;
     for (int l = l0; l < a.L - 1; ++l) {
@@ -209,7 +211,8 @@ __device__ void block_vcycle(const MgArgs& a, int l0) {
     __shared__ uint8_t s_lab[MG_SMEM_CELLS];
     MgLevel C = a.lv[lc];
     const int npad = (C.W + 2) * (C.H + 2) * (C.D + 2);
-    if (lc > 0 && npad <= MG_SMEM_CELLS) {  // (a single-level hierarchy's x is the output: keep it global)
+    const bool in_smem = lc > 0 && npad <= MG_SMEM_CELLS;  // a single-level hierarchy's x is the output
+    if (in_smem) {
         for (int c = t0; c < npad; c += st) {
             s_lab[c] = C.lab[c];
             s_b[c] = C.b[c];
@@ -229,15 +232,21 @@ __device__ void block_vcycle(const MgArgs& a, int l0) {
         op_sweep(C, 1, t0, st); __syncthreads();
         if (it + 1 < a.nu_coarse || lc == 0) {
             op_sweep(C, 0, t0, st); __syncthreads();
-        } else {
+        } else if (lc > l0) {
             op_prolong_red(a.lv[lc - 1], C, a.omega, t0, st); __syncthreads();
         }
     }
+    if (in_smem && lc == l0) {  // the grid prolongation reads this level from global memory
+        for (int c = t0; c < npad; c += st) a.lv[lc].x[c] = s_x[c];
+        __syncthreads();
+    }
     for (int l = lc - 1; l >= l0; --l) {
         op_sweep(a.lv[l], 1, t0, st); __syncthreads();
-        if (l > 0) op_prolong_red(a.lv[l - 1], a.lv[l], a.omega, t0, st);
-        else op_sweep(a.lv[l], 0, t0, st);
-        __syncthreads();
+        if (l == 0) {
+            op_sweep(a.lv[0], 0, t0, st); __syncthreads();
+        } else if (l > l0) {
+            op_prolong_red(a.lv[l - 1], a.lv[l], a.omega, t0, st); __syncthreads();
+        }
     }
 }
 
@@ -262,6 +271,11 @@ __device__ bool vcycle(const MgArgs& a) {
     }
     if (blockIdx.x == 0) block_vcycle(a, G);
     if (!grid_barrier(a.bar, nb, a.status)) return false;
+    if (G > 0) {  // level G's last red sweep, fused with its prolongation into level G - 1
+        if (G == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
+        else op_prolong_red(a.lv[G - 1], a.lv[G], a.omega, t0, st);
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
+    }
     for (int l = G - 1; l >= 0; --l) {
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 1, t0, st);
         else op_sweep(a.lv[l], 1, t0, st);
