@@ -122,7 +122,9 @@ def test_unet_training_lowers_the_heldout_loss(trained):
     from fluidprjct_b200 import learned
     after = learned.eval_loss(trained["net"], trained["held"], range(12))
     print("held-out loss", trained["loss0"], "->", after, "history", trained["hist"])
-    assert np.isfinite(after) and after < 0.25 * trained["loss0"] and after < 1.0
+    # the training pairs come from FLIP steps whose P2G sums with float atomics,
+    # so the trajectory differs a little between runs: the bound is loose
+    assert np.isfinite(after) and after < 0.2 * trained["loss0"] and after < 2.0
 
 
 def test_learned_guess_keeps_mg_iterations(trained):
