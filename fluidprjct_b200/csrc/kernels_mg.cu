@@ -32,7 +32,7 @@ namespace fp {
 
 namespace {
 
-constexpr int MG_THREADS = 512;
+constexpr int MG_THREADS = 1024;
 constexpr int MG_SMEM_CELLS = 1024;  // padded coarsest level held in shared memory
 
 struct MgArgs {
