@@ -26,7 +26,7 @@ SOURCES = [
     "kernels_body.cu",
     "kernels_mg.cu",
     "kernels_unet.cu",
-    "kernels_unet_tc.cu",
+    "kernels_unet_tma.cu",
     "unet.cu",
     "solver.cu",
     "noalloc.cu",

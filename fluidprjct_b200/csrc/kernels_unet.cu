@@ -1,24 +1,18 @@
 // kernels_unet.cu -- kernels of the learned pressure preconditioner (a 3D
 // U-Net; the layer table is in unet.hpp).
 //
-// Convolutions are implicit GEMMs on the BF16 tensor cores (mma.sync
-// m16n8k16, FP32 accumulation):
-//   k_conv3  y[v][co] = sum_t sum_ci x[v + off(t)][ci] w[t][co][ci], one
-//            output brick of 8x8x4 voxels (M = 256) per step of a persistent
-//            CTA.  The zero-padded input halo (10x10x6 voxels, every input
-//            channel) is staged in shared memory with cp.async.  The CTA's
-//            output-channel group of the weights stays resident in shared
-//            memory for all of its bricks.  The input may be the
-//            concatenation [up2(xa) | xb] of a 2x-upsampled coarse tensor and
-//            a same-level one: the upsampling is an index shift in the halo
-//            load, never a tensor in memory.  The backward data pass of a
-//            layer is the same kernel, run on the flipped, transposed
-//            weights.
+// The forward and backward-data convolutions run on tcgen05
+// (kernels_unet_tma.cu).  This file holds the rest, with the weight gradient
+// on the BF16 mma.sync path (m16n8k16, FP32 accumulation):
 //   k_corr3  weight gradients dw[t][co][ci] = sum_v g[v][co] x[v+off(t)][ci]
-//            (M = COUT, N = CIN, K = voxels).  Each CTA accumulates its tap
-//            group over its bricks in registers and writes one partial.  The
-//            partials are summed in a fixed order, so gradients are
-//            deterministic.
+//            (M = COUT, N = CIN, K = voxels), over bricks of 8x8x4 voxels
+//            whose zero-padded input halo (10x10x6, every input channel) is
+//            staged with cp.async.  The input may be the concatenation
+//            [up2(xa) | xb] of a 2x-upsampled coarse tensor and a same-level
+//            one: the upsampling is an index shift in the halo load.  Each
+//            CTA accumulates its tap group over its bricks in registers and
+//            writes one partial.  The partials are summed in a fixed order,
+//            so gradients are deterministic.
 // Smem rows are padded by 16 bytes, so each 8-row ldmatrix phase hits eight
 // distinct 16-byte bank groups.
 #include <algorithm>
@@ -43,11 +37,6 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool pred
                  "r"(pred ? 16 : 0));
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-__device__ __forceinline__ void ldsm_x4(unsigned& r0, unsigned& r1, unsigned& r2, unsigned& r3, unsigned addr) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-                 : "r"(addr));
-}
 __device__ __forceinline__ void ldsm_x4_t(unsigned& r0, unsigned& r1, unsigned& r2, unsigned& r3, unsigned addr) {
     asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
                  : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
@@ -82,109 +71,6 @@ __device__ __forceinline__ void load_halo(bf16* sx, const bf16* __restrict__ xa,
         else
             src = in ? xb + ((int64_t(gz) * lv.H + gy) * lv.W + gx) * CB + (ch * 8 - CA) : xb;
         cp_async16(sx + hv * RS + ch * 8, src, in);
-    }
-}
-
-template <int CA, int CB, int COUT, int NCO, int EPI>
-__global__ void __launch_bounds__(THREADS) k_conv3(ConvArgs a) {
-    constexpr int CIN = CA + CB;
-    constexpr int RS = CIN + 8;
-    constexpr int NT = NCO / 8;
-    static_assert(CIN % 16 == 0 && NCO % 16 == 0 && COUT % NCO == 0, "channel tiling");
-    static_assert(EPI != EPI_HEAD || (NCO == 16 && COUT == 16), "head needs all 16 channels");
-    extern __shared__ __align__(16) unsigned char smem[];
-    bf16* sx = reinterpret_cast<bf16*>(smem);
-    bf16* sw = sx + HALO * RS;
-    const int cog = blockIdx.y;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-    for (int i = tid; i < 27 * NCO * (CIN / 8); i += THREADS) {
-        const int ch = i % (CIN / 8), row = i / (CIN / 8);
-        const int tap = row / NCO, co = row % NCO;
-        cp_async16(sw + row * RS + ch * 8, a.w + (int64_t(tap) * COUT + cog * NCO + co) * CIN + ch * 8, true);
-    }
-    const int nbx = (a.lv.W + BX - 1) / BX, nby = (a.lv.H + BY - 1) / BY, nbz = (a.lv.D + BZ - 1) / BZ;
-    const int nbricks = nbx * nby * nbz;
-    // per-lane ldmatrix rows: A (voxel rows of a 16-voxel M-tile), B (output channels)
-    const int ar = (lane & 7) + 8 * ((lane >> 3) & 1), akoff = 8 * (lane >> 4);
-    const int bco = (lane & 7) + 8 * (lane >> 4), bkoff = 8 * ((lane >> 3) & 1);
-    const int g = lane >> 2, tq = lane & 3;
-    int abase[2];
-#pragma unroll
-    for (int m = 0; m < 2; ++m) {
-        const int mt = warp * 2 + m, z = mt >> 2, yy = (mt & 3) * 2;
-        abase[m] = ((z + 1) * HY + (yy + (ar >> 3) + 1)) * HX + ((ar & 7) + 1);
-    }
-    const unsigned sx_s = smem_addr(sx), sw_s = smem_addr(sw);
-
-    for (int brick = blockIdx.x; brick < nbricks; brick += gridDim.x) {
-        const int bx = brick % nbx, by = (brick / nbx) % nby, bz = brick / (nbx * nby);
-        load_halo<CA, CB, RS>(sx, a.xa, a.xb, a.lv, a.lc, bx * BX - 1, by * BY - 1, bz * BZ - 1);
-        cp_async_wait_all();
-        __syncthreads();
-
-        float acc[2][NT][4];
-#pragma unroll
-        for (int m = 0; m < 2; ++m)
-#pragma unroll
-            for (int j = 0; j < NT; ++j) acc[m][j][0] = acc[m][j][1] = acc[m][j][2] = acc[m][j][3] = 0.0f;
-
-#pragma unroll 1
-        for (int tap = 0; tap < 27; ++tap) {
-            const int toff = ((tap / 9 - 1) * HY + ((tap / 3) % 3 - 1)) * HX + (tap % 3 - 1);
-#pragma unroll
-            for (int kc = 0; kc < CIN / 16; ++kc) {
-                unsigned b[NT][2];
-#pragma unroll
-                for (int j = 0; j < NT; j += 2)
-                    ldsm_x4(b[j][0], b[j][1], b[j + 1][0], b[j + 1][1],
-                            sw_s + ((tap * NCO + j * 8 + bco) * RS + kc * 16 + bkoff) * 2);
-#pragma unroll
-                for (int m = 0; m < 2; ++m) {
-                    unsigned a0, a1, a2, a3;
-                    ldsm_x4(a0, a1, a2, a3, sx_s + ((abase[m] + toff) * RS + kc * 16 + akoff) * 2);
-#pragma unroll
-                    for (int j = 0; j < NT; ++j) mma16816(acc[m][j], a0, a1, a2, a3, b[j][0], b[j][1]);
-                }
-            }
-        }
-
-        // epilogue: rows g (y = yy) and g + 8 (y = yy + 1), x = g
-#pragma unroll
-        for (int m = 0; m < 2; ++m) {
-            const int mt = warp * 2 + m, z = mt >> 2, yy = (mt & 3) * 2;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int gx = bx * BX + g, gy = by * BY + yy + h, gz = bz * BZ + z;
-                const bool in = gx < a.lv.W && gy < a.lv.H && gz < a.lv.D;
-                const int64_t vox = (int64_t(gz) * a.lv.H + gy) * a.lv.W + gx;
-                float hsum = 0.0f;
-#pragma unroll
-                for (int j = 0; j < NT; ++j) {
-                    const int co = cog * NCO + j * 8 + 2 * tq;
-                    float v0 = acc[m][j][2 * h], v1 = acc[m][j][2 * h + 1];
-                    if (EPI == EPI_RELU || EPI == EPI_HEAD) {
-                        v0 = fmaxf(v0, 0.0f);
-                        v1 = fmaxf(v1, 0.0f);
-                    }
-                    if (EPI == EPI_MASK && in) {
-                        const __nv_bfloat162 mk = *reinterpret_cast<const __nv_bfloat162*>(a.mask + vox * COUT + co);
-                        if (!(__bfloat162float(mk.x) > 0.0f)) v0 = 0.0f;
-                        if (!(__bfloat162float(mk.y) > 0.0f)) v1 = 0.0f;
-                    }
-                    const __nv_bfloat162 o = __floats2bfloat162_rn(v0, v1);
-                    if (in) *reinterpret_cast<__nv_bfloat162*>(a.y + vox * COUT + co) = o;
-                    if (EPI == EPI_HEAD)
-                        hsum += __bfloat162float(o.x) * a.head_w[co] + __bfloat162float(o.y) * a.head_w[co + 1];
-                }
-                if (EPI == EPI_HEAD) {
-                    hsum += __shfl_xor_sync(0xffffffffu, hsum, 1);
-                    hsum += __shfl_xor_sync(0xffffffffu, hsum, 2);
-                    if (in && tq == 0) a.head_out[vox] = hsum;
-                }
-            }
-        }
-        __syncthreads();  // the next brick overwrites the halo
     }
 }
 
@@ -608,25 +494,6 @@ int nbricks_of(const Lvl& lv) {
     return ((lv.W + BX - 1) / BX) * ((lv.H + BY - 1) / BY) * ((lv.D + BZ - 1) / BZ);
 }
 
-template <int CA, int CB, int COUT, int NCO, int EPI>
-int run_conv(const ConvArgs& a, cudaStream_t st) {
-    constexpr int CIN = CA + CB;
-    constexpr size_t smem = size_t(HALO * (CIN + 8) + 27 * NCO * (CIN + 8)) * sizeof(bf16);
-    static int per_sm = -1;
-    auto kern = k_conv3<CA, CB, COUT, NCO, EPI>;
-    if (per_sm < 0) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
-        if (per_sm < 1) per_sm = 1;
-    }
-    const int groups = COUT / NCO;
-    const int nb = nbricks_of(a.lv);
-    const int gx = std::max(1, std::min(nb, per_sm * sm_count() / groups));
-    kern<<<dim3(gx, groups), THREADS, smem, st>>>(a);
-    return int(cudaPeekAtLastError());
-}
-
 template <int CA, int CB, int COUT, int TPC>
 int run_corr(const CorrArgs& a, int nblk, cudaStream_t st) {
     constexpr int CIN = CA + CB;
@@ -645,33 +512,6 @@ int run_corr(const CorrArgs& a, int nblk, cudaStream_t st) {
 constexpr int kTpc[kLayers] = {27, 27, 9, 9, 3, 3, 3, 9, 9, 27};
 
 }  // namespace
-
-int conv_forward_layer(int layer, const ConvArgs& a, cudaStream_t st) {
-    switch (layer) {
-        case 0: case 1: return run_conv<0, 16, 16, 16, EPI_RELU>(a, st);
-        case 2: return run_conv<0, 16, 32, 32, EPI_RELU>(a, st);
-        case 3: case 7: return run_conv<0, 32, 32, 32, EPI_RELU>(a, st);
-        case 4: return run_conv<0, 32, 64, 32, EPI_RELU>(a, st);
-        case 5: return run_conv<0, 64, 64, 16, EPI_RELU>(a, st);
-        case 6: return run_conv<64, 32, 32, 16, EPI_RELU>(a, st);
-        case 8: return run_conv<32, 16, 16, 16, EPI_RELU>(a, st);
-        case 9: return run_conv<0, 16, 16, 16, EPI_HEAD>(a, st);
-    }
-    return int(cudaErrorInvalidValue);
-}
-
-int conv_backward_layer(int layer, const ConvArgs& a, cudaStream_t st) {
-    switch (layer) {
-        case 9: case 1: return run_conv<0, 16, 16, 16, EPI_MASK>(a, st);
-        case 8: return run_conv<0, 16, 48, 48, EPI_RAW>(a, st);
-        case 7: case 3: return run_conv<0, 32, 32, 32, EPI_MASK>(a, st);
-        case 6: return run_conv<0, 32, 96, 32, EPI_RAW>(a, st);
-        case 5: return run_conv<0, 64, 64, 16, EPI_MASK>(a, st);
-        case 4: return run_conv<0, 64, 32, 16, EPI_RAW>(a, st);
-        case 2: return run_conv<0, 32, 16, 16, EPI_RAW>(a, st);
-    }
-    return int(cudaErrorInvalidValue);
-}
 
 int corr_blocks(int layer, const Lvl& lv) {
     const int groups = 27 / kTpc[layer];

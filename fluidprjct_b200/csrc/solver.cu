@@ -380,7 +380,7 @@ int solve_system(fp_solver* s, float* p_out) {
                 return s->cuda_fail(cudaGetLastError(), "U-Net forward");
             unet::launch_output_compact(pb.nf, pb.fidx, real, unet::net_level0(s->net), unet::net_out(s->net),
                                         unet::net_scal(s->net), s->d_x0c, s->st);
-            s->launches += 1 + 14 + 1;  // rhs scatter, network (2 scale/input + 10 conv + 2 pool), guess
+            s->launches += 1 + 16 + 1;  // rhs scatter, network (2 scale/input, 10 conv, 2 pool, 2 concat), guess
             cudaEventRecord(s->ev_net, s->st);
             x0 = s->d_x0c;
         }

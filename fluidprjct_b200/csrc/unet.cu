@@ -40,6 +40,7 @@ struct fp_unet {
     double* h_loss = nullptr;
     // forward
     bf16 *X0, *a0, *e0, *q0, *a1, *e1, *q1, *a2, *e2, *d1a, *d1, *d0a, *d0;
+    bf16 *cat6, *cat8;  // [up2(e2) | e1] and [up2(d1) | e0], the decoder layers' inputs
     float* out = nullptr;
     // backward
     bf16 *g9, *g8, *raw8, *g7, *g6, *raw6, *g5, *g4, *gq1, *g3, *g2, *gq0, *g1, *g0;
@@ -76,18 +77,24 @@ const float* net_out(const fp_unet* u) { return u->out; }
 const float* net_scal(const fp_unet* u) { return u->scal; }
 const int* net_status(const fp_unet* u) { return u->d_status; }
 
+// A 3x3x3 convolution layer.  A decoder layer's input [up2(xa) | xb] is first
+// materialised in u->cat6 / u->cat8, because the convolution reads its input
+// through one TMA tensor map.
 static int conv_fwd(fp_unet* u, int l, const bf16* xa, const bf16* xb, bf16* y, cudaStream_t st) {
-    ConvArgs a{};
-    a.xa = xa;
-    a.xb = xb;
+    TmaConvArgs a{};
     a.w = u->wf + layer_offset(l);
     a.y = y;
     a.lv = u->L[kSpec[l].level];
-    a.lc = kSpec[l].level < 2 ? u->L[kSpec[l].level + 1] : a.lv;
     a.head_w = u->w32 + layer_offset(kLayers);
     a.head_out = u->out;
     a.status = u->d_status;
-    return conv_forward_layer_tc(l, a, st);
+    const bf16* in = xb;
+    if (kSpec[l].ca > 0) {
+        bf16* cat = l == 6 ? u->cat6 : u->cat8;
+        launch_upcat(xa, kSpec[l].ca, xb, kSpec[l].cb, a.lv, cat, st);
+        in = cat;
+    }
+    return conv_forward_layer_tma(l, in, a, st);
 }
 
 // Forward pass: u->out (net level 0) and u->scal (s, 1/s).
@@ -110,7 +117,7 @@ int forward_on(fp_unet* u, const uint8_t* labels, const float* rhs, cudaStream_t
     return e;
 }
 
-int forward_kernel_count() { return 2 + 10 + 2; }
+int forward_kernel_count() { return 2 + 10 + 2 + 2; }
 
 }  // namespace unet
 }  // namespace fp
@@ -126,15 +133,13 @@ int device_status(fp_unet* u, const char* what) {
 }
 
 int conv_bwd(fp_unet* u, int l, const bf16* g, const bf16* mask, bf16* y, cudaStream_t st) {
-    ConvArgs a{};
-    a.xb = g;
+    TmaConvArgs a{};
     a.w = u->wt + layer_offset(l);
     a.y = y;
     a.mask = mask;
     a.lv = u->L[kSpec[l].level];
-    a.lc = a.lv;
     a.status = u->d_status;
-    return conv_backward_layer_tc(l, a, st);
+    return conv_backward_layer_tma(l, g, a, st);
 }
 
 int wgrad(fp_unet* u, int l, const bf16* xa, const bf16* xb, const bf16* g, cudaStream_t st) {
@@ -248,6 +253,8 @@ int fp_unet_create(int W, int H, int D, int train, uint64_t seed, fp_unet** out)
     u->d1 = u->alloc<bf16>(n1 * 32);
     u->d0a = u->alloc<bf16>(n0 * 16);
     u->d0 = u->alloc<bf16>(n0 * 16);
+    u->cat6 = u->alloc<bf16>(n1 * 96);
+    u->cat8 = u->alloc<bf16>(n0 * 48);
     u->out = u->alloc<float>(n0);
     if (u->train) {
         u->m = u->alloc<float>(kParams);

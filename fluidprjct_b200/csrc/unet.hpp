@@ -45,19 +45,6 @@ struct Lvl {
     __host__ __device__ int64_t n() const { return int64_t(W) * H * D; }
 };
 
-// Arguments of the 3x3x3 convolution kernel (forward and backward-data).
-struct ConvArgs {
-    const bf16* xa;        // coarse input (CA channels) read 2x-upsampled, or null
-    const bf16* xb;        // same-level input (CB channels)
-    const bf16* w;         // [27][COUT][CA+CB]
-    bf16* y;               // output [V][COUT]
-    const bf16* mask;      // EPI_MASK: output is zeroed where mask[V][c] <= 0
-    const float* head_w;   // EPI_HEAD: 16 head weights
-    float* head_out;       // EPI_HEAD: one FP32 value per voxel
-    Lvl lv, lc;            // this level, the coarse level of xa
-    int* status;           // set to nonzero if a bounded device wait gave up
-};
-
 // Arguments of the weight-gradient kernel: dw[t][co][ci] = sum_v g[v][co] x[v + off(t)][ci].
 struct CorrArgs {
     const bf16* xa;
@@ -69,12 +56,23 @@ struct CorrArgs {
 
 enum { EPI_RELU = 0, EPI_MASK = 1, EPI_RAW = 2, EPI_HEAD = 3 };
 
+// Arguments of the TMA-fed convolution (kernels_unet_tma.cu); its input is
+// one [V][CIN] tensor read through a tensor map.
+struct TmaConvArgs {
+    bf16* y;               // output [V][COUT]
+    const bf16* mask;      // EPI_MASK: output is zeroed where mask[V][c] <= 0
+    const float* head_w;   // EPI_HEAD: 16 head weights
+    float* head_out;       // EPI_HEAD: one FP32 value per voxel
+    const bf16* w;         // [27][COUT][CIN]
+    Lvl lv;                // the level of input and output
+    int* status;           // set to nonzero if a bounded device wait gave up
+};
+int conv_forward_layer_tma(int layer, const bf16* in, const TmaConvArgs& a, cudaStream_t st);
+int conv_backward_layer_tma(int layer, const bf16* in, const TmaConvArgs& a, cudaStream_t st);
+// out = [up2(coarse) | skip] on the fine level (ca + cb channels).
+void launch_upcat(const bf16* coarse, int ca, const bf16* skip, int cb, Lvl fine, bf16* out, cudaStream_t st);
+
 // Launchers (kernels_unet.cu).  Each returns 0 or a cudaError_t value.
-int conv_forward_layer(int layer, const ConvArgs& a, cudaStream_t st);   // EPI_RELU, or EPI_HEAD for L9
-int conv_backward_layer(int layer, const ConvArgs& a, cudaStream_t st);  // data gradient of layer (1..9)
-// The same convolutions on tcgen05 (kernels_unet_tc.cu).
-int conv_forward_layer_tc(int layer, const ConvArgs& a, cudaStream_t st);
-int conv_backward_layer_tc(int layer, const ConvArgs& a, cudaStream_t st);
 int corr_layer(int layer, const CorrArgs& a, int nblk, cudaStream_t st);
 int corr_blocks(int layer, const Lvl& lv);                               // gridDim.x for corr_layer
 void reduce_partials(const float* part, int nblk, int64_t n, float* out, cudaStream_t st);
