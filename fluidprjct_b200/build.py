@@ -27,6 +27,7 @@ SOURCES = [
     "kernels_mg.cu",
     "kernels_unet.cu",
     "kernels_unet_tma.cu",
+    "kernels_ref2d.cu",
     "unet.cu",
     "solver.cu",
     "noalloc.cu",

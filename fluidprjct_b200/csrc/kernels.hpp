@@ -144,4 +144,28 @@ void launch_pack(const float* pos, const float* vel, int64_t np, float4* pos4, f
 int csr_cg_solve(int n, const int* offsets, const int* cols, const double* vals, const double* b, double* x, double tol,
                  int maxit, int* iters, double* relres, cudaStream_t st);
 
+// -------- the reference's own 2D step, scheme "ref2d" (kernels_ref2d.cu) --------
+// Scratch: start[(W+4)*(H+4)+1] (bins of cells -2..W+1 x -2..H+1), list, key,
+// rank [np], keep [np+1], misc[3] (non-finite u and v velocities, capped
+// substep loops).
+struct R2Scratch {
+    int *start, *list, *key, *rank, *keep, *misc;
+};
+void launch_r2_label(const uint8_t* base, uint8_t* labels, const float4* pos, int64_t np, Dims g, float dx,
+                     cudaStream_t st);
+// mode 0: u, v = P2G; mode 1: u*, v* = P2G and u, v = P2G + gravity (5 launches)
+void launch_r2_p2g(const float4* pos, const float4* vel, int64_t np, Dims g, float dx, float dt, int mode,
+                   R2Scratch& sc, float* u, float* v, float* us, float* vs, cudaStream_t st);
+void launch_r2_forces(float* u, float* v, Dims g, float dt, cudaStream_t st);
+void launch_r2_project(float* u, float* v, const float* p, const uint8_t* labels, Dims g, float dx, float dt,
+                       cudaStream_t st);
+// flags: 1 G2P, 2 advection, 4 clean-up (sets sc.keep)
+void launch_r2_particles(float4* pos, float4* vel, int64_t np, const float* u, const float* v, const float* us,
+                         const float* vs, const uint8_t* labels, Dims g, float dx, float dt, float alpha, int flags,
+                         R2Scratch& sc, cudaStream_t st);
+// kept particles of sc.keep, in order, to pos2/vel2 (w = new index); the
+// count lands in sc.keep[np] (2 launches)
+void launch_r2_compact(const float4* pos, const float4* vel, int64_t np, R2Scratch& sc, float4* pos2, float4* vel2,
+                       cudaStream_t st);
+
 }  // namespace fp

@@ -129,6 +129,11 @@ struct fp_solver {
     int* h_nf = nullptr;
     int* d_bad = nullptr;   // first non-finite particle of an upload
     int* h_bad = nullptr;
+    // scheme ref2d: bins over (W+4)*(H+4) cells, particle lists and keep flags
+    R2Scratch r2{};
+    int r2_nb = 0;
+    int64_t r2_cap = 0;
+    int* h_r2 = nullptr;    // pinned: [0] particles kept, [1] capped substep loops
     // body
     BodyKin body{};
     HostBody hb;
@@ -150,6 +155,11 @@ struct fp_solver {
 
 namespace {
 
+void free_r2(fp_solver* s) {
+    dfree(s->r2.start); dfree(s->r2.misc);
+    s->r2_nb = 0;
+}
+
 void free_grid(fp_solver* s) {
     dfree(s->d_base); dfree(s->d_labels); dfree(s->d_bodymark);
     dfree(s->d_u); dfree(s->d_v); dfree(s->d_w); dfree(s->d_us); dfree(s->d_vs); dfree(s->d_ws);
@@ -165,6 +175,7 @@ void free_grid(fp_solver* s) {
     dfree(s->d_mgp); dfree(s->d_mgq); dfree(s->d_mgx); dfree(s->d_mgr);
     dfree(s->d_rhs_dense); dfree(s->d_x0c);
     if (s->net) { fp_unet_destroy(s->net); s->net = nullptr; }
+    free_r2(s);
     s->have_grid = false;
 }
 
@@ -176,8 +187,10 @@ void free_body(fp_solver* s) {
 void free_particles(fp_solver* s) {
     dfree(s->d_pos); dfree(s->d_vel); dfree(s->d_pos2); dfree(s->d_vel2);
     dfree(s->d_key); dfree(s->d_rank); dfree(s->d_io);
-    s->np = s->cap = 0;
+    dfree(s->r2.list); dfree(s->r2.keep);
+    s->np = s->cap = s->r2_cap = 0;
 }
+
 
 // (Re)create the inference network for the current grid from learned_path.
 int load_net(fp_solver* s) {
@@ -540,6 +553,116 @@ void phase_g2p_advect(fp_solver* s, int do_g2p, int do_adv) {
     if (do_adv) s->sorted = false;
 }
 
+// ---------------------------------------------------------------- scheme ref2d
+// FluidSolver2D.cu's own step (kernels_ref2d.cu); particles stay in order.
+bool ref2d(const fp_solver* s) { return s->cfg.scheme == FP_SCHEME_REF2D; }
+
+int r2_alloc(fp_solver* s) {
+    const int nb = (s->W + 4) * (s->H + 4);
+    cudaError_t e = cudaSuccess;
+    if (s->r2_nb != nb) {
+        free_r2(s);
+        e = dalloc(&s->r2.start, size_t(nb) + 1);
+        if (e == cudaSuccess) e = dalloc(&s->r2.misc, size_t(4));
+        if (e != cudaSuccess) { free_r2(s); return s->cuda_fail(e, "device allocation of the 2D bins"); }
+        s->r2_nb = nb;
+    }
+    if (s->r2_cap < s->cap || !s->r2.list) {
+        dfree(s->r2.list); dfree(s->r2.keep);
+        const int64_t n = std::max<int64_t>(s->cap, 1);
+        e = dalloc(&s->r2.list, size_t(n));
+        if (e == cudaSuccess) e = dalloc(&s->r2.keep, size_t(n) + 1);
+        if (e != cudaSuccess) return s->cuda_fail(e, "device allocation of the 2D particle lists");
+        s->r2_cap = n;
+    }
+    s->r2.key = s->d_key;
+    s->r2.rank = s->d_rank;
+    return FP_OK;
+}
+
+void r2_label(fp_solver* s) {
+    launch_r2_label(s->d_base, s->d_labels, s->d_pos, s->np, s->g, s->cfg.dx, s->st);
+    s->launches += s->np > 0 ? 2 : 1;
+}
+
+void r2_p2g(fp_solver* s, int mode) {
+    launch_r2_p2g(s->d_pos, s->d_vel, s->np, s->g, s->cfg.dx, s->cfg.dt, mode, s->r2, s->d_u, s->d_v, s->d_us, s->d_vs,
+                  s->st);
+    s->launches += s->np > 0 ? 5 : 3;
+}
+
+int r2_pressure(fp_solver* s) {
+    // the 2D system has no w faces: keep the depth-1 w grid at zero
+    cudaMemsetAsync(s->d_w, 0, sizeof(float) * s->g.nw(), s->st);
+    return phase_pressure(s);
+}
+
+void r2_project(fp_solver* s) {
+    launch_r2_project(s->d_u, s->d_v, s->d_p, s->d_labels, s->g, s->cfg.dx, s->cfg.dt, s->st);
+    s->launches += 1;
+}
+
+void r2_particles(fp_solver* s, int flags) {
+    if (s->np == 0) return;
+    launch_r2_particles(s->d_pos, s->d_vel, s->np, s->d_u, s->d_v, s->d_us, s->d_vs, s->d_labels, s->g, s->cfg.dx,
+                        s->cfg.dt, s->cfg.pic_weight, flags, s->r2, s->st);
+    s->launches += 1;
+}
+
+// After r2_particles with the clean-up flag: drop deleted particles (order
+// kept), read the new count and the capped-loop count.
+int r2_compact(fp_solver* s, bool advected) {
+    if (s->np == 0) return FP_OK;
+    launch_r2_compact(s->d_pos, s->d_vel, s->np, s->r2, s->d_pos2, s->d_vel2, s->st);
+    s->launches += 2;
+    cudaMemcpyAsync(s->h_r2, s->r2.keep + s->np, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+    if (advected) cudaMemcpyAsync(s->h_r2 + 1, s->r2.misc + 2, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+    cudaError_t e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "2D particle clean-up");
+    std::swap(s->d_pos, s->d_pos2);
+    std::swap(s->d_vel, s->d_vel2);
+    s->stats.particles_removed = s->np - s->h_r2[0];
+    if (advected) s->stats.advect_capped = s->h_r2[1];
+    s->np = s->h_r2[0];
+    return FP_OK;
+}
+
+// frameStep, FluidSolver2D.cu:1302-1331
+int one_step_ref2d(fp_solver* s) {
+    int rc = r2_alloc(s);
+    if (rc) return rc;
+    cudaEventRecord(s->ev[0], s->st);
+    r2_label(s);
+    cudaEventRecord(s->ev[1], s->st);
+    r2_p2g(s, 1);  // P2G + save + forces
+    cudaEventRecord(s->ev[2], s->st);
+    rc = r2_pressure(s);
+    cudaEventRecord(s->ev[3], s->st);
+    if (rc != FP_OK) return rc;
+    r2_project(s);
+    cudaEventRecord(s->ev[4], s->st);
+    r2_particles(s, 7);  // G2P, advection, clean-up
+    cudaEventRecord(s->ev[5], s->st);
+    rc = r2_compact(s, true);
+    if (rc != FP_OK) return rc;
+    float t[5];
+    for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&t[i], s->ev[i], s->ev[i + 1]);
+    s->stats.t_label = t[0];
+    s->stats.t_p2g = t[1];
+    s->stats.t_forces = 0.0f;
+    s->stats.t_pressure = t[2];
+    s->stats.t_project = t[3];
+    s->stats.t_body = 0.0f;
+    s->stats.t_g2p = 0.0f;
+    s->stats.t_advect = t[4];
+    cudaEventElapsedTime(&s->stats.t_total, s->ev[0], s->ev[5]);
+    ++s->steps;
+    s->stats.step = s->steps;
+    s->stats.num_particles = s->np;
+    s->stats.kernel_launches = s->launches;
+    return FP_OK;
+}
+
 int check_ready(fp_solver* s) {
     if (!s) return FP_ERR_ARG;
     if (!s->have_grid) return s->fail(FP_ERR_STATE, "labels not loaded");
@@ -550,6 +673,7 @@ int check_ready(fp_solver* s) {
 }
 
 int one_step(fp_solver* s) {
+    if (ref2d(s)) return one_step_ref2d(s);
     cudaEventRecord(s->ev[0], s->st);
     phase_label(s);
     cudaEventRecord(s->ev[1], s->st);
@@ -679,6 +803,12 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
         delete s;
         return FP_ERR_ARG;
     }
+    if ((s->cfg.scheme != FP_SCHEME_DEFAULT && s->cfg.scheme != FP_SCHEME_REF2D) ||
+        (s->cfg.scheme == FP_SCHEME_REF2D && s->cfg.dim != 2)) {
+        std::fprintf(stderr, "fp_create: scheme %d with dim %d\n", s->cfg.scheme, s->cfg.dim);
+        delete s;
+        return FP_ERR_ARG;
+    }
     cudaError_t e = cudaSuccess;
     if (s->cfg.device >= 0) e = cudaSetDevice(s->cfg.device);  // the calling thread's device from here on
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
@@ -691,6 +821,7 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_bad, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&s->d_bad, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_bforce, sizeof(double) * 6);
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_r2, sizeof(int) * 2);
     if (e != cudaSuccess) {
         std::fprintf(stderr, "fp_create: %s\n", cudaGetErrorString(e));
         fp_destroy(s);
@@ -707,6 +838,7 @@ int fp_destroy(fp_solver* s) {
     free_particles(s);
     free_body(s);
     if (s->h_bforce) cudaFreeHost(s->h_bforce);
+    if (s->h_r2) cudaFreeHost(s->h_r2);
     for (auto& ev : s->ev) if (ev) cudaEventDestroy(ev);
     for (auto& ev : s->ev_pcg) if (ev) cudaEventDestroy(ev);
     if (s->ev_net) cudaEventDestroy(s->ev_net);
@@ -899,18 +1031,23 @@ int fp_run(fp_solver* s, int frames) {
         csv = std::fopen(cp.c_str(), "w");
         if (csv) std::fprintf(csv, "frame,centerX1,centerX2,centerX3,angleX1,angleX2,angleX3\n");
     }
-    phase_label(s);  // run() labels once before the loop (FluidSolver3D.cu:3110)
     std::vector<float> pos, vel;
-    for (int64_t i = 0; i <= int64_t(frames) * ipf; ++i) {  // inclusive bound, :3111
+    // FluidSolver3D::run labels once before its loop and takes frames * ipf + 1
+    // steps (FluidSolver3D.cu:3110-3111); FluidSolver2D::run takes max_steps
+    // steps and writes every one of them (FluidSolver2D.cu:1333-1342).
+    const bool r2 = ref2d(s);
+    if (!r2) phase_label(s);
+    const int64_t last = r2 ? int64_t(frames) - 1 : int64_t(frames) * ipf;
+    for (int64_t i = 0; i <= last; ++i) {
         rc = one_step(s);
         if (rc) break;
-        if (i % ipf == 0 && s->cfg.output_format != FP_OUT_NONE) {
+        if ((r2 || i % ipf == 0) && s->cfg.output_format != FP_OUT_NONE) {
             pos.resize(size_t(s->np) * 3);
             vel.resize(size_t(s->np) * 3);
             rc = fp_get_particles(s, pos.data(), vel.data(), s->np);
             if (rc) break;
             const char* ext = s->cfg.output_format == FP_OUT_OFF ? ".off" : ".ply";
-            std::string path = tmpl + std::to_string(i / ipf) + ext;
+            std::string path = tmpl + std::to_string(r2 ? i : i / ipf) + ext;
             if (!io::write_particles(path, pos.data(), vel.data(), s->np, s->cfg.output_format, s->err)) {
                 rc = FP_ERR_IO;
                 break;
@@ -930,6 +1067,30 @@ int fp_run(fp_solver* s, int frames) {
 int fp_run_phase(fp_solver* s, int phase) {
     int rc = check_ready(s);
     if (rc) return rc;
+    if (ref2d(s)) {
+        rc = r2_alloc(s);
+        if (rc) return rc;
+        switch (phase) {
+            case FP_PHASE_LABEL: r2_label(s); break;
+            case FP_PHASE_P2G: r2_p2g(s, 0); break;
+            case FP_PHASE_SAVE: phase_save(s); break;
+            case FP_PHASE_FORCES: launch_r2_forces(s->d_u, s->d_v, s->g, s->cfg.dt, s->st); s->launches += 1; break;
+            case FP_PHASE_PRESSURE: rc = r2_pressure(s); break;
+            case FP_PHASE_PROJECT: r2_project(s); break;
+            case FP_PHASE_BODY: break;
+            case FP_PHASE_G2P: r2_particles(s, 1); break;
+            case FP_PHASE_ADVECT:
+                r2_particles(s, 2);
+                if (s->np) cudaMemcpyAsync(s->h_r2 + 1, s->r2.misc + 2, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+                break;
+            case FP_PHASE_CLEANUP: r2_particles(s, 4); rc = r2_compact(s, false); break;
+            default: return s->fail(FP_ERR_ARG, "unknown phase");
+        }
+        cudaError_t e = cudaStreamSynchronize(s->st);
+        if (e != cudaSuccess) return s->cuda_fail(e, "phase");
+        if (phase == FP_PHASE_ADVECT && s->np) s->stats.advect_capped = s->h_r2[1];
+        return rc;
+    }
     switch (phase) {
         case FP_PHASE_LABEL: phase_label(s); break;
         case FP_PHASE_P2G: phase_p2g(s, 0); break;

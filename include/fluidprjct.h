@@ -65,6 +65,15 @@ enum { FP_SOLVER_PCG = 0, FP_SOLVER_PCG_MIXED = 1, FP_SOLVER_PCG_MG = 2, FP_SOLV
  * FluidSolver3D.cu:1241-1330) or midpoint RK2 with the same substepping. */
 enum { FP_ADVECT_RK3REF = 0, FP_ADVECT_RK2 = 1 };
 
+/* Step scheme.  FP_SCHEME_DEFAULT runs the 3D scheme of FluidSolver3D.cu on
+ * any grid (a 2D grid is its depth-1 case).  FP_SCHEME_REF2D (dim = 2 only)
+ * runs FluidSolver2D.cu's own step (:1302-1331): cell-centre-weighted P2G,
+ * VEL_UNKNOWN faces, 1D-linear G2P, Euler advection with projection into the
+ * nearest SOLID cell, and particle deletion; particles keep their order and
+ * fp_num_particles shrinks as they are deleted.  Its fp_config.advection and
+ * cfl are unused (the reference fixes Euler and C = 1). */
+enum { FP_SCHEME_DEFAULT = 0, FP_SCHEME_REF2D = 1 };
+
 /* Grid selectors for fp_get_grid / fp_set_grid.  FP_GRID_RHS (read only) is
  * the dense right-hand side of the last pressure solve, zero off FLUID cells
  * (the reference's RHS, FluidSolver3D.cu:1518-1596, before compaction). */
@@ -73,7 +82,8 @@ enum { FP_GRID_U = 0, FP_GRID_V = 1, FP_GRID_W = 2, FP_GRID_U_SAVED = 3, FP_GRID
 
 /* Step phases for fp_run_phase, in frameStep order (FluidSolver3D.cu:3030-3098). */
 enum { FP_PHASE_LABEL = 0, FP_PHASE_P2G = 1, FP_PHASE_SAVE = 2, FP_PHASE_FORCES = 3, FP_PHASE_PRESSURE = 4,
-       FP_PHASE_PROJECT = 5, FP_PHASE_BODY = 6, FP_PHASE_G2P = 7, FP_PHASE_ADVECT = 8 };
+       FP_PHASE_PROJECT = 5, FP_PHASE_BODY = 6, FP_PHASE_G2P = 7, FP_PHASE_ADVECT = 8,
+       FP_PHASE_CLEANUP = 9 /* FP_SCHEME_REF2D only: cleanUpParticles, FluidSolver2D.cu:1171-1204 */ };
 
 /* Solver configuration.  Keys and defaults follow main.cpp:17-52 and the
  * member initialisers of FluidSolver3D.cuh:72-80,160-166; the fields after
@@ -100,6 +110,7 @@ typedef struct fp_config {
     float    body_radius;          /* analytic sphere SDF radius; 0 = SDF file     */
     float    body_density;         /* sphere density relative to water            */
     int      device;               /* CUDA device ordinal; -1 = current device     */
+    int      scheme;               /* FP_SCHEME_* (default FP_SCHEME_DEFAULT)      */
 } fp_config;
 
 /* Per-step statistics: the reference's cudaEvent phase timers
@@ -123,6 +134,10 @@ typedef struct fp_step_stats {
     int64_t kernel_launches;   /* kernels this library launched, cumulative     */
     float   t_pcg;             /* device time of the pressure solve, last step  */
     float   t_learned;         /* of which the learned initial guess            */
+    int64_t particles_removed; /* FP_SCHEME_REF2D: deleted by the last clean-up  */
+    int32_t advect_capped;     /* FP_SCHEME_REF2D: particles whose substep loop
+                                  hit its bound in the last step                */
+    int32_t pad2_;
 } fp_step_stats;
 
 typedef struct fp_solver fp_solver;

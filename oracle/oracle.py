@@ -1,10 +1,12 @@
-"""ctypes binding of the CPU oracle (``oracle/fluid_oracle.cpp``).
+"""ctypes binding of the CPU oracle (``oracle/fluid_oracle.cpp``,
+``oracle/ref2d_oracle.cpp``).
 
 TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
 and ``bench.py``'s CPU-baseline / reference legs, never by the product package.
 The oracle restates Ship-Vano/FluidPrjct's 3D PIC/FLIP step
-(``src/FluidSim/FluidSolver3D.cu``) on the CPU; see the header of
-``fluid_oracle.cpp`` for the arithmetic modes and the pins.
+(``src/FluidSim/FluidSolver3D.cu``, class ``Sim3``) and its own 2D step
+(``src/FluidSim/FluidSolver2D.cu``, class ``Ref2D``) on the CPU; the headers
+of the two C++ files give the arithmetic modes and the pins.
 """
 from __future__ import annotations
 
@@ -19,13 +21,14 @@ _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 _lib = None
 
 GRID_U, GRID_V, GRID_W, GRID_US, GRID_VS, GRID_WS, GRID_P = range(7)
-PH_LABEL, PH_P2G, PH_SAVE, PH_FORCES, PH_PRESSURE, PH_PROJECT, PH_BODY, PH_G2P, PH_ADVECT = range(9)
+PH_LABEL, PH_P2G, PH_SAVE, PH_FORCES, PH_PRESSURE, PH_PROJECT, PH_BODY, PH_G2P, PH_ADVECT, PH_CLEANUP = range(10)
+VEL_UNKNOWN = float(np.float32(-2.0 ** 31))  # INT_MIN stored in a float grid (utility.cuh:56)
 
 
 def build(force: bool = False) -> str:
     """Compile the oracle with its Makefile (g++, OpenMP) and return the .so path."""
-    src = os.path.join(_HERE, "fluid_oracle.cpp")
-    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+    srcs = [os.path.join(_HERE, f) for f in ("fluid_oracle.cpp", "ref2d_oracle.cpp")]
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < max(map(os.path.getmtime, srcs)):
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 
@@ -70,6 +73,22 @@ def lib():
         L.or3_apply.argtypes = [P, P, P]
         L.or3_stats.argtypes = [P, P]
         L.or_num_threads.restype = I
+        L.or2r_create.argtypes = [I, I, D, D, I]
+        L.or2r_create.restype = P
+        L.or2r_destroy.argtypes = [P]
+        L.or2r_set_params.argtypes = [P, D, D, I]
+        L.or2r_set_labels.argtypes = [P, P]
+        L.or2r_get_labels.argtypes = [P, P]
+        L.or2r_set_particles.argtypes = [P, I64, P, P]
+        L.or2r_num_particles.argtypes = [P]
+        L.or2r_num_particles.restype = I64
+        L.or2r_get_particles.argtypes = [P, P, P]
+        L.or2r_grid_len.argtypes = [P, I]
+        L.or2r_grid_len.restype = I64
+        L.or2r_grid_io.argtypes = [P, I, P, I]
+        L.or2r_phase.argtypes = [P, I]
+        L.or2r_step.argtypes = [P, I]
+        L.or2r_stats.argtypes = [P, P]
     return _lib
 
 
@@ -254,6 +273,69 @@ class Sim3:
         out = np.zeros(3, np.float64)
         lib().or3_stats(self.h, _p(out))
         return {"iters": int(out[0]), "relres": float(out[1]), "nf": int(out[2])}
+
+
+class Ref2D:
+    """Oracle of the reference's own 2D step (FluidSolver2D.cu); fp64=False
+    follows its FP32 expression order.  Phases as in ``Sim3`` plus
+    PH_CLEANUP; labels are (H, W), particles n x 3 with z ignored."""
+
+    def __init__(self, W, H, dx, dt, fp64=False, pic_weight=0.5, tol=1e-12, maxit=100000):
+        self.W, self.H = W, H
+        self.h = lib().or2r_create(W, H, dx, dt, int(fp64))
+        lib().or2r_set_params(self.h, pic_weight, tol, maxit)
+
+    def close(self):
+        if self.h:
+            lib().or2r_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_labels(self, labels):
+        lab = np.ascontiguousarray(labels, np.uint8).reshape(-1)
+        assert lab.size == self.W * self.H
+        lib().or2r_set_labels(self.h, _p(lab))
+
+    def labels(self):
+        out = np.zeros(self.W * self.H, np.uint8)
+        lib().or2r_get_labels(self.h, _p(out))
+        return out.reshape(self.H, self.W)
+
+    def set_particles(self, pos, vel=None):
+        pos = np.ascontiguousarray(pos, np.float32)
+        v = None if vel is None else np.ascontiguousarray(vel, np.float32)
+        lib().or2r_set_particles(self.h, len(pos), _p(pos), None if v is None else _p(v))
+
+    def particles(self):
+        n = lib().or2r_num_particles(self.h)
+        pos = np.zeros((n, 3), np.float64)
+        vel = np.zeros((n, 3), np.float64)
+        lib().or2r_get_particles(self.h, _p(pos), _p(vel))
+        return pos, vel
+
+    def grid(self, which):
+        n = lib().or2r_grid_len(self.h, which)
+        out = np.zeros(n, np.float64)
+        lib().or2r_grid_io(self.h, which, _p(out), 0)
+        return out
+
+    def set_grid(self, which, data):
+        n = lib().or2r_grid_len(self.h, which)
+        a = np.ascontiguousarray(data, np.float64).reshape(-1)
+        assert a.size == n
+        lib().or2r_grid_io(self.h, which, _p(a), 1)
+
+    def phase(self, ph):
+        return lib().or2r_phase(self.h, ph)
+
+    def step(self, n=1):
+        return lib().or2r_step(self.h, n)
+
+    def stats(self):
+        out = np.zeros(4, np.int64)
+        lib().or2r_stats(self.h, _p(out))
+        return {"nf": int(out[0]), "cg_iters": int(out[1]), "removed": int(out[2]), "capped": int(out[3])}
 
 
 def num_threads() -> int:

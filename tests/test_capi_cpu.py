@@ -42,6 +42,18 @@ def test_config_defaults_match_reference():
     assert list(c.body_pos) == pytest.approx([0.5, 0.5, 0.5])
     assert c.output_template == b"InputData/particles_"
     assert c.solver == capi.SOLVER_PCG and c.advection == capi.ADVECT_RK3REF
+    assert c.scheme == capi.SCHEME_DEFAULT
+    # the ctypes mirrors have the C sizes (int64 + int32 x 2 appended to the stats)
+    assert C.sizeof(capi.FpStepStats) % 8 == 0
+
+
+def test_create_rejects_bad_schemes():
+    """fp_create checks the configuration before touching the GPU."""
+    from fluidprjct_b200 import capi
+    for kw in ({"dim": 3, "scheme": capi.SCHEME_REF2D}, {"dim": 2, "scheme": 7}):
+        cfg = capi.default_config(**kw)
+        h = C.c_void_p()
+        assert capi.lib().fp_create(C.byref(cfg), C.byref(h)) == capi.FP_ERR_ARG and not h.value
 
 
 def test_config_json(tmp_path):
