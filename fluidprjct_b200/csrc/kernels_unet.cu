@@ -67,9 +67,9 @@ __device__ __forceinline__ void load_halo(bf16* sx, const bf16* __restrict__ xa,
         const bool in = gx >= 0 && gx < lv.W && gy >= 0 && gy < lv.H && gz >= 0 && gz < lv.D;
         const bf16* src;
         if (CA > 0 && ch * 8 < CA)
-            src = in ? xa + ((int64_t(gz >> 1) * lc.H + (gy >> 1)) * lc.W + (gx >> 1)) * CA + ch * 8 : xa;
+            src = in ? xa + blk8(lc.n(), (int64_t(gz >> 1) * lc.H + (gy >> 1)) * lc.W + (gx >> 1), ch) : xa;
         else
-            src = in ? xb + ((int64_t(gz) * lv.H + gy) * lv.W + gx) * CB + (ch * 8 - CA) : xb;
+            src = in ? xb + blk8(lv.n(), (int64_t(gz) * lv.H + gy) * lv.W + gx, ch - CA / 8) : xb;
         cp_async16(sx + hv * RS + ch * 8, src, in);
     }
 }
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(THREADS) k_corr3(CorrArgs a) {
             const int ch = i % (COUT / 8), v = i / (COUT / 8);
             const int gx = bx * BX + (v & 7), gy = by * BY + ((v >> 3) & 7), gz = bz * BZ + (v >> 6);
             const bool in = gx < a.lv.W && gy < a.lv.H && gz < a.lv.D;
-            const bf16* src = in ? a.g + ((int64_t(gz) * a.lv.H + gy) * a.lv.W + gx) * COUT + ch * 8 : a.g;
+            const bf16* src = in ? a.g + blk8(a.lv.n(), (int64_t(gz) * a.lv.H + gy) * a.lv.W + gx, ch) : a.g;
             cp_async16(sg + v * GS + ch * 8, src, in);
         }
         cp_async_wait_all();
@@ -234,9 +234,8 @@ __global__ void k_input(const uint8_t* __restrict__ lab, const float* __restrict
     v[1] = __float2bfloat16_rn(l == 1 ? 1.0f : 0.0f);
     v[2] = __float2bfloat16_rn(l == 2 ? 1.0f : 0.0f);
     v[3] = __float2bfloat16_rn((l == 0 || l == 3) ? 1.0f : 0.0f);
-    uint4* dst = reinterpret_cast<uint4*>(x0 + t * 16);
-    dst[0] = reinterpret_cast<const uint4*>(v)[0];
-    dst[1] = reinterpret_cast<const uint4*>(v)[1];
+    *reinterpret_cast<uint4*>(x0 + blk8(net.n(), t, 0)) = reinterpret_cast<const uint4*>(v)[0];
+    *reinterpret_cast<uint4*>(x0 + blk8(net.n(), t, 1)) = reinterpret_cast<const uint4*>(v)[1];
 }
 
 __device__ __forceinline__ void load8(const bf16* p, float* f) {
@@ -257,27 +256,27 @@ __device__ __forceinline__ void store8(bf16* p, const float* f) {
     *reinterpret_cast<uint4*>(p) = u;
 }
 
-// One thread per (coarse voxel, 8 channels).  Fine dims are even.
+// One thread per (coarse voxel, 8 channels), voxels fastest.  Fine dims are even.
 __global__ void k_pool(const bf16* __restrict__ e, Lvl fine, int C, bf16* __restrict__ q) {
     const int CH = C / 8;
     const Lvl cl{fine.W / 2, fine.H / 2, fine.D / 2};
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= cl.n() * CH) return;
-    const int ch = int(t % CH);
-    const int64_t V = t / CH;
+    const int64_t V = t % cl.n();
+    const int ch = int(t / cl.n());
     const int I = int(V % cl.W), J = int((V / cl.W) % cl.H), K = int(V / (int64_t(cl.W) * cl.H));
     float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int dz = 0; dz < 2; ++dz)
         for (int dy = 0; dy < 2; ++dy)
             for (int dx = 0; dx < 2; ++dx) {
                 float f[8];
-                load8(e + ((int64_t(2 * K + dz) * fine.H + 2 * J + dy) * fine.W + 2 * I + dx) * C + ch * 8, f);
+                load8(e + blk8(fine.n(), (int64_t(2 * K + dz) * fine.H + 2 * J + dy) * fine.W + 2 * I + dx, ch), f);
 #pragma unroll
                 for (int c = 0; c < 8; ++c) s[c] += f[c];
             }
 #pragma unroll
     for (int c = 0; c < 8; ++c) s[c] *= 0.125f;
-    store8(q + V * C + ch * 8, s);
+    store8(q + blk8(cl.n(), V, ch), s);
 }
 
 // g[V][c] = (sum over the 8 children of raw[child][c]) * (act[V][c] > 0), c < C.
@@ -287,23 +286,23 @@ __global__ void k_sum_children_mask(const bf16* __restrict__ raw, Lvl fine, int 
     const Lvl cl{fine.W / 2, fine.H / 2, fine.D / 2};
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= cl.n() * CH) return;
-    const int ch = int(t % CH);
-    const int64_t V = t / CH;
+    const int64_t V = t % cl.n();
+    const int ch = int(t / cl.n());
     const int I = int(V % cl.W), J = int((V / cl.W) % cl.H), K = int(V / (int64_t(cl.W) * cl.H));
     float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int dz = 0; dz < 2; ++dz)
         for (int dy = 0; dy < 2; ++dy)
             for (int dx = 0; dx < 2; ++dx) {
                 float f[8];
-                load8(raw + ((int64_t(2 * K + dz) * fine.H + 2 * J + dy) * fine.W + 2 * I + dx) * ctot + ch * 8, f);
+                load8(raw + blk8(fine.n(), (int64_t(2 * K + dz) * fine.H + 2 * J + dy) * fine.W + 2 * I + dx, ch), f);
 #pragma unroll
                 for (int c = 0; c < 8; ++c) s[c] += f[c];
             }
     float m[8];
-    load8(act + V * C + ch * 8, m);
+    load8(act + blk8(cl.n(), V, ch), m);
 #pragma unroll
     for (int c = 0; c < 8; ++c) s[c] = m[c] > 0.0f ? s[c] : 0.0f;
-    store8(gout + V * C + ch * 8, s);
+    store8(gout + blk8(cl.n(), V, ch), s);
 }
 
 // g[v][c] = (raw[v][ca + c] + gq[v>>1][c] / 8) * (act[v][c] > 0), c < C.
@@ -312,17 +311,17 @@ __global__ void k_skip_combine(const bf16* __restrict__ raw, Lvl fine, int ctot,
     const int CH = C / 8;
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= fine.n() * CH) return;
-    const int ch = int(t % CH);
-    const int64_t v = t / CH;
+    const int64_t v = t % fine.n();
+    const int ch = int(t / fine.n());
     const int i = int(v % fine.W), j = int((v / fine.W) % fine.H), k = int(v / (int64_t(fine.W) * fine.H));
     const Lvl cl{fine.W / 2, fine.H / 2, fine.D / 2};
     float r[8], q[8], m[8];
-    load8(raw + v * ctot + ca + ch * 8, r);
-    load8(gq + ((int64_t(k >> 1) * cl.H + (j >> 1)) * cl.W + (i >> 1)) * C + ch * 8, q);
-    load8(act + v * C + ch * 8, m);
+    load8(raw + blk8(fine.n(), v, ca / 8 + ch), r);
+    load8(gq + blk8(cl.n(), (int64_t(k >> 1) * cl.H + (j >> 1)) * cl.W + (i >> 1), ch), q);
+    load8(act + blk8(fine.n(), v, ch), m);
 #pragma unroll
     for (int c = 0; c < 8; ++c) r[c] = m[c] > 0.0f ? r[c] + 0.125f * q[c] : 0.0f;
-    store8(gout + v * C + ch * 8, r);
+    store8(gout + blk8(fine.n(), v, ch), r);
 }
 
 __global__ void __launch_bounds__(THREADS) k_loss_part(const uint8_t* __restrict__ lab, const float* __restrict__ p,
@@ -377,15 +376,15 @@ __global__ void __launch_bounds__(THREADS) k_head_bwd(const uint8_t* __restrict_
             go = (out[t] - tv) * k2;
         }
         float f[16], o[16];
-        load8(d0 + t * 16, f);
-        load8(d0 + t * 16 + 8, f + 8);
+        load8(d0 + blk8(net.n(), t, 0), f);
+        load8(d0 + blk8(net.n(), t, 1), f + 8);
 #pragma unroll
         for (int c = 0; c < 16; ++c) {
             o[c] = f[c] > 0.0f ? go * hw[c] : 0.0f;
             hp[c] += double(go) * double(f[c]);
         }
-        store8(g9 + t * 16, o);
-        store8(g9 + t * 16 + 8, o + 8);
+        store8(g9 + blk8(net.n(), t, 0), o);
+        store8(g9 + blk8(net.n(), t, 1), o + 8);
     }
     block_sum_d<16>(hp, sh);
     if (threadIdx.x == 0)

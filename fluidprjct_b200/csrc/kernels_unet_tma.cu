@@ -117,11 +117,38 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Two accumulator sets, each TZ tiles of NCO columns (a power of two >= 32).
+// Layers with 16 output channels stack the three z taps in N ("dz in N"):
+// halo plane p (0 <= p < HZ), shifted by (dy, dx), is multiplied once by
+// [W(dz=-1); W(0); W(+1)] (N = 48) into its own 48 accumulator columns; the
+// dz block of plane p feeds output tile zo = p - 1 - dz.  Output tile zo adds
+// plane zo's dz=-1 block, plane zo+1's dz=0 block and plane zo+2's dz=+1
+// block: the same TMEM lanes, so the sum stays in one thread.  Each A tile is
+// read 9 times per group instead of 27, which is what the 16-wide MMAs are
+// bound by (their shared-memory operand reads).  Every MMA has the same shape
+// (changing N between consecutive MMAs stalls the tensor pipe).  The edge
+// planes' unused dz blocks overlap in pairs: plane 0 uses only dz = -1 and
+// plane 5 only dz = +1, plane 1 drops dz = +1 and plane 4 dz = -1, so one
+// set needs 240 columns instead of 288:
+//   plane   0    5    1    4    2    3
+//   column  0   16   64   96  144  192     (blocks of 16 per dz = -1, 0, +1)
+static_assert(TZ == 4, "the dz-in-N column table is laid out for four tiles");
+__host__ __device__ constexpr int dzn_col(int p) {
+    return p == 0 ? 0 : p == 5 ? 16 : p == 1 ? 64 : p == 4 ? 96 : p == 2 ? 144 : 192;
+}
+constexpr int DZN_SET_COLS = 240;
+// first column of output tile zo's dz partial
+__host__ __device__ constexpr int dzn_block_col(int zo, int dz) { return dzn_col(zo + 1 + dz) + (dz + 1) * 16; }
+
+// NSET accumulator sets of TZ tiles x NCO columns, or of the dz-in-N
+// blocks, allocated as a power of two >= 32.  Two sets let a brick's
+// epilogue overlap the next brick's MMAs inside the CTA; one set leaves
+// room for two CTAs per SM, whose MMA streams then interleave.
 template <int NCO>
+constexpr int set_cols() { return NCO == 16 ? DZN_SET_COLS : TZ * NCO; }
+template <int NCO, int NSET>
 constexpr int tmem_cols() {
-    return (2 * TZ * NCO <= 32) ? 32 : (2 * TZ * NCO <= 64) ? 64 : (2 * TZ * NCO <= 128) ? 128
-                                                                  : (2 * TZ * NCO <= 256) ? 256 : 512;
+    constexpr int c = NSET * set_cols<NCO>();
+    return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512;
 }
 template <int CIN, int NCO, int NST>
 constexpr size_t smem_bytes() {
@@ -129,11 +156,16 @@ constexpr size_t smem_bytes() {
     return size_t(NST) * STAGE_BYTES + size_t(27) * CIN * NCO * 2 + 8 * (2 * NST + 5) + 16 + 128;
 }
 
-template <int CIN, int COUT, int NCO, int EPI, int NST>
+template <int CIN, int COUT, int NCO, int EPI, int NST, int NSET>
 __global__ void __launch_bounds__(THREADS) k_conv3_tma(const __grid_constant__ CUtensorMap tin, TmaConvArgs a) {
     constexpr int G = CIN / 16;
-    constexpr int LA = NST - 1;  // loads in flight ahead of the MMAs
-    constexpr int NCOLS = tmem_cols<NCO>();
+    // loads issued ahead of the MMAs; with four or more stages two MMA batches
+    // stay in flight (the stage wait then covers the batch before the last)
+    constexpr int LA = NST >= 4 ? NST - 2 : NST - 1;
+    constexpr int NCOLS = tmem_cols<NCO, NSET>();
+    static_assert(NSET == 1 || NSET == 2, "accumulator sets");
+    constexpr bool DZN = NCO == 16;
+    constexpr uint32_t SET = uint32_t(set_cols<NCO>());
     constexpr uint32_t IDESC = umma_idesc_bf16(NCO);
     static_assert(CIN % 16 == 0 && NCO % 16 == 0 && NCO <= 48 && COUT % NCO == 0 && NST >= 2, "tiling");
     static_assert(EPI != EPI_HEAD || (NCO == 16 && COUT == 16), "the head needs all 16 channels");
@@ -170,10 +202,20 @@ __global__ void __launch_bounds__(THREADS) k_conv3_tma(const __grid_constant__ C
         mbar_init(spare, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
+    // weights, K-major: [tap][chunk][co][8], or [dy,dx][chunk][dz][co][8] for dz in N
     for (int i = tid; i < 27 * NCO * (CIN / 8); i += THREADS) {
-        const int co = i % NCO, c = (i / NCO) % (CIN / 8), tap = i / (NCO * (CIN / 8));
-        cp_async16(sB + uint32_t(((tap * (CIN / 8) + c) * NCO + co) * 16),
-                   a.w + (int64_t(tap) * COUT + cog * NCO + co) * CIN + c * 8);
+        int co, c, tap;
+        if constexpr (DZN) {
+            co = i % 16;
+            const int dz = (i / 16) % 3;
+            c = (i / 48) % (CIN / 8);
+            tap = dz * 9 + i / (48 * (CIN / 8));
+        } else {
+            co = i % NCO;
+            c = (i / NCO) % (CIN / 8);
+            tap = i / (NCO * (CIN / 8));
+        }
+        cp_async16(sB + uint32_t(i * 16), a.w + (int64_t(tap) * COUT + cog * NCO + co) * CIN + c * 8);
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -198,25 +240,43 @@ __global__ void __launch_bounds__(THREADS) k_conv3_tma(const __grid_constant__ C
             auto mma_step = [&](int t) {
                 const int sl = t % NST, use = t / NST, i = t / G, g = t % G;
                 if (!mbar_wait_bounded(full0 + 8u * sl, uint32_t(use & 1))) return fail();
-                if (g == 0 && i >= 2 && !mbar_wait_bounded(acce0 + 8u * (i & 1), uint32_t(((i >> 1) - 1) & 1)))
+                if (g == 0 && i >= NSET &&
+                    !mbar_wait_bounded(acce0 + 8u * (i % NSET), uint32_t((i / NSET - 1) & 1)))
                     return fail();
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const uint32_t stage = sStage + uint32_t(sl * STAGE_BYTES);
-                const uint32_t set = uint32_t(i & 1) * uint32_t(TZ * NCO);
-                // taps outer, tiles inner: the tiles' accumulation chains interleave
+                const uint32_t set = uint32_t(i % NSET) * SET;
+                if constexpr (DZN) {
+                    // shifts outer, planes inner: six accumulation chains interleave
 #pragma unroll 1
-                for (int tap = 0; tap < 27; ++tap) {
-                    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-                    const uint64_t bd = umma_desc(sB + uint32_t((tap * (CIN / 8) + 2 * g) * NCO * 16), NCO * 16, 128);
+                    for (int sh = 0; sh < 9; ++sh) {
+                        const int dy = sh / 3 - 1, dx = sh % 3 - 1;
+                        const uint64_t bd =
+                            umma_desc(sB + uint32_t((sh * (CIN / 8) + 2 * g) * 3 * 16 * 16), 3 * 16 * 16, 128);
 #pragma unroll
-                    for (int zo = 0; zo < TZ; ++zo) {
-                        const int hv0 = ((zo + 1 + dz) * HY + (1 + dy)) * HX + (1 + dx);
-                        const uint64_t ad = umma_desc(stage + uint32_t(hv0 * 16), PLANE_BYTES, HX * 16);
-                        umma_bf16(tmem + set + uint32_t(zo * NCO), ad, bd, IDESC, (g | tap) != 0 ? 1u : 0u);
+                        for (int p = 0; p < HZ; ++p) {
+                            const int hv0 = (p * HY + (1 + dy)) * HX + (1 + dx);
+                            const uint64_t ad = umma_desc(stage + uint32_t(hv0 * 16), PLANE_BYTES, HX * 16);
+                            umma_bf16(tmem + set + uint32_t(dzn_col(p)), ad, bd, umma_idesc_bf16(48),
+                                      (g | sh) != 0 ? 1u : 0u);
+                        }
+                    }
+                } else {
+                    // taps outer, tiles inner: the tiles' accumulation chains interleave
+#pragma unroll 1
+                    for (int tap = 0; tap < 27; ++tap) {
+                        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+                        const uint64_t bd = umma_desc(sB + uint32_t((tap * (CIN / 8) + 2 * g) * NCO * 16), NCO * 16, 128);
+#pragma unroll
+                        for (int zo = 0; zo < TZ; ++zo) {
+                            const int hv0 = ((zo + 1 + dz) * HY + (1 + dy)) * HX + (1 + dx);
+                            const uint64_t ad = umma_desc(stage + uint32_t(hv0 * 16), PLANE_BYTES, HX * 16);
+                            umma_bf16(tmem + set + uint32_t(zo * NCO), ad, bd, IDESC, (g | tap) != 0 ? 1u : 0u);
+                        }
                     }
                 }
                 umma_commit(empty0 + 8u * sl);
-                if (g == G - 1) umma_commit(accf0 + 8u * (i & 1));
+                if (g == G - 1) umma_commit(accf0 + 8u * (i % NSET));
             };
             for (int s = 0; s < steps && ok; ++s) {
                 const int sl = s % NST, use = s / NST, i = s / G, g = s % G;
@@ -228,9 +288,10 @@ __global__ void __launch_bounds__(THREADS) k_conv3_tma(const __grid_constant__ C
                 const int bx = brick % nbx, by = (brick / nbx) % nby, bz = brick / (nbx * nby);
                 const uint32_t stage = sStage + uint32_t(sl * STAGE_BYTES);
                 mbar_expect_tx(full0 + 8u * sl, STAGE_BYTES);
-                tma_load_4d(stage, &tin, full0 + 8u * sl, 16 * g, bx * TX - 1, by * TY - 1, bz * TZ - 1);
-                tma_load_4d(stage + PLANE_BYTES, &tin, full0 + 8u * sl, 16 * g + 8, bx * TX - 1, by * TY - 1,
-                            bz * TZ - 1);
+                // (8 channels x 10 voxels) rows of 160 bytes; x = 8 (bx TX - 1) is a multiple of 8 elements
+                tma_load_4d(stage, &tin, full0 + 8u * sl, 8 * (bx * TX - 1), by * TY - 1, bz * TZ - 1, 2 * g);
+                tma_load_4d(stage + PLANE_BYTES, &tin, full0 + 8u * sl, 8 * (bx * TX - 1), by * TY - 1, bz * TZ - 1,
+                            2 * g + 1);
                 if (s >= LA) mma_step(s - LA);
             }
             for (int t = max(0, steps - LA); t < steps && ok; ++t) mma_step(t);
@@ -245,7 +306,7 @@ __global__ void __launch_bounds__(THREADS) k_conv3_tma(const __grid_constant__ C
         // epilogue warps: TMEM lanes 32 * warp .. 32 * warp + 31
         for (int i = 0; i < mine; ++i) {
             bool got = true;
-            if (lane == 0) got = mbar_wait_bounded(accf0 + 8u * (i & 1), uint32_t((i >> 1) & 1));
+            if (lane == 0) got = mbar_wait_bounded(accf0 + 8u * (i % NSET), uint32_t((i / NSET) & 1));
             got = __shfl_sync(0xffffffffu, got ? 1 : 0, 0) != 0;
             if (!got || *(volatile int*)&s_abort) {
                 if (lane == 0 && !got && a.status) atomicExch(a.status, DEV_TIMEOUT_CODE);
@@ -254,18 +315,29 @@ __global__ void __launch_bounds__(THREADS) k_conv3_tma(const __grid_constant__ C
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             const int brick = int(blockIdx.x) + i * int(gridDim.x);
             const int bx = brick % nbx, by = (brick / nbx) % nby, bz = brick / (nbx * nby);
-            const uint32_t set = uint32_t(i & 1) * uint32_t(TZ * NCO);
-#pragma unroll 1
+            const uint32_t set = uint32_t(i % NSET) * SET;
+            const uint32_t lanes = tmem + (uint32_t(warp * 32) << 16) + set;
+#pragma unroll
             for (int zo = 0; zo < TZ; ++zo) {
                 float v[NCO];
+                if constexpr (DZN) {
+                    float v1[16], v2[16];
+                    tmem_ld16(lanes + uint32_t(dzn_block_col(zo, -1)), v);
+                    tmem_ld16(lanes + uint32_t(dzn_block_col(zo, 0)), v1);
+                    tmem_ld16(lanes + uint32_t(dzn_block_col(zo, 1)), v2);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-                for (int j = 0; j < NCO / 16; ++j)
-                    tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + set + uint32_t(zo * NCO + 16 * j), v + 16 * j);
-                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                    for (int q = 0; q < 16; ++q) v[q] = (v[q] + v1[q]) + v2[q];
+                } else {
+#pragma unroll
+                    for (int j = 0; j < NCO / 16; ++j) tmem_ld16(lanes + uint32_t(zo * NCO + 16 * j), v + 16 * j);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                }
                 const int m = warp * 32 + lane;
                 const int gx = bx * TX + (m & 7), gy = by * TY + (m >> 3), gz = bz * TZ + zo;
                 if (gx >= a.lv.W || gy >= a.lv.H || gz >= a.lv.D) continue;
                 const int64_t vox = (int64_t(gz) * a.lv.H + gy) * a.lv.W + gx;
+                const int64_t nv = a.lv.n();
                 if (EPI == EPI_RELU || EPI == EPI_HEAD) {
 #pragma unroll
                     for (int q = 0; q < NCO; ++q) v[q] = fmaxf(v[q], 0.0f);
@@ -273,7 +345,7 @@ __global__ void __launch_bounds__(THREADS) k_conv3_tma(const __grid_constant__ C
                 if (EPI == EPI_MASK) {
 #pragma unroll
                     for (int q = 0; q < NCO / 8; ++q) {
-                        const uint4 mk = *reinterpret_cast<const uint4*>(a.mask + vox * COUT + cog * NCO + 8 * q);
+                        const uint4 mk = *reinterpret_cast<const uint4*>(a.mask + blk8(nv, vox, cog * (NCO / 8) + q));
                         const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&mk);
 #pragma unroll
                         for (int e = 0; e < 4; ++e) {
@@ -296,13 +368,13 @@ __global__ void __launch_bounds__(THREADS) k_conv3_tma(const __grid_constant__ C
                             hsum += f.x * a.head_w[8 * q + 2 * e] + f.y * a.head_w[8 * q + 2 * e + 1];
                         }
                     }
-                    *reinterpret_cast<uint4*>(a.y + vox * COUT + cog * NCO + 8 * q) = u;
+                    *reinterpret_cast<uint4*>(a.y + blk8(nv, vox, cog * (NCO / 8) + q)) = u;
                 }
                 if (EPI == EPI_HEAD) a.head_out[vox] = hsum;
             }
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(acce0 + 8u * (i & 1));
+            if (lane == 0) mbar_arrive(acce0 + 8u * (i % NSET));
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -311,22 +383,18 @@ __global__ void __launch_bounds__(THREADS) k_conv3_tma(const __grid_constant__ C
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(NCOLS));
 }
 
-// [up2(coarse) | skip]: the concatenated input of a decoder layer, materialised
-// so that TMA can read it.  One thread per (voxel, 8 channels).
-__global__ void k_upcat(const bf16* __restrict__ coarse, int ca, const bf16* __restrict__ skip, int cb, Lvl fine,
-                        bf16* __restrict__ out) {
-    const int ct = ca + cb, ch = ct / 8;
+// up2(coarse) into the first ca / 8 channel blocks of a decoder layer's input
+// [up2(coarse) | skip]; the skip tensor already lives in the blocks after
+// them.  One thread per (fine voxel, 8 channels), voxels fastest.
+__global__ void k_upcat(const bf16* __restrict__ coarse, int ca, Lvl fine, bf16* __restrict__ out) {
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= fine.n() * ch) return;
-    const int c = int(t % ch);
-    const int64_t v = t / ch;
+    if (t >= fine.n() * (ca / 8)) return;
+    const int64_t v = t % fine.n();
+    const int c = int(t / fine.n());
     const int i = int(v % fine.W), j = int((v / fine.W) % fine.H), k = int(v / (int64_t(fine.W) * fine.H));
     const Lvl cl{fine.W / 2, fine.H / 2, fine.D / 2};
-    const uint4 val = c * 8 < ca
-                          ? *reinterpret_cast<const uint4*>(
-                                coarse + ((int64_t(k >> 1) * cl.H + (j >> 1)) * cl.W + (i >> 1)) * ca + c * 8)
-                          : *reinterpret_cast<const uint4*>(skip + v * cb + (c * 8 - ca));
-    *reinterpret_cast<uint4*>(out + v * ct + c * 8) = val;
+    *reinterpret_cast<uint4*>(out + blk8(fine.n(), v, c)) = *reinterpret_cast<const uint4*>(
+        coarse + blk8(cl.n(), (int64_t(k >> 1) * cl.H + (j >> 1)) * cl.W + (i >> 1), c));
 }
 
 // ---- host side
@@ -345,25 +413,36 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     return g_encode;
 }
 
-// Tensor map of a [D][H][W][C] bf16 tensor read in 8-channel x 10 x 18 x 4 boxes.
+// Tensor map of a channel-blocked [C/8][D][H][W][8] bf16 tensor seen as
+// (8 W, H, D, C / 8): one box is an 8-channel halo plane of HX x HY x HZ
+// voxels, HY * HZ rows of 160 contiguous bytes.
 bool make_map(CUtensorMap* map, const bf16* ptr, int C, const Lvl& lv) {
     auto enc = encoder();
     if (!enc) return false;
-    const cuuint64_t dims[4] = {cuuint64_t(C), cuuint64_t(lv.W), cuuint64_t(lv.H), cuuint64_t(lv.D)};
-    const cuuint64_t strides[3] = {cuuint64_t(C) * 2, cuuint64_t(lv.W) * C * 2, cuuint64_t(lv.H) * lv.W * C * 2};
-    const cuuint32_t box[4] = {8, HX, HY, HZ};
+    const cuuint64_t dims[4] = {cuuint64_t(lv.W) * 8, cuuint64_t(lv.H), cuuint64_t(lv.D), cuuint64_t(C / 8)};
+    const cuuint64_t strides[3] = {cuuint64_t(lv.W) * 16, cuuint64_t(lv.H) * lv.W * 16,
+                                   cuuint64_t(lv.D) * lv.H * lv.W * 16};
+    const cuuint32_t box[4] = {8 * HX, HY, HZ, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(ptr), dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int CIN, int COUT, int NCO, int EPI, int NST = 2>
+// Pipelines: wide layers (NCO >= 32) run two CTAs per SM with two stages and
+// two accumulator sets; 16-wide layers with CIN <= 48 run two CTAs per SM
+// with one set; wider inputs run one CTA per SM with two sets and 4-5 stages.
+template <int CIN, int NCO>
+constexpr int pick_nst() { return NCO != 16 || CIN <= 48 ? 2 : CIN <= 64 ? 5 : 4; }
+template <int CIN, int NCO>
+constexpr int pick_nset() { return NCO == 16 && CIN <= 48 ? 1 : 2; }
+
+template <int CIN, int COUT, int NCO, int EPI, int NST = pick_nst<CIN, NCO>(), int NSET = pick_nset<CIN, NCO>()>
 int run_tma(const bf16* in, const TmaConvArgs& a, cudaStream_t st) {
     constexpr size_t smem = smem_bytes<CIN, NCO, NST>();
     static_assert(smem <= 232448, "shared memory of one CTA");
     static int per_sm = -1;
-    auto kern = k_conv3_tma<CIN, COUT, NCO, EPI, NST>;
+    auto kern = k_conv3_tma<CIN, COUT, NCO, EPI, NST, NSET>;
     if (per_sm < 0) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
@@ -378,7 +457,7 @@ int run_tma(const bf16* in, const TmaConvArgs& a, cudaStream_t st) {
         // resident CTAs per SM: shared memory (1 KB reserved per CTA), threads and
         // the 512 TMEM columns (the CTAs never wait on each other, so a grid above
         // the true residency only queues)
-        per_sm = std::max(1, std::min({smem_sm / int(smem + 1024), 2048 / THREADS, 512 / tmem_cols<NCO>()}));
+        per_sm = std::max(1, std::min({smem_sm / int(smem + 1024), 2048 / THREADS, 512 / tmem_cols<NCO, NSET>()}));
     }
     CUtensorMap map;
     std::memset(&map, 0, sizeof map);
@@ -419,9 +498,9 @@ int conv_backward_layer_tma(int layer, const bf16* in, const TmaConvArgs& a, cud
     return int(cudaErrorInvalidValue);
 }
 
-void launch_upcat(const bf16* coarse, int ca, const bf16* skip, int cb, Lvl fine, bf16* out, cudaStream_t st) {
-    const int64_t n = fine.n() * ((ca + cb) / 8);
-    k_upcat<<<unsigned((n + 255) / 256), 256, 0, st>>>(coarse, ca, skip, cb, fine, out);
+void launch_upcat(const bf16* coarse, int ca, Lvl fine, bf16* out, cudaStream_t st) {
+    const int64_t n = fine.n() * (ca / 8);
+    k_upcat<<<unsigned((n + 255) / 256), 256, 0, st>>>(coarse, ca, fine, out);
 }
 
 }  // namespace unet

@@ -77,9 +77,10 @@ const float* net_out(const fp_unet* u) { return u->out; }
 const float* net_scal(const fp_unet* u) { return u->scal; }
 const int* net_status(const fp_unet* u) { return u->d_status; }
 
-// A 3x3x3 convolution layer.  A decoder layer's input [up2(xa) | xb] is first
-// materialised in u->cat6 / u->cat8, because the convolution reads its input
-// through one TMA tensor map.
+// A 3x3x3 convolution layer.  A decoder layer reads [up2(xa) | xb] through
+// one TMA tensor map from u->cat6 / u->cat8: the skip tensor xb (e1, e0) is
+// written there by its own layer (the channel blocks after up2(xa)), and
+// up2(xa) is filled in here.
 static int conv_fwd(fp_unet* u, int l, const bf16* xa, const bf16* xb, bf16* y, cudaStream_t st) {
     TmaConvArgs a{};
     a.w = u->wf + layer_offset(l);
@@ -91,7 +92,7 @@ static int conv_fwd(fp_unet* u, int l, const bf16* xa, const bf16* xb, bf16* y, 
     const bf16* in = xb;
     if (kSpec[l].ca > 0) {
         bf16* cat = l == 6 ? u->cat6 : u->cat8;
-        launch_upcat(xa, kSpec[l].ca, xb, kSpec[l].cb, a.lv, cat, st);
+        launch_upcat(xa, kSpec[l].ca, a.lv, cat, st);
         in = cat;
     }
     return conv_forward_layer_tma(l, in, a, st);
@@ -242,10 +243,12 @@ int fp_unet_create(int W, int H, int D, int train, uint64_t seed, fp_unet** out)
     u->d_status = u->alloc<int>(1);
     u->X0 = u->alloc<bf16>(n0 * 16);
     u->a0 = u->alloc<bf16>(n0 * 16);
-    u->e0 = u->alloc<bf16>(n0 * 16);
+    u->cat8 = u->alloc<bf16>(n0 * 48);
+    u->e0 = u->cat8 ? u->cat8 + n0 * 32 : nullptr;  // channel blocks 4-5 of [up2(d1) | e0]
     u->q0 = u->alloc<bf16>(n1 * 16);
     u->a1 = u->alloc<bf16>(n1 * 32);
-    u->e1 = u->alloc<bf16>(n1 * 32);
+    u->cat6 = u->alloc<bf16>(n1 * 96);
+    u->e1 = u->cat6 ? u->cat6 + n1 * 64 : nullptr;  // channel blocks 8-11 of [up2(e2) | e1]
     u->q1 = u->alloc<bf16>(n2 * 32);
     u->a2 = u->alloc<bf16>(n2 * 64);
     u->e2 = u->alloc<bf16>(n2 * 64);
@@ -253,8 +256,6 @@ int fp_unet_create(int W, int H, int D, int train, uint64_t seed, fp_unet** out)
     u->d1 = u->alloc<bf16>(n1 * 32);
     u->d0a = u->alloc<bf16>(n0 * 16);
     u->d0 = u->alloc<bf16>(n0 * 16);
-    u->cat6 = u->alloc<bf16>(n1 * 96);
-    u->cat8 = u->alloc<bf16>(n0 * 48);
     u->out = u->alloc<float>(n0);
     if (u->train) {
         u->m = u->alloc<float>(kParams);

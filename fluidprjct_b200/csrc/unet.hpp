@@ -45,6 +45,13 @@ struct Lvl {
     __host__ __device__ int64_t n() const { return int64_t(W) * H * D; }
 };
 
+// Activations and their gradients are channel-blocked: channel c of voxel v
+// on a level of n voxels is element blk8(n, v, c / 8) + c % 8.  Eight channels
+// of a row of voxels are then contiguous, which is what the convolutions'
+// tensor maps read, and a channel concatenation [A | B] is A's blocks
+// followed by B's.
+__host__ __device__ inline int64_t blk8(int64_t n, int64_t v, int cb) { return (int64_t(cb) * n + v) * 8; }
+
 // Arguments of the weight-gradient kernel: dw[t][co][ci] = sum_v g[v][co] x[v + off(t)][ci].
 struct CorrArgs {
     const bf16* xa;
@@ -69,8 +76,8 @@ struct TmaConvArgs {
 };
 int conv_forward_layer_tma(int layer, const bf16* in, const TmaConvArgs& a, cudaStream_t st);
 int conv_backward_layer_tma(int layer, const bf16* in, const TmaConvArgs& a, cudaStream_t st);
-// out = [up2(coarse) | skip] on the fine level (ca + cb channels).
-void launch_upcat(const bf16* coarse, int ca, const bf16* skip, int cb, Lvl fine, bf16* out, cudaStream_t st);
+// The first ca / 8 channel blocks of out = up2(coarse) on the fine level.
+void launch_upcat(const bf16* coarse, int ca, Lvl fine, bf16* out, cudaStream_t st);
 
 // Launchers (kernels_unet.cu).  Each returns 0 or a cudaError_t value.
 int corr_layer(int layer, const CorrArgs& a, int nblk, cudaStream_t st);
