@@ -471,12 +471,14 @@ int run_tma(const bf16* in, const TmaConvArgs& a, cudaStream_t st) {
 
 }  // namespace
 
+// Every layer runs in 16-channel output groups (blockIdx.y): the dz-in-N
+// MMAs, and for CIN <= 48 two CTAs per SM.
 int conv_forward_layer_tma(int layer, const bf16* in, const TmaConvArgs& a, cudaStream_t st) {
     switch (layer) {
         case 0: case 1: return run_tma<16, 16, 16, EPI_RELU>(in, a, st);
-        case 2: return run_tma<16, 32, 32, EPI_RELU>(in, a, st);
-        case 3: case 7: return run_tma<32, 32, 32, EPI_RELU>(in, a, st);
-        case 4: return run_tma<32, 64, 32, EPI_RELU>(in, a, st);
+        case 2: return run_tma<16, 32, 16, EPI_RELU>(in, a, st);
+        case 3: case 7: return run_tma<32, 32, 16, EPI_RELU>(in, a, st);
+        case 4: return run_tma<32, 64, 16, EPI_RELU>(in, a, st);
         case 5: return run_tma<64, 64, 16, EPI_RELU>(in, a, st);
         case 6: return run_tma<96, 32, 16, EPI_RELU>(in, a, st);
         case 8: return run_tma<48, 16, 16, EPI_RELU>(in, a, st);
@@ -488,9 +490,9 @@ int conv_forward_layer_tma(int layer, const bf16* in, const TmaConvArgs& a, cuda
 int conv_backward_layer_tma(int layer, const bf16* in, const TmaConvArgs& a, cudaStream_t st) {
     switch (layer) {
         case 9: case 1: return run_tma<16, 16, 16, EPI_MASK>(in, a, st);
-        case 8: return run_tma<16, 48, 48, EPI_RAW>(in, a, st);
-        case 7: case 3: return run_tma<32, 32, 32, EPI_MASK>(in, a, st);
-        case 6: return run_tma<32, 96, 32, EPI_RAW>(in, a, st);
+        case 8: return run_tma<16, 48, 16, EPI_RAW>(in, a, st);
+        case 7: case 3: return run_tma<32, 32, 16, EPI_MASK>(in, a, st);
+        case 6: return run_tma<32, 96, 16, EPI_RAW>(in, a, st);
         case 5: return run_tma<64, 64, 16, EPI_MASK>(in, a, st);
         case 4: return run_tma<64, 32, 16, EPI_RAW>(in, a, st);
         case 2: return run_tma<32, 16, 16, EPI_RAW>(in, a, st);
