@@ -28,6 +28,7 @@ SOURCES = [
     "kernels_unet.cu",
     "kernels_unet_tma.cu",
     "kernels_ref2d.cu",
+    "kernels_scene.cu",
     "unet.cu",
     "solver.cu",
     "noalloc.cu",

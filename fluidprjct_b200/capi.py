@@ -83,6 +83,11 @@ _SIGS = {
     "fp_set_labels": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int]),
     "fp_get_dims": (C.c_int, [_P, _P, _P, _P]),
     "fp_load_sdf": (C.c_int, [_P, C.c_char_p]),
+    "fp_set_paddle": (C.c_int, [_P, C.c_float, C.c_float, C.c_float]),
+    "fp_set_labels_from_levelsets": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int]),
+    "fp_read_levelset_file": (C.c_int, [C.c_char_p, _P, _P]),
+    "fp_scene_seabed": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32,
+                                  C.c_float]),
     "fp_seed_particles": (C.c_int, [_P, C.c_int, C.c_uint32]),
     "fp_set_particles": (C.c_int, [_P, _P, _P, C.c_int64]),
     "fp_load_ply": (C.c_int, [_P, C.c_char_p]),
@@ -143,6 +148,17 @@ def declared_symbols():
 
 def ptr(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
+
+
+def read_levelset_file(path) -> np.ndarray:
+    """A 2D level-set file of the reference's DistrGen tools as an (H, W) array."""
+    dims = np.zeros(2, np.int32)
+    rc = lib().fp_read_levelset_file(str(path).encode(), ptr(dims), None)
+    if rc != FP_OK:
+        raise FluidError(rc, f"cannot read level-set file {path}")
+    out = np.zeros(int(dims[0]) * int(dims[1]), np.float32)
+    lib().fp_read_levelset_file(str(path).encode(), ptr(dims), ptr(out))
+    return out.reshape(int(dims[1]), int(dims[0]))
 
 
 def default_config(**kw) -> FpConfig:
@@ -213,6 +229,23 @@ class Solver:
         """Body SDF from a reference SDF file, or the analytic sphere of the
         config (body_radius, body_density) when path is None."""
         return self._check(lib().fp_load_sdf(self._h, None if path is None else str(path).encode()))
+
+    def set_labels_from_levelsets(self, solid: np.ndarray, fluid: np.ndarray):
+        """Labels from solid and fluid level sets ((H, W) or (D, H, W) arrays)."""
+        s = np.ascontiguousarray(solid, np.float32)
+        f = np.ascontiguousarray(fluid, np.float32)
+        if s.shape != f.shape or s.ndim not in (2, 3):
+            raise ValueError("level sets must have the same (H, W) or (D, H, W) shape")
+        D, H, W = (1,) + s.shape if s.ndim == 2 else s.shape
+        return self._check(lib().fp_set_labels_from_levelsets(self._h, ptr(s), ptr(f), W, H, D))
+
+    def scene_seabed(self, W, H, D, level=0.45, bed_base=0.15, bed_amp=0.05, seed=4, water_xmin=0.0):
+        """The seabed scene labelled on the GPU (see scenes.seabed)."""
+        return self._check(lib().fp_scene_seabed(self._h, W, H, D, level, bed_base, bed_amp, seed, water_xmin))
+
+    def set_paddle(self, x_rest, amplitude, period):
+        """Wave paddle: BODY where x < x_rest + amplitude sin(2 pi t / period)."""
+        return self._check(lib().fp_set_paddle(self._h, x_rest, amplitude, period))
 
     def seed_particles(self, ppc, seed):
         return self._check(lib().fp_seed_particles(self._h, ppc, seed))

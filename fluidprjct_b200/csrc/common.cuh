@@ -128,7 +128,9 @@ __device__ __forceinline__ float3 interp_vel(const float* __restrict__ u, const 
 // Rigid-body geometry for marking and the force integral: an analytic
 // sphere, or the reference's voxel SDF (RigidBody, utility.cuh:195-491) with
 // its rotation (row-major, world = R * local) and local centre of mass.
-enum : int { BODY_SPHERE = 0, BODY_SDF = 1 };
+// Body shapes: analytic sphere, the reference's voxel SDF, and a wave paddle
+// (the half-space x < com.x, moved by a prescribed law, not by the fluid).
+enum : int { BODY_SPHERE = 0, BODY_SDF = 1, BODY_PADDLE = 2 };
 struct BodyShape {
     int kind;
     float3 com;          // body position (centre of mass) in world space

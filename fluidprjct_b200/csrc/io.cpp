@@ -58,6 +58,24 @@ bool read_labels2d(const std::string& path, int& W, int& H, std::vector<uint8_t>
     return true;
 }
 
+bool read_levelset2d(const std::string& path, char& kind, int& W, int& H, std::vector<float>& out, std::string& err) {
+    std::ifstream f(path);
+    if (!f) { err = "cannot open level-set file: " + path; return false; }
+    std::string k;
+    if (!(f >> k >> W >> H) || k.size() != 1 || W <= 0 || H <= 0) { err = "bad level-set header in " + path; return false; }
+    kind = k[0];
+    out.assign(size_t(W) * H, 0.0f);
+    // rows in file order j = 0..h-1 of the generator; its row 0 is the top,
+    // the order generate_combined_labels_simple writes and the 2D label reader reads
+    for (int j = H - 1; j >= 0; --j)
+        for (int i = 0; i < W; ++i) {
+            float v;
+            if (!(f >> v)) { err = "level-set file truncated: " + path; return false; }
+            out[size_t(i) + size_t(j) * W] = v;
+        }
+    return true;
+}
+
 // ---------------------------------------------------------------- PLY
 namespace {
 int type_size(const std::string& t) {

@@ -17,6 +17,9 @@ bool read_labels3d(const std::string& path, int& W, int& H, int& D, std::vector<
 // 2D label file (FluidSolver2D::init, FluidSolver2D.cu:52-104): "W H" then rows
 // from the top (j = H-1) to the bottom, columns ascending.
 bool read_labels2d(const std::string& path, int& W, int& H, std::vector<uint8_t>& out, std::string& err);
+// 2D level-set file of DistrGen/fluidLevelSets.py: "<S|F> w h", then h rows of
+// w floats from the top row (j = h-1) down; out[i + j*w].
+bool read_levelset2d(const std::string& path, char& kind, int& W, int& H, std::vector<float>& out, std::string& err);
 
 // PLY vertices (ascii or binary_little_endian; float or double x y z and
 // optional vx vy vz).  The reference writes ascii positions only

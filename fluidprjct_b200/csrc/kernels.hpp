@@ -144,6 +144,11 @@ void launch_pack(const float* pos, const float* vel, int64_t np, float4* pos4, f
 int csr_cg_solve(int n, const int* offsets, const int* cols, const double* vals, const double* b, double* x, double tol,
                  int maxit, int* iters, double* relres, cudaStream_t st);
 
+// -------- scene generation (kernels_scene.cu) --------
+void launch_seabed_labels(uint8_t* labels, int W, int H, int D, double dx, double level, double bed_base,
+                          double bed_amp, uint64_t seed, double water_xmin, cudaStream_t st);
+void launch_levelset_labels(const float* solid, const float* fluid, int64_t n, uint8_t* labels, cudaStream_t st);
+
 // -------- the reference's own 2D step, scheme "ref2d" (kernels_ref2d.cu) --------
 // Scratch: start[(W+4)*(H+4)+1] (bins of cells -2..W+1 x -2..H+1), list, key,
 // rank [np], keep [np+1], misc[3] (non-finite u and v velocities, capped

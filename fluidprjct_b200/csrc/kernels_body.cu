@@ -29,6 +29,7 @@ __device__ __forceinline__ float sdf_at(const BodyShape& b, float3 x) {
     // Explicitly rounded (no contraction) so BODY marks match a CPU evaluation bit for bit.
     if (b.kind == BODY_SPHERE)
         return sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(d.x, d.x), __fmul_rn(d.y, d.y)), __fmul_rn(d.z, d.z))) - b.radius;
+    if (b.kind == BODY_PADDLE) return d.x;  // signed distance to the paddle face x = com.x
     // Voxel SDF: local = R^T (x - pos) + local_com; coordinate (local - origin)/cell.
     const float lx = b.rot[0] * d.x + b.rot[3] * d.y + b.rot[6] * d.z + b.local_com.x;
     const float ly = b.rot[1] * d.x + b.rot[4] * d.y + b.rot[7] * d.z + b.local_com.y;

@@ -60,6 +60,16 @@ struct HostBody {
     // voxel SDF
     int nx = 0, ny = 0, nz = 0;
     float origin[3] = {0, 0, 0}, cell = 1, local_com[3] = {0, 0, 0};
+    // paddle: face at x0 + amp sin(2 pi t / period), t since fp_set_paddle
+    double pad_x0 = 0, pad_amp = 0, pad_period = 1, pad_t = 0;
+
+    void paddle_at(double t) {
+        const double w = 2.0 * 3.14159265358979323846 / pad_period;
+        pos[0] = pad_x0 + pad_amp * std::sin(w * t);
+        vel[0] = pad_amp * w * std::cos(w * t);
+        vel[1] = vel[2] = 0.0;
+        omega[0] = omega[1] = omega[2] = 0.0;
+    }
 
     // update_rotation_matrix (utility.cuh:470-484)
     void update_rotation() {
@@ -540,7 +550,13 @@ int phase_body(fp_solver* s) {
         s->stats.body_force[a] = h.force[a];
         s->stats.body_torque[a] = h.torque[a];
     }
-    h.integrate(double(s->cfg.dt));
+    if (h.kind == BODY_PADDLE) {  // prescribed motion; the force is the fluid's load on the paddle
+        for (int a = 0; a < 3; ++a) s->stats.body_force[a] = h.force[a] = s->h_bforce[a];
+        h.pad_t += double(s->cfg.dt);
+        h.paddle_at(h.pad_t);
+    } else {
+        h.integrate(double(s->cfg.dt));
+    }
     fill_body_stats(s);
     return FP_OK;
 }
@@ -738,6 +754,21 @@ int fp_read_label_file(const char* path, int dim, int* dims, uint8_t* out) {
     return FP_OK;
 }
 
+int fp_read_levelset_file(const char* path, int* dims, float* out) {
+    if (!path || !dims) return FP_ERR_ARG;
+    std::vector<float> v;
+    std::string err;
+    char kind = 0;
+    int W = 0, H = 0;
+    if (!io::read_levelset2d(path, kind, W, H, v, err)) {
+        std::fprintf(stderr, "fp_read_levelset_file: %s\n", err.c_str());
+        return FP_ERR_IO;
+    }
+    dims[0] = W; dims[1] = H;
+    if (out) std::memcpy(out, v.data(), sizeof(float) * v.size());
+    return FP_OK;
+}
+
 int fp_read_ply_file(const char* path, int64_t* n, float* pos, float* vel, int* has_vel) {
     if (!path || !n) return FP_ERR_ARG;
     std::vector<float> p, v;
@@ -872,6 +903,47 @@ int fp_set_labels(fp_solver* s, const uint8_t* labels, int W, int H, int D) {
     return FP_OK;
 }
 
+// Labels already in s->d_labels (no BODY cells): the SOLID map becomes the base.
+static int labels_from_device(fp_solver* s) {
+    cudaError_t e = cudaMemcpyAsync(s->d_base, s->d_labels, size_t(s->g.nc()), cudaMemcpyDeviceToDevice, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "scene labels");
+    return FP_OK;
+}
+
+int fp_set_labels_from_levelsets(fp_solver* s, const float* solid, const float* fluid, int W, int H, int D) {
+    if (!s || !solid || !fluid || W <= 0 || H <= 0 || D <= 0)
+        return s ? s->fail(FP_ERR_ARG, "bad level sets") : FP_ERR_ARG;
+    int rc = alloc_grid(s, W, H, D);
+    if (rc) return rc;
+    const int64_t nc = int64_t(W) * H * D;
+    float *ds = nullptr, *df = nullptr;
+    cudaError_t e = dalloc(&ds, size_t(nc));
+    if (e == cudaSuccess) e = dalloc(&df, size_t(nc));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, solid, sizeof(float) * nc, cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(df, fluid, sizeof(float) * nc, cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) {
+        launch_levelset_labels(ds, df, nc, s->d_labels, s->st);
+        s->launches += 1;
+        e = cudaStreamSynchronize(s->st);
+    }
+    dfree(ds);
+    dfree(df);
+    if (e != cudaSuccess) return s->cuda_fail(e, "level-set labels");
+    return labels_from_device(s);
+}
+
+int fp_scene_seabed(fp_solver* s, int W, int H, int D, float level, float bed_base, float bed_amp, uint32_t seed,
+                    float water_xmin) {
+    if (!s || W < 3 || H < 3 || D < 3) return s ? s->fail(FP_ERR_ARG, "seabed grid too small") : FP_ERR_ARG;
+    int rc = alloc_grid(s, W, H, D);
+    if (rc) return rc;
+    launch_seabed_labels(s->d_labels, W, H, D, double(s->cfg.dx), double(level), double(bed_base), double(bed_amp),
+                         uint64_t(seed), double(water_xmin), s->st);
+    s->launches += 1;
+    return labels_from_device(s);
+}
+
 int fp_load_labels(fp_solver* s, const char* path) {
     if (!s || !path) return FP_ERR_ARG;
     std::vector<uint8_t> lab;
@@ -935,6 +1007,34 @@ int fp_load_sdf(fp_solver* s, const char* path) {
     launch_apply_mark(s->d_labels, s->d_bodymark, s->g, s->st);
     e = cudaStreamSynchronize(s->st);
     if (e != cudaSuccess) return s->cuda_fail(e, "body marking");
+    fill_body_stats(s);
+    return FP_OK;
+}
+
+int fp_set_paddle(fp_solver* s, float x_rest, float amplitude, float period) {
+    if (!s) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "labels must be loaded before the paddle");
+    if (!(period > 0.0f) || !std::isfinite(x_rest) || !std::isfinite(amplitude))
+        return s->fail(FP_ERR_ARG, "paddle needs a finite rest position and amplitude and a positive period");
+    free_body(s);
+    HostBody& h = s->hb;
+    h = HostBody();
+    h.kind = BODY_PADDLE;
+    h.pad_x0 = x_rest;
+    h.pad_amp = amplitude;
+    h.pad_period = period;
+    h.pos[1] = 0.5 * s->H * s->cfg.dx;  // torque reference: the face centre
+    h.pos[2] = 0.5 * s->D * s->cfg.dx;
+    h.paddle_at(0.0);
+    cudaError_t e = dalloc(&s->d_bpart, size_t(body_force_partials()));
+    if (e == cudaSuccess) e = dalloc(&s->d_bforce, 6);
+    if (e != cudaSuccess) { free_body(s); return s->cuda_fail(e, "paddle"); }
+    h.loaded = true;
+    s->cfg.active_body = 1;
+    launch_mark_body(s->d_bodymark, s->g, body_shape(s), s->st);
+    launch_apply_mark(s->d_labels, s->d_bodymark, s->g, s->st);
+    e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "paddle marking");
     fill_body_stats(s);
     return FP_OK;
 }

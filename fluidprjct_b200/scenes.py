@@ -83,40 +83,63 @@ def random_boxes(seed, n=128, max_boxes=3, sphere=True):
     return lab
 
 
+_SM64 = (np.uint64(0x9E3779B97F4A7C15), np.uint64(0xBF58476D1CE4E5B9), np.uint64(0x94D049BB133111EB))
+
+
+def _splitmix64(x):
+    x = x + _SM64[0]
+    x = (x ^ (x >> np.uint64(30))) * _SM64[1]
+    x = (x ^ (x >> np.uint64(27))) * _SM64[2]
+    return x ^ (x >> np.uint64(31))
+
+
+def _lattice(seed, o, a, b):
+    """Lattice value in [0, 1) at integer points (a, b) of octave o."""
+    key = (np.uint64(o) << np.uint64(42)) ^ (a.astype(np.uint64) << np.uint64(21)) ^ b.astype(np.uint64)
+    return (_splitmix64(np.uint64(seed) ^ _splitmix64(key)) >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+
+
 def value_noise_2d(shape, octaves=4, seed=4):
-    """Seeded multi-octave value noise in [0, 1] on an (nz, nx) grid."""
-    rng = np.random.default_rng(seed)
+    """Seeded multi-octave value noise in [0, 1] on an (nz, nx) grid: 4, 8, 16,
+    ... lattice cells per octave, smoothstep-weighted bilinear interpolation
+    of splitmix64-hashed lattice values, halving amplitudes.  The expressions
+    are the ones the GPU scene kernel evaluates (fp_scene_seabed), in the same
+    order, so both give the same bits."""
     nz, nx = shape
+    kk = np.arange(nz, dtype=np.float64)[:, None]
+    ii = np.arange(nx, dtype=np.float64)[None, :]
     out = np.zeros(shape, np.float64)
     amp, tot = 1.0, 0.0
     for o in range(octaves):
-        cells = 2 ** (o + 2)
-        lattice = rng.random((cells + 1, cells + 1))
-        zs = np.linspace(0, cells, nz, endpoint=False)
-        xs = np.linspace(0, cells, nx, endpoint=False)
-        z0, x0 = zs.astype(int), xs.astype(int)
-        fz, fx = zs - z0, xs - x0
-        fz = fz * fz * (3 - 2 * fz)
-        fx = fx * fx * (3 - 2 * fx)
-        a = lattice[z0][:, x0]
-        b = lattice[z0][:, x0 + 1]
-        c = lattice[z0 + 1][:, x0]
-        d = lattice[z0 + 1][:, x0 + 1]
-        top = a * (1 - fx)[None, :] + b * fx[None, :]
-        bot = c * (1 - fx)[None, :] + d * fx[None, :]
-        out += amp * (top * (1 - fz)[:, None] + bot * fz[:, None])
-        tot += amp
-        amp *= 0.5
+        cells = 4 << o
+        zs = kk * (float(cells) / float(nz))
+        xs = ii * (float(cells) / float(nx))
+        z0, x0 = np.broadcast_arrays(zs.astype(np.int64), xs.astype(np.int64))
+        fz = zs - zs.astype(np.int64)
+        fx = xs - xs.astype(np.int64)
+        fz = (fz * fz) * (3.0 - 2.0 * fz)
+        fx = (fx * fx) * (3.0 - 2.0 * fx)
+        top = _lattice(seed, o, z0, x0) * (1.0 - fx) + _lattice(seed, o, z0, x0 + 1) * fx
+        bot = _lattice(seed, o, z0 + 1, x0) * (1.0 - fx) + _lattice(seed, o, z0 + 1, x0 + 1) * fx
+        out = out + amp * (top * (1.0 - fz) + bot * fz)
+        tot = tot + amp
+        amp = amp * 0.5
     return out / tot
 
 
-def seabed(W=256, H=128, D=256, dx=1.0 / 128, level=0.45, seed=4):
-    """Large seabed scene: SOLID below 0.15 + 0.05*noise(x, z), water to y < level."""
+def seabed(W=256, H=128, D=256, dx=1.0 / 128, level=0.45, seed=4, bed_base=0.15, bed_amp=0.05, water_xmin=0.0):
+    """Large seabed scene: SOLID below bed_base + bed_amp * noise(x, z), water
+    to y < level for x >= water_xmin (the wave paddle's side of the tank).
+    The parameters are rounded to float32 like fp_scene_seabed's, which
+    generates the same labels on the GPU."""
+    f = lambda v: float(np.float32(v))
+    dx, level, bed_base, bed_amp, water_xmin = f(dx), f(level), f(bed_base), f(bed_amp), f(water_xmin)
     lab = _walls((D, H, W))
-    bed = 0.15 + 0.05 * value_noise_2d((D, W), 4, seed)  # (D, W) heights
+    bed = bed_base + bed_amp * value_noise_2d((D, W), 4, seed)  # (D, W) heights
     y = _centres(H, dx)
+    x = _centres(W, dx)
     solid = y[None, :, None] < bed[:, None, :]
-    water = (y < level)[None, :, None] & ~solid
+    water = (y < level)[None, :, None] & (x >= water_xmin)[None, None, :] & ~solid
     lab[solid] = SOLID
     lab[water & (lab != SOLID)] = FLUID
     return lab

@@ -161,11 +161,33 @@ const char* fp_last_error(const fp_solver* s);
  * grids; SOLID cells stay fixed for the whole run. */
 int fp_load_labels(fp_solver* s, const char* path);
 int fp_set_labels(fp_solver* s, const uint8_t* labels, int W, int H, int D);
+
+/* Labels from level sets, combined on the GPU as the reference's DistrGen
+ * tools do (fluidLabels.py: SOLID where solid < 0, else FLUID where
+ * fluid < 0, else AIR); host arrays of W*H*D floats in i + j*W + k*W*H order.
+ * fp_read_levelset_file reads one 2D level-set file of
+ * DistrGen/fluidLevelSets.py (dims = {W, H}; out may be NULL to query them). */
+int fp_set_labels_from_levelsets(fp_solver* s, const float* solid, const float* fluid, int W, int H, int D);
+int fp_read_levelset_file(const char* path, int* dims, float* out);
+
+/* The large seabed scene, labelled on the GPU: SOLID walls, SOLID below
+ * bed_base + bed_amp * noise(x, z) (four octaves of value noise, seeded),
+ * FLUID below y = level where x >= water_xmin, AIR elsewhere.  The grid
+ * spacing is fp_config.dx. */
+int fp_scene_seabed(fp_solver* s, int W, int H, int D, float level, float bed_base, float bed_amp, uint32_t seed,
+                    float water_xmin);
 int fp_get_dims(const fp_solver* s, int* W, int* H, int* D);
 
 /* Body SDF (RigidBody::loadSDF, utility.cuh:231-338) from a text file, or the
  * analytic sphere of fp_config.body_radius when path is NULL. */
 int fp_load_sdf(fp_solver* s, const char* path);
+
+/* Wave paddle (no reference counterpart; the large seabed scene's moving
+ * boundary): the half-space x < x_p(t) = x_rest + amplitude sin(2 pi t /
+ * period), t from this call, is a BODY region moving at dx_p/dt.  It takes
+ * the body slot (replacing an SDF body) and sets active_body; its motion is
+ * prescribed, and fp_step_stats.body_force reports the fluid's load on it. */
+int fp_set_paddle(fp_solver* s, float x_rest, float amplitude, float period);
 
 /* Particles: seeding of FLUID cells (seedParticles, FluidSolver3D.cu:213-297)
  * with a deterministic mt19937(seed); caller arrays; PLY files.  A

@@ -73,6 +73,15 @@ template <class R> inline R clamp01(R f) { return std::min(std::max(f, R(0)), R(
 // Rigid body (RigidBody, utility.cuh:195-491) with an analytic sphere SDF.
 struct OBody {
     bool loaded = false;
+    bool paddle = false;  // half-space x < pos[0] with prescribed motion (fp_set_paddle)
+    double pad_x0 = 0, pad_amp = 0, pad_period = 1, pad_t = 0;
+    void paddle_at(double t) {
+        const double w = 2.0 * 3.14159265358979323846 / pad_period;
+        pos[0] = pad_x0 + pad_amp * std::sin(w * t);
+        vel[0] = pad_amp * w * std::cos(w * t);
+        vel[1] = vel[2] = 0.0;
+        omega[0] = omega[1] = omega[2] = 0.0;
+    }
     double pos[3] = {0, 0, 0}, vel[3] = {0, 0, 0}, omega[3] = {0, 0, 0};
     double theta = 0, psi = 0, phi = 0, Rm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     double mass = 1, inertia = 1, radius = 0;
@@ -147,8 +156,10 @@ template <class R> struct Sim3 {
         j = std::min(std::max(j, 0), H - 1);
         k = std::min(std::max(k, 0), D - 1);
     }
-    // Sphere SDF in FP32 (the GPU's explicitly rounded float evaluation).
+    // Body SDF in FP32 (the GPU's explicitly rounded float evaluation): the
+    // sphere, or the paddle's signed distance x - x_p.
     float sphere_sdf(float x, float y, float z) const {
+        if (ob.paddle) return x - float(ob.pos[0]);
         const float cx = float(ob.pos[0]), cy = float(ob.pos[1]), cz = float(ob.pos[2]);
         const float dxp = x - cx, dyp = y - cy, dzp = z - cz;
         const float s2 = (dxp * dxp + dyp * dyp) + dzp * dzp;
@@ -588,7 +599,13 @@ template <class R> struct Sim3 {
         body_force(f);
         const double g[3] = {0.0, double(-9.81f), 0.0};
         for (int a = 0; a < 3; ++a) { ob.force[a] = ob.mass * g[a] + f[a]; ob.torque[a] = f[3 + a]; }
-        ob.integrate(double(float(dt)));
+        if (ob.paddle) {
+            for (int a = 0; a < 3; ++a) ob.force[a] = f[a];
+            ob.pad_t += double(float(dt));
+            ob.paddle_at(ob.pad_t);
+        } else {
+            ob.integrate(double(float(dt)));
+        }
         sync_body_kin();
     }
     void sync_body_kin() {
@@ -907,6 +924,19 @@ void or3_set_sphere(void* p, const double* pos, double r, double m) {
         for (int a = 0; a < 3; ++a) s.ob.pos[a] = pos[a];
         s.ob.radius = r; s.ob.mass = m; s.ob.inertia = 0.4 * m * r * r;
         s.ob.update_rotation();
+        s.sync_body_kin();
+        return 0;
+    });
+}
+// Wave paddle (fp_set_paddle): BODY where x < x0 + amp sin(2 pi t / period).
+void or3_set_paddle(void* p, double x0, double amp, double period) {
+    with(static_cast<Handle*>(p), [&](auto& s) {
+        s.ob = OBody();
+        s.ob.loaded = true;
+        s.ob.paddle = true;
+        s.ob.pad_x0 = double(float(x0)); s.ob.pad_amp = double(float(amp)); s.ob.pad_period = double(float(period));
+        s.ob.pos[1] = 0.5 * s.H * double(float(s.dx)); s.ob.pos[2] = 0.5 * s.D * double(float(s.dx));
+        s.ob.paddle_at(0.0);
         s.sync_body_kin();
         return 0;
     });

@@ -55,6 +55,7 @@ def lib():
         L.or3_set_body.argtypes = [P, P, P, P]
         L.or3_set_rk2.argtypes = [P, I]
         L.or3_set_sphere.argtypes = [P, P, D, D]
+        L.or3_set_paddle.argtypes = [P, D, D, D]
         L.or3_body_state.argtypes = [P, P]
         L.or3_body_force.argtypes = [P, P]
         L.or3_set_labels.argtypes = [P, P]
@@ -200,6 +201,9 @@ class Sim3:
     def set_sphere(self, pos, radius, mass):
         a = np.ascontiguousarray(pos, np.float64)
         lib().or3_set_sphere(self.h, _p(a), radius, mass)
+
+    def set_paddle(self, x_rest, amplitude, period):
+        lib().or3_set_paddle(self.h, x_rest, amplitude, period)
 
     def body_state(self):
         out = np.zeros(18, np.float64)
