@@ -29,6 +29,7 @@ SOURCES = [
     "kernels_unet_tma.cu",
     "kernels_ref2d.cu",
     "kernels_scene.cu",
+    "kernels_extrap.cu",
     "unet.cu",
     "solver.cu",
     "noalloc.cu",

@@ -144,6 +144,15 @@ void launch_pack(const float* pos, const float* vel, int64_t np, float4* pos4, f
 int csr_cg_solve(int n, const int* offsets, const int* cols, const double* vals, const double* b, double* x, double tol,
                  int maxit, int* iters, double* relres, cudaStream_t st);
 
+// -------- velocity extrapolation (kernels_extrap.cu) --------
+// Values equal to VEL_UNKNOWN on an nx x ny face grid, depth waves; the first
+// front reads neighbour markers at row stride front_stride.  mark: nx*ny ints.
+// Returns the number of launches.
+int launch_extrapolate_unknown(float* v, int nx, int ny, int depth, int front_stride, int* mark, cudaStream_t st);
+// Faces of component axis (0 u, 1 v, 2 w) with no FLUID side, depth waves.
+int launch_extrapolate_from_fluid(float* v, int axis, const uint8_t* labels, Dims g, int depth, int* mark,
+                                  cudaStream_t st);
+
 // -------- scene generation (kernels_scene.cu) --------
 void launch_seabed_labels(uint8_t* labels, int W, int H, int D, double dx, double level, double bed_base,
                           double bed_amp, uint64_t seed, double water_xmin, cudaStream_t st);

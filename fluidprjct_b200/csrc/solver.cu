@@ -144,6 +144,7 @@ struct fp_solver {
     int r2_nb = 0;
     int64_t r2_cap = 0;
     int* h_r2 = nullptr;    // pinned: [0] particles kept, [1] capped substep loops
+    int* d_extmark = nullptr;  // wavefront markers of the velocity extrapolation (largest face grid)
     // body
     BodyKin body{};
     HostBody hb;
@@ -186,6 +187,7 @@ void free_grid(fp_solver* s) {
     dfree(s->d_rhs_dense); dfree(s->d_x0c);
     if (s->net) { fp_unet_destroy(s->net); s->net = nullptr; }
     free_r2(s);
+    dfree(s->d_extmark);
     s->have_grid = false;
 }
 
@@ -569,6 +571,36 @@ void phase_g2p_advect(fp_solver* s, int do_g2p, int do_adv) {
     if (do_adv) s->sorted = false;
 }
 
+// ---------------------------------------------------------------- extrapolation
+int ext_alloc(fp_solver* s) {
+    if (s->d_extmark) return FP_OK;
+    const int64_t n = std::max({s->g.nu(), s->g.nv(), s->g.nw()});
+    cudaError_t e = dalloc(&s->d_extmark, size_t(n));
+    if (e != cudaSuccess) return s->cuda_fail(e, "device allocation of the extrapolation markers");
+    return FP_OK;
+}
+
+// The 2D step's first commented-out call (after P2G, depth 2) or second one
+// (after G2P, depth W for u and H for v).  checkNeighbors reads at stride W.
+int r2_extrapolate(fp_solver* s, bool after_g2p) {
+    int rc = ext_alloc(s);
+    if (rc) return rc;
+    s->launches += launch_extrapolate_unknown(s->d_u, s->W + 1, s->H, after_g2p ? s->W : 2, s->W, s->d_extmark, s->st);
+    s->launches += launch_extrapolate_unknown(s->d_v, s->W, s->H + 1, after_g2p ? s->H : 2, s->W, s->d_extmark, s->st);
+    return FP_OK;
+}
+
+// Default scheme: cfg.extrapolate layers into faces with no FLUID side.
+int extrapolate_3d(fp_solver* s) {
+    int rc = ext_alloc(s);
+    if (rc) return rc;
+    float* comp[3] = {s->d_u, s->d_v, s->d_w};
+    for (int a = 0; a < (s->D > 1 ? 3 : 2); ++a)
+        s->launches += launch_extrapolate_from_fluid(comp[a], a, s->d_labels, s->g, s->cfg.extrapolate, s->d_extmark,
+                                                     s->st);
+    return FP_OK;
+}
+
 // ---------------------------------------------------------------- scheme ref2d
 // FluidSolver2D.cu's own step (kernels_ref2d.cu); particles stay in order.
 bool ref2d(const fp_solver* s) { return s->cfg.scheme == FP_SCHEME_REF2D; }
@@ -650,14 +682,31 @@ int one_step_ref2d(fp_solver* s) {
     cudaEventRecord(s->ev[0], s->st);
     r2_label(s);
     cudaEventRecord(s->ev[1], s->st);
-    r2_p2g(s, 1);  // P2G + save + forces
+    const bool ext = s->cfg.extrapolate != 0;
+    if (ext) {  // P2G, extrapolation, save, forces
+        r2_p2g(s, 0);
+        rc = r2_extrapolate(s, false);
+        if (rc) return rc;
+        phase_save(s);
+        launch_r2_forces(s->d_u, s->d_v, s->g, s->cfg.dt, s->st);
+        s->launches += 1;
+    } else {
+        r2_p2g(s, 1);  // P2G + save + forces
+    }
     cudaEventRecord(s->ev[2], s->st);
     rc = r2_pressure(s);
     cudaEventRecord(s->ev[3], s->st);
     if (rc != FP_OK) return rc;
     r2_project(s);
     cudaEventRecord(s->ev[4], s->st);
-    r2_particles(s, 7);  // G2P, advection, clean-up
+    if (ext) {  // G2P, extrapolation, then advection and clean-up
+        r2_particles(s, 1);
+        rc = r2_extrapolate(s, true);
+        if (rc) return rc;
+        r2_particles(s, 6);
+    } else {
+        r2_particles(s, 7);  // G2P, advection, clean-up
+    }
     cudaEventRecord(s->ev[5], s->st);
     rc = r2_compact(s, true);
     if (rc != FP_OK) return rc;
@@ -705,7 +754,14 @@ int one_step(fp_solver* s) {
     if (rc != FP_OK) return rc;
     cudaEventRecord(s->ev[6], s->st);
     cudaEventRecord(s->ev[7], s->st);
-    phase_g2p_advect(s, 1, 1);
+    if (s->cfg.extrapolate > 0) {
+        phase_g2p_advect(s, 1, 0);
+        rc = extrapolate_3d(s);
+        if (rc != FP_OK) return rc;
+        phase_g2p_advect(s, 0, 1);
+    } else {
+        phase_g2p_advect(s, 1, 1);
+    }
     cudaEventRecord(s->ev[8], s->st);
     cudaError_t e = cudaEventSynchronize(s->ev[8]);
     if (e != cudaSuccess) return s->cuda_fail(e, "step");
@@ -831,6 +887,10 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     if (!(s->cfg.dx > 0) || !(s->cfg.dt > 0) || (s->cfg.dim != 2 && s->cfg.dim != 3)) { delete s; return FP_ERR_ARG; }
     if (s->cfg.solver < FP_SOLVER_PCG || s->cfg.solver > FP_SOLVER_PCG_LEARNED) {
         std::fprintf(stderr, "fp_create: solver %d is not available in this build\n", s->cfg.solver);
+        delete s;
+        return FP_ERR_ARG;
+    }
+    if (s->cfg.extrapolate < 0) {
         delete s;
         return FP_ERR_ARG;
     }
@@ -1172,7 +1232,10 @@ int fp_run_phase(fp_solver* s, int phase) {
         if (rc) return rc;
         switch (phase) {
             case FP_PHASE_LABEL: r2_label(s); break;
-            case FP_PHASE_P2G: r2_p2g(s, 0); break;
+            case FP_PHASE_P2G:
+                r2_p2g(s, 0);
+                if (s->cfg.extrapolate) rc = r2_extrapolate(s, false);
+                break;
             case FP_PHASE_SAVE: phase_save(s); break;
             case FP_PHASE_FORCES: launch_r2_forces(s->d_u, s->d_v, s->g, s->cfg.dt, s->st); s->launches += 1; break;
             case FP_PHASE_PRESSURE: rc = r2_pressure(s); break;
@@ -1180,6 +1243,10 @@ int fp_run_phase(fp_solver* s, int phase) {
             case FP_PHASE_BODY: break;
             case FP_PHASE_G2P: r2_particles(s, 1); break;
             case FP_PHASE_ADVECT:
+                if (s->cfg.extrapolate) {
+                    rc = r2_extrapolate(s, true);
+                    if (rc) return rc;
+                }
                 r2_particles(s, 2);
                 if (s->np) cudaMemcpyAsync(s->h_r2 + 1, s->r2.misc + 2, sizeof(int), cudaMemcpyDeviceToHost, s->st);
                 break;
@@ -1200,7 +1267,10 @@ int fp_run_phase(fp_solver* s, int phase) {
         case FP_PHASE_PROJECT: phase_project(s); break;
         case FP_PHASE_BODY: rc = phase_body(s); break;
         case FP_PHASE_G2P: phase_g2p_advect(s, 1, 0); break;
-        case FP_PHASE_ADVECT: phase_g2p_advect(s, 0, 1); break;
+        case FP_PHASE_ADVECT:
+            if (s->cfg.extrapolate > 0) rc = extrapolate_3d(s);
+            if (rc == FP_OK) phase_g2p_advect(s, 0, 1);
+            break;
         default: return s->fail(FP_ERR_ARG, "unknown phase");
     }
     cudaError_t e = cudaStreamSynchronize(s->st);

@@ -111,6 +111,13 @@ typedef struct fp_config {
     float    body_density;         /* sphere density relative to water            */
     int      device;               /* CUDA device ordinal; -1 = current device     */
     int      scheme;               /* FP_SCHEME_* (default FP_SCHEME_DEFAULT)      */
+    int      extrapolate;          /* velocity extrapolation (extrapolateGridFluidData,
+                                      FluidSolver2D.cu:1207-1295), off by default:
+                                      FP_SCHEME_REF2D: nonzero enables the 2D step's
+                                      two commented-out calls with their depths;
+                                      default scheme: this many wavefront layers into
+                                      faces with no FLUID side, between G2P and
+                                      advection */
 } fp_config;
 
 /* Per-step statistics: the reference's cudaEvent phase timers

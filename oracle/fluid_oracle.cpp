@@ -122,6 +122,7 @@ template <class R> struct Sim3 {
     std::vector<uint8_t> labels;
     std::vector<R> u, v, w, us, vs, ws, p;
     std::vector<R> px, py, pz, vx, vy, vz;
+    int extrap = 0;  // layers of velocity extrapolation between G2P and advection
     int last_iters = 0;
     double last_res = 0.0;
     int last_nf = 0;
@@ -614,6 +615,49 @@ template <class R> struct Sim3 {
         body.com = {R(float(ob.pos[0])), R(float(ob.pos[1])), R(float(ob.pos[2]))};
     }
 
+    // Velocity extrapolation into faces with no FLUID side (the wavefront
+    // scheme of FluidSolver2D.cu:1207-1295 on the 26-neighbourhood), extrap layers.
+    void extrapolate(std::vector<R>& g, int axis) const {
+        const int nx = W + (axis == 0), ny = H + (axis == 1), nz = D + (axis == 2);
+        auto id = [&](int i, int j, int k) { return size_t(i) + size_t(j) * nx + size_t(k) * nx * ny; };
+        auto lab_or_solid = [&](int i, int j, int k) -> uint8_t {
+            return (i < 0 || i >= W || j < 0 || j >= H || k < 0 || k >= D) ? SOLID : labels[cidx(i, j, k)];
+        };
+        std::vector<int> d(size_t(nx) * ny * nz);
+        for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) {
+            const uint8_t a = lab_or_solid(i, j, k);
+            const uint8_t b = lab_or_solid(i - (axis == 0), j - (axis == 1), k - (axis == 2));
+            d[id(i, j, k)] = (a == FLUID || b == FLUID) ? 0 : INT32_MAX;
+        }
+        auto for_nb = [&](int i, int j, int k, auto f) {
+            for (int ox = -1; ox <= 1; ++ox) for (int oy = 1; oy >= -1; --oy) for (int oz = -1; oz <= 1; ++oz) {
+                if (ox == 0 && oy == 0 && oz == 0) continue;
+                const int a = i + ox, b = j + oy, e = k + oz;
+                if (a < 0 || a >= nx || b < 0 || b >= ny || e < 0 || e >= nz) continue;
+                f(a, b, e);
+            }
+        };
+        for (int wave = 1; wave <= extrap; ++wave) {
+            std::vector<size_t> front;
+            for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) {
+                if (d[id(i, j, k)] != INT32_MAX) continue;
+                bool adj = false;
+                for_nb(i, j, k, [&](int a, int b, int e) { adj = adj || d[id(a, b, e)] == wave - 1; });
+                if (adj) front.push_back(id(i, j, k));
+            }
+            for (size_t c : front) d[c] = wave;
+            for (size_t c : front) {
+                const int i = int(c % nx), j = int((c / nx) % ny), k = int(c / (size_t(nx) * ny));
+                R avg = R(0);
+                int used = 0;
+                for_nb(i, j, k, [&](int a, int b, int e) {
+                    if (d[id(a, b, e)] < wave) { avg = R(avg + g[id(a, b, e)]); ++used; }
+                });
+                g[c] = R(avg / R(used));
+            }
+        }
+    }
+
     // frameStep (:3030-3098).
     int phase(int ph) {
         switch (ph) {
@@ -625,7 +669,10 @@ template <class R> struct Sim3 {
             case 5: project(); return 0;
             case 6: body_phase(); return 0;
             case 7: g2p(); return 0;
-            case 8: advect(); return 0;
+            case 8:
+                if (extrap > 0) { extrapolate(u, 0); extrapolate(v, 1); if (D > 1) extrapolate(w, 2); }
+                advect();
+                return 0;
         }
         return -99;
     }
@@ -852,6 +899,9 @@ void or3_set_params(void* p, double pic_weight, double cfl, double tol, int maxi
         using R = std::decay_t<decltype(s.dx)>;
         s.alpha = R(float(pic_weight)); s.cfl = R(float(cfl)); s.tol = tol; s.maxit = maxit; return 0;
     });
+}
+void or3_set_extrap(void* p, int layers) {
+    with(static_cast<Handle*>(p), [&](auto& s) { s.extrap = layers; return 0; });
 }
 void or3_set_rk2(void* p, int rk2) {
     with(static_cast<Handle*>(p), [&](auto& s) { s.rk2 = rk2; return 0; });

@@ -56,6 +56,8 @@ def lib():
         L.or3_set_rk2.argtypes = [P, I]
         L.or3_set_sphere.argtypes = [P, P, D, D]
         L.or3_set_paddle.argtypes = [P, D, D, D]
+        L.or3_set_extrap.argtypes = [P, I]
+        L.or2r_set_extrap.argtypes = [P, I]
         L.or3_body_state.argtypes = [P, P]
         L.or3_body_force.argtypes = [P, P]
         L.or3_set_labels.argtypes = [P, P]
@@ -205,6 +207,10 @@ class Sim3:
     def set_paddle(self, x_rest, amplitude, period):
         lib().or3_set_paddle(self.h, x_rest, amplitude, period)
 
+    def set_extrapolate(self, layers):
+        """Velocity extrapolation layers between G2P and advection (0 = off)."""
+        lib().or3_set_extrap(self.h, layers)
+
     def body_state(self):
         out = np.zeros(18, np.float64)
         lib().or3_body_state(self.h, _p(out))
@@ -300,6 +306,10 @@ class Ref2D:
         lab = np.ascontiguousarray(labels, np.uint8).reshape(-1)
         assert lab.size == self.W * self.H
         lib().or2r_set_labels(self.h, _p(lab))
+
+    def set_extrapolate(self, on):
+        """The step's commented-out extrapolateGridFluidData calls."""
+        lib().or2r_set_extrap(self.h, int(bool(on)))
 
     def labels(self):
         out = np.zeros(self.W * self.H, np.uint8)

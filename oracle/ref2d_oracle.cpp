@@ -86,6 +86,7 @@ struct Ref2D {
     std::vector<R> u, v, us, vs, p;
     std::vector<R> px, py, vx, vy;
     int nf = 0, cg_iters = 0, capped = 0;
+    bool extrap = false;  // the step's commented-out extrapolateGridFluidData calls (:1309-1310, :1325-1326)
     int64_t removed = 0;
 
     int64_t nu() const { return int64_t(W + 1) * H; }
@@ -152,6 +153,43 @@ struct Ref2D {
         }
         for (int64_t f = 0; f < nu(); ++f) u[f] = ud[f] != R(0) ? R(un[f] / ud[f]) : R(0);
         for (int64_t f = 0; f < nv(); ++f) v[f] = vd[f] != R(0) ? R(vn[f] / vd[f]) : R(0);
+    }
+    // extrapolateGridFluidData, :1207-1295, in the reference's sequential form.
+    // Its initial front reads neighbour markers at stride W (checkNeighbors,
+    // :1049-1066) whatever the grid's own width x.
+    void extrapolate(std::vector<R>& g, int x, int y, int depth) const {
+        std::vector<int> d(size_t(x) * y);
+        for (int j = 0; j < y; ++j)
+            for (int i = 0; i < x; ++i) d[size_t(i) + size_t(j) * x] = g[size_t(i) + size_t(j) * x] != R(kVelUnknown) ? 0 : INT_MAX;
+        static const int nb[8][2] = {{-1, 1}, {-1, 0}, {-1, -1}, {0, 1}, {0, -1}, {1, 1}, {1, 0}, {1, -1}};
+        std::vector<std::vector<std::pair<int, int>>> fronts(1);
+        for (int i = 0; i < x; ++i)
+            for (int j = 0; j < y; ++j) {
+                if (d[size_t(i) + size_t(j) * x] == 0) continue;
+                bool known_nb = false;
+                for (auto& n : nb) {
+                    const int a = i + n[0], b = j + n[1];
+                    if (a >= 0 && a < x && b >= 0 && b < y && d[size_t(a) + size_t(b) * W] == 0) { known_nb = true; break; }
+                }
+                if (known_nb) { d[size_t(i) + size_t(j) * x] = 1; fronts[0].push_back({i, j}); }
+            }
+        for (int cur = 0; cur < depth; ++cur) {
+            std::vector<std::pair<int, int>> next;
+            for (auto [i, j] : fronts[size_t(cur)]) {
+                const int dc = d[size_t(i) + size_t(j) * x];
+                R avg = R(0);
+                int used = 0;
+                for (auto& n : nb) {
+                    const int a = i + n[0], b = j + n[1];
+                    if (!(a >= 0 && a < x && b >= 0 && b < y)) continue;
+                    int& dn = d[size_t(a) + size_t(b) * x];
+                    if (dn < dc) { avg = R(avg + g[size_t(a) + size_t(b) * x]); ++used; }
+                    else if (dn == INT_MAX) { dn = dc + 1; next.push_back({a, b}); }
+                }
+                g[size_t(i) + size_t(j) * x] = R(avg / R(used));
+            }
+            fronts.push_back(next);
+        }
     }
     void save() { us = u; vs = v; }
     void forces() {
@@ -358,14 +396,20 @@ struct Ref2D {
     int phase(int ph) {
         switch (ph) {
             case 0: label(); return 0;
-            case 1: p2g(); return 0;
+            case 1:
+                p2g();
+                if (extrap) { extrapolate(u, W + 1, H, 2); extrapolate(v, W, H + 1, 2); }
+                return 0;
             case 2: save(); return 0;
             case 3: forces(); return 0;
             case 4: return pressure();
             case 5: project(); return 0;
             case 6: return 0;
             case 7: g2p(); return 0;
-            case 8: advect(); return 0;
+            case 8:
+                if (extrap) { extrapolate(u, W + 1, H, W); extrapolate(v, W, H + 1, H); }
+                advect();
+                return 0;
             case 9: cleanup(); return 0;
         }
         return -99;
@@ -400,6 +444,9 @@ void or2r_set_params(void* p, double alpha, double tol, int maxit) {
         using R = std::decay_t<decltype(s.dx)>;
         s.alpha = R(float(alpha)); s.tol = tol; s.maxit = maxit; return 0;
     });
+}
+void or2r_set_extrap(void* p, int on) {
+    with2(static_cast<Handle2*>(p), [&](auto& s) { s.extrap = on != 0; return 0; });
 }
 void or2r_set_labels(void* p, const uint8_t* l) {
     with2(static_cast<Handle2*>(p), [&](auto& s) { std::memcpy(s.labels.data(), l, s.labels.size()); return 0; });

@@ -285,3 +285,30 @@ def test_errors_are_reported_not_thrown(tmp_path):
     with pytest.raises(capi.FluidError) as e:
         s.load_labels(tmp_path / "nope.txt")
     assert e.value.code == capi.FP_ERR_IO
+
+
+@pytest.mark.parametrize("layers", [1, 3])
+def test_velocity_extrapolation_matches_oracle(O, layers):
+    """fp_config.extrapolate = layers: between G2P and advection, faces with
+    no FLUID side take wavefront means of older faces (26-neighbourhood).
+    From identical grids the extrapolated grids are bit-exact."""
+    from fluidprjct_b200 import capi
+    dx, dt = 0.05, 0.004
+    lab, pos, vel = _scene(O)
+    s, o = _pair(O, lab, pos, vel, dx, dt, extrapolate=layers)
+    o.set_extrapolate(layers)
+    rng = np.random.default_rng(9)
+    s.phase(capi.PHASE_LABEL); o.phase(O.PH_LABEL)
+    grids = ((capi.GRID_U, O.GRID_U), (capi.GRID_V, O.GRID_V), (capi.GRID_W, O.GRID_W))
+    for g, go in grids:
+        f = rng.uniform(-1, 1, s.grid_shape(g)).astype(np.float32)
+        s.set_grid(g, f)
+        o.set_grid(go, f.astype(np.float64))
+    before = [s.grid(g).copy() for g, _ in grids]
+    s.phase(capi.PHASE_ADVECT); o.phase(O.PH_ADVECT)
+    changed = 0
+    for (g, go), b in zip(grids, before):
+        a = s.grid(g)
+        assert np.array_equal(a.ravel(), o.grid(go).astype(np.float32)), g
+        changed += int((a != b).sum())
+    assert changed > 100

@@ -16,7 +16,7 @@ from conftest import rel_l2
 pytestmark = pytest.mark.gpu
 
 
-def _scene(O, n=32, ppc=4, seed=0, dt=0.005, jitter=0.3, alpha=0.05):
+def _scene(O, n=32, ppc=4, seed=0, dt=0.005, jitter=0.3, alpha=0.05, extrapolate=0):
     from fluidprjct_b200 import capi, scenes
     lab = scenes.dam_break_2d(n)
     dx = 1.0 / n
@@ -24,10 +24,11 @@ def _scene(O, n=32, ppc=4, seed=0, dt=0.005, jitter=0.3, alpha=0.05):
     vel = np.zeros_like(pos)
     vel[:, :2] = np.random.default_rng(seed).uniform(-jitter, jitter, (len(pos), 2))
     s = capi.Solver(dim=2, dx=dx, dt=dt, pic_weight=alpha, solver="pcg_mg", tol=1e-9, scheme="ref2d",
-                    output_format=capi.OUT_NONE)
+                    output_format=capi.OUT_NONE, extrapolate=extrapolate)
     s.set_labels(lab)
     s.set_particles(pos, vel)
     o = O.Ref2D(n, n, dx, dt, pic_weight=alpha, tol=1e-13)
+    o.set_extrapolate(extrapolate)
     o.set_labels(lab)
     o.set_particles(pos, vel)
     return s, o, lab
@@ -39,9 +40,12 @@ def _same(a, b):
     return a.shape == b.shape and np.array_equal(a, b, equal_nan=True)
 
 
-def test_ref2d_phases_bit_exact(O):
+@pytest.mark.parametrize("extrapolate", [0, 1])
+def test_ref2d_phases_bit_exact(O, extrapolate):
+    """With extrapolate = 1 the step's two commented-out extrapolateGridFluidData
+    calls run too (after P2G, and between G2P and advection)."""
     from fluidprjct_b200 import capi
-    s, o, lab = _scene(O)
+    s, o, lab = _scene(O, extrapolate=extrapolate)
     for k in range(3):  # three steps, phase by phase
         s.phase(capi.PHASE_LABEL); o.phase(O.PH_LABEL)
         assert np.array_equal(s.labels().reshape(o.labels().shape), o.labels())

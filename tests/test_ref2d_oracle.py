@@ -245,3 +245,31 @@ def test_dam_break_runs_and_keeps_particles(O):
     assert np.isfinite(po).all() and np.isfinite(vo).all()
     assert len(po) == len(pos)
     assert po[:, 1].mean() < y0
+
+
+def test_extrapolation_waves_and_stride_quirk(O):
+    """extrapolateGridFluidData (:1207-1295), enabled in the G2P -> advection
+    gap: a VEL_UNKNOWN face next to known faces becomes the mean of its known
+    8-neighbours (wave 1), the next ring the mean of older waves (wave 2).
+    The initial front of the u grid reads markers at stride W, not W + 1
+    (checkNeighbors, :1049-1066)."""
+    W, H = 6, 5
+    r = O.Ref2D(W, H, 0.2, 0.01)
+    r.set_extrapolate(True)
+    lab = _box(W, H)
+    r.set_labels(lab)
+    r.set_particles(np.zeros((0, 3), np.float32))
+    v = np.full((H + 1, W), VU, np.float64)
+    v[0, :3] = [1.0, 2.0, 4.0]                     # known values in the bottom row
+    r.set_grid(O.GRID_V, v)
+    u = np.full((H, W + 1), VU, np.float64)
+    u[1, 0] = 8.0                                  # one known u face, (i, j) = (0, 1): true index 7
+    r.set_grid(O.GRID_U, u)
+    r.phase(O.PH_ADVECT)
+    uo = r.grid(O.GRID_U).reshape(H, W + 1)
+    # The first front tests markers at a + b*W = 7, i.e. cell (1, 1): the
+    # neighbours of (1, 1) join wave 1.  (0, 0) and (0, 2) are true neighbours
+    # of the known face and take its value; (2, 0..2) have no older neighbour
+    # and become 0/0 = NaN, as in the reference; (1, 1) itself is not in wave 1.
+    assert uo[0, 0] == 8.0 and uo[2, 0] == 8.0
+    assert np.isnan(uo[0, 2]) and np.isnan(uo[1, 2]) and np.isnan(uo[2, 2])
