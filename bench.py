@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--frames", type=int, default=0,
+                    help="also time fp_run's frame output (binary and ASCII PLY) over this many frames")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--solver", default="pcg_mg", choices=["pcg", "pcg_mixed", "pcg_mg", "pcg_learned"],
                     help="pressure solver of the timed steps")
@@ -313,6 +315,10 @@ def run_ours(args, rank, local, world):
                       "h2d_bytes_per_step": int(np_ * 24), "d2h_bytes_per_step": int(np_ * 24), "steps": k,
                       "path": "fp_set_particles(pinned host pos, vel) + fp_step + fp_get_particles"}
 
+    # ---- frame output of fp_run (optional) ----
+    if args.frames > 0 and rank == 0:
+        out["frame_output"] = frame_output(s, args.frames)
+
     # ---- CPU baseline (rank 0, N = 1) ----
     if not args.no_cpu and rank == 0 and world == 1:
         out["cpu_baseline"] = cpu_baseline(lab, args.n, args.ppc, args.cpu_seconds)
@@ -324,6 +330,52 @@ def run_ours(args, rank, local, world):
     s.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def frame_output(s, frames):
+    """Wall time of fp_run(frames) with one frame per step, for no output,
+    binary PLY and ASCII PLY, against the synchronous alternative (the same
+    steps, then per frame a download and a file write on the calling
+    thread).  fp_run overlaps the writes with the following steps."""
+    import copy
+    import tempfile
+
+    import numpy as np
+
+    from fluidprjct_b200 import capi
+    res = {"frames": frames, "particles": s.num_particles}
+    cfg = copy.copy(s.cfg)
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, fmt, ipf in (("none", capi.OUT_NONE, 1), ("binary", capi.OUT_PLY_BINARY, 1),
+                               ("ascii", capi.OUT_PLY, 1), ("binary_every10", capi.OUT_PLY_BINARY, 10),
+                               ("ascii_every10", capi.OUT_PLY, 10)):
+            cfg.output_format = fmt
+            cfg.iter_per_frame = ipf
+            cfg.output_template = os.path.join(tmp, name + "_").encode()
+            r = capi.Solver(cfg)
+            r.set_labels(s.labels())
+            pos, vel = s.particles()
+            r.set_particles(pos, vel)
+            r.step(1)
+            t0 = time.perf_counter()
+            r.run(frames)  # frames * ipf + 1 steps, frames + 1 files
+            res[name + "_ms_per_frame"] = round((time.perf_counter() - t0) * 1000.0 / (frames + 1), 3)
+            if fmt != capi.OUT_NONE:
+                f0 = os.path.join(tmp, name + "_0.ply")
+                res[name + "_bytes_per_frame"] = os.path.getsize(f0)
+                # synchronous alternative: the steps, then download and write on this thread
+                hp, hv = np.zeros_like(pos), np.zeros_like(vel)
+                t0 = time.perf_counter()
+                for i in range(frames + 1):
+                    r.step(ipf if i else 1)
+                    r.particles(out=(hp, hv))
+                    capi.lib().fp_write_particle_file(os.path.join(tmp, f"sync_{i}.ply").encode(), capi.ptr(hp),
+                                                      capi.ptr(hv), len(hp), fmt)
+                res[name + "_sync_ms_per_frame"] = round((time.perf_counter() - t0) * 1000.0 / (frames + 1), 3)
+            r.close()
+            for f in os.listdir(tmp):
+                os.remove(os.path.join(tmp, f))
+    return res
 
 
 def cpu_baseline(lab, n, ppc, seconds):

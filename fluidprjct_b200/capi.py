@@ -86,6 +86,7 @@ _SIGS = {
     "fp_set_paddle": (C.c_int, [_P, C.c_float, C.c_float, C.c_float]),
     "fp_set_labels_from_levelsets": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int]),
     "fp_read_levelset_file": (C.c_int, [C.c_char_p, _P, _P]),
+    "fp_write_particle_file": (C.c_int, [C.c_char_p, _P, _P, C.c_int64, C.c_int]),
     "fp_scene_seabed": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32,
                                   C.c_float]),
     "fp_seed_particles": (C.c_int, [_P, C.c_int, C.c_uint32]),

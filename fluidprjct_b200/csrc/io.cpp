@@ -3,12 +3,14 @@
 
 #include <algorithm>
 #include <cctype>
+#include <charconv>
 #include <cmath>
 #include <cstring>
 #include <fstream>
 #include <map>
 #include <random>
 #include <sstream>
+#include <thread>
 
 namespace fp::io {
 
@@ -168,40 +170,78 @@ bool read_ply(const std::string& path, std::vector<float>& pos, std::vector<floa
     return true;
 }
 
-bool write_particles(const std::string& path, const float* pos, const float* vel, int64_t n, int format,
-                     std::string& err) {
-    if (format == FP_OUT_NONE) return true;
-    if (format == FP_OUT_PLY_BINARY) {
-        std::ofstream f(path, std::ios::binary);
-        if (!f) { err = "cannot write " + path; return false; }
-        f << "ply\nformat binary_little_endian 1.0\nelement vertex " << n
-          << "\nproperty float x\nproperty float y\nproperty float z\nproperty float vx\nproperty float vy\n"
-             "property float vz\nend_header\n";
-        std::vector<float> rec(size_t(6) * size_t(std::min<int64_t>(n, 1 << 16)));
-        for (int64_t b = 0; b < n; b += (1 << 16)) {
-            int64_t m = std::min<int64_t>(n - b, 1 << 16);
-            for (int64_t q = 0; q < m; ++q) {
-                for (int c = 0; c < 3; ++c) {
-                    rec[6 * q + c] = pos[3 * (b + q) + c];
-                    rec[6 * q + 3 + c] = vel ? vel[3 * (b + q) + c] : 0.0f;
-                }
-            }
-            f.write(reinterpret_cast<const char*>(rec.data()), std::streamsize(sizeof(float) * 6 * m));
-        }
-        if (!f) { err = "write failed: " + path; return false; }
-        return true;
-    }
-    std::ofstream f(path);
+namespace {
+const char* kBinaryHeader =
+    "\nproperty float x\nproperty float y\nproperty float z\nproperty float vx\nproperty float vy\n"
+    "property float vz\nend_header\n";
+
+// ASCII PLY / OFF of positions pos[stride * q + 0..2]: "x y z" per line as an
+// ostream of floats prints them (saveParticlesToPLY, utility.cu:91-127), %g
+// with 6 significant digits, i.e. std::to_chars in general format with
+// precision 6.  Chunks are formatted in parallel and written in order.
+bool write_ascii(const std::string& path, const float* pos, int stride, int64_t n, int format, std::string& err) {
+    std::ofstream f(path, std::ios::binary);
     if (!f) { err = "cannot write " + path; return false; }
     if (format == FP_OUT_OFF) {
         f << "OFF\n" << n << " 0 0\n";
     } else {
         f << "ply\nformat ascii 1.0\nelement vertex " << n << "\nproperty float x\nproperty float y\nproperty float z\nend_header\n";
     }
-    char buf[96];
-    for (int64_t q = 0; q < n; ++q) {
-        int len = std::snprintf(buf, sizeof buf, "%g %g %g\n", double(pos[3 * q]), double(pos[3 * q + 1]), double(pos[3 * q + 2]));
-        f.write(buf, len);
+    const int64_t chunk = 1 << 18;
+    const int64_t nchunks = (n + chunk - 1) / chunk;
+    const int nthreads = int(std::max<int64_t>(1, std::min<int64_t>(nchunks, std::max(1u, std::thread::hardware_concurrency()))));
+    std::vector<std::string> text(size_t(std::max<int64_t>(nchunks, 0)));
+    auto format_chunk = [&](int64_t c) {
+        std::string& out = text[size_t(c)];
+        const int64_t b = c * chunk, e = std::min(n, b + chunk);
+        out.resize(size_t(e - b) * 48);
+        char* p = out.data();
+        for (int64_t q = b; q < e; ++q)
+            for (int a = 0; a < 3; ++a) {
+                p = std::to_chars(p, p + 16, double(pos[stride * q + a]), std::chars_format::general, 6).ptr;
+                *p++ = a < 2 ? ' ' : '\n';
+            }
+        out.resize(size_t(p - out.data()));
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; ++t)
+        pool.emplace_back([&, t] {
+            for (int64_t c = t; c < nchunks; c += nthreads) format_chunk(c);
+        });
+    for (auto& th : pool) th.join();
+    for (const auto& s : text) f.write(s.data(), std::streamsize(s.size()));
+    if (!f) { err = "write failed: " + path; return false; }
+    return true;
+}
+}  // namespace
+
+bool write_frame_records(const std::string& path, const float* rec, int64_t n, int format, std::string& err) {
+    if (format == FP_OUT_NONE) return true;
+    if (format != FP_OUT_PLY_BINARY) return write_ascii(path, rec, 6, n, format, err);
+    std::ofstream f(path, std::ios::binary);
+    if (!f) { err = "cannot write " + path; return false; }
+    f << "ply\nformat binary_little_endian 1.0\nelement vertex " << n << kBinaryHeader;
+    f.write(reinterpret_cast<const char*>(rec), std::streamsize(sizeof(float) * 6 * size_t(n)));
+    if (!f) { err = "write failed: " + path; return false; }
+    return true;
+}
+
+bool write_particles(const std::string& path, const float* pos, const float* vel, int64_t n, int format,
+                     std::string& err) {
+    if (format == FP_OUT_NONE) return true;
+    if (format != FP_OUT_PLY_BINARY) return write_ascii(path, pos, 3, n, format, err);
+    std::ofstream f(path, std::ios::binary);
+    if (!f) { err = "cannot write " + path; return false; }
+    f << "ply\nformat binary_little_endian 1.0\nelement vertex " << n << kBinaryHeader;
+    std::vector<float> rec(size_t(6) * size_t(std::min<int64_t>(n, 1 << 16)));
+    for (int64_t b = 0; b < n; b += (1 << 16)) {
+        const int64_t m = std::min<int64_t>(n - b, 1 << 16);
+        for (int64_t q = 0; q < m; ++q)
+            for (int c = 0; c < 3; ++c) {
+                rec[size_t(6 * q + c)] = pos[3 * (b + q) + c];
+                rec[size_t(6 * q + 3 + c)] = vel ? vel[3 * (b + q) + c] : 0.0f;
+            }
+        f.write(reinterpret_cast<const char*>(rec.data()), std::streamsize(sizeof(float) * 6 * m));
     }
     if (!f) { err = "write failed: " + path; return false; }
     return true;

@@ -27,6 +27,9 @@ bool read_levelset2d(const std::string& path, char& kind, int& W, int& H, std::v
 bool read_ply(const std::string& path, std::vector<float>& pos, std::vector<float>& vel, bool& has_vel, std::string& err);
 // format: FP_OUT_PLY (ascii, positions; utility.cu:91-109), FP_OUT_OFF
 // (utility.cu:111-127), FP_OUT_PLY_BINARY (little-endian float x y z vx vy vz).
+// A frame from records x y z vx vy vz (6 floats per particle): binary PLY
+// writes them as they are; ASCII PLY / OFF format the positions.
+bool write_frame_records(const std::string& path, const float* rec, int64_t n, int format, std::string& err);
 bool write_particles(const std::string& path, const float* pos, const float* vel, int64_t n, int format,
                      std::string& err);
 

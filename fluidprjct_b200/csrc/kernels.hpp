@@ -135,6 +135,8 @@ int body_force_partials();
 // -------- particle order helpers --------
 // out[pid] = in[slot] for the xyz part of float4 arrays (pid in pos.w bits).
 void launch_unsort(const float4* pos, const float4* vel, int64_t np, float* pos_out, float* vel_out, cudaStream_t st);
+// rec[6 pid + 0..5] = x y z vx vy vz (frame records in the original order).
+void launch_unsort_records(const float4* pos, const float4* vel, int64_t np, float* rec, cudaStream_t st);
 // AoS to float4 (w = original index); the lowest index holding a non-finite
 // value goes to *bad (set to INT_MAX before the call), if bad is not null.
 void launch_pack(const float* pos, const float* vel, int64_t np, float4* pos4, float4* vel4, int* bad,

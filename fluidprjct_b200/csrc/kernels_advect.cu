@@ -129,6 +129,16 @@ __global__ void k_unsort(const float4* __restrict__ pos, const float4* __restric
     if (vel_out) { const float4 V = vel[q]; vel_out[3 * id] = V.x; vel_out[3 * id + 1] = V.y; vel_out[3 * id + 2] = V.z; }
 }
 
+// Frame records x y z vx vy vz in the original order (the binary PLY layout).
+__global__ void k_unsort_records(const float4* __restrict__ pos, const float4* __restrict__ vel, int64_t np,
+                                 float* __restrict__ rec) {
+    const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= np) return;
+    const float4 P = pos[q], V = vel[q];
+    float* r = rec + 6 * int64_t(__float_as_int(P.w));
+    r[0] = P.x; r[1] = P.y; r[2] = P.z; r[3] = V.x; r[4] = V.y; r[5] = V.z;
+}
+
 // AoS (x y z) arrays to float4 pos (w = original index) and vel.  The
 // lowest index of a particle with a non-finite value goes to *bad (the
 // caller sets it to INT_MAX first).
@@ -157,6 +167,11 @@ void launch_g2p_advect(float4* pos, float4* vel, int64_t np, const float* u, con
 void launch_unsort(const float4* pos, const float4* vel, int64_t np, float* pos_out, float* vel_out, cudaStream_t st) {
     if (np == 0) return;
     k_unsort<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, pos_out, vel_out);
+}
+
+void launch_unsort_records(const float4* pos, const float4* vel, int64_t np, float* rec, cudaStream_t st) {
+    if (np == 0) return;
+    k_unsort_records<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, rec);
 }
 
 void launch_pack(const float* pos, const float* vel, int64_t np, float4* pos4, float4* vel4, int* bad,

@@ -12,9 +12,13 @@
 //   g2p+adv : one kernel per particle
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/fluidprjct.h"
@@ -825,6 +829,16 @@ int fp_read_levelset_file(const char* path, int* dims, float* out) {
     return FP_OK;
 }
 
+int fp_write_particle_file(const char* path, const float* pos, const float* vel, int64_t n, int format) {
+    if (!path || n < 0 || (n > 0 && !pos) || format < FP_OUT_PLY || format > FP_OUT_NONE) return FP_ERR_ARG;
+    std::string err;
+    if (!io::write_particles(path, pos, vel, n, format, err)) {
+        std::fprintf(stderr, "fp_write_particle_file: %s\n", err.c_str());
+        return FP_ERR_IO;
+    }
+    return FP_OK;
+}
+
 int fp_read_ply_file(const char* path, int64_t* n, float* pos, float* vel, int* has_vel) {
     if (!path || !n) return FP_ERR_ARG;
     std::vector<float> p, v;
@@ -1180,6 +1194,94 @@ int fp_step(fp_solver* s, int n) {
     return FP_OK;
 }
 
+// Frame output of fp_run off the step's critical path: each frame's particles
+// go (unsort kernel packing x y z vx vy vz records, then D2H on the solver
+// stream) into one of two pinned buffers, and a writer thread writes the file
+// (one write for binary PLY) once the copy's event has
+// completed, while the host goes on issuing steps.  A buffer is reused only
+// after its previous file is written.
+struct FrameWriter {
+    fp_solver* s;
+    int format;
+    float* h[2] = {nullptr, nullptr};  // pos | vel, 6 * cap floats each
+    int64_t cap = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool busy[2] = {false, false};
+    struct Job { int buf; int64_t n; std::string path; };
+    std::deque<Job> jobs;
+    std::mutex m;
+    std::condition_variable cv;
+    bool stop = false, failed = false;
+    std::string err;
+    std::thread th;
+
+    FrameWriter(fp_solver* sv, int fmt) : s(sv), format(fmt) {}
+    int start(int64_t n) {
+        cap = std::max<int64_t>(n, 1);
+        for (int b = 0; b < 2; ++b) {
+            if (cudaMallocHost(&h[b], sizeof(float) * 6 * size_t(cap)) != cudaSuccess ||
+                cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming) != cudaSuccess)
+                return s->cuda_fail(cudaGetLastError(), "frame buffers");
+        }
+        th = std::thread([this] { loop(); });
+        return FP_OK;
+    }
+    void loop() {
+        for (;;) {
+            Job j;
+            {
+                std::unique_lock<std::mutex> lk(m);
+                cv.wait(lk, [&] { return stop || !jobs.empty(); });
+                if (jobs.empty()) return;
+                j = jobs.front();
+                jobs.pop_front();
+            }
+            std::string e;
+            bool ok = cudaEventSynchronize(ev[j.buf]) == cudaSuccess &&
+                      io::write_frame_records(j.path, h[j.buf], j.n, format, e);
+            std::lock_guard<std::mutex> lk(m);
+            if (!ok && !failed) { failed = true; err = e.empty() ? "frame copy failed" : e; }
+            busy[j.buf] = false;
+            cv.notify_all();
+        }
+    }
+    // Queues frame `path` from buffer b; waits while b still holds an unwritten frame.
+    int submit(int b, const std::string& path) {
+        {
+            std::unique_lock<std::mutex> lk(m);
+            cv.wait(lk, [&] { return !busy[b] || failed; });
+            if (failed) return s->fail(FP_ERR_IO, err);
+        }
+        const int64_t n = s->np;
+        if (n > cap) return s->fail(FP_ERR_STATE, "particle count grew during fp_run");
+        if (n > 0) {
+            launch_unsort_records(s->d_pos, s->d_vel, n, s->d_io, s->st);
+            s->launches += 1;
+            cudaMemcpyAsync(h[b], s->d_io, sizeof(float) * 6 * size_t(n), cudaMemcpyDeviceToHost, s->st);
+        }
+        cudaEventRecord(ev[b], s->st);
+        std::lock_guard<std::mutex> lk(m);
+        busy[b] = true;
+        jobs.push_back(Job{b, n, path});
+        cv.notify_all();
+        return FP_OK;
+    }
+    int finish() {
+        {
+            std::lock_guard<std::mutex> lk(m);
+            stop = true;
+            cv.notify_all();
+        }
+        if (th.joinable()) th.join();
+        for (int b = 0; b < 2; ++b) {
+            if (h[b]) cudaFreeHost(h[b]);
+            if (ev[b]) cudaEventDestroy(ev[b]);
+        }
+        if (failed) return s->fail(FP_ERR_IO, err);
+        return FP_OK;
+    }
+};
+
 int fp_run(fp_solver* s, int frames) {
     int rc = check_ready(s);
     if (rc) return rc;
@@ -1191,7 +1293,14 @@ int fp_run(fp_solver* s, int frames) {
         csv = std::fopen(cp.c_str(), "w");
         if (csv) std::fprintf(csv, "frame,centerX1,centerX2,centerX3,angleX1,angleX2,angleX3\n");
     }
-    std::vector<float> pos, vel;
+    const bool out = s->cfg.output_format != FP_OUT_NONE;
+    FrameWriter writer(s, s->cfg.output_format);
+    if (out && (rc = writer.start(s->np)) != FP_OK) {
+        writer.finish();
+        if (csv) std::fclose(csv);
+        return rc;
+    }
+    int64_t frame = 0;
     // FluidSolver3D::run labels once before its loop and takes frames * ipf + 1
     // steps (FluidSolver3D.cu:3110-3111); FluidSolver2D::run takes max_steps
     // steps and writes every one of them (FluidSolver2D.cu:1333-1342).
@@ -1201,17 +1310,10 @@ int fp_run(fp_solver* s, int frames) {
     for (int64_t i = 0; i <= last; ++i) {
         rc = one_step(s);
         if (rc) break;
-        if ((r2 || i % ipf == 0) && s->cfg.output_format != FP_OUT_NONE) {
-            pos.resize(size_t(s->np) * 3);
-            vel.resize(size_t(s->np) * 3);
-            rc = fp_get_particles(s, pos.data(), vel.data(), s->np);
-            if (rc) break;
+        if ((r2 || i % ipf == 0) && out) {
             const char* ext = s->cfg.output_format == FP_OUT_OFF ? ".off" : ".ply";
-            std::string path = tmpl + std::to_string(r2 ? i : i / ipf) + ext;
-            if (!io::write_particles(path, pos.data(), vel.data(), s->np, s->cfg.output_format, s->err)) {
-                rc = FP_ERR_IO;
-                break;
-            }
+            rc = writer.submit(int(frame++ & 1), tmpl + std::to_string(r2 ? i : i / ipf) + ext);
+            if (rc) break;
             if (csv) {
                 std::fprintf(csv, "%lld,%g,%g,%g,%g,%g,%g\n", (long long)(i / ipf), s->stats.body_pos[0],
                              s->stats.body_pos[1], s->stats.body_pos[2], s->stats.body_angles[0],
@@ -1221,6 +1323,10 @@ int fp_run(fp_solver* s, int frames) {
         }
     }
     if (csv) std::fclose(csv);
+    if (out) {
+        const int wrc = writer.finish();
+        if (rc == FP_OK) rc = wrc;
+    }
     return rc;
 }
 

@@ -160,3 +160,38 @@ def test_scene_file_round_trip(tmp_path):
     p = tmp_path / "s.txt"
     scenes.write_labels3d(p, lab)
     assert np.array_equal(capi.read_label_file(p, 3), lab)
+
+
+def test_particle_writer_formats(tmp_path):
+    """ASCII PLY / OFF lines are "x y z" as an ostream of floats prints them
+    (saveParticlesToPLY, utility.cu:91-127): %g with six significant digits.
+    Binary PLY round-trips exactly through the reader."""
+    from fluidprjct_b200 import capi
+    rng = np.random.default_rng(0)
+    odd = [0.0, -0.0, 1e-5, 1.23456789e-5, 1e-4, 123456.7, 1234567.0, 1e-30, -7.5e20, 0.5, 1 / 3, 2 / 3, 3.4e38,
+           -2.0 ** -126, 9.999995, 99999.95]
+    pos = np.concatenate([rng.uniform(-2, 2, 3 * 300_000), odd, [0.25, 0.5]]).astype(np.float32).reshape(-1, 3)
+    vel = rng.uniform(-1, 1, pos.shape).astype(np.float32)
+    lib = capi.lib()
+    p = tmp_path / "a.ply"
+    assert lib.fp_write_particle_file(str(p).encode(), capi.ptr(pos), None, len(pos), capi.OUT_PLY) == 0
+    lines = p.read_bytes().decode().split("\n")
+    assert lines[:6] == ["ply", "format ascii 1.0", f"element vertex {len(pos)}", "property float x",
+                         "property float y", "property float z"] and lines[6] == "end_header"
+    body = lines[7:-1]
+    assert len(body) == len(pos)
+    idx = list(range(0, len(pos), 997)) + list(range(len(pos) - 8, len(pos)))
+    for q in idx:
+        assert body[q] == "%g %g %g" % tuple(float(v) for v in pos[q]), q
+    o = tmp_path / "a.off"
+    assert lib.fp_write_particle_file(str(o).encode(), capi.ptr(pos), None, len(pos), capi.OUT_OFF) == 0
+    assert o.read_text().split("\n")[:2] == ["OFF", f"{len(pos)} 0 0"]
+    b = tmp_path / "b.ply"
+    assert lib.fp_write_particle_file(str(b).encode(), capi.ptr(pos), capi.ptr(vel), len(pos),
+                                      capi.OUT_PLY_BINARY) == 0
+    n = C.c_int64()
+    hv = C.c_int()
+    lib.fp_read_ply_file(str(b).encode(), C.byref(n), None, None, C.byref(hv))
+    p2, v2 = np.zeros_like(pos), np.zeros_like(vel)
+    lib.fp_read_ply_file(str(b).encode(), C.byref(n), capi.ptr(p2), capi.ptr(v2), C.byref(hv))
+    assert n.value == len(pos) and hv.value == 1 and np.array_equal(p2, pos) and np.array_equal(v2, vel)
