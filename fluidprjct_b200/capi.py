@@ -20,6 +20,7 @@ OUT_PLY, OUT_OFF, OUT_PLY_BINARY, OUT_NONE = 0, 1, 2, 3
 SOLVER_PCG, SOLVER_PCG_MIXED, SOLVER_PCG_MG, SOLVER_PCG_LEARNED = 0, 1, 2, 3
 ADVECT_RK3REF, ADVECT_RK2 = 0, 1
 SCHEME_DEFAULT, SCHEME_REF2D = 0, 1
+BODY_FORCES_FACE_FRACTION, BODY_FORCES_REFERENCE = 0, 1
 GRID_U, GRID_V, GRID_W, GRID_U_SAVED, GRID_V_SAVED, GRID_W_SAVED, GRID_P, GRID_RHS = range(8)
 (PHASE_LABEL, PHASE_P2G, PHASE_SAVE, PHASE_FORCES, PHASE_PRESSURE, PHASE_PROJECT, PHASE_BODY, PHASE_G2P,
  PHASE_ADVECT, PHASE_CLEANUP) = range(10)
@@ -35,7 +36,7 @@ class FpConfig(C.Structure):
         ("active_body", C.c_int), ("body_pos", C.c_float * 3), ("body_mass", C.c_float),
         ("ppc", C.c_int), ("seed", C.c_uint32), ("solver", C.c_int), ("advection", C.c_int), ("cfl", C.c_float),
         ("tol", C.c_double), ("max_iters", C.c_int), ("body_radius", C.c_float), ("body_density", C.c_float),
-        ("device", C.c_int), ("scheme", C.c_int), ("extrapolate", C.c_int),
+        ("device", C.c_int), ("scheme", C.c_int), ("extrapolate", C.c_int), ("body_forces", C.c_int),
     ]
 
 
@@ -176,6 +177,8 @@ def default_config(**kw) -> FpConfig:
             cfg.advection = {"rk3ref": ADVECT_RK3REF, "rk2": ADVECT_RK2}[v]
         elif k == "scheme" and isinstance(v, str):
             cfg.scheme = {"default": SCHEME_DEFAULT, "ref2d": SCHEME_REF2D}[v]
+        elif k == "body_forces" and isinstance(v, str):
+            cfg.body_forces = {"face_fraction": BODY_FORCES_FACE_FRACTION, "reference": BODY_FORCES_REFERENCE}[v]
         else:
             setattr(cfg, k, v)
     return cfg

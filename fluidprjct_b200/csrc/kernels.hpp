@@ -131,6 +131,21 @@ void launch_apply_mark(uint8_t* labels, const uint8_t* mark, Dims g, cudaStream_
 void launch_body_force(const float* p, const uint8_t* labels, Dims g, const BodyShape& b, double* part, double* out,
                        cudaStream_t st);
 int body_force_partials();
+// The reference's body forces: out[0..5] = panel drag + lift force and torque
+// about cm, out[6..7] = body volume and submerged volume from the SDF voxels.
+// part holds body_force_partials() doubles; pos/start are the cell-sorted
+// particles.  sdf = null samples the analytic sphere |x - local_com| - radius.
+struct RefBuoyancy {
+    const float* sdf;
+    int sw, sh, sd;
+    float cs;
+    float3 origin, local_com, com;
+    float radius;
+    float rot[9];
+};
+void launch_ref_body_forces(const uint8_t* labels, const float* u, const float* v, const float* w, Dims g, float3 cm,
+                            float3 bvel, const RefBuoyancy& b, const float4* pos, const int* start, double* part,
+                            double* out, cudaStream_t st);
 
 // -------- particle order helpers --------
 // out[pid] = in[slot] for the xyz part of float4 arrays (pid in pos.w bits).

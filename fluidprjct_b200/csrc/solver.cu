@@ -64,6 +64,7 @@ struct HostBody {
     // voxel SDF
     int nx = 0, ny = 0, nz = 0;
     float origin[3] = {0, 0, 0}, cell = 1, local_com[3] = {0, 0, 0};
+    std::vector<float> sdf_host;  // voxel SDF values (surface-point output)
     // paddle: face at x0 + amp sin(2 pi t / period), t since fp_set_paddle
     double pad_x0 = 0, pad_amp = 0, pad_period = 1, pad_t = 0;
 
@@ -542,8 +543,82 @@ void phase_project(fp_solver* s) {
 
 // updateBody (FluidSolver3D.cu:2793-2846): fluid force and torque from the
 // pressure (FP64 reduction on the GPU), gravity m*g, then integrate.
+// The SDF voxel grid of the body for the reference's buoyancy and surface
+// points: the file's grid, or the analytic sphere sampled on a grid of
+// spacing dx / 2 centred on its centre of mass (local_com = 0).
+RefBuoyancy ref_voxels(const fp_solver* s) {
+    const HostBody& h = s->hb;
+    RefBuoyancy b{};
+    b.com = make_float3(float(h.pos[0]), float(h.pos[1]), float(h.pos[2]));
+    for (int i = 0; i < 9; ++i) b.rot[i] = float(h.R[i]);
+    if (h.kind == BODY_SDF) {
+        b.sdf = s->d_sdf;
+        b.sw = h.nx; b.sh = h.ny; b.sd = h.nz;
+        b.cs = h.cell;
+        b.origin = make_float3(h.origin[0], h.origin[1], h.origin[2]);
+        b.local_com = make_float3(h.local_com[0], h.local_com[1], h.local_com[2]);
+    } else {
+        b.sdf = nullptr;
+        b.cs = 0.5f * s->cfg.dx;
+        const int n = int(std::ceil(2.0 * (h.radius + 2.0 * b.cs) / b.cs));
+        b.sw = b.sh = b.sd = n;
+        const float o = -0.5f * float(n) * b.cs;
+        b.origin = make_float3(o, o, o);
+        b.local_com = make_float3(0.0f, 0.0f, 0.0f);
+        b.radius = float(h.radius);
+    }
+    return b;
+}
+
+// generateSurfacePoints(0.5 dx) (utility.cuh:339-374): voxel corners with
+// |sdf| < dx / 2, rotated about the local centre of mass into the world.
+void body_surface_points(const fp_solver* s, std::vector<float>& pts) {
+    pts.clear();
+    const HostBody& h = s->hb;
+    const RefBuoyancy b = ref_voxels(s);
+    const float lim = 0.5f * s->cfg.dx;
+    for (int k = 0; k < b.sd; ++k)
+        for (int j = 0; j < b.sh; ++j)
+            for (int i = 0; i < b.sw; ++i) {
+                const float plx = b.origin.x + float(i) * b.cs, ply = b.origin.y + float(j) * b.cs,
+                            plz = b.origin.z + float(k) * b.cs;
+                const float cx = plx - b.local_com.x, cy = ply - b.local_com.y, cz = plz - b.local_com.z;
+                float sdf;
+                if (h.kind == BODY_SDF) sdf = h.sdf_host[size_t(i) + size_t(j) * b.sw + size_t(k) * b.sw * b.sh];
+                else sdf = std::sqrt((cx * cx + cy * cy) + cz * cz) - b.radius;
+                if (!(std::fabs(sdf) < lim)) continue;
+                pts.push_back(b.com.x + ((b.rot[0] * cx + b.rot[1] * cy) + b.rot[2] * cz));
+                pts.push_back(b.com.y + ((b.rot[3] * cx + b.rot[4] * cy) + b.rot[5] * cz));
+                pts.push_back(b.com.z + ((b.rot[6] * cx + b.rot[7] * cy) + b.rot[8] * cz));
+            }
+}
+
 int phase_body(fp_solver* s) {
     if (!body_on(s)) return FP_OK;
+    if (s->cfg.body_forces == FP_BODY_FORCES_REFERENCE && s->hb.kind != BODY_PADDLE) {
+        // updateBody (FluidSolver3D.cu:2793-2846): F = m g + panel drag/lift,
+        // then applyBuoyancy adds -rho V_submerged g; the panel torque only.
+        HostBody& h = s->hb;
+        if (!s->sorted) phase_label(s);  // the buoyancy searches the cell-sorted particles
+        const float3 cm = make_float3(float(h.pos[0]), float(h.pos[1]), float(h.pos[2]));
+        const float3 bv = make_float3(float(h.vel[0]), float(h.vel[1]), float(h.vel[2]));
+        launch_ref_body_forces(s->d_labels, s->d_u, s->d_v, s->d_w, s->g, cm, bv, ref_voxels(s), s->d_pos, s->d_start,
+                               s->d_bpart, s->d_bforce, s->st);
+        s->launches += 4;
+        cudaMemcpyAsync(s->h_bforce, s->d_bforce, sizeof(double) * 8, cudaMemcpyDeviceToHost, s->st);
+        cudaError_t e = cudaStreamSynchronize(s->st);
+        if (e != cudaSuccess) return s->cuda_fail(e, "reference body forces");
+        const double buoy = 1000.0 * s->h_bforce[7] * -double(kGravity[1]);
+        for (int a = 0; a < 3; ++a) {
+            h.force[a] = h.mass * double(kGravity[a]) + s->h_bforce[a] + (a == 1 ? buoy : 0.0);
+            h.torque[a] = s->h_bforce[3 + a];
+            s->stats.body_force[a] = h.force[a];
+            s->stats.body_torque[a] = h.torque[a];
+        }
+        h.integrate(double(s->cfg.dt));
+        fill_body_stats(s);
+        return FP_OK;
+    }
     launch_body_force(s->d_p, s->d_labels, s->g, body_shape(s), s->d_bpart, s->d_bforce, s->st);
     s->launches += 2;
     cudaMemcpyAsync(s->h_bforce, s->d_bforce, sizeof(double) * 6, cudaMemcpyDeviceToHost, s->st);
@@ -904,7 +979,8 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
         delete s;
         return FP_ERR_ARG;
     }
-    if (s->cfg.extrapolate < 0) {
+    if (s->cfg.extrapolate < 0 ||
+        (s->cfg.body_forces != FP_BODY_FORCES_FACE_FRACTION && s->cfg.body_forces != FP_BODY_FORCES_REFERENCE)) {
         delete s;
         return FP_ERR_ARG;
     }
@@ -925,7 +1001,7 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_nf, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_bad, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&s->d_bad, sizeof(int));
-    if (e == cudaSuccess) e = cudaMallocHost(&s->h_bforce, sizeof(double) * 6);
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_bforce, sizeof(double) * 8);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_r2, sizeof(int) * 2);
     if (e != cudaSuccess) {
         std::fprintf(stderr, "fp_create: %s\n", cudaGetErrorString(e));
@@ -1072,8 +1148,9 @@ int fp_load_sdf(fp_solver* s, const char* path) {
         if (e == cudaSuccess) e = cudaMemcpy(s->d_sdf, data.data(), sizeof(float) * data.size(), cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess) e = dalloc(&s->d_bpart, size_t(body_force_partials()));
-    if (e == cudaSuccess) e = dalloc(&s->d_bforce, 6);
+    if (e == cudaSuccess) e = dalloc(&s->d_bforce, 8);
     if (e != cudaSuccess) { free_body(s); return s->cuda_fail(e, "body upload"); }
+    h.sdf_host = std::move(data);
     h.loaded = true;
     s->cfg.active_body = 1;
     // init's marking before seeding (FluidSolver3D.cu:177-193)
@@ -1101,7 +1178,7 @@ int fp_set_paddle(fp_solver* s, float x_rest, float amplitude, float period) {
     h.pos[2] = 0.5 * s->D * s->cfg.dx;
     h.paddle_at(0.0);
     cudaError_t e = dalloc(&s->d_bpart, size_t(body_force_partials()));
-    if (e == cudaSuccess) e = dalloc(&s->d_bforce, 6);
+    if (e == cudaSuccess) e = dalloc(&s->d_bforce, 8);
     if (e != cudaSuccess) { free_body(s); return s->cuda_fail(e, "paddle"); }
     h.loaded = true;
     s->cfg.active_body = 1;
@@ -1314,6 +1391,15 @@ int fp_run(fp_solver* s, int frames) {
             const char* ext = s->cfg.output_format == FP_OUT_OFF ? ".off" : ".ply";
             rc = writer.submit(int(frame++ & 1), tmpl + std::to_string(r2 ? i : i / ipf) + ext);
             if (rc) break;
+            if (body_on(s) && s->hb.kind != BODY_PADDLE) {  // body_<frame>.ply (run, :3130-3132)
+                std::vector<float> pts;
+                body_surface_points(s, pts);
+                const std::string bp = frame_dir(tmpl) + "/body_" + std::to_string(i / ipf) + ".ply";
+                if (!io::write_particles(bp, pts.data(), nullptr, int64_t(pts.size() / 3), FP_OUT_PLY, s->err)) {
+                    rc = FP_ERR_IO;
+                    break;
+                }
+            }
             if (csv) {
                 std::fprintf(csv, "%lld,%g,%g,%g,%g,%g,%g\n", (long long)(i / ipf), s->stats.body_pos[0],
                              s->stats.body_pos[1], s->stats.body_pos[2], s->stats.body_angles[0],

@@ -74,6 +74,14 @@ enum { FP_ADVECT_RK3REF = 0, FP_ADVECT_RK2 = 1 };
  * cfl are unused (the reference fixes Euler and C = 1). */
 enum { FP_SCHEME_DEFAULT = 0, FP_SCHEME_REF2D = 1 };
 
+/* Fluid force on the rigid body.  FP_BODY_FORCES_FACE_FRACTION (default):
+ * the pressure integral over SDF face fractions, an FP64 reduction.
+ * FP_BODY_FORCES_REFERENCE: the reference's panel drag and lift
+ * (DragLiftForceCalculator, FluidSolver3D.cu:2674-2791; Cd = Cl = 0.1) plus
+ * its voxel buoyancy (applyBuoyancy, :2917-3026), summed in FP64; the
+ * analytic sphere is sampled on a voxel grid of spacing dx / 2 for it. */
+enum { FP_BODY_FORCES_FACE_FRACTION = 0, FP_BODY_FORCES_REFERENCE = 1 };
+
 /* Grid selectors for fp_get_grid / fp_set_grid.  FP_GRID_RHS (read only) is
  * the dense right-hand side of the last pressure solve, zero off FLUID cells
  * (the reference's RHS, FluidSolver3D.cu:1518-1596, before compaction). */
@@ -118,6 +126,7 @@ typedef struct fp_config {
                                       default scheme: this many wavefront layers into
                                       faces with no FLUID side, between G2P and
                                       advection */
+    int      body_forces;          /* FP_BODY_FORCES_* (default face fractions)   */
 } fp_config;
 
 /* Per-step statistics: the reference's cudaEvent phase timers

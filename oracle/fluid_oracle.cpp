@@ -123,6 +123,8 @@ template <class R> struct Sim3 {
     std::vector<R> u, v, w, us, vs, ws, p;
     std::vector<R> px, py, pz, vx, vy, vz;
     int extrap = 0;  // layers of velocity extrapolation between G2P and advection
+    int ref_forces = 0;  // 1: the reference's panel drag/lift and voxel buoyancy
+    double ref_out[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // last reference force, torque, volumes
     int last_iters = 0;
     double last_res = 0.0;
     int last_nf = 0;
@@ -593,9 +595,102 @@ template <class R> struct Sim3 {
                 out[3] += ry * fz - rz * fy; out[4] += rz * fx - rx * fz; out[5] += rx * fy - ry * fx;
             }
     }
+    // The reference's body forces (FP32 panels and voxels, FP64 sums):
+    // DragLiftForceCalculator (:2674-2791) over BODY cells' FLUID faces, and
+    // applyBuoyancy (:2917-3026) over the sphere sampled on a dx/2 voxel grid.
+    void ref_body_forces(double out[8]) const {
+        for (int m = 0; m < 8; ++m) out[m] = 0.0;
+        const float fdx = float(dx), rho = 1000.0f;
+        const float cmx = float(ob.pos[0]), cmy = float(ob.pos[1]), cmz = float(ob.pos[2]);
+        const float bvx = float(ob.vel[0]), bvy = float(ob.vel[1]), bvz = float(ob.vel[2]);
+        auto cross = [](float ax, float ay, float az, float bx, float by, float bz, float& cx, float& cy, float& cz) {
+            cx = ay * bz - az * by; cy = az * bx - ax * bz; cz = ax * by - ay * bx;
+        };
+        for (int k = 0; k < D; ++k) for (int j = 0; j < H; ++j) for (int i = 0; i < W; ++i) {
+            if (labels[cidx(i, j, k)] != BODY) continue;
+            for (int dir = 0; dir < 6; ++dir) {
+                const int ax = dir >> 1, sg = (dir & 1) ? -1 : 1;
+                const int ni = i + (ax == 0) * sg, nj = j + (ax == 1) * sg, nk = k + (ax == 2) * sg;
+                if (ni < 0 || ni >= W || nj < 0 || nj >= H || nk < 0 || nk >= D) continue;
+                if (labels[cidx(ni, nj, nk)] != FLUID) continue;
+                const float nx = ax == 0 ? float(sg) : 0.0f, ny = ax == 1 ? float(sg) : 0.0f, nz = ax == 2 ? float(sg) : 0.0f;
+                const float fcx = (float(i) + 0.5f) * fdx + (nx * 0.5f) * fdx;
+                const float fcy = (float(j) + 0.5f) * fdx + (ny * 0.5f) * fdx;
+                const float fcz = (float(k) + 0.5f) * fdx + (nz * 0.5f) * fdx;
+                const float rx = fcx - cmx, ry = fcy - cmy, rz = fcz - cmz;
+                const V3<R> up = interp_vel(mk(R(fcx), R(fcy), R(fcz)));
+                const float urx = bvx - float(up.x), ury = bvy - float(up.y), urz = bvz - float(up.z);
+                const float ua = std::sqrt((urx * urx + ury * ury) + urz * urz);
+                const float area = fdx * fdx;
+                float A = 0.0f;
+                const float nu = (nx * urx + ny * ury) + nz * urz;
+                if (nu > 0.0f) A = (nu / ua * 0.5f + (1.0f - 0.5f)) * area;
+                const float sd = float(-0.5 * double(rho) * double(0.1f) * double(A) * double(ua));
+                const float fdx_ = urx * sd, fdy = ury * sd, fdz = urz * sd;
+                float cx, cy, cz;
+                cross(nx, ny, nz, urx, ury, urz, cx, cy, cz);
+                const float cxa = std::sqrt((cx * cx + cy * cy) + cz * cz);
+                float lx, ly, lz;
+                cross(urx, ury, urz, cx / cxa, cy / cxa, cz / cxa, lx, ly, lz);
+                const float sl = (((-0.5f * rho) * 0.1f) * A) * ua;
+                const float flx = lx * sl, fly = ly * sl, flz = lz * sl;
+                float t1x, t1y, t1z, t2x, t2y, t2z;
+                cross(rx, ry, rz, fdx_, fdy, fdz, t1x, t1y, t1z);
+                cross(rx, ry, rz, flx, fly, flz, t2x, t2y, t2z);
+                out[0] += double(fdx_ + flx); out[1] += double(fdy + fly); out[2] += double(fdz + flz);
+                out[3] += double(t1x + t2x); out[4] += double(t1y + t2y); out[5] += double(t1z + t2z);
+            }
+        }
+        // buoyancy voxels: sphere on a grid of spacing dx/2 centred on the centre of mass
+        const float cs = 0.5f * fdx;
+        const int n = int(std::ceil(2.0 * (ob.radius + 2.0 * cs) / cs));
+        const float o = -0.5f * float(n) * cs, r = float(ob.radius);
+        float Rf[9];
+        for (int m = 0; m < 9; ++m) Rf[m] = float(ob.Rm[m]);
+        std::vector<std::vector<int>> bins(nc());
+        for (size_t q = 0; q < np(); ++q) {
+            int i, j, k;
+            cell_of(px[q], py[q], pz[q], i, j, k);
+            bins[cidx(i, j, k)].push_back(int(q));
+        }
+        const float rad = 2.0f * fdx;
+        for (int k = 0; k < n; ++k) for (int j = 0; j < n; ++j) for (int i = 0; i < n; ++i) {
+            const float plx = o + float(i) * cs, ply = o + float(j) * cs, plz = o + float(k) * cs;
+            const float sdf = std::sqrt((plx * plx + ply * ply) + plz * plz) - r;
+            if (sdf > 0.0f) continue;
+            const float vx = cmx + ((Rf[0] * plx + Rf[1] * ply) + Rf[2] * plz);
+            const float vy = cmy + ((Rf[3] * plx + Rf[4] * ply) + Rf[5] * plz);
+            const float vz = cmz + ((Rf[6] * plx + Rf[7] * ply) + Rf[8] * plz);
+            float vol = (cs * cs) * cs;
+            if (sdf > -cs) vol = vol * (0.5f - (0.5f * sdf) / cs);
+            out[6] += double(vol);
+            const int ii = std::min(std::max(int(vx / fdx), 0), W - 1), jj = std::min(std::max(int(vy / fdx), 0), H - 1),
+                      kk = std::min(std::max(int(vz / fdx), 0), D - 1);
+            bool sub = labels[cidx(ii, jj, kk)] == FLUID;
+            for (int q : bins[cidx(ii, jj, kk)]) {
+                if (sub) break;
+                const float ex = float(px[q]) - vx, ey = float(py[q]) - vy, ez = float(pz[q]) - vz;
+                sub = std::sqrt((ex * ex + ey * ey) + ez * ez) < rad;
+            }
+            if (sub) out[7] += double(vol);
+        }
+    }
+
     // updateBody (:2793-2846) with the pressure-integral force.
     void body_phase() {
         if (!ob.loaded) return;
+        if (ref_forces && !ob.paddle) {
+            ref_body_forces(ref_out);
+            const double g[3] = {0.0, double(-9.81f), 0.0};
+            const double buoy = 1000.0 * ref_out[7] * double(9.81f);
+            for (int a = 0; a < 3; ++a) {
+                ob.force[a] = ob.mass * g[a] + ref_out[a] + (a == 1 ? buoy : 0.0);
+                ob.torque[a] = ref_out[3 + a];
+            }
+            ob.integrate(double(float(dt)));
+            sync_body_kin();
+            return;
+        }
         double f[6];
         body_force(f);
         const double g[3] = {0.0, double(-9.81f), 0.0};
@@ -900,6 +995,12 @@ void or3_set_params(void* p, double pic_weight, double cfl, double tol, int maxi
         s.alpha = R(float(pic_weight)); s.cfl = R(float(cfl)); s.tol = tol; s.maxit = maxit; return 0;
     });
 }
+void or3_set_ref_forces(void* p, int on) {
+    with(static_cast<Handle*>(p), [&](auto& s) { s.ref_forces = on; return 0; });
+}
+void or3_ref_forces(void* p, double* out) {  // out[8]: of the last body phase
+    with(static_cast<Handle*>(p), [&](auto& s) { for (int m = 0; m < 8; ++m) out[m] = s.ref_out[m]; return 0; });
+}
 void or3_set_extrap(void* p, int layers) {
     with(static_cast<Handle*>(p), [&](auto& s) { s.extrap = layers; return 0; });
 }
@@ -912,6 +1013,8 @@ void or3_set_body(void* p, const double* vel, const double* omega, const double*
         s.body.vel = {R(float(vel[0])), R(float(vel[1])), R(float(vel[2]))};
         s.body.omega = {R(float(omega[0])), R(float(omega[1])), R(float(omega[2]))};
         s.body.com = {R(float(com[0])), R(float(com[1])), R(float(com[2]))};
+        if (s.ob.loaded)  // the loaded body's own state too (fp_set_body_state)
+            for (int a = 0; a < 3; ++a) { s.ob.vel[a] = vel[a]; s.ob.omega[a] = omega[a]; s.ob.pos[a] = com[a]; }
         return 0;
     });
 }

@@ -57,6 +57,8 @@ def lib():
         L.or3_set_sphere.argtypes = [P, P, D, D]
         L.or3_set_paddle.argtypes = [P, D, D, D]
         L.or3_set_extrap.argtypes = [P, I]
+        L.or3_set_ref_forces.argtypes = [P, I]
+        L.or3_ref_forces.argtypes = [P, P]
         L.or2r_set_extrap.argtypes = [P, I]
         L.or3_body_state.argtypes = [P, P]
         L.or3_body_force.argtypes = [P, P]
@@ -210,6 +212,16 @@ class Sim3:
     def set_extrapolate(self, layers):
         """Velocity extrapolation layers between G2P and advection (0 = off)."""
         lib().or3_set_extrap(self.h, layers)
+
+    def set_reference_forces(self, on=True):
+        """The reference's panel drag/lift and voxel buoyancy in the body phase."""
+        lib().or3_set_ref_forces(self.h, int(bool(on)))
+
+    def reference_forces(self):
+        """Force, torque, body volume, submerged volume of the last body phase."""
+        out = np.zeros(8, np.float64)
+        lib().or3_ref_forces(self.h, _p(out))
+        return out
 
     def body_state(self):
         out = np.zeros(18, np.float64)

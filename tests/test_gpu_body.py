@@ -13,12 +13,12 @@ from conftest import rel_l2
 pytestmark = pytest.mark.gpu
 
 
-def _pool(O, n=40, level=0.7, c=(0.5, 0.35, 0.5), r=0.12, density=0.5, seed=3, dt=0.002):
+def _pool(O, n=40, level=0.7, c=(0.5, 0.35, 0.5), r=0.12, density=0.5, seed=3, dt=0.002, **kw):
     from fluidprjct_b200 import capi, scenes
     dx = 1.0 / n
     lab = scenes.box_3d(n, n, n, dx, 2.0, level, 2.0)
     s = capi.Solver(dx=dx, dt=dt, pic_weight=0.05, solver="pcg_mixed", tol=1e-9, body_radius=r,
-                    body_density=density, body_pos=c, active_body=1)
+                    body_density=density, body_pos=c, active_body=1, **kw)
     s.set_labels(lab)
     s.load_sdf(None)
     marked = s.labels()
@@ -99,3 +99,79 @@ def test_rigid_body_drop_160(O):
     # in the air the body falls freely: v_y = -g t after 5 steps
     assert abs(st["body_vel"][1] - (-9.81 * 0.002 * 5)) < 1e-3
     assert abs(st["body_pos"][0] - 0.5) < 1e-6 and abs(st["body_pos"][2] - 0.5) < 1e-6
+
+
+def test_reference_body_forces_match_oracle(O):
+    """body_forces = reference: the panel drag/lift of DragLiftForceCalculator
+    (FluidSolver3D.cu:2674-2791) and the voxel buoyancy of applyBuoyancy
+    (:2917-3026).  From the same labels, particles and (random) face
+    velocities, the GPU force and torque match the oracle's."""
+    from fluidprjct_b200 import capi
+    s, o, lab, pos, mass = _pool(O, n=40, c=(0.5, 0.4, 0.5), r=0.12, body_forces="reference")
+    o.set_reference_forces(True)
+    s.phase(capi.PHASE_LABEL)
+    o.phase(O.PH_LABEL)
+    bv, om, c = [0.05, -0.2, 0.1], [0.0, 0.0, 0.0], [0.5, 0.4, 0.5]
+    s.set_body_state(c, bv, om)
+    o.set_body(np.array(bv), np.array(om), np.array(c))
+    rng = np.random.default_rng(4)
+    for g, go in ((capi.GRID_U, O.GRID_U), (capi.GRID_V, O.GRID_V), (capi.GRID_W, O.GRID_W)):
+        f = rng.uniform(-1, 1, s.grid_shape(g)).astype(np.float32)
+        s.set_grid(g, f)
+        o.set_grid(go, f.astype(np.float64))
+    s.phase(capi.PHASE_BODY)
+    o.phase(O.PH_BODY)
+    st = s.stats()
+    ref = o.reference_forces()
+    g = float(np.float32(-9.81))
+    V = 4.0 / 3.0 * np.pi * float(np.float32(0.12)) ** 3
+    # The voxels sample the sphere's volume.  The reference skips voxels with
+    # 0 < sdf < cs although its fraction 1/2 - sdf/(2 cs) would count half of
+    # them: about half a voxel shell (7.8 % of V here) is missing.  Only voxels
+    # whose cell is FLUID (or holds a particle within 2 dx) count as
+    # submerged, so a submerged body's interior (BODY cells, no particles)
+    # does not: the reference's buoyancy is a surface shell's.
+    assert 0.88 < ref[6] / V < 1.0 and 0.0 < ref[7] < 0.5 * ref[6]
+    assert np.isfinite(ref).all() and abs(ref[0]) > 0
+    f_ref = mass * np.array([0.0, g, 0.0]) + ref[:3] + np.array([0.0, 1000.0 * ref[7] * -g, 0.0])
+    assert np.allclose(st["body_force"], f_ref, rtol=1e-5, atol=1e-5 * np.abs(ref[:3]).max())
+    assert np.allclose(st["body_torque"], ref[3:6], rtol=1e-5, atol=1e-5 * np.abs(ref[3:6]).max())
+
+
+def test_reference_lift_is_nan_where_the_reference_is(O):
+    """The reference normalises n x u_rel for the lift (:2769-2771): a panel
+    whose interpolated fluid velocity equals the body's (its stencil touches
+    only faces set to the body velocity by the projection) gives 0/0, and the
+    NaN survives the zero panel area.  A sphere at rest in still water hits
+    that on its first step; the restatement does too, in the same place."""
+    from fluidprjct_b200 import capi
+    s, o, lab, pos, mass = _pool(O, n=40, c=(0.5, 0.4, 0.5), r=0.12, body_forces="reference")
+    o.set_reference_forces(True)
+    for ph_s, ph_o in ((capi.PHASE_LABEL, O.PH_LABEL), (capi.PHASE_P2G, O.PH_P2G), (capi.PHASE_SAVE, O.PH_SAVE),
+                       (capi.PHASE_FORCES, O.PH_FORCES), (capi.PHASE_PRESSURE, O.PH_PRESSURE)):
+        s.phase(ph_s)
+        o.phase(ph_o)
+    o.set_grid(O.GRID_P, s.grid(capi.GRID_P).astype(np.float64))
+    s.phase(capi.PHASE_PROJECT)
+    o.phase(O.PH_PROJECT)
+    for g, go in ((capi.GRID_U, O.GRID_U), (capi.GRID_V, O.GRID_V), (capi.GRID_W, O.GRID_W)):
+        o.set_grid(go, s.grid(g).astype(np.float64))
+    s.phase(capi.PHASE_BODY)
+    o.phase(O.PH_BODY)
+    assert np.array_equal(np.isnan(s.stats()["body_force"]), np.isnan(o.body_state()["force"]))
+    assert np.isnan(o.reference_forces()[:3]).any()
+
+
+def test_run_writes_body_surface_points(O, tmp_path):
+    """fp_run writes body_<frame>.ply beside the frames: the SDF voxel corners
+    with |sdf| < dx/2 (generateSurfacePoints(0.5 dx), utility.cuh:339-374)."""
+    from fluidprjct_b200 import capi
+    s, o, lab, pos, mass = _pool(O, n=32, c=(0.5, 0.5, 0.5), r=0.15, output_format=capi.OUT_PLY_BINARY,
+                                 output_template=str(tmp_path / "p_"), iter_per_frame=2)
+    s.run(2)
+    names = sorted(f.name for f in tmp_path.iterdir())
+    assert names == ["body_0.ply", "body_1.ply", "body_2.ply", "csvRes.csv", "p_0.ply", "p_1.ply", "p_2.ply"]
+    pts, _ = capi.read_ply_file(tmp_path / "body_2.ply")
+    c = np.array(s.stats()["body_pos"])
+    d = np.linalg.norm(pts - c, axis=1)
+    assert len(pts) > 500 and np.all(np.abs(d - 0.15) < 0.5 / 32 + 1e-4)
