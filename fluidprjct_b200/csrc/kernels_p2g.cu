@@ -101,8 +101,10 @@ __device__ __forceinline__ void splat_cell(const float4* __restrict__ pos, const
             }
 }
 
+// Three CTAs per SM: 80 registers and no spills, against 126 registers and
+// two CTAs unbounded; the walk over a cell's particles is latency-bound.
 template <int BX, int BY, int BZ, int NT>
-__global__ void __launch_bounds__(NT) k_p2g(const float4* __restrict__ pos, const float4* __restrict__ vel,
+__global__ void __launch_bounds__(NT, 3) k_p2g(const float4* __restrict__ pos, const float4* __restrict__ vel,
                                             const int* __restrict__ start, Dims g, float dt, float3 grav,
                                             float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
                                             float* __restrict__ us, float* __restrict__ vs, float* __restrict__ ws,
