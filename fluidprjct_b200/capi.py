@@ -37,6 +37,7 @@ class FpConfig(C.Structure):
         ("ppc", C.c_int), ("seed", C.c_uint32), ("solver", C.c_int), ("advection", C.c_int), ("cfl", C.c_float),
         ("tol", C.c_double), ("max_iters", C.c_int), ("body_radius", C.c_float), ("body_density", C.c_float),
         ("device", C.c_int), ("scheme", C.c_int), ("extrapolate", C.c_int), ("body_forces", C.c_int),
+        ("mg_sweeps", C.c_int),
     ]
 
 

@@ -70,8 +70,10 @@ void launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStre
 // entry and on exit.
 // x0: compact initial guess (scaled on the device by its energy-optimal
 // factor), or null to start from x = 0.
+// nu0: red-black sweep pairs before and after the coarse correction on the
+// finest level (coarser levels take one pair; the cycle stays symmetric).
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
-                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0 = nullptr);
+                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0 = nullptr, int nu0 = 2);
 
 // -------- labelling and the particle sort (kernels_sort.cu) --------
 // counts[nc] must be zero on entry.  Writes key/rank per particle.

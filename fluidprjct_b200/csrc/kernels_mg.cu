@@ -40,6 +40,7 @@ struct MgArgs {
     float rscale;                // restriction scale (1/4 in 3D, 1/2 in 2D)
     float omega;                 // over-relaxation of the coarse-grid correction
     int nu_coarse;               // symmetric sweep pairs on the coarsest level
+    int nu0;                     // red-black sweep pairs before and after on level 0 (coarser: 1)
     MgLevel lv[MG_MAX_LEVELS];
     double* p;                   // level-0 padded dense Krylov vectors (FP64)
     double* q;
@@ -262,10 +263,18 @@ __device__ bool vcycle(const MgArgs& a) {
     if (!grid_barrier(a.bar, nb, a.status)) return false;
     const int G = min(a.G, a.L - 1);
     const int nf = *a.nf;
+    // one grid-wide sweep of level l (colour 0 red, 1 black) and a barrier
+    auto sweep = [&](int l, int color) {
+        if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, color, t0, st);
+        else op_sweep(a.lv[l], color, t0, st);
+        return grid_barrier(a.bar, nb, a.status);
+    };
     for (int l = 0; l < G; ++l) {
-        if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 1, t0, st);
-        else op_sweep(a.lv[l], 1, t0, st);
-        if (!grid_barrier(a.bar, nb, a.status)) return false;
+        // pre-smoothing (red, black)^nu (nu = nu0 on level 0, else 1); the first
+        // red sweep is fused upstream
+        if (!sweep(l, 1)) return false;
+        for (int e = 1; e < (l == 0 ? a.nu0 : 1); ++e)
+            if (!sweep(l, 0) || !sweep(l, 1)) return false;
         op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
@@ -277,9 +286,12 @@ __device__ bool vcycle(const MgArgs& a) {
         if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
     for (int l = G - 1; l >= 0; --l) {
-        if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 1, t0, st);
-        else op_sweep(a.lv[l], 1, t0, st);
-        if (!grid_barrier(a.bar, nb, a.status)) return false;
+        // post-smoothing (black, red)^nu, the reverse of the pre-smoothing; the
+        // first red sweep was fused with the prolongation, the last red sweep
+        // with the next prolongation
+        if (!sweep(l, 1)) return false;
+        for (int e = 1; e < (l == 0 ? a.nu0 : 1); ++e)
+            if (!sweep(l, 0) || !sweep(l, 1)) return false;
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 0, t0, st);
         else if (l == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
         else op_prolong_red(a.lv[l - 1], a.lv[l], a.omega, t0, st);
@@ -510,7 +522,7 @@ void launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStre
 }
 
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
-                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0) {
+                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0, int nu0) {
     const int nb = mg_max_blocks();
     int* status = &pb.out->status;
     cudaMemsetAsync(pb.bar, 0, sizeof(GridBar), st);
@@ -530,6 +542,7 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     // every omega up to 2 on dam-break, pool and random-box scenes.
     a.omega = 1.7f;
     a.nu_coarse = 2;
+    a.nu0 = std::max(1, nu0);
     a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
     a.X = static_cast<double*>(pb.X);
     a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;

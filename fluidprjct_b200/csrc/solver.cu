@@ -418,7 +418,8 @@ int solve_system(fp_solver* s, float* p_out) {
         // counts as stalled and hands over to the plain PCG.
         constexpr int kLearnedMaxit = 300;
         int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr, pb.b, tol,
-                                   learned ? std::min(maxit, kLearnedMaxit) : maxit, s->st, x0)
+                                   learned ? std::min(maxit, kLearnedMaxit) : maxit, s->st, x0,
+                                   s->cfg.mg_sweeps > 0 ? s->cfg.mg_sweeps : 2)
                    : launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st);
         cudaEventRecord(s->ev_pcg[1], s->st);
         if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");

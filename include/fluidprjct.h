@@ -127,6 +127,10 @@ typedef struct fp_config {
                                       faces with no FLUID side, between G2P and
                                       advection */
     int      body_forces;          /* FP_BODY_FORCES_* (default face fractions)   */
+    int      mg_sweeps;            /* FP_SOLVER_PCG_MG / _LEARNED: red-black sweep
+                                      pairs before and after the coarse correction
+                                      on the finest level (coarser levels: one);
+                                      0 = the default, 2                           */
 } fp_config;
 
 /* Per-step statistics: the reference's cudaEvent phase timers
