@@ -540,7 +540,7 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     // 31 -> 14 at 256^2 in a float64 model of this V-cycle).  Any omega > 0
     // keeps the preconditioner symmetric; in that model PCG converged for
     // every omega up to 2 on dam-break, pool and random-box scenes.
-    a.omega = 1.7f;
+    a.omega = 1.9f;
     a.nu_coarse = 2;
     a.nu0 = std::max(1, nu0);
     a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
