@@ -50,7 +50,8 @@ struct PressureBufs {
 
 // -------- multigrid-preconditioned PCG (kernels_mg.cu) --------
 constexpr int MG_MAX_LEVELS = 8;
-constexpr int MG_BLOCK_CELLS = 512;  // levels at most this big are swept by one block
+constexpr int MG_BLOCK_CELLS = 4096;           // levels at most this big are solved by one block ...
+constexpr int MG_SMEM_BUDGET = 180 * 1024;     // ... in shared memory, when their copies fit in this
 // One multigrid level: padded dense grids with a SOLID / zero halo.
 struct MgLevel {
     int W, H, D;    // interior cells
@@ -59,11 +60,17 @@ struct MgLevel {
     float* x;       // correction (level 0: the preconditioned residual z)
     float* b;       // right-hand side (level 0: the residual r)
 };
-// Fills lv[].W/H/D/sy/sz of the level hierarchy for a W x H x D grid; returns L.
+// Fills lv[].W/H/D/sy/sz of the level hierarchy for a W x H x D grid (down to
+// at most 2 cells per axis, or MG_MAX_LEVELS levels); returns L.
 int mg_levels_for(int W, int H, int D, MgLevel* lv);
 int mg_max_blocks();
-// Level labels from the cell labels (per solve).
-void launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStream_t st);
+// First block-solved level G of the hierarchy and the shared memory its
+// copies take (0: the block levels stay in global memory).
+int mg_split(const MgLevel* lv, int L, int* smem_bytes);
+// Level labels from the cell labels (per solve): level 0 and the grid-wide
+// levels; the solver kernel coarsens the shared-memory levels itself.
+// Returns the number of launches.
+int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStream_t st);
 // MG-preconditioned PCG (FP32 V-cycle, FP64 Krylov vectors and reductions) for
 // A x = rhs (compact) to ||r||/||rhs|| <= tol; solution in pb.X (FP64
 // compact).  p, q, xs, r are level-0 padded dense FP64 work grids, zero at

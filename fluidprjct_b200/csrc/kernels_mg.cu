@@ -18,7 +18,9 @@
 //     sums the red children.  Level 0 works on the compact FLUID list.
 // Levels with more than MG_BLOCK_CELLS cells are swept by the whole grid with a
 // grid barrier between sweeps; the remaining coarse levels are done by block 0
-// alone with __syncthreads.  The whole PCG runs in one persistent cooperative
+// alone with __syncthreads, on shared-memory copies (labels coarsened there at
+// kernel start; the first block level's b and x copied in and its x copied
+// back out per cycle).  The whole PCG runs in one persistent cooperative
 // launch with the bounded grid barrier.  Precision split: the V-cycle works in
 // FP32; the Krylov vectors (x, r, p, q) and all dot products are FP64, so the
 // recurrence residual tracks the true residual down to the 1e-6 target
@@ -33,10 +35,10 @@ namespace fp {
 namespace {
 
 constexpr int MG_THREADS = 1024;
-constexpr int MG_SMEM_CELLS = 1024;  // padded coarsest level held in shared memory
 
 struct MgArgs {
     int L, G;                    // levels; levels [0, G) are grid-wide
+    int smem;                    // bytes of the shared-memory copies of levels [G, L); 0: none
     float rscale;                // restriction scale (1/4 in 3D, 1/2 in 2D)
     float omega;                 // over-relaxation of the coarse-grid correction
     int nu_coarse;               // symmetric sweep pairs on the coarsest level
@@ -115,8 +117,22 @@ __device__ void op0_sweep(const MgLevel& L, const int* fidx, const uint8_t* dg, 
     }
 }
 // ---- level operations over a (t0, stride) share of the work ----
-// Gauss-Seidel update of the FLUID cells of one colour.
+// Gauss-Seidel update of the FLUID cells of one colour.  With an even width
+// the work items are the cells of that colour only: cell i2 of a row is
+// i = 2 i2 + ((j + k + colour) & 1).
 __device__ void op_sweep(const MgLevel& L, int color, int t0, int stride) {
+    if ((L.W & 1) == 0) {
+        const int hw = L.W >> 1, n = hw * L.H * L.D;
+        for (int t = t0; t < n; t += stride) {
+            const int i2 = t % hw, r = t / hw, j = r % L.H, k = r / L.H;
+            const int i = 2 * i2 + ((j + k + color) & 1);
+            const int c = (i + 1) + (j + 1) * L.sy + (k + 1) * L.sz;
+            if (L.lab[c] != FLUID) continue;
+            const int d = lv_diag(L, c);
+            L.x[c] = d > 0 ? (L.b[c] + lv_nbsum(L, c)) / float(d) : 0.0f;
+        }
+        return;
+    }
     const int n = L.W * L.H * L.D;
     for (int t = t0; t < n; t += stride) {
         int i, j, k;
@@ -193,37 +209,238 @@ __device__ void op0_prolong_red(const MgLevel& F, const MgLevel& Cl, float omega
     }
 }
 
-// V-cycle over levels [l0, L) by block 0 alone.  Level l0's first sweep is
-// already done (fused into the step that wrote its right-hand side).  With
-// l0 > 0 the stage stops after level l0's last black sweep: the final red
-// sweep of level l0 is the grid-wide prolongation into level l0 - 1, which
-// recomputes it.  With l0 == 0 it finishes level 0 itself.
-__device__ void block_vcycle(const MgArgs& a, int l0) {
+// Coarse label of cell t of level Cl, with Dirichlet priority: AIR if any
+// child is AIR, else FLUID if any child is FLUID, else SOLID.
+__device__ __forceinline__ void coarsen_cell(const MgLevel& F, const MgLevel& Cl, int t) {
+    int I, J, K;
+    const int cc = lv_cell(Cl, t, I, J, K);
+    bool air = false, fluid = false;
+    for (int c3 = 0; c3 < 2; ++c3)
+        for (int b3 = 0; b3 < 2; ++b3)
+            for (int a3 = 0; a3 < 2; ++a3) {
+                const int i = 2 * I + a3, j = 2 * J + b3, k = 2 * K + c3;
+                if (i >= F.W || j >= F.H || k >= F.D) continue;
+                const uint8_t l = F.lab[(i + 1) + (j + 1) * F.sy + (k + 1) * F.sz];
+                air |= l == AIR;
+                fluid |= l == FLUID;
+            }
+    Cl.lab[cc] = air ? AIR : (fluid ? FLUID : SOLID);
+}
+
+// ---- the block stage: levels [G, L) solved by block 0 alone ----
+// Shared-memory form.  Per level: x, b and rs (the red cells' residuals) as
+// FP32 padded grids; lab (labels, used while setting up) and code (FLUID:
+// 1 + diagonal, else 0) as bytes; ent, the level's FLUID cells (red ones from
+// the front, black ones from the back; padded index | parent's padded index
+// on the next level << 16) and kid (first child's padded index on the level
+// above).  Built once per solve at kernel start; afterwards each operation
+// walks a FLUID list (no index decoding, no label tests).  Only FLUID cells are
+// written, so every other cell stays zero.
+struct BlkLevel {
+    MgLevel m;            // dims, strides and the x, b, lab pointers
+    float* rs;
+    uint8_t* code;
+    uint32_t* ent;
+    uint32_t* kid;
+    int cells;            // interior cells
+    int nred, nblack;     // FLUID cells of each colour
+};
+
+__host__ __device__ __forceinline__ int mg_npad(const MgLevel& L) { return (L.W + 2) * (L.H + 2) * (L.D + 2); }
+__host__ __device__ __forceinline__ int mg_cells(const MgLevel& L) { return L.W * L.H * L.D; }
+// Bytes of the block levels [G, L): every level's three FP32 grids (padded
+// cells rounded up to 4), then the two entry arrays (cells rounded up to 4),
+// then the two byte grids (padded cells rounded up to 16).  The same walk
+// sizes the launch and places the arrays (block_levels_init).
+__host__ __device__ __forceinline__ int mg_smem_bytes(const MgLevel* lv, int G, int L) {
+    int f = 0, e = 0, by = 0;
+    for (int l = G; l < L; ++l) {
+        f += 3 * ((mg_npad(lv[l]) + 3) & ~3);
+        e += 2 * ((mg_cells(lv[l]) + 3) & ~3);
+        by += 2 * ((mg_npad(lv[l]) + 15) & ~15);
+    }
+    return 4 * f + 4 * e + by;
+}
+
+extern __shared__ __align__(16) unsigned char mg_smem[];
+
+// Block 0 at kernel start.  Returns the number of levels that carry FLUID
+// cells (at least G + 1): the deepest of them is the cycle's coarsest level.
+__device__ int block_levels_init(const MgArgs& a, BlkLevel* S) {
+    const int G = a.G, L = a.L, t0 = threadIdx.x, st = blockDim.x;
+    __shared__ int s_levels;
+    if (t0 == 0) {
+        float* f = reinterpret_cast<float*>(mg_smem);
+        for (int l = G; l < L; ++l) {
+            const int n4 = (mg_npad(a.lv[l]) + 3) & ~3;
+            S[l].m = a.lv[l];
+            S[l].m.x = f; f += n4;
+            S[l].m.b = f; f += n4;
+            S[l].rs = f; f += n4;
+        }
+        uint32_t* e = reinterpret_cast<uint32_t*>(f);
+        for (int l = G; l < L; ++l) {
+            const int c4 = (mg_cells(a.lv[l]) + 3) & ~3;
+            S[l].ent = e; e += c4;
+            S[l].kid = e; e += c4;
+        }
+        uint8_t* by = reinterpret_cast<uint8_t*>(e);
+        for (int l = G; l < L; ++l) {
+            const int n16 = (mg_npad(a.lv[l]) + 15) & ~15;
+            S[l].m.lab = by; by += n16;
+            S[l].code = by; by += n16;
+            S[l].cells = mg_cells(a.lv[l]);
+            S[l].nred = S[l].nblack = 0;
+        }
+    }
+    uint4* z = reinterpret_cast<uint4*>(mg_smem);
+    for (int i = t0; i < a.smem / 16; i += st) z[i] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    for (int c = t0; c < mg_npad(a.lv[G]); c += st) S[G].m.lab[c] = a.lv[G].lab[c];
+    __syncthreads();
+    for (int l = G + 1; l < L; ++l) {
+        for (int t = t0; t < S[l].cells; t += st) coarsen_cell(S[l - 1].m, S[l].m, t);
+        __syncthreads();
+    }
+    for (int l = G; l < L; ++l) {
+        BlkLevel& B = S[l];
+        for (int t = t0; t < B.cells; t += st) {
+            int i, j, k;
+            const int c = lv_cell(B.m, t, i, j, k);
+            if (B.m.lab[c] != FLUID) continue;
+            B.code[c] = uint8_t(1 + lv_diag(B.m, c));
+            const int slot = ((i + j + k) & 1) == 0 ? atomicAdd(&B.nred, 1) : B.cells - 1 - atomicAdd(&B.nblack, 1);
+            const int pc = l + 1 < L ? ((i >> 1) + 1) + ((j >> 1) + 1) * S[l + 1].m.sy + ((k >> 1) + 1) * S[l + 1].m.sz : 0;
+            B.ent[slot] = uint32_t(c) | (uint32_t(pc) << 16);
+            if (l > G) B.kid[slot] = uint32_t((2 * i + 1) + (2 * j + 1) * S[l - 1].m.sy + (2 * k + 1) * S[l - 1].m.sz);
+        }
+    }
+    __syncthreads();
+    if (t0 == 0) {
+        int n = G + 1;
+        for (int l = G; l < L; ++l)
+            if (S[l].nred + S[l].nblack > 0) n = l + 1;
+        s_levels = n;
+    }
+    __syncthreads();
+    return s_levels;
+}
+
+// Slot of the t-th FLUID cell of level B (red ones first).
+__device__ __forceinline__ int bl_slot(const BlkLevel& B, int t) {
+    return t < B.nred ? t : B.cells - B.nblack + (t - B.nred);
+}
+// Gauss-Seidel update of the FLUID cells of one colour.
+__device__ void bl_sweep(const BlkLevel& B, int color, int t0, int st) {
+    const int n = color == 0 ? B.nred : B.nblack;
+    const uint32_t* e = color == 0 ? B.ent : B.ent + (B.cells - B.nblack);
+    for (int t = t0; t < n; t += st) {
+        const int c = int(e[t] & 0xFFFFu);
+        const int d = B.code[c] - 1;
+        B.m.x[c] = d > 0 ? (B.m.b[c] + lv_nbsum(B.m, c)) / float(d) : 0.0f;
+    }
+}
+// rs = b - A x on the red FLUID cells (after a black sweep the black ones vanish).
+__device__ void bl_residual(const BlkLevel& B, int t0, int st) {
+    for (int t = t0; t < B.nred; t += st) {
+        const int c = int(B.ent[t] & 0xFFFFu);
+        B.rs[c] = B.m.b[c] - (float(B.code[c] - 1) * B.m.x[c] - lv_nbsum(B.m, c));
+    }
+}
+// Restriction into C fused with C's first sweep: b = scale * (sum of the
+// children's rs, in the dense restriction's order; black, non-FLUID and
+// out-of-grid children read zero), x = b/d on red cells, 0 on black ones.
+__device__ void bl_restrict(const BlkLevel& F, const BlkLevel& C, float scale, int t0, int st) {
+    const int n = C.nred + C.nblack, sy = F.m.sy, sz = F.m.sz;
+    for (int t = t0; t < n; t += st) {
+        const int slot = bl_slot(C, t);
+        const int cc = int(C.ent[slot] & 0xFFFFu);
+        const float* r = F.rs + C.kid[slot];
+        float s = 0.0f;
+        s += r[0]; s += r[1]; s += r[sy]; s += r[sy + 1];
+        s += r[sz]; s += r[sz + 1]; s += r[sz + sy]; s += r[sz + sy + 1];
+        s *= scale;
+        C.m.b[cc] = s;
+        const int d = C.code[cc] - 1;
+        C.m.x[cc] = (t < C.nred && d > 0) ? s / float(d) : 0.0f;
+    }
+}
+// Prolongation: every FLUID cell of F adds omega * its parent's x when the
+// parent is FLUID (the parent level's red cells are already swept).
+__device__ void bl_prolong(const BlkLevel& F, const BlkLevel& C, float omega, int t0, int st) {
+    const int n = F.nred + F.nblack;
+    for (int t = t0; t < n; t += st) {
+        const uint32_t e = F.ent[bl_slot(F, t)];
+        const int c = int(e & 0xFFFFu), pc = int(e >> 16);
+        if (C.code[pc] > 0) F.m.x[c] += omega * C.m.x[pc];
+    }
+}
+
+// V-cycle over the shared-memory levels [l0, nl) by block 0 (nl from
+// block_levels_init).  Level l0's first sweep is already done: the grid-wide
+// restriction wrote its b and x, which are copied in.  The stage stops after
+// level l0's last black sweep and copies its x back out: the final red sweep
+// of level l0 is the grid-wide prolongation into level l0 - 1, which
+// recomputes it from that copy.
+__device__ void block_vcycle_smem(const MgArgs& a, int l0, int nl, const BlkLevel* S) {
+    const int t0 = threadIdx.x, st = blockDim.x;
+    const BlkLevel& B0 = S[l0];
+    const MgLevel& G0 = a.lv[l0];
+    for (int t = t0; t < B0.nred + B0.nblack; t += st) {
+        const int c = int(B0.ent[bl_slot(B0, t)] & 0xFFFFu);
+        B0.m.b[c] = G0.b[c];
+        B0.m.x[c] = G0.x[c];
+    }
+    __syncthreads();
+    const int lc = nl - 1;
+    for (int l = l0; l < lc; ++l) {
+        bl_sweep(S[l], 1, t0, st); __syncthreads();
+        bl_residual(S[l], t0, st); __syncthreads();
+        bl_restrict(S[l], S[l + 1], a.rscale, t0, st); __syncthreads();
+    }
+    const BlkLevel& C = S[lc];
+    bl_sweep(C, 1, t0, st); __syncthreads();
+    for (int it = 1; it < a.nu_coarse; ++it) {
+        bl_sweep(C, 0, t0, st); __syncthreads();
+        bl_sweep(C, 1, t0, st); __syncthreads();
+    }
+    for (int it = 0; it < a.nu_coarse; ++it) {
+        bl_sweep(C, 1, t0, st); __syncthreads();
+        if (it + 1 < a.nu_coarse) {
+            bl_sweep(C, 0, t0, st); __syncthreads();
+        } else if (lc > l0) {
+            bl_sweep(C, 0, t0, st); __syncthreads();
+            bl_prolong(S[lc - 1], C, a.omega, t0, st); __syncthreads();
+        }
+    }
+    for (int l = lc - 1; l >= l0; --l) {
+        bl_sweep(S[l], 1, t0, st); __syncthreads();
+        if (l > l0) {
+            bl_sweep(S[l], 0, t0, st); __syncthreads();
+            bl_prolong(S[l - 1], S[l], a.omega, t0, st); __syncthreads();
+        }
+    }
+    // the grid barrier that follows begins with __syncthreads
+    for (int t = t0; t < B0.nred + B0.nblack; t += st) {
+        const int c = int(B0.ent[bl_slot(B0, t)] & 0xFFFFu);
+        a.lv[l0].x[c] = B0.m.x[c];
+    }
+}
+
+// Global-memory form (the block levels do not fit in shared memory, or the
+// hierarchy has one level): V-cycle over levels [l0, L) of a.lv by block 0.
+// Level l0's first sweep is already done (fused into the step that wrote its
+// right-hand side).  With l0 > 0 the stage stops after level l0's last black
+// sweep: the final red sweep of level l0 is the grid-wide prolongation into
+// level l0 - 1, which recomputes it.  With l0 == 0 it finishes level 0 itself.
+__device__ void block_vcycle_global(const MgArgs& a, int l0) {
     const int t0 = threadIdx.x, st = blockDim.x;
     for (int l = l0; l < a.L - 1; ++l) {
         op_sweep(a.lv[l], 1, t0, st); __syncthreads();
         op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st); __syncthreads();
     }
     const int lc = a.L - 1;
-    // The coarsest level lives in shared memory when it fits: its sweeps then
-    // cost no global-memory latency (level-op pointers are generic, so the
-    // same operations run on the shared copy).
-    __shared__ float s_x[MG_SMEM_CELLS], s_b[MG_SMEM_CELLS];
-    __shared__ uint8_t s_lab[MG_SMEM_CELLS];
-    MgLevel C = a.lv[lc];
-    const int npad = (C.W + 2) * (C.H + 2) * (C.D + 2);
-    const bool in_smem = lc > 0 && npad <= MG_SMEM_CELLS;  // a single-level hierarchy's x is the output
-    if (in_smem) {
-        for (int c = t0; c < npad; c += st) {
-            s_lab[c] = C.lab[c];
-            s_b[c] = C.b[c];
-            s_x[c] = C.x[c];
-        }
-        C.lab = s_lab;
-        C.b = s_b;
-        C.x = s_x;
-        __syncthreads();
-    }
+    const MgLevel& C = a.lv[lc];
     op_sweep(C, 1, t0, st); __syncthreads();
     for (int it = 1; it < a.nu_coarse; ++it) {
         op_sweep(C, 0, t0, st); __syncthreads();
@@ -237,10 +454,6 @@ __device__ void block_vcycle(const MgArgs& a, int l0) {
             op_prolong_red(a.lv[lc - 1], C, a.omega, t0, st); __syncthreads();
         }
     }
-    if (in_smem && lc == l0) {  // the grid prolongation reads this level from global memory
-        for (int c = t0; c < npad; c += st) a.lv[lc].x[c] = s_x[c];
-        __syncthreads();
-    }
     for (int l = lc - 1; l >= l0; --l) {
         op_sweep(a.lv[l], 1, t0, st); __syncthreads();
         if (l == 0) {
@@ -253,14 +466,13 @@ __device__ void block_vcycle(const MgArgs& a, int l0) {
 
 // z = V-cycle(r) with r = lv[0].b, z = lv[0].x.  The caller has already done
 // the first (red) sweep of level 0: z = b/d on red FLUID cells, 0 on black
-// ones.  Starts and ends with a grid barrier; returns false if a barrier
-// timed out.  Grid-wide levels take four barriers each: black sweep,
+// ones, and a grid barrier since.  Ends with a grid barrier; returns false if
+// a barrier timed out.  Grid-wide levels take four barriers each: black sweep,
 // restriction (with the next level's first sweep), black sweep, red sweep
 // (with the prolongation into the finer level).
-__device__ bool vcycle(const MgArgs& a) {
+__device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
     const unsigned nb = gridDim.x;
-    if (!grid_barrier(a.bar, nb, a.status)) return false;
     const int G = min(a.G, a.L - 1);
     const int nf = *a.nf;
     // one grid-wide sweep of level l (colour 0 red, 1 black) and a barrier
@@ -278,7 +490,10 @@ __device__ bool vcycle(const MgArgs& a) {
         op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
-    if (blockIdx.x == 0) block_vcycle(a, G);
+    if (blockIdx.x == 0) {
+        if (a.smem) block_vcycle_smem(a, G, nl, S);
+        else block_vcycle_global(a, G);
+    }
     if (!grid_barrier(a.bar, nb, a.status)) return false;
     if (G > 0) {  // level G's last red sweep, fused with its prolongation into level G - 1
         if (G == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
@@ -322,7 +537,10 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     };
     auto total = [&]() { double3 t = grid_sum3(a.part + (red & 1) * 3 * nb, nb); ++red; return t; };
     const int sy = F.sy, sz = F.sz;
+    __shared__ BlkLevel s_lv[MG_MAX_LEVELS];  // block 0: the shared-memory block levels
+    const int nl = (blockIdx.x == 0 && a.smem) ? block_levels_init(a, s_lv) : a.L;
 
+    double rrl = 0.0;
     for (int n = t0; n < nf; n += st) {
         const int c = a.fidx[n];
         const double rv = double(a.rhs[n]);
@@ -330,6 +548,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         b0[c] = float(rv);
         z[c] = first_red0(float(rv), a.diag[n]);  // the V-cycle's first sweep
         a.xs[c] = a.x0 ? double(a.x0[n]) : 0.0;
+        rrl += rv * rv;
     }
     double bb_warm = 0.0;  // ||b||^2 when started from a guess
     if (a.x0) {
@@ -352,6 +571,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         const double3 t = total();
         const double alpha = (t.y > 0.0 && isfinite(t.x / t.y)) ? t.x / t.y : 0.0;
         bb_warm = t.z;  // all reads of x ended before the barrier above
+        rrl = 0.0;
         for (int n = t0; n < nf; n += st) {
             const int c = a.fidx[n];
             a.xs[c] *= alpha;
@@ -359,85 +579,102 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
             r[c] = rv;
             b0[c] = float(rv);
             z[c] = first_red0(float(rv), a.diag[n]);
+            rrl += rv * rv;
         }
     }
-    if (!vcycle(a)) return;
-    {
-        double rz = 0.0, rr = 0.0;
-        for (int n = t0; n < nf; n += st) {
-            const int c = a.fidx[n];
-            const double zv = double(z[c]);
-            rz += r[c] * zv;
-            rr += r[c] * r[c];
-            a.p[c] = zv;
-        }
-        partial(rz, rr, 0.0);
-    }
+    partial(rrl, 0.0, 0.0);
     if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
-    double3 tot = total();
-    double rz = tot.x, rr = tot.y;
-    const double bb = a.x0 ? bb_warm : tot.y;
-    const double rr0 = tot.y;
+    double rr = total().x;
+    const double bb = a.x0 ? bb_warm : rr;
+    const double rr0 = rr;
     const double thr = a.tol * a.tol * bb;
+    // Preconditioned CG in the Chronopoulos-Gear form: after the V-cycle one
+    // pass forms w = A z, gamma = (r, z) and delta = (z, w); one more updates
+    // p = z + beta p, s = w + beta s (= A p), x += alpha p, r -= alpha s and
+    // starts the next cycle, with beta = gamma / gamma_old and
+    // alpha = gamma / (delta - beta gamma / alpha_old).  Two grid-wide passes
+    // per iteration besides the cycle.  w is kept in the compact X buffer
+    // (the solution is written there only at the end); s lives in q.
+    double* w = a.X;
+    double gam = 0.0, gam_old = 0.0, alpha_old = 1.0;
     int it = 0, stt = DEV_OK;
     while (rr > thr && bb > 0.0) {
         if (it >= a.maxit) { stt = DEV_MAXIT; break; }
-        // q = A p, (p, q)
-        double pq = 0.0;
+        if (!vcycle(a, s_lv, nl)) return;  // z = M^-1 r
+        double gl = 0.0, dl = 0.0;
+        constexpr int U3 = 3;  // three cells in flight fit the register budget with FP64 sums
+        for (int base = t0; base < nf; base += U3 * st) {
+            Cells<U3> k;
+            load_cells(k, a.fidx, a.diag, nf, base, st, 1 + sy + sz);
+            float zc[U3];
+            double zn[U3], rc[U3];  // A z exactly: FP32 values summed in FP64
+#pragma unroll
+            for (int u = 0; u < U3; ++u) {
+                const float* zp = z + k.c[u];
+                zc[u] = zp[0];
+                zn[u] = (double(zp[1]) + double(zp[-1])) + (double(zp[sy]) + double(zp[-sy])) +
+                        (double(zp[sz]) + double(zp[-sz]));
+                rc[u] = r[k.c[u]];
+            }
+#pragma unroll
+            for (int u = 0; u < U3; ++u) {
+                if (!k.ok[u]) continue;
+                const double zv = double(zc[u]);
+                const double wv = double(k.db[u] & 0x7F) * zv - zn[u];
+                w[base + u * st] = wv;
+                gl += rc[u] * zv;
+                dl += zv * wv;
+            }
+        }
+        partial(gl, dl, 0.0);
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+        const double3 t = total();
+        gam = t.x;
+        if (isnan(t.x) || isnan(t.y)) { stt = DEV_NAN; break; }
+        const double beta = it > 0 ? gam / gam_old : 0.0;
+        const double den = it > 0 ? t.y - beta * gam / alpha_old : t.y;
+        if (!(den > 0.0)) { stt = DEV_BREAKDOWN; break; }
+        const double alpha = gam / den;
+        rrl = 0.0;
         constexpr int U2 = 2;  // FP64: two cells in flight fit the register budget
         for (int base = t0; base < nf; base += U2 * st) {
             Cells<U2> k;
             load_cells(k, a.fidx, a.diag, nf, base, st, 1 + sy + sz);
-            double pc[U2], ns[U2];
+            double pv[U2], sv[U2], xv[U2], rv[U2], wv[U2];
+            float zc[U2];
 #pragma unroll
             for (int u = 0; u < U2; ++u) {
-                const double* pp = a.p + k.c[u];
-                pc[u] = pp[0];
-                ns[u] = (pp[1] + pp[-1]) + (pp[sy] + pp[-sy]) + (pp[sz] + pp[-sz]);
+                const int c = k.c[u];
+                zc[u] = z[c];
+                pv[u] = a.p[c];
+                sv[u] = a.q[c];
+                xv[u] = a.xs[c];
+                rv[u] = r[c];
+                wv[u] = k.ok[u] ? w[base + u * st] : 0.0;
             }
 #pragma unroll
             for (int u = 0; u < U2; ++u) {
                 if (!k.ok[u]) continue;
-                const double qv = double(k.db[u] & 0x7F) * pc[u] - ns[u];
-                a.q[k.c[u]] = qv;
-                pq += pc[u] * qv;
+                const int c = k.c[u];
+                const double pn = it > 0 ? double(zc[u]) + beta * pv[u] : double(zc[u]);
+                const double sn = it > 0 ? wv[u] + beta * sv[u] : wv[u];
+                a.p[c] = pn;
+                a.q[c] = sn;
+                a.xs[c] = xv[u] + alpha * pn;
+                const double rn = rv[u] - alpha * sn;
+                r[c] = rn;
+                b0[c] = float(rn);
+                z[c] = first_red0(float(rn), k.db[u]);
+                rrl += rn * rn;
             }
         }
-        partial(pq, 0.0, 0.0);
+        partial(rrl, 0.0, 0.0);
         if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
-        const double pqs = total().x;
-        if (!(pqs > 0.0) || isnan(pqs)) { stt = isnan(pqs) ? DEV_NAN : DEV_BREAKDOWN; break; }
-        const double alpha = rz / pqs;
-        double rrl = 0.0;
-        for (int n = t0; n < nf; n += st) {
-            const int c = a.fidx[n];
-            a.xs[c] += alpha * a.p[c];
-            const double rv = r[c] - alpha * a.q[c];
-            r[c] = rv;
-            b0[c] = float(rv);
-            z[c] = first_red0(float(rv), a.diag[n]);
-            rrl += rv * rv;
-        }
-        if (!vcycle(a)) return;  // z = M^-1 r (begins with a barrier)
-        double rzl = 0.0;
-        for (int n = t0; n < nf; n += st) {
-            const int c = a.fidx[n];
-            rzl += r[c] * double(z[c]);
-        }
-        partial(rzl, rrl, 0.0);
-        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
-        tot = total();
+        rr = total().x;
         ++it;
-        if (isnan(tot.x) || isnan(tot.y)) { stt = DEV_NAN; break; }
-        rr = tot.y;
-        if (rr <= thr) break;
-        const double beta = tot.x / rz;
-        rz = tot.x;
-        for (int n = t0; n < nf; n += st) {
-            const int c = a.fidx[n];
-            a.p[c] = double(z[c]) + beta * a.p[c];
-        }
-        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+        if (isnan(rr)) { stt = DEV_NAN; break; }
+        gam_old = gam;
+        alpha_old = alpha;
     }
     // compact solution; zero the level-0 work grids at the FLUID cells so the
     // next solve starts from zero whatever cells are fluid then
@@ -452,7 +689,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         atomicCAS(a.status, DEV_OK, stt);
         a.out->rr = rr;
         a.out->bb = bb;
-        a.out->rz = rz;
+        a.out->rz = gam;
         a.out->rr0 = rr0;
     }
 }
@@ -471,20 +708,7 @@ __global__ void k_pad_labels(const uint8_t* __restrict__ lab, Dims g, MgLevel L)
 // any child FLUID, else SOLID.
 __global__ void k_coarsen(MgLevel F, MgLevel Cl) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= Cl.W * Cl.H * Cl.D) return;
-    int I, J, K;
-    const int cc = lv_cell(Cl, t, I, J, K);
-    bool air = false, fluid = false;
-    for (int c3 = 0; c3 < 2; ++c3)
-        for (int b3 = 0; b3 < 2; ++b3)
-            for (int a3 = 0; a3 < 2; ++a3) {
-                const int i = 2 * I + a3, j = 2 * J + b3, k = 2 * K + c3;
-                if (i >= F.W || j >= F.H || k >= F.D) continue;
-                const uint8_t l = F.lab[(i + 1) + (j + 1) * F.sy + (k + 1) * F.sz];
-                air |= l == AIR;
-                fluid |= l == FLUID;
-            }
-    Cl.lab[cc] = air ? AIR : (fluid ? FLUID : SOLID);
+    if (t < Cl.W * Cl.H * Cl.D) coarsen_cell(F, Cl, t);
 }
 
 }  // namespace
@@ -496,7 +720,7 @@ int mg_levels_for(int W, int H, int D, MgLevel* lv) {
         lv[L].W = w; lv[L].H = h; lv[L].D = d;
         lv[L].sy = w + 2; lv[L].sz = (w + 2) * (h + 2);
         ++L;
-        if (int64_t(w) * h * d <= 512 || (w <= 2 && h <= 2 && d <= 2)) break;
+        if (w <= 2 && h <= 2 && d <= 2) break;
         w = (w + 1) / 2; h = (h + 1) / 2; d = (d + 1) / 2;
     }
     return L;
@@ -508,17 +732,36 @@ int mg_max_blocks() {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_mg, MG_THREADS, 0);
+    cudaFuncSetAttribute(k_pcg_mg, cudaFuncAttributeMaxDynamicSharedMemorySize, MG_SMEM_BUDGET);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_mg, MG_THREADS, MG_SMEM_BUDGET);
     cached = sms * std::max(1, per);
     return cached;
 }
 
-void launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStream_t st) {
+int mg_split(const MgLevel* lv, int L, int* smem_bytes) {
+    *smem_bytes = 0;
+    if (L <= 1) return 0;
+    int G = 1;  // level 0 is always swept grid-wide on its FLUID list
+    for (int l = 0; l < L; ++l)
+        if (int64_t(lv[l].W) * lv[l].H * lv[l].D > MG_BLOCK_CELLS) G = std::max(G, l + 1);
+    for (G = std::min(G, L - 1); G < L; ++G) {
+        const int b = mg_smem_bytes(lv, G, L);
+        // the FLUID lists hold padded indices in 16 bits
+        if (b <= MG_SMEM_BUDGET && mg_npad(lv[G]) <= 65535) { *smem_bytes = b; return G; }
+    }
+    return L - 1;  // not even the coarsest level fits: the block levels stay in global memory
+}
+
+int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStream_t st) {
+    int smem = 0;
+    const int G = mg_split(lv, L, &smem);
+    const int last = smem ? G : L - 1;  // deeper shared-memory levels: coarsened by the solver kernel
     k_pad_labels<<<unsigned((g.nc() + 255) / 256), 256, 0, st>>>(labels, g, lv[0]);
-    for (int l = 1; l < L; ++l) {
+    for (int l = 1; l <= last; ++l) {
         const int n = lv[l].W * lv[l].H * lv[l].D;
         k_coarsen<<<(n + 255) / 256, 256, 0, st>>>(lv[l - 1], lv[l]);
     }
+    return 1 + last;
 }
 
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
@@ -529,11 +772,8 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     cudaMemsetAsync(status, 0, sizeof(int), st);
     MgArgs a;
     a.L = L;
-    a.G = 0;
-    for (int l = 0; l < L; ++l) {
-        a.lv[l] = lv[l];
-        if (int64_t(lv[l].W) * lv[l].H * lv[l].D > MG_BLOCK_CELLS) a.G = l + 1;
-    }
+    a.G = mg_split(lv, L, &a.smem);
+    for (int l = 0; l < L; ++l) a.lv[l] = lv[l];
     a.rscale = g.D > 1 ? 0.25f : 0.5f;
     // The piecewise-constant prolongation underestimates the coarse correction;
     // scaling it by 1.7 roughly halves the PCG iterations (29 -> 15 at 128^3,
@@ -548,7 +788,7 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;
     a.tol = tol; a.maxit = maxit;
     void* args[] = {&a};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_mg, dim3(nb), dim3(MG_THREADS), args, 0, st);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_mg, dim3(nb), dim3(MG_THREADS), args, size_t(a.smem), st);
     return e == cudaSuccess ? 0 : int(e);
 }
 

@@ -398,8 +398,7 @@ int solve_system(fp_solver* s, float* p_out) {
         const bool mg = s->cfg.solver != FP_SOLVER_PCG;
         if (learned && !s->net) return s->fail(FP_ERR_STATE, "learned solver: no weights loaded (fp_load_learned)");
         if (mg) {
-            launch_mg_setup(s->d_labels, s->g, s->mg, s->mgL, s->st);
-            s->launches += s->mgL;
+            s->launches += launch_mg_setup(s->d_labels, s->g, s->mg, s->mgL, s->st);
         }
         cudaEventRecord(s->ev_pcg[0], s->st);
         const float* x0 = nullptr;
