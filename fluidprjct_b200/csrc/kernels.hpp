@@ -59,6 +59,7 @@ struct MgLevel {
     uint8_t* lab;   // labels (BODY folded into SOLID)
     float* x;       // correction (level 0: the preconditioned residual z)
     float* b;       // right-hand side (level 0: the residual r)
+    uint8_t* code;  // per solve: FLUID cells 1 + diagonal, every other cell 0
 };
 // Fills lv[].W/H/D/sy/sz of the level hierarchy for a W x H x D grid (down to
 // at most 2 cells per axis, or MG_MAX_LEVELS levels); returns L.

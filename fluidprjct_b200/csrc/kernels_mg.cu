@@ -117,6 +117,15 @@ __device__ void op0_sweep(const MgLevel& L, const int* fidx, const uint8_t* dg, 
     }
 }
 // ---- level operations over a (t0, stride) share of the work ----
+// They read the level's code (FLUID: 1 + diagonal, else 0) instead of labels,
+// and issue a cell's loads together, masked by the code afterwards: every
+// load is of an interior cell or its halo, so it stays in bounds.
+// Gauss-Seidel update of one FLUID cell (code dc > 0).
+__device__ __forceinline__ void gs_update(const MgLevel& L, int c) {
+    const int dc = L.code[c];
+    const float bv = L.b[c], nb = lv_nbsum(L, c);
+    if (dc > 0) L.x[c] = dc > 1 ? (bv + nb) / float(dc - 1) : 0.0f;
+}
 // Gauss-Seidel update of the FLUID cells of one colour.  With an even width
 // the work items are the cells of that colour only: cell i2 of a row is
 // i = 2 i2 + ((j + k + colour) & 1).
@@ -126,10 +135,7 @@ __device__ void op_sweep(const MgLevel& L, int color, int t0, int stride) {
         for (int t = t0; t < n; t += stride) {
             const int i2 = t % hw, r = t / hw, j = r % L.H, k = r / L.H;
             const int i = 2 * i2 + ((j + k + color) & 1);
-            const int c = (i + 1) + (j + 1) * L.sy + (k + 1) * L.sz;
-            if (L.lab[c] != FLUID) continue;
-            const int d = lv_diag(L, c);
-            L.x[c] = d > 0 ? (L.b[c] + lv_nbsum(L, c)) / float(d) : 0.0f;
+            gs_update(L, (i + 1) + (j + 1) * L.sy + (k + 1) * L.sz);
         }
         return;
     }
@@ -137,37 +143,38 @@ __device__ void op_sweep(const MgLevel& L, int color, int t0, int stride) {
     for (int t = t0; t < n; t += stride) {
         int i, j, k;
         const int c = lv_cell(L, t, i, j, k);
-        if (((i + j + k) & 1) != color || L.lab[c] != FLUID) continue;
-        const int d = lv_diag(L, c);
-        L.x[c] = d > 0 ? (L.b[c] + lv_nbsum(L, c)) / float(d) : 0.0f;
+        if (((i + j + k) & 1) == color) gs_update(L, c);
     }
+}
+// Residual b - A x of fine cell c if it is FLUID, else 0.
+__device__ __forceinline__ float fine_residual(const MgLevel& F, int c) {
+    const int dc = F.code[c];
+    const float bv = F.b[c], xv = F.x[c], nb = lv_nbsum(F, c);
+    return dc > 0 ? bv - (float(dc - 1) * xv - nb) : 0.0f;
 }
 // Restriction to the next level fused with that level's first sweep:
 // b_coarse = scale * sum over the red FLUID children of (b - A x), then
-// x_coarse = b/d on red FLUID cells, 0 elsewhere.
+// x_coarse = b/d on red FLUID cells, 0 elsewhere.  After the black sweep the
+// black residuals vanish, so only the red children (offsets with an even
+// coordinate sum) are read, in k, j, i order.  A child beyond
+// an odd-sized fine level (every 2D level in z) is skipped: its stencil would
+// leave the padded grid.
 __device__ void op_restrict_first(const MgLevel& F, const MgLevel& Cl, float scale, int t0, int stride) {
     const int n = Cl.W * Cl.H * Cl.D;
     for (int t = t0; t < n; t += stride) {
         int I, J, K;
         const int cc = lv_cell(Cl, t, I, J, K);
+        const int dc = Cl.code[cc];
         float s = 0.0f, xv = 0.0f;
-        if (Cl.lab[cc] == FLUID) {
-            for (int c3 = 0; c3 < 2; ++c3)
-                for (int b3 = 0; b3 < 2; ++b3)
-                    for (int a3 = 0; a3 < 2; ++a3) {
-                        const int i = 2 * I + a3, j = 2 * J + b3, k = 2 * K + c3;
-                        if (i >= F.W || j >= F.H || k >= F.D) continue;
-                        // after the black sweep the black residuals vanish: sum red children only
-                        if (((i + j + k) & 1) != 0) continue;
-                        const int c = (i + 1) + (j + 1) * F.sy + (k + 1) * F.sz;
-                        if (F.lab[c] != FLUID) continue;
-                        s += F.b[c] - (float(lv_diag(F, c)) * F.x[c] - lv_nbsum(F, c));
-                    }
+        if (dc > 0) {
+            const bool ii = 2 * I + 1 < F.W, jj = 2 * J + 1 < F.H, kk = 2 * K + 1 < F.D;
+            const int c0 = (2 * I + 1) + (2 * J + 1) * F.sy + (2 * K + 1) * F.sz;
+            s += fine_residual(F, c0);
+            if (ii && jj) s += fine_residual(F, c0 + 1 + F.sy);
+            if (ii && kk) s += fine_residual(F, c0 + 1 + F.sz);
+            if (jj && kk) s += fine_residual(F, c0 + F.sy + F.sz);
             s *= scale;
-            if (((I + J + K) & 1) == 0) {
-                const int d = lv_diag(Cl, cc);
-                xv = d > 0 ? s / float(d) : 0.0f;
-            }
+            if (((I + J + K) & 1) == 0) xv = dc > 1 ? s / float(dc - 1) : 0.0f;
         }
         Cl.b[cc] = s;
         Cl.x[cc] = xv;
@@ -179,10 +186,15 @@ __device__ void op_restrict_first(const MgLevel& F, const MgLevel& Cl, float sca
 // by each of its children from the final black neighbours, with the same
 // arithmetic, so all eight see the same bits) and a black parent's is final.
 // The coarse x is not needed after this, so it is not written back.
-__device__ __forceinline__ float parent_value(const MgLevel& Cl, int cc, int I, int J, int K) {
-    if (((I + J + K) & 1) != 0) return Cl.x[cc];
-    const int d = lv_diag(Cl, cc);
-    return d > 0 ? (Cl.b[cc] + lv_nbsum(Cl, cc)) / float(d) : 0.0f;
+__device__ __forceinline__ void prolong_one(const MgLevel& F, int c, const MgLevel& Cl, float omega, int i, int j,
+                                            int k) {
+    const int I = i >> 1, J = j >> 1, K = k >> 1;
+    const int cc = (I + 1) + (J + 1) * Cl.sy + (K + 1) * Cl.sz;
+    const int dc = Cl.code[cc];
+    const float xc = Cl.x[cc], bc = Cl.b[cc], nb = lv_nbsum(Cl, cc), xf = F.x[c];
+    if (dc == 0) return;
+    const float v = ((I + J + K) & 1) != 0 ? xc : (dc > 1 ? (bc + nb) / float(dc - 1) : 0.0f);
+    F.x[c] = xf + omega * v;
 }
 // ... over every cell of the fine level F (dense levels)
 __device__ void op_prolong_red(const MgLevel& F, const MgLevel& Cl, float omega, int t0, int stride) {
@@ -190,11 +202,7 @@ __device__ void op_prolong_red(const MgLevel& F, const MgLevel& Cl, float omega,
     for (int t = t0; t < n; t += stride) {
         int i, j, k;
         const int c = lv_cell(F, t, i, j, k);
-        if (F.lab[c] != FLUID) continue;
-        const int I = i >> 1, J = j >> 1, K = k >> 1;
-        const int cc = (I + 1) + (J + 1) * Cl.sy + (K + 1) * Cl.sz;
-        if (Cl.lab[cc] != FLUID) continue;
-        F.x[c] += omega * parent_value(Cl, cc, I, J, K);
+        if (F.code[c] != 0) prolong_one(F, c, Cl, omega, i, j, k);
     }
 }
 // ... over the level-0 FLUID list
@@ -203,9 +211,16 @@ __device__ void op0_prolong_red(const MgLevel& F, const MgLevel& Cl, float omega
     for (int n = t0; n < nf; n += stride) {
         const int c = fidx[n];
         const int i = c % F.sy - 1, j = (c / F.sy) % (F.H + 2) - 1, k = c / F.sz - 1;
-        const int I = i >> 1, J = j >> 1, K = k >> 1;
-        const int cc = (I + 1) + (J + 1) * Cl.sy + (K + 1) * Cl.sz;
-        if (Cl.lab[cc] == FLUID) F.x[c] += omega * parent_value(Cl, cc, I, J, K);
+        prolong_one(F, c, Cl, omega, i, j, k);
+    }
+}
+// Codes of the interior cells of a dense level from its labels.
+__device__ void op_codes(const MgLevel& L, int t0, int stride) {
+    const int n = L.W * L.H * L.D;
+    for (int t = t0; t < n; t += stride) {
+        int i, j, k;
+        const int c = lv_cell(L, t, i, j, k);
+        L.code[c] = L.lab[c] == FLUID ? uint8_t(1 + lv_diag(L, c)) : uint8_t(0);
     }
 }
 
@@ -540,10 +555,15 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     __shared__ BlkLevel s_lv[MG_MAX_LEVELS];  // block 0: the shared-memory block levels
     const int nl = (blockIdx.x == 0 && a.smem) ? block_levels_init(a, s_lv) : a.L;
 
+    // level codes: level 0 on its FLUID cells (zero elsewhere, restored at the
+    // end), the dense grid-wide levels (and, without shared-memory copies, the
+    // block levels) over all their cells
+    for (int l = 1; l <= (a.smem ? a.G : a.L - 1); ++l) op_codes(a.lv[l], t0, st);
     double rrl = 0.0;
     for (int n = t0; n < nf; n += st) {
         const int c = a.fidx[n];
         const double rv = double(a.rhs[n]);
+        F.code[c] = uint8_t(1 + (a.diag[n] & 0x7F));
         r[c] = rv;
         b0[c] = float(rv);
         z[c] = first_red0(float(rv), a.diag[n]);  // the V-cycle's first sweep
@@ -682,7 +702,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     for (int n = t0; n < nf; n += st) {
         const int c = a.fidx[n];
         a.X[n] = a.xs[c];
-        a.xs[c] = 0.0; a.p[c] = 0.0; a.q[c] = 0.0; r[c] = 0.0; b0[c] = 0.0f; z[c] = 0.0f;
+        a.xs[c] = 0.0; a.p[c] = 0.0; a.q[c] = 0.0; r[c] = 0.0; b0[c] = 0.0f; z[c] = 0.0f; F.code[c] = 0;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.out->iters = it;

@@ -186,7 +186,9 @@ void free_grid(fp_solver* s) {
     for (int i = 0; i < 2; ++i) { dfree(pb.R[i]); dfree(pb.Wv[i]); dfree(pb.S[i]); }
     dfree(pb.invd); dfree(pb.P); dfree(pb.X);
     dfree(pb.x64); dfree(pb.xd); dfree(pb.part); dfree(pb.bar); dfree(pb.out); dfree(pb.red);
-    for (int l = 0; l < s->mgL; ++l) { dfree(s->mg[l].lab); dfree(s->mg[l].x); dfree(s->mg[l].b); }
+    for (int l = 0; l < s->mgL; ++l) {
+        dfree(s->mg[l].lab); dfree(s->mg[l].x); dfree(s->mg[l].b); dfree(s->mg[l].code);
+    }
     s->mgL = 0;
     dfree(s->d_mgp); dfree(s->d_mgq); dfree(s->d_mgx); dfree(s->d_mgr);
     dfree(s->d_rhs_dense); dfree(s->d_x0c);
@@ -261,9 +263,10 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
         for (int l = 0; l < s->mgL && e == cudaSuccess; ++l) {
             MgLevel& L = s->mg[l];
             const size_t np_ = size_t(L.W + 2) * (L.H + 2) * (L.D + 2);
-            ck(dalloc(&L.lab, np_)); ck(dalloc(&L.x, np_)); ck(dalloc(&L.b, np_));
+            ck(dalloc(&L.lab, np_)); ck(dalloc(&L.x, np_)); ck(dalloc(&L.b, np_)); ck(dalloc(&L.code, np_));
             if (e == cudaSuccess) {
                 ck(cudaMemsetAsync(L.lab, 0, np_, s->st));  // SOLID halo
+                ck(cudaMemsetAsync(L.code, 0, np_, s->st));
                 ck(cudaMemsetAsync(L.x, 0, np_ * sizeof(float), s->st));
                 ck(cudaMemsetAsync(L.b, 0, np_ * sizeof(float), s->st));
             }
