@@ -88,24 +88,44 @@ struct Cells {
     uint8_t db[N];
     bool ok[N];
 };
-// Lanes past the end of the list get `safe`, the padded index of interior cell
-// (0,0,0): it and its six stencil neighbours lie inside every level-0 grid, so
-// the unconditional loads of an idle lane stay in bounds (its result is dropped).
+// A thread's cells are n = t0 + q * stride for trips q = 0, 1, ...  Its first
+// UNR cells (q < UNR) are cached for the whole solve in shared memory, in its
+// own column (only the thread itself reads them): padded index and diag byte,
+// or `safe` and 0 past the end of the list.  `safe` is the padded index of
+// interior cell (0,0,0): it and its six stencil neighbours lie inside every
+// level-0 grid, so the unconditional loads of an idle lane stay in bounds (its
+// result is dropped).
+__shared__ int s_fc[UNR * MG_THREADS];
+__shared__ uint8_t s_fd[UNR * MG_THREADS];
+__device__ __forceinline__ void cache_cells(const int* fidx, const uint8_t* dg, int nf, int t0, int stride, int safe) {
+#pragma unroll
+    for (int q = 0; q < UNR; ++q) {
+        const int n = t0 + q * stride;
+        s_fc[q * MG_THREADS + threadIdx.x] = n < nf ? fidx[n] : safe;
+        s_fd[q * MG_THREADS + threadIdx.x] = n < nf ? dg[n] : 0;
+    }
+}
+// Cells of trips q0 .. q0 + N - 1 (base = t0 + q0 * stride).
 template <int N>
-__device__ __forceinline__ void load_cells(Cells<N>& k, const int* fidx, const uint8_t* dg, int nf, int base, int stride,
-                                           int safe) {
+__device__ __forceinline__ void load_cells(Cells<N>& k, const int* fidx, const uint8_t* dg, int nf, int base, int q0,
+                                           int stride, int safe) {
 #pragma unroll
     for (int u = 0; u < N; ++u) {
-        const int n = base + u * stride;
+        const int n = base + u * stride, q = q0 + u;
         k.ok[u] = n < nf;
-        k.c[u] = k.ok[u] ? fidx[n] : safe;
-        k.db[u] = k.ok[u] ? dg[n] : 0;
+        if (q < UNR) {
+            k.c[u] = s_fc[q * MG_THREADS + threadIdx.x];
+            k.db[u] = s_fd[q * MG_THREADS + threadIdx.x];
+        } else {
+            k.c[u] = k.ok[u] ? fidx[n] : safe;
+            k.db[u] = k.ok[u] ? dg[n] : 0;
+        }
     }
 }
 __device__ void op0_sweep(const MgLevel& L, const int* fidx, const uint8_t* dg, int nf, int color, int t0, int stride) {
-    for (int base = t0; base < nf; base += UNR * stride) {
+    for (int base = t0, q0 = 0; base < nf; base += UNR * stride, q0 += UNR) {
         Cells<> k;
-        load_cells(k, fidx, dg, nf, base, stride, 1 + L.sy + L.sz);
+        load_cells(k, fidx, dg, nf, base, q0, stride, 1 + L.sy + L.sz);
         float b[UNR], nb[UNR];
 #pragma unroll
         for (int u = 0; u < UNR; ++u) { b[u] = L.b[k.c[u]]; nb[u] = lv_nbsum(L, k.c[u]); }
@@ -208,8 +228,8 @@ __device__ void op_prolong_red(const MgLevel& F, const MgLevel& Cl, float omega,
 // ... over the level-0 FLUID list
 __device__ void op0_prolong_red(const MgLevel& F, const MgLevel& Cl, float omega, const int* fidx, int nf, int t0,
                                 int stride) {
-    for (int n = t0; n < nf; n += stride) {
-        const int c = fidx[n];
+    for (int n = t0, q = 0; n < nf; n += stride, ++q) {
+        const int c = q < UNR ? s_fc[q * MG_THREADS + threadIdx.x] : fidx[n];
         const int i = c % F.sy - 1, j = (c / F.sy) % (F.H + 2) - 1, k = c / F.sz - 1;
         prolong_one(F, c, Cl, omega, i, j, k);
     }
@@ -559,6 +579,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     // end), the dense grid-wide levels (and, without shared-memory copies, the
     // block levels) over all their cells
     for (int l = 1; l <= (a.smem ? a.G : a.L - 1); ++l) op_codes(a.lv[l], t0, st);
+    cache_cells(a.fidx, a.diag, nf, t0, st, 1 + sy + sz);
     double rrl = 0.0;
     for (int n = t0; n < nf; n += st) {
         const int c = a.fidx[n];
@@ -623,9 +644,9 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         if (!vcycle(a, s_lv, nl)) return;  // z = M^-1 r
         double gl = 0.0, dl = 0.0;
         constexpr int U3 = 3;  // three cells in flight fit the register budget with FP64 sums
-        for (int base = t0; base < nf; base += U3 * st) {
+        for (int base = t0, q0 = 0; base < nf; base += U3 * st, q0 += U3) {
             Cells<U3> k;
-            load_cells(k, a.fidx, a.diag, nf, base, st, 1 + sy + sz);
+            load_cells(k, a.fidx, a.diag, nf, base, q0, st, 1 + sy + sz);
             float zc[U3];
             double zn[U3], rc[U3];  // A z exactly: FP32 values summed in FP64
 #pragma unroll
@@ -657,9 +678,9 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         const double alpha = gam / den;
         rrl = 0.0;
         constexpr int U2 = 2;  // FP64: two cells in flight fit the register budget
-        for (int base = t0; base < nf; base += U2 * st) {
+        for (int base = t0, q0 = 0; base < nf; base += U2 * st, q0 += U2) {
             Cells<U2> k;
-            load_cells(k, a.fidx, a.diag, nf, base, st, 1 + sy + sz);
+            load_cells(k, a.fidx, a.diag, nf, base, q0, st, 1 + sy + sz);
             double pv[U2], sv[U2], xv[U2], rv[U2], wv[U2];
             float zc[U2];
 #pragma unroll
