@@ -212,12 +212,15 @@ def run_ours(args, rank, local, world):
     solve_ms = [p["t_pcg"] - p["t_learned"] for p in per]  # the network's share is timed apart
     if args.solver in ("pcg_mg", "pcg_learned"):
         kernel = "k_pcg_mg"
-        # per MG-PCG iteration: Krylov loops 117 B per FLUID cell (FP64 p, q, x, r;
-        # FP32 z; index and diagonal), level-0 V-cycle 75 B per FLUID cell plus
-        # 5 B per cell for the restriction, coarser levels 7 B per fine cell
-        solve_bytes = [(192.0 * p["num_fluid_cells"] + 12.0 * nc) * p["pcg_iters"] for p in per]
-        note = ("192 B per fluid cell + 12 B per cell per MG-PCG iteration; the kernel is bound by its "
-                "~26 grid barriers per V-cycle, not by HBM")
+        # per MG-PCG iteration, each array read or written once per pass:
+        # Krylov passes 104 B per FLUID cell (w = A z pass: z, r, w; update
+        # pass: z, w, p, s, x, r, and the cycle's b and z), level-0 V-cycle
+        # 85 B per FLUID cell (seven sweeps of b, x and half of x written;
+        # restriction; prolongation), coarser grid-wide levels 5 B per fine
+        # cell; the block-solved levels live in shared memory
+        solve_bytes = [(189.0 * p["num_fluid_cells"] + 5.0 * nc) * p["pcg_iters"] for p in per]
+        note = ("189 B per fluid cell + 5 B per cell per MG-PCG iteration; the kernel is bound by its "
+                "~20 grid barriers per iteration and L2 latency (the working set stays in L2), not by HBM")
     else:
         kernel = "k_pcg_cg"
         solve_bytes = [41.0 * p["num_fluid_cells"] * p["pcg_iters"] + 17.0 * p["num_fluid_cells"] * p["outer_iters"]
