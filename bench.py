@@ -129,10 +129,10 @@ def make_scene(n, ppc):
     return scenes.dam_break_3d(n)
 
 
-def new_solver(lab, device, solver="pcg", n=N_GRID, ppc=PPC):
+def new_solver(lab, device, solver="pcg", n=N_GRID, ppc=PPC, warm_start=1):
     from fluidprjct_b200 import capi
     s = capi.Solver(dx=1.0 / n, dt=DT, pic_weight=PIC, advection="rk2", solver=solver, tol=1e-6, max_iters=20000,
-                    device=device, output_format=capi.OUT_NONE)
+                    device=device, output_format=capi.OUT_NONE, warm_start=warm_start)
     s.set_labels(lab)
     if solver == "pcg_learned":
         from fluidprjct_b200.learned import DEFAULT_WEIGHTS
@@ -247,7 +247,8 @@ def run_ours(args, rank, local, world):
     solver_desc = {
         "pcg": "plain PCG (Jacobi, FP64 vectors)",
         "pcg_mixed": "pcg_mixed (Jacobi PCG, FP32 stencil/vectors, FP64 reductions, FP64 refinement)",
-        "pcg_mg": "pcg_mg (FP32 multigrid V-cycle preconditioner, FP64 Krylov vectors and reductions)",
+        "pcg_mg": "pcg_mg (FP32 multigrid V-cycle preconditioner, FP64 Krylov vectors and reductions, "
+                  "warm-started from the previous step's pressure)",
         "pcg_learned": "pcg_learned (U-Net initial guess + pcg_mg, plain PCG fallback)",
     }[args.solver]
 
@@ -263,12 +264,14 @@ def run_ours(args, rank, local, world):
            "ns_per_particle_step": round(ms_step * 1e6 / np_, 3),
            "clocks": clk, "gpu_launches": int(launches), "roofline": roofline, "phases": phases}
 
-    # ---- PCG time-to-1e-6: plain vs mixed (refinement) on the same scene ----
+    # ---- PCG time-to-1e-6 of each solver on the same scene, all from x = 0 (the
+    # learned one from its network guess), and MG warm-started as in the step ----
     if not args.no_variants and rank == 0:
         var = {}
-        for name in ("pcg", "pcg_mixed", "pcg_mg", "pcg_learned"):
+        for name, solver, warm in (("pcg", "pcg", 0), ("pcg_mixed", "pcg_mixed", 0), ("pcg_mg", "pcg_mg", 0),
+                                   ("pcg_learned", "pcg_learned", 0), ("pcg_mg_warm", "pcg_mg", 1)):
             try:
-                v = new_solver(lab, local, name, args.n, args.ppc)
+                v = new_solver(lab, local, solver, args.n, args.ppc, warm)
             except Exception as e:  # variant not available in this build
                 var[name] = {"unavailable": str(e)}
                 continue

@@ -38,6 +38,7 @@ class FpConfig(C.Structure):
         ("tol", C.c_double), ("max_iters", C.c_int), ("body_radius", C.c_float), ("body_density", C.c_float),
         ("device", C.c_int), ("scheme", C.c_int), ("extrapolate", C.c_int), ("body_forces", C.c_int),
         ("mg_sweeps", C.c_int),
+        ("warm_start", C.c_int),
     ]
 
 

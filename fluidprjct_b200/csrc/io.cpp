@@ -436,6 +436,8 @@ bool load_config_json(const std::string& path, fp_config& cfg, std::string* labe
     num("max_iters", cfg.max_iters);
     num("body_radius", cfg.body_radius);
     num("body_density", cfg.body_density);
+    num("mg_sweeps", cfg.mg_sweeps);
+    num("warm_start", cfg.warm_start);
     if (strv("solver", s)) {
         if (s == "pcg") cfg.solver = FP_SOLVER_PCG;
         else if (s == "pcg_mixed") cfg.solver = FP_SOLVER_PCG_MIXED;

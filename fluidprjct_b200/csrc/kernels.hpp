@@ -80,8 +80,11 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStrea
 // factor), or null to start from x = 0.
 // nu0: red-black sweep pairs before and after the coarse correction on the
 // finest level (coarser levels take one pair; the cycle stays symmetric).
+// pprev: without x0, a dense W x H x D guess (the previous step's pressure),
+// gathered at the FLUID cells and scaled like x0; null to start from zero.
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
-                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0 = nullptr, int nu0 = 2);
+                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0 = nullptr, int nu0 = 2,
+                  const float* pprev = nullptr);
 
 // -------- labelling and the particle sort (kernels_sort.cu) --------
 // counts[nc] must be zero on entry.  Writes key/rank per particle.

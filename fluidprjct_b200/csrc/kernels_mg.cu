@@ -49,7 +49,8 @@ struct MgArgs {
     double* xs;
     double* r;
     const float* rhs;            // compact right-hand side
-    const float* x0;             // compact initial guess, or null for x = 0
+    const float* x0;             // compact initial guess, or null
+    const float* pprev;          // dense W x H x D guess (the previous pressure) when x0 is null, or null
     const int* fidx;             // compact FLUID list (level-0 padded index)
     const uint8_t* diag;         // compact diagonal, bit 7 = red/black colour
     const int* nf;
@@ -588,11 +589,20 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         r[c] = rv;
         b0[c] = float(rv);
         z[c] = first_red0(float(rv), a.diag[n]);  // the V-cycle's first sweep
-        a.xs[c] = a.x0 ? double(a.x0[n]) : 0.0;
+        float g0 = 0.0f;
+        if (a.x0) {
+            g0 = a.x0[n];
+        } else if (a.pprev) {
+            const int i = c % sy - 1, j = (c / sy) % (F.H + 2) - 1, k = c / sz - 1;
+            g0 = a.pprev[(int64_t(k) * F.H + j) * F.W + i];
+            if (!isfinite(g0)) g0 = 0.0f;
+        }
+        a.xs[c] = double(g0);
         rrl += rv * rv;
     }
+    const bool guess = a.x0 || a.pprev;
     double bb_warm = 0.0;  // ||b||^2 when started from a guess
-    if (a.x0) {
+    if (guess) {
         // Scale the guess by its energy-optimal factor alpha = (x0, b) / (x0, A x0):
         // the A-norm error of alpha x0 is never above that of x = 0.  Then r = b - A x.
         if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
@@ -626,7 +636,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     partial(rrl, 0.0, 0.0);
     if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
     double rr = total().x;
-    const double bb = a.x0 ? bb_warm : rr;
+    const double bb = guess ? bb_warm : rr;
     const double rr0 = rr;
     const double thr = a.tol * a.tol * bb;
     // Preconditioned CG in the Chronopoulos-Gear form: after the V-cycle one
@@ -806,7 +816,8 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStrea
 }
 
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
-                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0, int nu0) {
+                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0, int nu0,
+                  const float* pprev) {
     const int nb = mg_max_blocks();
     int* status = &pb.out->status;
     cudaMemsetAsync(pb.bar, 0, sizeof(GridBar), st);
@@ -824,7 +835,7 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     a.omega = 1.9f;
     a.nu_coarse = 2;
     a.nu0 = std::max(1, nu0);
-    a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
+    a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.pprev = x0 ? nullptr : pprev; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
     a.X = static_cast<double*>(pb.X);
     a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;
     a.tol = tol; a.maxit = maxit;

@@ -38,7 +38,9 @@ __device__ __forceinline__ int64_t padded_index(int i, int j, int k, const Dims&
 
 __device__ __forceinline__ bool solidish(uint8_t l) { return l == SOLID || l == BODY; }
 
-// Pass 1 of the fluid compaction: tile counts of FLUID cells; zero p.
+// Pass 1 of the fluid compaction: tile counts of FLUID cells; zero p off the
+// fluid (the solve writes every FLUID cell; until then they keep the previous
+// pressure, which a warm-started MG solve reads as its guess).
 __global__ void __launch_bounds__(SCAN_BLOCK) k_fluid_tiles(const uint8_t* __restrict__ labels, int64_t nc,
                                                             float* __restrict__ p, int* __restrict__ tile_sums) {
     int64_t e0 = int64_t(blockIdx.x) * SCAN_TILE + int64_t(threadIdx.x) * SCAN_ITEMS;
@@ -47,8 +49,9 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_fluid_tiles(const uint8_t* __res
     for (int t = 0; t < SCAN_ITEMS; ++t) {
         int64_t e = e0 + t;
         if (e < nc) {
-            s += labels[e] == FLUID;
-            p[e] = 0.0f;
+            const bool f = labels[e] == FLUID;
+            s += f;
+            if (!f) p[e] = 0.0f;
         }
     }
     int total;

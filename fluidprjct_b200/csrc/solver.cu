@@ -421,7 +421,8 @@ int solve_system(fp_solver* s, float* p_out) {
         constexpr int kLearnedMaxit = 300;
         int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr, pb.b, tol,
                                    learned ? std::min(maxit, kLearnedMaxit) : maxit, s->st, x0,
-                                   s->cfg.mg_sweeps > 0 ? s->cfg.mg_sweeps : 2)
+                                   s->cfg.mg_sweeps > 0 ? s->cfg.mg_sweeps : 2,
+                                   s->cfg.warm_start && p_out == s->d_p ? p_out : nullptr)
                    : launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st);
         cudaEventRecord(s->ev_pcg[1], s->st);
         if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
@@ -446,9 +447,10 @@ int solve_system(fp_solver* s, float* p_out) {
         dev_status = s->h_out->status;
         outer = 1;
         cudaEventElapsedTime(&pcg_ms, s->ev_pcg[0], s->ev_pcg[1]);
+        if (mg && (learned || (s->cfg.warm_start && p_out == s->d_p)))
+            guess_relres = s->h_out->bb > 0 ? float(std::sqrt(s->h_out->rr0 / s->h_out->bb)) : 0.0f;
         if (learned) {
             cudaEventElapsedTime(&learned_ms, s->ev_pcg[0], s->ev_net);
-            guess_relres = s->h_out->bb > 0 ? float(std::sqrt(s->h_out->rr0 / s->h_out->bb)) : 0.0f;
             const double rel = s->h_red[1] > 0 ? std::sqrt(s->h_red[0] / s->h_red[1]) : 0.0;
             if (*s->h_nf > 0 && dev_status != DEV_TIMEOUT && (dev_status != DEV_OK || !(rel <= tol))) {
                 // fallback: the plain FP64 PCG from x = 0
@@ -956,6 +958,7 @@ int fp_config_default(fp_config* c) {
     c->body_radius = 0.0f;
     c->body_density = 0.5f;
     c->device = -1;
+    c->warm_start = 1;
     return FP_OK;
 }
 

@@ -131,6 +131,11 @@ typedef struct fp_config {
                                       pairs before and after the coarse correction
                                       on the finest level (coarser levels: one);
                                       0 = the default, 2                           */
+    int      warm_start;           /* FP_SOLVER_PCG_MG: nonzero (the default)
+                                      starts each solve from the pressure of the
+                                      previous step, scaled by its energy-optimal
+                                      factor; the stopping test stays relative
+                                      to ||b||.  0: from x = 0                  */
 } fp_config;
 
 /* Per-step statistics: the reference's cudaEvent phase timers
@@ -147,8 +152,10 @@ typedef struct fp_step_stats {
     double  residual;          /* final true relative residual ||b-Ax||/||b||    */
     float   t_label, t_p2g, t_forces, t_pressure, t_project, t_body, t_g2p, t_advect;
     float   t_total;
-    float   guess_relres;      /* ||b - A x0|| / ||b|| of the learned initial guess
-                                  (1 for solves that start from x = 0)           */
+    float   guess_relres;      /* ||b - A x0|| / ||b|| of the initial guess (the
+                                  learned one, or the previous pressure with
+                                  warm_start), after its energy-optimal scaling;
+                                  1 for solves that start from x = 0            */
     double  body_pos[3], body_vel[3], body_omega[3], body_angles[3];
     double  body_force[3], body_torque[3];
     int64_t kernel_launches;   /* kernels this library launched, cumulative     */

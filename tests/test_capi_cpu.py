@@ -43,6 +43,8 @@ def test_config_defaults_match_reference():
     assert c.output_template == b"InputData/particles_"
     assert c.solver == capi.SOLVER_PCG and c.advection == capi.ADVECT_RK3REF
     assert c.scheme == capi.SCHEME_DEFAULT
+    # additions: MG warm start on, the finest level's sweep pairs at their default
+    assert (c.warm_start, c.mg_sweeps) == (1, 0)
     # the ctypes mirrors have the C sizes (int64 + int32 x 2 appended to the stats)
     assert C.sizeof(capi.FpStepStats) % 8 == 0
 
@@ -64,7 +66,7 @@ def test_config_json(tmp_path):
                  ' "inputLabelData": "InputData/labels_gaussian.txt", "frameAmount": 280,\n'
                  ' "outputTemplate": "OutputData/particles_", "body_x": 0.5, "body_y": 0.2, "body_z": 0.5,\n'
                  ' "body_mass": 0.03, "activeBody": true, "solver": "pcg_mixed", "advection": "rk2",'
-                 ' "seed": 7, "nested": {"a": [1, 2, {"b": null}]}}')
+                 ' "seed": 7, "mg_sweeps": 3, "warm_start": 0, "nested": {"a": [1, 2, {"b": null}]}}')
     cfg = capi.default_config()
     lab = C.create_string_buffer(256)
     frames = C.c_int(0)
@@ -77,6 +79,7 @@ def test_config_json(tmp_path):
     assert cfg.output_template == b"OutputData/particles_" and cfg.output_format == capi.OUT_PLY
     assert lab.value == b"InputData/labels_gaussian.txt" and frames.value == 280
     assert cfg.solver == capi.SOLVER_PCG_MIXED and cfg.advection == capi.ADVECT_RK2 and cfg.seed == 7
+    assert (cfg.mg_sweeps, cfg.warm_start) == (3, 0)
     bad = tmp_path / "bad.json"
     bad.write_text('{"dt": 0.1, "solver": "magic"}')
     assert capi.lib().fp_config_load_json(str(bad).encode(), C.byref(cfg), None, 0, None) == capi.FP_ERR_IO

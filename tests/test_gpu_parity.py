@@ -269,6 +269,32 @@ def test_dam_break_128_properties(O, solver):
     assert -9.81 * 0.002 * 1.2 < vel[:, 1].mean() < 0.0
 
 
+def test_mg_warm_start_from_previous_pressure():
+    """warm_start (the default for pcg_mg) starts each solve from the previous
+    step's pressure, scaled by its energy-optimal factor.  The first solve has a
+    zero guess; later ones reach the same 1e-6 target in fewer iterations, and
+    the pressures of warm and cold runs agree within the tolerance."""
+    from fluidprjct_b200 import capi, scenes
+    lab = scenes.dam_break_3d(64)
+    runs = {}
+    for ws in (0, 1):
+        s = _solver(dx=1 / 64, dt=0.004, pic_weight=0.05, tol=1e-6, solver="pcg_mg", warm_start=ws)
+        s.set_labels(lab)
+        s.seed_particles(8, 1)
+        its, guess = [], []
+        for _ in range(10):
+            s.step(1)
+            st = s.stats()
+            assert st["solve_status"] == 0 and st["residual"] <= 1e-6
+            its.append(st["pcg_iters"])
+            guess.append(st["guess_relres"])
+        runs[ws] = (its, guess, s.grid(capi.GRID_P))
+    cold, warm = runs[0], runs[1]
+    assert cold[1] == [1.0] * 10 and warm[1][0] == 1.0 and all(0.0 < g < 10.0 for g in warm[1][1:])
+    assert sum(warm[0][1:]) < sum(cold[0][1:])
+    assert rel_l2(warm[2], cold[2]) <= 1e-4
+
+
 def test_errors_are_reported_not_thrown(tmp_path):
     from fluidprjct_b200 import capi
     s = _solver(dx=0.1, dt=0.01)
