@@ -528,6 +528,18 @@ int solve_system(fp_solver* s, float* p_out) {
     else if (dev_status == DEV_TIMEOUT) status = FP_ERR_TIMEOUT;
     else if (dev_status != DEV_OK) status = FP_ERR_SOLVER;
     s->stats.solve_status = status;
+    if (status == FP_ERR_TIMEOUT && s->mgL > 0) {
+        // a solve that gave up mid-way leaves the MG work grids and level-0
+        // codes non-zero; restore the zero state the next solve relies on
+        for (int l = 0; l < s->mgL; ++l) {
+            const size_t np_ = size_t(s->mg[l].W + 2) * (s->mg[l].H + 2) * (s->mg[l].D + 2);
+            cudaMemsetAsync(s->mg[l].x, 0, np_ * sizeof(float), s->st);
+            cudaMemsetAsync(s->mg[l].b, 0, np_ * sizeof(float), s->st);
+            cudaMemsetAsync(s->mg[l].code, 0, np_, s->st);
+        }
+        for (double* a : {s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr})
+            cudaMemsetAsync(a, 0, sizeof(double) * size_t(s->padded), s->st);
+    }
     if (status == FP_ERR_TIMEOUT) return s->fail(status, "PCG grid barrier timed out");
     if (dev_status == DEV_NAN) return s->fail(status, "PCG produced NaN");
     return FP_OK;  // no-fluid, breakdown and iteration cap are reported in stats; the step continues
