@@ -101,6 +101,37 @@ def test_rigid_body_drop_160(O):
     assert abs(st["body_pos"][0] - 0.5) < 1e-6 and abs(st["body_pos"][2] - 0.5) < 1e-6
 
 
+def _float_height(density, y0, n=64, steps=1500):
+    from fluidprjct_b200 import capi, scenes
+    s = capi.Solver(dx=1.0 / n, dt=0.002, pic_weight=0.05, solver="pcg_mg", tol=1e-6, body_radius=0.12,
+                    body_density=density, body_pos=(0.5, y0, 0.5), active_body=1, advection="rk2",
+                    output_format=capi.OUT_NONE)
+    s.set_labels(scenes.pool_3d(n, 0.5))
+    s.load_sdf(None)
+    s.seed_particles(8, 2)
+    ys = []
+    for _ in range(steps):
+        s.step(1)
+        st = s.stats()
+        assert st["solve_status"] == 0
+        ys.append(st["body_pos"][1])
+    return np.array(ys[-500:])
+
+
+def test_sphere_floats_at_its_archimedes_depth():
+    """The physical check of the face-fraction coupling: a sphere (r = 0.12)
+    dropped from above a still pool (64^3, water to y = 0.5) settles where
+    buoyancy balances its weight.  At half the water's density it floats half
+    submerged (centre at the waterline, 0.5036 with the displaced water); at a
+    quarter it floats a quarter submerged, its centre 0.042 higher (submerged
+    cap height h with h^2 (3r - h) = r^3, h / 2r = 0.326).  The last 500 of
+    1500 steps (3 s) stay within about a cell of those heights."""
+    half = _float_height(0.5, 0.6)
+    quarter = _float_height(0.25, 0.65)
+    assert abs(half.mean() - 0.5036) < 0.02 and half.std() < 0.01
+    assert abs((quarter.mean() - half.mean()) - 0.042) < 0.015 and quarter.std() < 0.01
+
+
 def test_reference_body_forces_match_oracle(O):
     """body_forces = reference: the panel drag/lift of DragLiftForceCalculator
     (FluidSolver3D.cu:2674-2791) and the voxel buoyancy of applyBuoyancy
