@@ -35,6 +35,13 @@ namespace fp {
 namespace {
 
 constexpr int MG_THREADS = 1024;
+// Over-relaxation of every red-black Gauss-Seidel update (pre- and
+// post-smoothing alike, so the cycle stays symmetric): x <- x + w (y - x),
+// y = (b + neighbours) / d.  1 is plain Gauss-Seidel; 1.1 took a 128^3 dam
+// break from 13.6 to 12.2 iterations per solve (1.05: 12.8, 1.15: 12.1 but
+// more from x = 0, 1.2: 12.4, 1.3: 14.0).
+constexpr float MG_SOR = 1.1f;
+__device__ __forceinline__ float sor(float x, float y) { return MG_SOR == 1.0f ? y : x + MG_SOR * (y - x); }
 
 struct MgArgs {
     int L, G;                    // levels; levels [0, G) are grid-wide
@@ -127,13 +134,17 @@ __device__ void op0_sweep(const MgLevel& L, const int* fidx, const uint8_t* dg, 
     for (int base = t0, q0 = 0; base < nf; base += UNR * stride, q0 += UNR) {
         Cells<> k;
         load_cells(k, fidx, dg, nf, base, q0, stride, 1 + L.sy + L.sz);
-        float b[UNR], nb[UNR];
+        float b[UNR], nb[UNR], xo[UNR];
 #pragma unroll
-        for (int u = 0; u < UNR; ++u) { b[u] = L.b[k.c[u]]; nb[u] = lv_nbsum(L, k.c[u]); }
+        for (int u = 0; u < UNR; ++u) {
+            b[u] = L.b[k.c[u]];
+            nb[u] = lv_nbsum(L, k.c[u]);
+            xo[u] = MG_SOR == 1.0f ? 0.0f : L.x[k.c[u]];
+        }
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
             const int d = k.db[u] & 0x7F;
-            if (k.ok[u] && (k.db[u] >> 7) == color) L.x[k.c[u]] = d > 0 ? (b[u] + nb[u]) / float(d) : 0.0f;
+            if (k.ok[u] && (k.db[u] >> 7) == color) L.x[k.c[u]] = d > 0 ? sor(xo[u], (b[u] + nb[u]) / float(d)) : 0.0f;
         }
     }
 }
@@ -144,8 +155,8 @@ __device__ void op0_sweep(const MgLevel& L, const int* fidx, const uint8_t* dg, 
 // Gauss-Seidel update of one FLUID cell (code dc > 0).
 __device__ __forceinline__ void gs_update(const MgLevel& L, int c) {
     const int dc = L.code[c];
-    const float bv = L.b[c], nb = lv_nbsum(L, c);
-    if (dc > 0) L.x[c] = dc > 1 ? (bv + nb) / float(dc - 1) : 0.0f;
+    const float bv = L.b[c], nb = lv_nbsum(L, c), xo = MG_SOR == 1.0f ? 0.0f : L.x[c];
+    if (dc > 0) L.x[c] = dc > 1 ? sor(xo, (bv + nb) / float(dc - 1)) : 0.0f;
 }
 // Gauss-Seidel update of the FLUID cells of one colour.  With an even width
 // the work items are the cells of that colour only: cell i2 of a row is
@@ -195,7 +206,7 @@ __device__ void op_restrict_first(const MgLevel& F, const MgLevel& Cl, float sca
             if (ii && kk) s += fine_residual(F, c0 + 1 + F.sz);
             if (jj && kk) s += fine_residual(F, c0 + F.sy + F.sz);
             s *= scale;
-            if (((I + J + K) & 1) == 0) xv = dc > 1 ? s / float(dc - 1) : 0.0f;
+            if (((I + J + K) & 1) == 0) xv = dc > 1 ? sor(0.0f, s / float(dc - 1)) : 0.0f;
         }
         Cl.b[cc] = s;
         Cl.x[cc] = xv;
@@ -214,7 +225,7 @@ __device__ __forceinline__ void prolong_one(const MgLevel& F, int c, const MgLev
     const int dc = Cl.code[cc];
     const float xc = Cl.x[cc], bc = Cl.b[cc], nb = lv_nbsum(Cl, cc), xf = F.x[c];
     if (dc == 0) return;
-    const float v = ((I + J + K) & 1) != 0 ? xc : (dc > 1 ? (bc + nb) / float(dc - 1) : 0.0f);
+    const float v = ((I + J + K) & 1) != 0 ? xc : (dc > 1 ? sor(xc, (bc + nb) / float(dc - 1)) : 0.0f);
     F.x[c] = xf + omega * v;
 }
 // ... over every cell of the fine level F (dense levels)
@@ -373,7 +384,7 @@ __device__ void bl_sweep(const BlkLevel& B, int color, int t0, int st) {
     for (int t = t0; t < n; t += st) {
         const int c = int(e[t] & 0xFFFFu);
         const int d = B.code[c] - 1;
-        B.m.x[c] = d > 0 ? (B.m.b[c] + lv_nbsum(B.m, c)) / float(d) : 0.0f;
+        B.m.x[c] = d > 0 ? sor(B.m.x[c], (B.m.b[c] + lv_nbsum(B.m, c)) / float(d)) : 0.0f;
     }
 }
 // rs = b - A x on the red FLUID cells (after a black sweep the black ones vanish).
@@ -398,7 +409,7 @@ __device__ void bl_restrict(const BlkLevel& F, const BlkLevel& C, float scale, i
         s *= scale;
         C.m.b[cc] = s;
         const int d = C.code[cc] - 1;
-        C.m.x[cc] = (t < C.nred && d > 0) ? s / float(d) : 0.0f;
+        C.m.x[cc] = (t < C.nred && d > 0) ? sor(0.0f, s / float(d)) : 0.0f;
     }
 }
 // Prolongation: every FLUID cell of F adds omega * its parent's x when the
@@ -554,7 +565,7 @@ __device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
 // Level-0 first sweep value of one FLUID cell: b/d on red cells, 0 on black.
 __device__ __forceinline__ float first_red0(float b, uint8_t db) {
     const int d = db & 0x7F;
-    return ((db >> 7) == 0 && d > 0) ? b / float(d) : 0.0f;
+    return ((db >> 7) == 0 && d > 0) ? sor(0.0f, b / float(d)) : 0.0f;
 }
 
 __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
@@ -831,8 +842,10 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     // scaling it by 1.7 roughly halves the PCG iterations (29 -> 15 at 128^3,
     // 31 -> 14 at 256^2 in a float64 model of this V-cycle).  Any omega > 0
     // keeps the preconditioner symmetric; in that model PCG converged for
-    // every omega up to 2 on dam-break, pool and random-box scenes.
-    a.omega = 1.9f;
+    // every omega up to 2 on dam-break, pool and random-box scenes.  With the
+    // over-relaxed smoother, 1.8 is as fast as 1.9 on the dam break and
+    // faster on random boxes (14 against 15 iterations).
+    a.omega = 1.8f;
     a.nu_coarse = 2;
     a.nu0 = std::max(1, nu0);
     a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.pprev = x0 ? nullptr : pprev; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
