@@ -833,7 +833,10 @@ int check_ready(fp_solver* s) {
     return FP_OK;
 }
 
-int one_step(fp_solver* s) {
+// finish: wait for the step and fill its phase timers.  fp_step skips that for
+// all but the last of its steps, so the host goes on issuing the next step
+// while the GPU completes this one (the solve's own read-back still waits).
+int one_step(fp_solver* s, bool finish = true) {
     if (ref2d(s)) return one_step_ref2d(s);
     cudaEventRecord(s->ev[0], s->st);
     phase_label(s);
@@ -859,6 +862,11 @@ int one_step(fp_solver* s) {
         phase_g2p_advect(s, 1, 1);
     }
     cudaEventRecord(s->ev[8], s->st);
+    ++s->steps;
+    s->stats.step = s->steps;
+    s->stats.num_particles = s->np;
+    s->stats.kernel_launches = s->launches;
+    if (!finish) return FP_OK;
     cudaError_t e = cudaEventSynchronize(s->ev[8]);
     if (e != cudaSuccess) return s->cuda_fail(e, "step");
     float t[8];
@@ -872,10 +880,6 @@ int one_step(fp_solver* s) {
     s->stats.t_g2p = 0.0f;
     s->stats.t_advect = t[7];
     cudaEventElapsedTime(&s->stats.t_total, s->ev[0], s->ev[8]);
-    ++s->steps;
-    s->stats.step = s->steps;
-    s->stats.num_particles = s->np;
-    s->stats.kernel_launches = s->launches;
     return FP_OK;
 }
 
@@ -1283,7 +1287,7 @@ int fp_step(fp_solver* s, int n) {
     int rc = check_ready(s);
     if (rc) return rc;
     for (int i = 0; i < n; ++i) {
-        rc = one_step(s);
+        rc = one_step(s, i + 1 == n);
         if (rc) return rc;
     }
     return FP_OK;

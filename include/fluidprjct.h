@@ -227,7 +227,9 @@ int fp_save_ply(fp_solver* s, const char* path, int format);
 int64_t fp_num_particles(const fp_solver* s);
 int fp_get_particles(fp_solver* s, float* pos, float* vel, int64_t n);
 
-/* One full step (frameStep, FluidSolver3D.cu:3030-3098), n times. */
+/* One full step (frameStep, FluidSolver3D.cu:3030-3098), n times.  Returns
+ * when the last step has finished; fp_stats then holds that step's phase
+ * timers (the earlier steps of the call are not waited for). */
 int fp_step(fp_solver* s, int n);
 
 /* run() (FluidSolver3D.cu:3100-3163): frames*iter_per_frame + 1 steps with
