@@ -58,6 +58,18 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
 
 
+def max_over_ranks(value, device):
+    """The largest of a float over the ranks of the default process group (the
+    slowest replica's time); the value itself without a group or with one rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -206,11 +218,7 @@ def run_ours(args, rank, local, world):
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     launches = per[-1]["kernel_launches"] - l0
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, "cuda")
     ms_step = ms / args.steps
     value = world * args.steps / (ms / 1000.0)
 
@@ -319,12 +327,7 @@ def run_ours(args, rank, local, world):
             s.particles(out=(hpn, hvn))                    # D2H of the step's result, the next input
         a1.record(stream)
         a1.synchronize()
-        ems = a0.elapsed_time(a1)
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(a0.elapsed_time(a1), "cuda")
         out["e2e"] = {"value": round(world * k / (ems / 1000.0), 3), "unit": "steps/s",
                       "h2d_bytes_per_step": int(np_ * 24), "d2h_bytes_per_step": int(np_ * 24), "steps": k,
                       "path": "fp_set_particles(pinned host pos, vel) + fp_step + fp_get_particles"}
