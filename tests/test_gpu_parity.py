@@ -269,6 +269,42 @@ def test_dam_break_128_properties(O, solver):
     assert -9.81 * 0.002 * 1.2 < vel[:, 1].mean() < 0.0
 
 
+@pytest.mark.parametrize("dims", [(100, 60, 84), (90, 70, 1)])
+def test_mg_on_odd_sized_levels(dims):
+    """MG on grids whose grid-wide coarse levels have odd sizes: 100x60x84
+    has a 25x15x21 level swept by the whole grid, and every 2D level is odd in
+    z.  The restriction then skips children beyond the fine level, and the
+    coarse cells' codes and halos are read at the edges.  The MG solution of a
+    FLIP step's system matches the plain FP64 PCG's to the tolerance."""
+    from fluidprjct_b200 import capi, scenes
+    W, H, D = dims
+    dim = 3 if D > 1 else 2
+    dx = 1.0 / W
+    lab = scenes.box_3d(W, H, D, dx, 0.55, 0.45 * H * dx, 0.7, xmin=0.1) if dim == 3 else _odd_2d(W, H)
+    s = capi.Solver(dim=dim, dx=dx, dt=0.003, pic_weight=0.05, solver="pcg_mg", tol=1e-6, output_format=capi.OUT_NONE,
+                    warm_start=0)
+    s.set_labels(lab)
+    s.seed_particles(8 if dim == 3 else 4, 5)
+    s.step(6)
+    rhs = s.grid(capi.GRID_RHS)
+    x_mg, it_mg, rr_mg, rc_mg = s.pressure_solve(rhs)
+    p = capi.Solver(dim=dim, dx=dx, dt=0.003, solver="pcg", tol=1e-10, output_format=capi.OUT_NONE)
+    p.set_labels(s.labels().reshape(lab.shape))  # the labels of the stepped state: the same system
+    x_pcg, it_pcg, rr_pcg, rc_pcg = p.pressure_solve(rhs)
+    assert rc_mg == capi.FP_OK and rc_pcg == capi.FP_OK
+    assert rr_mg <= 1e-6 and 0 < it_mg < it_pcg
+    assert rel_l2(x_mg, x_pcg) <= 1e-4
+
+
+def _odd_2d(W, H):
+    """2D box (H, W): walls, water in the lower left."""
+    lab = np.full((H, W), 2, np.uint8)
+    lab[0, :] = lab[-1, :] = 0
+    lab[:, 0] = lab[:, -1] = 0
+    lab[1:int(0.55 * H), 1:int(0.45 * W)] = 1
+    return lab
+
+
 def test_mg_warm_start_from_previous_pressure():
     """warm_start (the default for pcg_mg) starts each solve from the previous
     step's pressure, scaled by its energy-optimal factor.  The first solve has a
