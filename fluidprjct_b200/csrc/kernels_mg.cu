@@ -11,22 +11,25 @@
 //     or 1/2 (2D); prolongation adds the coarse value to every FLUID child.
 //     With these transfers R*A*P equals the coarse unit operator, and P is a
 //     multiple of R^T.
-//   * Smoother: red-black Gauss-Seidel, red then black going down, black then
-//     red coming up; the coarsest level does the same symmetric sweeps.  The
-//     V-cycle is therefore a symmetric positive definite preconditioner.
-//     After the black sweep only red cells carry a residual, so restriction
-//     sums the red children.  Level 0 works on the compact FLUID list.
+//   * Smoother: red-black Gauss-Seidel over-relaxed by MG_SOR, red then black
+//     going down, black then red coming up (two pairs on the finest level by
+//     default, one on the others); the coarsest level does the same symmetric
+//     sweeps.  The V-cycle is therefore a symmetric positive definite
+//     preconditioner.  After the black sweep only red cells carry a residual,
+//     so restriction sums the red children.  The coarse correction is scaled
+//     by omega.  Level 0 works on the compact FLUID list.
 // Levels with more than MG_BLOCK_CELLS cells are swept by the whole grid with a
 // grid barrier between sweeps; the remaining coarse levels are done by block 0
 // alone with __syncthreads, on shared-memory copies (labels coarsened there at
 // kernel start; the first block level's b and x copied in and its x copied
-// back out per cycle).  The whole PCG runs in one persistent cooperative
-// launch with the bounded grid barrier.  Precision split: the V-cycle works in
-// FP32; the Krylov vectors (x, r, p, q) and all dot products are FP64, so the
+// back out per cycle).  The whole PCG (Chronopoulos-Gear form, optionally
+// started from a guess) runs in one persistent cooperative launch with the
+// bounded grid barrier.  Precision split: the V-cycle works in FP32; the
+// Krylov vectors (x, r, p, s) and all dot products are FP64, so the
 // recurrence residual tracks the true residual down to the 1e-6 target
-// without restarts.  Loops over the FLUID list take four cells per thread per
-// trip with all loads issued before use (the solve is latency bound: the
-// 128^3 working set lives in L2).
+// without restarts.  Loops over the FLUID list take several cells per thread
+// per trip with all loads issued before use, the first four cached in shared
+// memory (the solve is latency bound: the 128^3 working set lives in L2).
 #include "kernels.hpp"
 #include "pcg_common.cuh"
 
@@ -512,11 +515,12 @@ __device__ void block_vcycle_global(const MgArgs& a, int l0) {
 }
 
 // z = V-cycle(r) with r = lv[0].b, z = lv[0].x.  The caller has already done
-// the first (red) sweep of level 0: z = b/d on red FLUID cells, 0 on black
-// ones, and a grid barrier since.  Ends with a grid barrier; returns false if
-// a barrier timed out.  Grid-wide levels take four barriers each: black sweep,
-// restriction (with the next level's first sweep), black sweep, red sweep
-// (with the prolongation into the finer level).
+// the first (red) sweep of level 0 (z = w b/d on red FLUID cells, 0 on black
+// ones) and a grid barrier since.  Ends with a grid barrier; returns false if
+// a barrier timed out.  Grid-wide levels take four barriers each with one
+// sweep pair (level 0 two more per extra pair): black sweep, restriction (with
+// the next level's first sweep), black sweep, red sweep (with the
+// prolongation into the finer level).  nl: the levels that hold FLUID cells.
 __device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
     const unsigned nb = gridDim.x;
