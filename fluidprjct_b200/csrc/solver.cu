@@ -138,6 +138,9 @@ struct fp_solver {
     float* d_rhs_dense = nullptr;  // dense right-hand side (network input, FP_GRID_RHS)
     float* d_x0c = nullptr;        // compact initial guess
     cudaEvent_t ev_net = nullptr;
+    // a PCG / MG solve whose read-back one_step has deferred (ev[9] marks it)
+    bool solve_pending = false;
+    bool pending_guess = false;
     // pinned result mirrors
     PcgOut* h_out = nullptr;
     double* h_red = nullptr;
@@ -385,7 +388,13 @@ void phase_save(fp_solver* s) {
 //   FP_SOLVER_PCG       one FP64-vector PCG to tol (the FP64 path);
 //   FP_SOLVER_PCG_MIXED FP64 iterative refinement: r = b - A x in FP64, an
 //                       FP32-vector PCG solves A c = r loosely, x += c.
-int solve_system(fp_solver* s, float* p_out) {
+int solve_tail(fp_solver* s, int inner_total, int outer, int dev_status, float pcg_ms, float learned_ms,
+               float guess_relres, int fallback);
+
+// defer: for the plain PCG and MG solvers, queue the read-back of the solve's
+// statistics behind ev[9] and return without waiting; solve_finalize then
+// waits and fills them (one_step issues the projection and advection first).
+int solve_system(fp_solver* s, float* p_out, bool defer = false) {
     PressureBufs& pb = s->pb;
     const double tol = s->cfg.tol;
     const int maxit = s->cfg.max_iters;
@@ -428,7 +437,7 @@ int solve_system(fp_solver* s, float* p_out) {
         if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
         // FP64 solution to p, its true residual, then clear the work grids at
         // this solve's FLUID cells (the residual check leaves x in R[0])
-        auto finish = [&](bool jacobi) -> cudaError_t {
+        auto finish_launch = [&](bool jacobi) {
             launch_scatter_p(pb, p_out, 1, s->g, s->st);
             launch_true_residual(pb, 1, s->g, s->st);
             launch_pcg_clear(pb, 1, jacobi ? 1 : 0, s->st);
@@ -436,8 +445,18 @@ int solve_system(fp_solver* s, float* p_out) {
             cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
             cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
             cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+        };
+        auto finish = [&](bool jacobi) -> cudaError_t {
+            finish_launch(jacobi);
             return cudaStreamSynchronize(s->st);
         };
+        if (defer && !learned) {
+            finish_launch(!mg);
+            cudaEventRecord(s->ev[9], s->st);
+            s->solve_pending = true;
+            s->pending_guess = mg && s->cfg.warm_start && p_out == s->d_p;
+            return FP_OK;
+        }
         if (learned)
             cudaMemcpyAsync(s->h_bad, unet::net_status(s->net), sizeof(int), cudaMemcpyDeviceToHost, s->st);
         ce = finish(!mg);
@@ -514,6 +533,25 @@ int solve_system(fp_solver* s, float* p_out) {
         // xd must be zero at the start of the next solve
         cudaMemsetAsync(pb.xd, 0, sizeof(double) * size_t(s->padded), s->st);
     }
+    return solve_tail(s, inner_total, outer, dev_status, pcg_ms, learned_ms, guess_relres, fallback);
+}
+
+// Waits for a deferred solve and fills its statistics and status.
+int solve_finalize(fp_solver* s) {
+    if (!s->solve_pending) return FP_OK;
+    s->solve_pending = false;
+    const cudaError_t ce = cudaEventSynchronize(s->ev[9]);
+    if (ce != cudaSuccess) return s->cuda_fail(ce, "pressure solve");
+    float pcg_ms = 0.0f;
+    cudaEventElapsedTime(&pcg_ms, s->ev_pcg[0], s->ev_pcg[1]);
+    const float guess = !s->pending_guess ? 1.0f
+                        : (s->h_out->bb > 0 ? float(std::sqrt(s->h_out->rr0 / s->h_out->bb)) : 0.0f);
+    return solve_tail(s, s->h_out->iters, 1, s->h_out->status, pcg_ms, 0.0f, guess, 0);
+}
+
+// The statistics and status of a finished solve (host copies of its results).
+int solve_tail(fp_solver* s, int inner_total, int outer, int dev_status, float pcg_ms, float learned_ms,
+               float guess_relres, int fallback) {
     s->pcg_ms = pcg_ms;
     s->stats.t_pcg = pcg_ms;
     s->stats.num_fluid_cells = *s->h_nf;
@@ -545,11 +583,11 @@ int solve_system(fp_solver* s, float* p_out) {
     return FP_OK;  // no-fluid, breakdown and iteration cap are reported in stats; the step continues
 }
 
-int phase_pressure(fp_solver* s) {
+int phase_pressure(fp_solver* s, bool defer = false) {
     s->launches += 3;  // fluid tiles, tile scan, fluid build
     BodyKin b = body_kin(s);
     launch_pressure_setup(s->d_labels, s->d_u, s->d_v, s->d_w, s->g, s->cfg.dt, b, nullptr, s->d_p, s->pb, s->st);
-    return solve_system(s, s->d_p);
+    return solve_system(s, s->d_p, defer);
 }
 
 void phase_project(fp_solver* s) {
@@ -844,24 +882,30 @@ int one_step(fp_solver* s, bool finish = true) {
     phase_p2g(s, 1);  // P2G + save + forces
     cudaEventRecord(s->ev[2], s->st);
     cudaEventRecord(s->ev[3], s->st);
-    int rc = phase_pressure(s);
+    // The solve's statistics are read back only after the projection and
+    // advection are issued (solve_finalize), so the GPU does not idle while
+    // the host reads them; a failed solve is still reported by this call.
+    int rc = phase_pressure(s, true);
     cudaEventRecord(s->ev[4], s->st);
-    if (rc != FP_OK) return rc;
+    auto fail_after = [&](int rc0) { const int r = solve_finalize(s); return rc0 != FP_OK ? rc0 : r; };
+    if (rc != FP_OK) return fail_after(rc);
     phase_project(s);
     cudaEventRecord(s->ev[5], s->st);
     rc = phase_body(s);
-    if (rc != FP_OK) return rc;
+    if (rc != FP_OK) return fail_after(rc);
     cudaEventRecord(s->ev[6], s->st);
     cudaEventRecord(s->ev[7], s->st);
     if (s->cfg.extrapolate > 0) {
         phase_g2p_advect(s, 1, 0);
         rc = extrapolate_3d(s);
-        if (rc != FP_OK) return rc;
+        if (rc != FP_OK) return fail_after(rc);
         phase_g2p_advect(s, 0, 1);
     } else {
         phase_g2p_advect(s, 1, 1);
     }
     cudaEventRecord(s->ev[8], s->st);
+    rc = solve_finalize(s);
+    if (rc != FP_OK) return rc;
     ++s->steps;
     s->stats.step = s->steps;
     s->stats.num_particles = s->np;
