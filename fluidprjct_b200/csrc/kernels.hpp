@@ -82,9 +82,12 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStrea
 // finest level (coarser levels take one pair; the cycle stays symmetric).
 // pprev: without x0, a dense W x H x D guess (the previous step's pressure),
 // gathered at the FLUID cells and scaled like x0; null to start from zero.
+// pout: the dense W x H x D pressure out (its non-FLUID cells must be zero),
+// or null.  The kernel also writes the true residual's ||rhs - A x||^2 and
+// ||rhs||^2 (FP64) to pb.red.
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
                   const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0 = nullptr, int nu0 = 2,
-                  const float* pprev = nullptr);
+                  const float* pprev = nullptr, float* pout = nullptr);
 
 // -------- labelling and the particle sort (kernels_sort.cu) --------
 // counts[nc] must be zero on entry.  Writes key/rank per particle.

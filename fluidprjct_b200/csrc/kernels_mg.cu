@@ -65,6 +65,8 @@ struct MgArgs {
     const uint8_t* diag;         // compact diagonal, bit 7 = red/black colour
     const int* nf;
     double* X;                   // compact solution out (FP64)
+    float* pout;                 // dense W x H x D pressure out (zero off the fluid already), or null
+    double* red;                 // [2] out: ||rhs - A x||^2 and ||rhs||^2 of the solution, in FP64
     double* part;
     GridBar* bar;
     int* status;
@@ -742,12 +744,36 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         gam_old = gam;
         alpha_old = alpha;
     }
-    // compact solution; zero the level-0 work grids at the FLUID cells so the
-    // next solve starts from zero whatever cells are fluid then
+    // The true residual of the FP64 solution, ||rhs - A x||^2 and ||rhs||^2,
+    // then the compact and dense solution; zero the level-0 work grids at the
+    // FLUID cells so the next solve starts from zero whatever cells are fluid.
     if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+    {
+        double e2 = 0.0, b2 = 0.0;
+        for (int n = t0; n < nf; n += st) {
+            const int c = a.fidx[n];
+            const double* xp = a.xs + c;
+            const double ax = double(a.diag[n] & 0x7F) * xp[0] -
+                              ((xp[1] + xp[-1]) + (xp[sy] + xp[-sy]) + (xp[sz] + xp[-sz]));
+            const double bv = double(a.rhs[n]), e = bv - ax;
+            e2 += e * e;
+            b2 += bv * bv;
+        }
+        partial(e2, b2, 0.0);
+    }
+    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+    {
+        const double3 t = total();
+        if (blockIdx.x == 0 && threadIdx.x == 0) { a.red[0] = t.x; a.red[1] = t.y; }
+    }
     for (int n = t0; n < nf; n += st) {
         const int c = a.fidx[n];
-        a.X[n] = a.xs[c];
+        const double xv = a.xs[c];
+        a.X[n] = xv;
+        if (a.pout) {
+            const int i = c % sy - 1, j = (c / sy) % (F.H + 2) - 1, k = c / sz - 1;
+            a.pout[(int64_t(k) * F.H + j) * F.W + i] = float(xv);
+        }
         a.xs[c] = 0.0; a.p[c] = 0.0; a.q[c] = 0.0; r[c] = 0.0; b0[c] = 0.0f; z[c] = 0.0f; F.code[c] = 0;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -832,7 +858,7 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStrea
 
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
                   const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0, int nu0,
-                  const float* pprev) {
+                  const float* pprev, float* pout) {
     const int nb = mg_max_blocks();
     int* status = &pb.out->status;
     cudaMemsetAsync(pb.bar, 0, sizeof(GridBar), st);
@@ -854,6 +880,8 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     a.nu0 = std::max(1, nu0);
     a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.pprev = x0 ? nullptr : pprev; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
     a.X = static_cast<double*>(pb.X);
+    a.pout = pout;
+    a.red = pb.red;
     a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;
     a.tol = tol; a.maxit = maxit;
     void* args[] = {&a};

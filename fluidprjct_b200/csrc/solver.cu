@@ -431,17 +431,22 @@ int solve_system(fp_solver* s, float* p_out, bool defer = false) {
         int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr, pb.b, tol,
                                    learned ? std::min(maxit, kLearnedMaxit) : maxit, s->st, x0,
                                    s->cfg.mg_sweeps > 0 ? s->cfg.mg_sweeps : 2,
-                                   s->cfg.warm_start && p_out == s->d_p ? p_out : nullptr)
+                                   s->cfg.warm_start && p_out == s->d_p ? p_out : nullptr, p_out)
                    : launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st);
         cudaEventRecord(s->ev_pcg[1], s->st);
         if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
         // FP64 solution to p, its true residual, then clear the work grids at
-        // this solve's FLUID cells (the residual check leaves x in R[0])
+        // this solve's FLUID cells (the residual check leaves x in R[0]); the
+        // MG kernel does all three itself
         auto finish_launch = [&](bool jacobi) {
-            launch_scatter_p(pb, p_out, 1, s->g, s->st);
-            launch_true_residual(pb, 1, s->g, s->st);
-            launch_pcg_clear(pb, 1, jacobi ? 1 : 0, s->st);
-            s->launches += (jacobi ? 1 : 0) + 1 + 1 + 3 + 1;  // [reset +] pcg, scatter, residual (3), clear
+            if (jacobi) {
+                launch_scatter_p(pb, p_out, 1, s->g, s->st);
+                launch_true_residual(pb, 1, s->g, s->st);
+                launch_pcg_clear(pb, 1, 1, s->st);
+                s->launches += 1 + 1 + 1 + 3 + 1;  // reset + pcg, scatter, residual (3), clear
+            } else {
+                s->launches += 1;  // the MG kernel
+            }
             cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
             cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
             cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
