@@ -269,6 +269,32 @@ def test_dam_break_128_properties(O, solver):
     assert -9.81 * 0.002 * 1.2 < vel[:, 1].mean() < 0.0
 
 
+def test_dam_break_128_full_length():
+    """Config 2 at full size and length: 200 steps (0.4 s) of the 128^3 dam
+    break with the bench's settings (MG, warm start, RK2).  Every solve
+    reaches 1e-6, no particle is lost, the collapsing column's front runs
+    along the floor, and the centre of mass falls."""
+    from fluidprjct_b200 import capi, scenes
+    s = _solver(dx=1 / 128, dt=0.002, pic_weight=0.05, tol=1e-6, solver="pcg_mg", advection="rk2",
+                output_format=capi.OUT_NONE)
+    s.set_labels(scenes.dam_break_3d(128))
+    s.seed_particles(8, 1)
+    n0 = s.num_particles
+    y0 = s.particles()[0][:, 1].mean()
+    its = []
+    for _ in range(200):
+        s.step(1)
+        st = s.stats()
+        assert st["solve_status"] == 0 and st["residual"] <= 1e-6
+        its.append(st["pcg_iters"])
+    pos, vel = s.particles()
+    assert pos.shape[0] == n0 and np.isfinite(pos).all() and np.isfinite(vel).all()
+    floor = pos[:, 1] < 0.1
+    assert pos[floor, 0].max() > 0.8           # the front crossed most of the tank (it started at x = 0.4)
+    assert pos[:, 1].mean() < 0.9 * y0        # potential energy released (y0 = 0.3)
+    assert max(its) < 40
+
+
 @pytest.mark.parametrize("dims", [(100, 60, 84), (90, 70, 1)])
 def test_mg_on_odd_sized_levels(dims):
     """MG on grids whose grid-wide coarse levels have odd sizes: 100x60x84
