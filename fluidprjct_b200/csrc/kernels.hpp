@@ -68,9 +68,9 @@ int mg_max_blocks();
 // First block-solved level G of the hierarchy and the shared memory its
 // copies take (0: the block levels stay in global memory).
 int mg_split(const MgLevel* lv, int L, int* smem_bytes);
-// Level labels from the cell labels (per solve): level 0 and the grid-wide
-// levels; the solver kernel coarsens the shared-memory levels itself.
-// Returns the number of launches.
+// Level labels from the cell labels (per solve): the grid-wide coarse levels;
+// the solver kernel coarsens the shared-memory levels itself.  Returns the
+// number of launches.
 int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStream_t st);
 // MG-preconditioned PCG (FP32 V-cycle, FP64 Krylov vectors and reductions) for
 // A x = rhs (compact) to ||r||/||rhs|| <= tol; solution in pb.X (FP64

@@ -786,21 +786,32 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     }
 }
 
-// Level-0 labels with a SOLID halo; BODY counts as SOLID (Neumann).
-__global__ void k_pad_labels(const uint8_t* __restrict__ lab, Dims g, MgLevel L) {
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= g.nc()) return;
-    int i, j, k;
-    const int c = lv_cell(L, int(t), i, j, k);
-    const uint8_t l = lab[t];
-    L.lab[c] = l == BODY ? SOLID : l;
-}
-
 // Coarse labels with Dirichlet priority: AIR if any child AIR, else FLUID if
 // any child FLUID, else SOLID.
 __global__ void k_coarsen(MgLevel F, MgLevel Cl) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < Cl.W * Cl.H * Cl.D) coarsen_cell(F, Cl, t);
+}
+
+// Level 1 straight from the cell labels, by the same rule (BODY, like SOLID,
+// is neither AIR nor FLUID); level 0 itself needs no padded label copy, as
+// its operations read the FLUID list's diagonal bytes and codes.
+__global__ void k_coarsen_cells(const uint8_t* __restrict__ lab, Dims g, MgLevel Cl) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= Cl.W * Cl.H * Cl.D) return;
+    int I, J, K;
+    const int cc = lv_cell(Cl, t, I, J, K);
+    bool air = false, fluid = false;
+    for (int c3 = 0; c3 < 2; ++c3)
+        for (int b3 = 0; b3 < 2; ++b3)
+            for (int a3 = 0; a3 < 2; ++a3) {
+                const int i = 2 * I + a3, j = 2 * J + b3, k = 2 * K + c3;
+                if (i >= g.W || j >= g.H || k >= g.D) continue;
+                const uint8_t l = lab[int64_t(i) + int64_t(j) * g.W + int64_t(k) * g.W * g.H];
+                air |= l == AIR;
+                fluid |= l == FLUID;
+            }
+    Cl.lab[cc] = air ? AIR : (fluid ? FLUID : SOLID);
 }
 
 }  // namespace
@@ -848,12 +859,12 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStrea
     int smem = 0;
     const int G = mg_split(lv, L, &smem);
     const int last = smem ? G : L - 1;  // deeper shared-memory levels: coarsened by the solver kernel
-    k_pad_labels<<<unsigned((g.nc() + 255) / 256), 256, 0, st>>>(labels, g, lv[0]);
     for (int l = 1; l <= last; ++l) {
         const int n = lv[l].W * lv[l].H * lv[l].D;
-        k_coarsen<<<(n + 255) / 256, 256, 0, st>>>(lv[l - 1], lv[l]);
+        if (l == 1) k_coarsen_cells<<<(n + 255) / 256, 256, 0, st>>>(labels, g, lv[1]);
+        else k_coarsen<<<(n + 255) / 256, 256, 0, st>>>(lv[l - 1], lv[l]);
     }
-    return 1 + last;
+    return last;
 }
 
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
