@@ -598,56 +598,105 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     // block levels) over all their cells
     for (int l = 1; l <= (a.smem ? a.G : a.L - 1); ++l) op_codes(a.lv[l], t0, st);
     cache_cells(a.fidx, a.diag, nf, t0, st, 1 + sy + sz);
-    double rrl = 0.0;
-    for (int n = t0; n < nf; n += st) {
-        const int c = a.fidx[n];
-        const double rv = double(a.rhs[n]);
-        F.code[c] = uint8_t(1 + (a.diag[n] & 0x7F));
-        r[c] = rv;
-        b0[c] = float(rv);
-        z[c] = first_red0(float(rv), a.diag[n]);  // the V-cycle's first sweep
-        float g0 = 0.0f;
-        if (a.x0) {
-            g0 = a.x0[n];
-        } else if (a.pprev) {
-            const int i = c % sy - 1, j = (c / sy) % (F.H + 2) - 1, k = c / sz - 1;
-            g0 = a.pprev[(int64_t(k) * F.H + j) * F.W + i];
-            if (!isfinite(g0)) g0 = 0.0f;
+    // r = rhs, the V-cycle's right-hand side and first sweep, the level-0
+    // codes and the guess.  A dense guess (the previous pressure, zero off the
+    // current fluid and outside the grid) also gets its stencil A g and the
+    // dot products here: it was complete before the launch, so its
+    // neighbours need no grid barrier.  A compact guess needs one.
+    const bool dense_guess = a.pprev != nullptr;
+    double rrl = 0.0, xb = 0.0, xq = 0.0;
+    constexpr int UI = 2;
+    for (int base = t0, q0 = 0; base < nf; base += UI * st, q0 += UI) {
+        Cells<UI> k;
+        load_cells(k, a.fidx, a.diag, nf, base, q0, st, 1 + sy + sz);
+        float bvf[UI], g[UI];
+        double qv[UI];
+#pragma unroll
+        for (int u = 0; u < UI; ++u) {
+            const int n = base + u * st;
+            bvf[u] = k.ok[u] ? a.rhs[n] : 0.0f;
+            g[u] = 0.0f;
+            qv[u] = 0.0;
+            if (!k.ok[u]) continue;
+            if (a.x0) {
+                g[u] = a.x0[n];
+            } else if (dense_guess) {
+                const int c = k.c[u];
+                const int i = c % sy - 1, j = (c / sy) % (F.H + 2) - 1, kk = c / sz - 1;
+                const int64_t e = (int64_t(kk) * F.H + j) * F.W + i, sY = F.W, sZ = int64_t(F.W) * F.H;
+                auto gv = [&](bool in, int64_t off) {
+                    const float v = in ? a.pprev[e + off] : 0.0f;
+                    return isfinite(v) ? double(v) : 0.0;
+                };
+                const double gc = gv(true, 0);
+                g[u] = float(gc);
+                qv[u] = double(k.db[u] & 0x7F) * gc - ((gv(i + 1 < F.W, 1) + gv(i > 0, -1)) +
+                                                        (gv(j + 1 < F.H, sY) + gv(j > 0, -sY)) +
+                                                        (gv(kk + 1 < F.D, sZ) + gv(kk > 0, -sZ)));
+            }
         }
-        a.xs[c] = double(g0);
-        rrl += rv * rv;
+#pragma unroll
+        for (int u = 0; u < UI; ++u) {
+            if (!k.ok[u]) continue;
+            const int c = k.c[u];
+            const double rv = double(bvf[u]);
+            F.code[c] = uint8_t(1 + (k.db[u] & 0x7F));
+            r[c] = rv;
+            b0[c] = float(rv);
+            z[c] = first_red0(float(rv), k.db[u]);  // the V-cycle's first sweep
+            a.xs[c] = double(g[u]);
+            if (dense_guess) {
+                a.q[c] = qv[u];
+                xb += double(g[u]) * rv;
+                xq += double(g[u]) * qv[u];
+            }
+            rrl += rv * rv;
+        }
     }
     const bool guess = a.x0 || a.pprev;
     double bb_warm = 0.0;  // ||b||^2 when started from a guess
     if (guess) {
         // Scale the guess by its energy-optimal factor alpha = (x0, b) / (x0, A x0):
         // the A-norm error of alpha x0 is never above that of x = 0.  Then r = b - A x.
-        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
-        double xb = 0.0, xq = 0.0, bbl = 0.0;
-        for (int n = t0; n < nf; n += st) {
-            const int c = a.fidx[n];
-            const double* xp = a.xs + c;
-            const double qv = double(a.diag[n] & 0x7F) * xp[0] -
-                              ((xp[1] + xp[-1]) + (xp[sy] + xp[-sy]) + (xp[sz] + xp[-sz]));
-            a.q[c] = qv;
-            xb += xp[0] * r[c];
-            xq += xp[0] * qv;
-            bbl += r[c] * r[c];
+        if (a.x0) {
+            if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+            for (int n = t0; n < nf; n += st) {
+                const int c = a.fidx[n];
+                const double* xp = a.xs + c;
+                const double qc = double(a.diag[n] & 0x7F) * xp[0] -
+                                  ((xp[1] + xp[-1]) + (xp[sy] + xp[-sy]) + (xp[sz] + xp[-sz]));
+                a.q[c] = qc;
+                xb += xp[0] * r[c];
+                xq += xp[0] * qc;
+            }
         }
-        partial(xb, xq, bbl);
+        partial(xb, xq, rrl);
         if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
         const double3 t = total();
         const double alpha = (t.y > 0.0 && isfinite(t.x / t.y)) ? t.x / t.y : 0.0;
         bb_warm = t.z;  // all reads of x ended before the barrier above
         rrl = 0.0;
-        for (int n = t0; n < nf; n += st) {
-            const int c = a.fidx[n];
-            a.xs[c] *= alpha;
-            const double rv = r[c] - alpha * a.q[c];
-            r[c] = rv;
-            b0[c] = float(rv);
-            z[c] = first_red0(float(rv), a.diag[n]);
-            rrl += rv * rv;
+        for (int base = t0, q0 = 0; base < nf; base += UI * st, q0 += UI) {
+            Cells<UI> k;
+            load_cells(k, a.fidx, a.diag, nf, base, q0, st, 1 + sy + sz);
+            double xv[UI], rv0[UI], qc[UI];
+#pragma unroll
+            for (int u = 0; u < UI; ++u) {
+                xv[u] = a.xs[k.c[u]];
+                rv0[u] = r[k.c[u]];
+                qc[u] = a.q[k.c[u]];
+            }
+#pragma unroll
+            for (int u = 0; u < UI; ++u) {
+                if (!k.ok[u]) continue;
+                const int c = k.c[u];
+                a.xs[c] = xv[u] * alpha;
+                const double rv = rv0[u] - alpha * qc[u];
+                r[c] = rv;
+                b0[c] = float(rv);
+                z[c] = first_red0(float(rv), k.db[u]);
+                rrl += rv * rv;
+            }
         }
     }
     partial(rrl, 0.0, 0.0);
