@@ -53,12 +53,16 @@ enum { FP_SOLID = 0, FP_FLUID = 1, FP_AIR = 2, FP_BODY = 3 };
 enum { FP_OUT_PLY = 0, FP_OUT_OFF = 1, FP_OUT_PLY_BINARY = 2, FP_OUT_NONE = 3 };
 
 /* Pressure solver variants (all matrix-free 7-point PCG on the GPU):
- *   FP_SOLVER_PCG         FP32 stencil and vectors, FP64 reductions, Jacobi
- *                         preconditioner ("plain" PCG);
- *   FP_SOLVER_PCG_MIXED   the same inner PCG inside an FP64 iterative-refinement
- *                         loop (true residual recomputed in FP64);
- *   FP_SOLVER_PCG_MG      geometric-multigrid V-cycle preconditioner;
- *   FP_SOLVER_PCG_LEARNED learned U-Net preconditioner, plain PCG fallback. */
+ *   FP_SOLVER_PCG         FP64 vectors and reductions, Jacobi preconditioner
+ *                         ("plain" PCG);
+ *   FP_SOLVER_PCG_MIXED   FP32 stencil and vectors with FP64 reductions, inside
+ *                         an FP64 iterative-refinement loop (true residual
+ *                         recomputed in FP64);
+ *   FP_SOLVER_PCG_MG      FP32 geometric-multigrid V-cycle preconditioner, FP64
+ *                         Krylov vectors and reductions; warm-started from the
+ *                         previous step's pressure (warm_start);
+ *   FP_SOLVER_PCG_LEARNED a learned U-Net's pressure guess as the initial
+ *                         iterate of the MG solve, plain PCG fallback. */
 enum { FP_SOLVER_PCG = 0, FP_SOLVER_PCG_MIXED = 1, FP_SOLVER_PCG_MG = 2, FP_SOLVER_PCG_LEARNED = 3 };
 
 /* Advection: the reference's adaptive Ralston RK3 (AdvectParticlesFunctor,
