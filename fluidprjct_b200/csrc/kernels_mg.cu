@@ -705,26 +705,30 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     const double bb = guess ? bb_warm : rr;
     const double rr0 = rr;
     const double thr = a.tol * a.tol * bb;
-    // Preconditioned CG in the Chronopoulos-Gear form: after the V-cycle one
-    // pass forms w = A z, gamma = (r, z) and delta = (z, w); one more updates
-    // p = z + beta p, s = w + beta s (= A p), x += alpha p, r -= alpha s and
-    // starts the next cycle, with beta = gamma / gamma_old and
-    // alpha = gamma / (delta - beta gamma / alpha_old).  Two grid-wide passes
-    // per iteration besides the cycle.  w is kept in the compact X buffer
-    // (the solution is written there only at the end); s lives in q.
+    // Flexible preconditioned CG in the Chronopoulos-Gear form: after the
+    // V-cycle one pass forms w = A z, gamma = (r, z), delta = (z, w) and
+    // zeta = (z, s_old); one more updates p = z + beta p, s = w + beta s
+    // (= A p), x += alpha p, r -= alpha s and starts the next cycle.  beta is
+    // the Polak-Ribiere choice (z, r - r_old) / gamma_old = -alpha_old zeta /
+    // gamma_old, and (p, A p) = delta + 2 beta zeta + beta^2 (p, A p)_old holds
+    // for any beta, so alpha = gamma / (p, A p) needs no symmetry of the
+    // V-cycle (over-relaxed smoothing makes it slightly non-symmetric).  Two
+    // grid-wide passes per iteration besides the cycle.  w is kept in the
+    // compact X buffer (the solution is written there only at the end); s
+    // lives in q.
     double* w = a.X;
-    double gam = 0.0, gam_old = 0.0, alpha_old = 1.0;
+    double gam = 0.0, gam_old = 0.0, alpha_old = 1.0, den_old = 1.0;
     int it = 0, stt = DEV_OK;
     while (rr > thr && bb > 0.0) {
         if (it >= a.maxit) { stt = DEV_MAXIT; break; }
         if (!vcycle(a, s_lv, nl)) return;  // z = M^-1 r
-        double gl = 0.0, dl = 0.0;
+        double gl = 0.0, dl = 0.0, sl = 0.0;
         constexpr int U3 = 3;  // three cells in flight fit the register budget with FP64 sums
         for (int base = t0, q0 = 0; base < nf; base += U3 * st, q0 += U3) {
             Cells<U3> k;
             load_cells(k, a.fidx, a.diag, nf, base, q0, st, 1 + sy + sz);
             float zc[U3];
-            double zn[U3], rc[U3];  // A z exactly: FP32 values summed in FP64
+            double zn[U3], rc[U3], sc[U3];  // A z exactly: FP32 values summed in FP64
 #pragma unroll
             for (int u = 0; u < U3; ++u) {
                 const float* zp = z + k.c[u];
@@ -732,6 +736,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
                 zn[u] = (double(zp[1]) + double(zp[-1])) + (double(zp[sy]) + double(zp[-sy])) +
                         (double(zp[sz]) + double(zp[-sz]));
                 rc[u] = r[k.c[u]];
+                sc[u] = a.q[k.c[u]];
             }
 #pragma unroll
             for (int u = 0; u < U3; ++u) {
@@ -741,15 +746,16 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
                 w[base + u * st] = wv;
                 gl += rc[u] * zv;
                 dl += zv * wv;
+                sl += zv * sc[u];
             }
         }
-        partial(gl, dl, 0.0);
+        partial(gl, dl, sl);
         if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
         const double3 t = total();
         gam = t.x;
-        if (isnan(t.x) || isnan(t.y)) { stt = DEV_NAN; break; }
-        const double beta = it > 0 ? gam / gam_old : 0.0;
-        const double den = it > 0 ? t.y - beta * gam / alpha_old : t.y;
+        if (isnan(t.x) || isnan(t.y) || isnan(t.z)) { stt = DEV_NAN; break; }
+        const double beta = it > 0 ? -alpha_old * t.z / gam_old : 0.0;
+        const double den = it > 0 ? t.y + beta * (2.0 * t.z + beta * den_old) : t.y;
         if (!(den > 0.0)) { stt = DEV_BREAKDOWN; break; }
         const double alpha = gam / den;
         rrl = 0.0;
@@ -792,6 +798,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         if (isnan(rr)) { stt = DEV_NAN; break; }
         gam_old = gam;
         alpha_old = alpha;
+        den_old = den;
     }
     // The true residual of the FP64 solution, ||rhs - A x||^2 and ||rhs||^2,
     // then the compact and dense solution; zero the level-0 work grids at the
