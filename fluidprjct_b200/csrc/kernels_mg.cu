@@ -22,9 +22,9 @@
 // grid barrier between sweeps; the remaining coarse levels are done by block 0
 // alone with __syncthreads, on shared-memory copies (labels coarsened there at
 // kernel start; the first block level's b and x copied in and its x copied
-// back out per cycle).  The whole PCG (Chronopoulos-Gear form, optionally
-// started from a guess) runs in one persistent cooperative launch with the
-// bounded grid barrier.  Precision split: the V-cycle works in FP32; the
+// back out per cycle).  The whole PCG (flexible, in the Chronopoulos-Gear
+// form, optionally started from a guess) runs in one persistent cooperative
+// launch with the bounded grid barrier.  Precision split: the V-cycle works in FP32; the
 // Krylov vectors (x, r, p, s) and all dot products are FP64, so the
 // recurrence residual tracks the true residual down to the 1e-6 target
 // without restarts.  Loops over the FLUID list take several cells per thread
