@@ -263,8 +263,8 @@ def run_ours(args, rank, local, world):
     solver_desc = {
         "pcg": "plain PCG (Jacobi, FP64 vectors)",
         "pcg_mixed": "pcg_mixed (Jacobi PCG, FP32 stencil/vectors, FP64 reductions, FP64 refinement)",
-        "pcg_mg": "pcg_mg (FP32 multigrid V-cycle preconditioner, FP64 Krylov vectors and reductions, "
-                  "warm-started from the previous step's pressure)",
+        "pcg_mg": "pcg_mg (flexible PCG with an FP32 multigrid V-cycle preconditioner, FP64 Krylov vectors and "
+                  "reductions, warm-started from the previous step's pressure)",
         "pcg_learned": "pcg_learned (U-Net initial guess + pcg_mg, plain PCG fallback)",
     }[args.solver]
 
