@@ -17,9 +17,12 @@
 //   * it holds systems of at most FP_NOALLOC_MAX_N unknowns (5 double vectors
 //     of that length, 10 MiB); larger systems are rejected with FP_ERR_ARG
 //     before any GPU work;
-//   * every call on a device uses the same array, so calls that overlap on
-//     the GPU (two host threads, or two streams running at once) race and
-//     corrupt each other's vectors; the caller serialises them;
+//   * every call on a device uses the same array, so the calls on one device
+//     take turns: each holds that device's host mutex from its first launch
+//     until its stream has drained (the call is synchronous; on an error path
+//     the stream is synchronised before the mutex is released), and calls
+//     from several host threads, on any streams, are serialised in-process
+//     (separate processes have separate contexts, each with its own array);
 //   * each call clears the scratch it relies on: the argument-check flag and
 //     the product vector before every SpMV; x starts at zero;
 //   * the first call on each device, with that device current, looks up the
@@ -45,10 +48,13 @@ static __device__ __align__(256) double g_csr_scratch[kScratchDoubles];
 
 std::mutex g_setup_mutex;
 double* g_scratch_ptr[kMaxDevices] = {nullptr};  // device address of g_csr_scratch, per device ordinal
+std::mutex g_call_mutex[kMaxDevices];            // held by the one call that owns a device's scratch
 
-int scratch_for_current_device(double** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FP_ERR_CUDA;
+int current_device(int* dev) {
+    return cudaGetDevice(dev) == cudaSuccess && *dev >= 0 && *dev < kMaxDevices ? FP_OK : FP_ERR_CUDA;
+}
+
+int scratch_for_device(int dev, double** out) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_ptr[dev]) {
         void* p = nullptr;
@@ -145,19 +151,10 @@ __global__ void na_direction(int n, const double* __restrict__ z, double beta, d
     if (i < n) d[i] = z[i] + beta * d[i];
 }
 
-}  // namespace
-
-extern "C" int fp_solve_csr_upper_noalloc(int n, const int* d_offsets, const int* d_cols, const double* d_vals,
-                                          const double* d_b, double* d_x, double tol, int max_iters, int* iters,
-                                          double* relres, void* stream) {
-    if (n <= 0 || !d_offsets || !d_cols || !d_vals || !d_b || !d_x) return FP_ERR_ARG;
-    if (n > kMaxN) {
-        std::fprintf(stderr, "fp_solve_csr_upper_noalloc: n = %d exceeds the scratch limit of %d unknowns\n", n,
-                     kMaxN);
-        return FP_ERR_ARG;
-    }
-    double* base = nullptr;
-    if (const int rc = scratch_for_current_device(&base)) return rc;
+// The solve proper, run by one call at a time per device on scratch base.
+int solve_on_scratch(double* base, int n, const int* d_offsets, const int* d_cols, const double* d_vals,
+                     const double* d_b, double* d_x, double tol, int max_iters, int* iters, double* relres,
+                     cudaStream_t st) {
     double* dg = base;
     double* r = base + size_t(kMaxN);
     double* d = base + 2 * size_t(kMaxN);
@@ -166,7 +163,6 @@ extern "C" int fp_solve_csr_upper_noalloc(int n, const int* d_offsets, const int
     double* part = base + 5 * size_t(kMaxN);
     double* res = part + kDotBlocks;
     double* bad = res + 1;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int blk = 128, grd = (n + blk - 1) / blk;
 
     auto read = [&](const double* src, double& out) {
@@ -216,4 +212,28 @@ extern "C" int fp_solve_csr_upper_noalloc(int n, const int* d_offsets, const int
     if (iters) *iters = it;
     if (relres) *relres = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
     return FP_OK;
+}
+
+}  // namespace
+
+extern "C" int fp_solve_csr_upper_noalloc(int n, const int* d_offsets, const int* d_cols, const double* d_vals,
+                                          const double* d_b, double* d_x, double tol, int max_iters, int* iters,
+                                          double* relres, void* stream) {
+    if (n <= 0 || !d_offsets || !d_cols || !d_vals || !d_b || !d_x) return FP_ERR_ARG;
+    if (n > kMaxN) {
+        std::fprintf(stderr, "fp_solve_csr_upper_noalloc: n = %d exceeds the scratch limit of %d unknowns\n", n,
+                     kMaxN);
+        return FP_ERR_ARG;
+    }
+    int dev = 0;
+    double* base = nullptr;
+    if (const int rc = current_device(&dev)) return rc;
+    if (const int rc = scratch_for_device(dev, &base)) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lock(g_call_mutex[dev]);
+    const int rc = solve_on_scratch(base, n, d_offsets, d_cols, d_vals, d_b, d_x, tol, max_iters, iters, relres, st);
+    // An early error return may leave launches queued on st: let them finish
+    // before the next call takes the scratch.
+    if (rc != FP_OK) cudaStreamSynchronize(st);
+    return rc;
 }

@@ -281,7 +281,9 @@ int fp_solve_csr_upper(int n, const int* offsets, const int* cols, const double*
  * call never allocates.  For hosts whose own pool allocator owns the GPU, and
  * for loops that cannot pay cudaMalloc's latency and device-wide sync.
  *   - n above FP_NOALLOC_MAX_N is rejected with FP_ERR_ARG;
- *   - all calls on a device share the array: overlapping calls race;
+ *   - all calls on a device share the array, so they take turns: a call
+ *     holds a per-device host lock until its stream has drained, and calls
+ *     from several host threads are serialised;
  *   - the first call on a device, with that device current, looks up the
  *     array's address; make it before any stream capture on that device.
  * stream may be NULL (the legacy default stream). */

@@ -95,3 +95,52 @@ def test_noalloc_rejects_oversize_and_malformed():
     it, rr = capi.solve_csr_upper_noalloc(2, *ptrs(cols_ok), tol=1e-14)
     torch.cuda.synchronize(dev)
     assert torch.equal(x.cpu(), torch.ones(2, dtype=torch.float64)) and it <= 1
+
+
+@pytest.mark.gpu
+def test_noalloc_calls_from_two_threads_take_turns(O):
+    """Two host threads, each on its own stream, solve different systems three
+    times each at once.  ctypes releases the GIL during the call, so the calls
+    overlap on the host; the per-device lock serialises them on the shared
+    scratch, and every answer matches the allocating solve."""
+    import threading
+
+    import torch
+    from fluidprjct_b200 import capi
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(11)
+    systems = [_poisson(O, 30, 28, 26, obstacle=True), _poisson(O, 24, 20, 18, obstacle=False)]
+    jobs = []
+    for off, cols, vals in systems:
+        b = rng.standard_normal(len(off) - 1)
+        x_ref, _, _ = capi.solve_csr_upper(off, cols, vals, b, tol=1e-12, max_iters=20000)
+        t = [torch.from_numpy(a).to(dev) for a in (off, cols, vals, np.ascontiguousarray(b, np.float64))]
+        jobs.append((t, x_ref))
+    torch.cuda.synchronize(dev)
+    results = [[] for _ in jobs]
+    errors = []
+
+    def work(j):
+        try:
+            (t_off, t_cols, t_vals, t_b), _ = jobs[j]
+            s = torch.cuda.Stream(dev)
+            for _ in range(3):
+                t_x = torch.full_like(t_b, float("nan"))
+                torch.cuda.synchronize(dev)
+                it, rr = capi.solve_csr_upper_noalloc(len(t_b), t_off.data_ptr(), t_cols.data_ptr(),
+                                                      t_vals.data_ptr(), t_b.data_ptr(), t_x.data_ptr(),
+                                                      tol=1e-12, max_iters=20000, stream=s.cuda_stream)
+                results[j].append((t_x.cpu().numpy(), rr))
+        except Exception as e:  # reported by the main thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(j,)) for j in range(len(jobs))]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join(timeout=120)
+    assert not errors and not any(th.is_alive() for th in threads)
+    for (_, x_ref), res in zip(jobs, results):
+        assert len(res) == 3
+        for x, rr in res:
+            assert rr <= 1e-12 and rel_l2(x, x_ref) <= 1e-9
