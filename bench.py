@@ -7,7 +7,7 @@ particles per cell (3,830,400 particles, octant-jittered, seed 1), zero initial
 velocity, gravity -9.81, dt = 0.002, FLIP 0.95 (PIC weight 0.05), RK2
 advection, 7-point PCG pressure solve (FP32 stencil and vectors, FP64
 reductions) to a 1e-6 relative residual.  Synthetic data; the particle state
-(2 x 61 MB float4 arrays) and the grids exceed nothing reusable across steps in
+(2 x 61 MB float4 arrays at 8 ppc) and the grids exceed nothing reusable across steps in
 L2 beyond what a real run keeps there, and the particle arrays alone are larger
 than the 126 MB L2.
 
@@ -276,7 +276,8 @@ def run_ours(args, rank, local, world):
                       "solver": solver_desc,
                       "tol": 1e-6,
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                      "l2": "inputs larger than L2 (particle arrays 2 x 61 MB + grids 58 MB per step)"},
+                      "l2": f"inputs larger than L2 (particle arrays 2 x {np_ * 16 / 1e6:.0f} MB + face grids "
+                            f"{24 * (args.n + 1) * args.n ** 2 / 1e6:.0f} MB per step)"},
            "ns_per_particle_step": round(ms_step * 1e6 / np_, 3),
            "clocks": clk, "gpu_launches": int(launches), "roofline": roofline, "phases": phases}
 
