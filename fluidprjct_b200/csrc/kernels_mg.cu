@@ -30,6 +30,7 @@
 // without restarts.  Loops over the FLUID list take several cells per thread
 // per trip with all loads issued before use, the first four cached in shared
 // memory (the solve is latency bound: the 128^3 working set lives in L2).
+#include "device_memo.hpp"
 #include "kernels.hpp"
 #include "pcg_common.cuh"
 
@@ -886,15 +887,14 @@ int mg_levels_for(int W, int H, int D, MgLevel* lv) {
 }
 
 int mg_max_blocks() {
-    static int cached = 0;
-    if (cached) return cached;
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(k_pcg_mg, cudaFuncAttributeMaxDynamicSharedMemorySize, MG_SMEM_BUDGET);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_mg, MG_THREADS, MG_SMEM_BUDGET);
-    cached = sms * std::max(1, per);
-    return cached;
+    static DeviceMemo memo;
+    return memo.get([](int dev) {
+        int sms = 0, per = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(k_pcg_mg, cudaFuncAttributeMaxDynamicSharedMemorySize, MG_SMEM_BUDGET);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg_mg, MG_THREADS, MG_SMEM_BUDGET);
+        return sms * std::max(1, per);
+    });
 }
 
 int mg_split(const MgLevel* lv, int L, int* smem_bytes) {

@@ -19,6 +19,7 @@
 // bounded software grid barrier that reports a timeout instead of hanging.
 #include <cstdio>
 
+#include "device_memo.hpp"
 #include "kernels.hpp"
 #include "pcg_common.cuh"
 #include "scan.cuh"
@@ -475,16 +476,14 @@ void launch_pressure_setup(const uint8_t* labels, const float* u, const float* v
 }
 
 int pcg_max_blocks() {
-    static int cached = 0;
-    if (cached) return cached;
-    int dev = 0, sms = 0, pf = 0, pd = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, k_pcg_cg<float>, PCG_THREADS, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd, k_pcg_cg<double>, PCG_THREADS, 0);
-    int per_sm = std::max(1, std::min(pf, pd));
-    cached = sms * per_sm;
-    return cached;
+    static DeviceMemo memo;
+    return memo.get([](int dev) {
+        int sms = 0, pf = 0, pd = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, k_pcg_cg<float>, PCG_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd, k_pcg_cg<double>, PCG_THREADS, 0);
+        return sms * std::max(1, std::min(pf, pd));
+    });
 }
 
 template <class T>

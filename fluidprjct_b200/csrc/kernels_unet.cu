@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cstdio>
 
+#include "device_memo.hpp"
 #include "unet.hpp"
 
 namespace fp {
@@ -478,15 +479,14 @@ __global__ void k_weights_bf16(const float* __restrict__ w, bf16* __restrict__ w
 }
 
 // ---------------------------------------------------------------- dispatch
-int g_sms = 0;
 int sm_count() {
-    if (!g_sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-        if (g_sms <= 0) g_sms = 148;
-    }
-    return g_sms;
+    static DeviceMemo memo;
+    const int n = memo.get([](int dev) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        return std::max(sms, 0);
+    });
+    return n > 0 ? n : 148;
 }
 
 int nbricks_of(const Lvl& lv) {
@@ -497,13 +497,13 @@ template <int CA, int CB, int COUT, int TPC>
 int run_corr(const CorrArgs& a, int nblk, cudaStream_t st) {
     constexpr int CIN = CA + CB;
     constexpr size_t smem = size_t(HALO * (CIN + 8) + BRICK * (COUT + 8)) * sizeof(bf16);
-    static bool init = false;
+    static DeviceMemo memo;
     auto kern = k_corr3<CA, CB, COUT, TPC>;
-    if (!init) {
+    memo.get([&](int) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        init = true;
-    }
+        return 1;
+    });
     kern<<<dim3(nblk, 27 / TPC), THREADS, smem, st>>>(a);
     return int(cudaPeekAtLastError());
 }

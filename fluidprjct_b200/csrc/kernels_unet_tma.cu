@@ -33,6 +33,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "device_memo.hpp"
 #include "unet.hpp"
 
 namespace fp {
@@ -400,7 +401,6 @@ __global__ void k_upcat(const bf16* __restrict__ coarse, int ca, Lvl fine, bf16*
 // ---- host side
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 std::once_flag g_encode_once;
-int g_sms = 0;
 
 PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     std::call_once(g_encode_once, [] {
@@ -441,30 +441,28 @@ template <int CIN, int COUT, int NCO, int EPI, int NST = pick_nst<CIN, NCO>(), i
 int run_tma(const bf16* in, const TmaConvArgs& a, cudaStream_t st) {
     constexpr size_t smem = smem_bytes<CIN, NCO, NST>();
     static_assert(smem <= 232448, "shared memory of one CTA");
-    static int per_sm = -1;
+    static DeviceMemo memo;
     auto kern = k_conv3_tma<CIN, COUT, NCO, EPI, NST, NSET>;
-    if (per_sm < 0) {
+    // resident CTAs on the device: shared memory (1 KB reserved per CTA),
+    // threads and the 512 TMEM columns per SM (the CTAs never wait on each
+    // other, so a grid above the true residency only queues)
+    const int resident = memo.get([&](int dev) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        int dev = 0, smem_sm = 0;
-        cudaGetDevice(&dev);
-        if (!g_sms) {
-            cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-            if (g_sms <= 0) g_sms = 148;
-        }
+        int sms = 0, smem_sm = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
         cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
         if (smem_sm <= 0) smem_sm = 233472;
-        // resident CTAs per SM: shared memory (1 KB reserved per CTA), threads and
-        // the 512 TMEM columns (the CTAs never wait on each other, so a grid above
-        // the true residency only queues)
-        per_sm = std::max(1, std::min({smem_sm / int(smem + 1024), 2048 / THREADS, 512 / tmem_cols<NCO, NSET>()}));
-    }
+        return sms * std::max(1, std::min({smem_sm / int(smem + 1024), 2048 / THREADS,
+                                           512 / tmem_cols<NCO, NSET>()}));
+    });
     CUtensorMap map;
     std::memset(&map, 0, sizeof map);
     if (!make_map(&map, in, CIN, a.lv)) return int(cudaErrorNotSupported);
     const int groups = COUT / NCO;
     const int nb = ((a.lv.W + TX - 1) / TX) * ((a.lv.H + TY - 1) / TY) * ((a.lv.D + TZ - 1) / TZ);
-    const int gx = std::max(1, std::min(nb, per_sm * g_sms / groups));
+    const int gx = std::max(1, std::min(nb, resident / groups));
     kern<<<dim3(gx, groups), THREADS, smem, st>>>(map, a);
     return int(cudaPeekAtLastError());
 }
