@@ -1264,7 +1264,10 @@ int fp_set_paddle(fp_solver* s, float x_rest, float amplitude, float period) {
 int fp_set_particles(fp_solver* s, const float* pos, const float* vel, int64_t n) {
     if (!s || n < 0 || (n > 0 && !pos)) return s ? s->fail(FP_ERR_ARG, "bad particle arrays") : FP_ERR_ARG;
     if (!s->have_grid) return s->fail(FP_ERR_STATE, "labels must be set before particles");
-    if (n >= (int64_t(1) << 31)) return s->fail(FP_ERR_ARG, "too many particles");
+    // Particle indices travel as int32 in the w lane, and the check below
+    // reports the lowest bad index into a word preset with bytes of 0x7F, so
+    // every index must stay below 0x7F7F7F7F (2,139,062,143).
+    if (n > 0x7F7F7F7FLL) return s->fail(FP_ERR_ARG, "too many particles (at most 2,139,062,143)");
     int rc = alloc_particles(s, n);
     if (rc) return rc;
     s->sorted = false;
@@ -1273,7 +1276,7 @@ int fp_set_particles(fp_solver* s, const float* pos, const float* vel, int64_t n
     float* dvel = s->d_io + 3 * n;
     cudaError_t e = cudaMemcpyAsync(dpos, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->st);
     if (e == cudaSuccess && vel) e = cudaMemcpyAsync(dvel, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s->st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_bad, 0x7F, sizeof(int), s->st);  // 0x7F7F7F7F > any index
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_bad, 0x7F, sizeof(int), s->st);  // 0x7F7F7F7F >= n > any index
     if (e != cudaSuccess) return s->cuda_fail(e, "particle upload");
     // pack into the second buffer and check every value on the device
     launch_pack(dpos, vel ? dvel : nullptr, n, s->d_pos2, s->d_vel2, s->d_bad, s->st);

@@ -223,7 +223,8 @@ int fp_set_paddle(fp_solver* s, float x_rest, float amplitude, float period);
 /* Particles: seeding of FLUID cells (seedParticles, FluidSolver3D.cu:213-297)
  * with a deterministic mt19937(seed); caller arrays; PLY files.  A
  * non-finite position or velocity is rejected with FP_ERR_ARG (checked on
- * the device); the solver then holds no particles. */
+ * the device); the solver then holds no particles.  At most 2,139,062,143
+ * particles (0x7F7F7F7F); more are rejected with FP_ERR_ARG. */
 int fp_seed_particles(fp_solver* s, int ppc, uint32_t seed);
 int fp_set_particles(fp_solver* s, const float* pos, const float* vel, int64_t n);
 int fp_load_ply(fp_solver* s, const char* path);

@@ -370,6 +370,9 @@ def test_errors_are_reported_not_thrown(tmp_path):
     with pytest.raises(capi.FluidError) as e:
         s.set_particles(bad)
     assert e.value.code == capi.FP_ERR_ARG
+    # a count above the 0x7F7F7F7F index limit is refused before the arrays are read
+    one = np.zeros((1, 3), np.float32)
+    assert capi.lib().fp_set_particles(s._h, capi.ptr(one), None, 0x7F7F7F7F + 1) == capi.FP_ERR_ARG
     with pytest.raises(capi.FluidError) as e:
         s.load_labels(tmp_path / "nope.txt")
     assert e.value.code == capi.FP_ERR_IO
