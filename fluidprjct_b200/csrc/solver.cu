@@ -292,6 +292,9 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     ck(cudaMemsetAsync(pb.invd, 0, pbytes, s->st));
     ck(cudaMemsetAsync(pb.xd, 0, sizeof(double) * size_t(s->padded), s->st));
     ck(cudaMemsetAsync(pb.bar, 0, sizeof(GridBar), s->st));
+    // No FLUID list until the first pressure set-up: the count starts at 0, so
+    // FP_GRID_RHS read before any step densifies nothing (an all-zero grid).
+    ck(cudaMemsetAsync(pb.nf, 0, sizeof(int), s->st));
     if (e != cudaSuccess) { free_grid(s); return s->cuda_fail(e, "grid initialisation"); }
     s->have_grid = true;
     s->sorted = false;

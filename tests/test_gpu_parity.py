@@ -366,6 +366,8 @@ def test_errors_are_reported_not_thrown(tmp_path):
     lab = np.zeros((4, 4, 4), np.uint8)
     lab[1:3, 1:3, 1:3] = 2
     s.set_labels(lab)
+    # before any step there is no FLUID list: the right-hand side reads as zeros
+    assert not s.grid(capi.GRID_RHS).any()
     bad = np.array([[0.1, np.nan, 0.1]], np.float32)
     with pytest.raises(capi.FluidError) as e:
         s.set_particles(bad)
