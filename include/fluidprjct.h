@@ -14,6 +14,9 @@
  *   - One solver per host thread; each solver owns one CUDA stream and all of
  *     its device memory.  Buffers passed in or out are host memory owned by
  *     the caller and are copied.
+ *   - fp_create makes fp_config.device current on the calling thread, which
+ *     then makes the solver's calls.  A process may drive solvers on several
+ *     GPUs at once, one thread each; launch set-up is kept per device.
  *   - Grids use the reference's layouts: cell (i,j,k) at i + j*W + k*W*H;
  *     u is (W+1) x H x D, v is W x (H+1) x D, w is W x H x (D+1), each with
  *     i fastest.  Labels: FP_SOLID 0, FP_FLUID 1, FP_AIR 2, FP_BODY 3
