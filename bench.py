@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--solver", default="pcg_mg", choices=["pcg", "pcg_mixed", "pcg_mg", "pcg_learned"],
                     help="pressure solver of the timed steps")
+    ap.add_argument("--no-parity", action="store_true", help="skip the parity leg against the FP64 oracle")
+    ap.add_argument("--no-extra", action="store_true", help="skip the 200-step run and the 16 ppc variant")
     return ap.parse_args()
 
 
@@ -159,6 +161,15 @@ def event_timer(stream_ptr):
     return st, (lambda: torch.cuda.Event(enable_timing=True))
 
 
+def step_bytes(np_, nc, nf, iters, outer=1):
+    """Algorithmic HBM bytes of one whole step (FP32 values, uint8 labels,
+    each array read or written once per phase): label 12 Np + 2 Nc, P2G
+    24 Np + 24 Nc, RHS 17 Nc, PCG 41 Nf per iteration + 17 Nf per outer
+    refinement, projection 29 Nc, G2P + advection 48 Np + 24 Nc; in all
+    84 Np + 96 Nc + 41 Nf iters + 17 Nf outer."""
+    return 84.0 * np_ + 96.0 * nc + 41.0 * nf * iters + 17.0 * nf * outer
+
+
 def algorithmic_bytes(np_, nc, nf):
     """Per-phase algorithmic HBM bytes (FP32 values, uint8 labels; each array
     read or written once per phase)."""
@@ -248,17 +259,29 @@ def run_ours(args, rank, local, world):
     phase_ms = {k: statistics.mean(p[k] for p in per) for k in ("t_label", "t_p2g", "t_pressure", "t_project",
                                                                  "t_advect", "t_total")}
     ab = algorithmic_bytes(np_, nc, nf)
+    def bw(key, ms):
+        g = ab[key] / ms / 1e6
+        return {"ms": round(ms, 4), "gbs": round(g, 1), "frac": round(g / peak, 4)}
     phases = {
-        "label": {"ms": phase_ms["t_label"], "gbs": ab["label"] / phase_ms["t_label"] / 1e6},
-        "p2g+save+forces": {"ms": phase_ms["t_p2g"], "gbs": ab["p2g"] / phase_ms["t_p2g"] / 1e6},
+        "label": bw("label", phase_ms["t_label"]),
+        "p2g+save+forces": dict(bw("p2g", phase_ms["t_p2g"]), kernel="k_p2g"),
         "pressure": {"ms": phase_ms["t_pressure"], "solve_ms": statistics.mean(solve_ms),
                      "learned_ms": statistics.mean(p["t_learned"] for p in per), "iters": statistics.mean(iters)},
-        "project": {"ms": phase_ms["t_project"], "gbs": ab["project"] / phase_ms["t_project"] / 1e6},
-        "g2p+advect": {"ms": phase_ms["t_advect"], "gbs": ab["g2p_advect"] / phase_ms["t_advect"] / 1e6},
+        "project": dict(bw("project", phase_ms["t_project"]), kernel="k_project"),
+        "g2p+advect": dict(bw("g2p_advect", phase_ms["t_advect"]), kernel="k_g2p_advect"),
     }
+    sb = statistics.mean(step_bytes(np_, nc, p["num_fluid_cells"], p["pcg_iters"], p["outer_iters"]) for p in per)
+    step_gbs = sb / (ms_step / 1000.0) / 1e9
+    # DRAM traffic of one captured launch, per iteration of that launch, times
+    # the timed solves' mean iterations: the same unit as the algorithmic bytes
+    t_launch = (traffic or {}).get(kernel + "_bytes_per_launch")
+    t_iters = (traffic or {}).get(kernel + "_iters")
+    traffic_launch = (t_launch / t_iters * statistics.mean(iters)) if (t_launch and t_iters) else t_launch
     roofline = {"kernel": kernel + " (persistent cooperative solver)", "bound": "hbm", "achieved": round(solve_gbs, 1),
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(solve_gbs / peak, 4),
-                "traffic": (traffic or {}).get(kernel + "_bytes_per_launch"),
+                "traffic": round(traffic_launch) if traffic_launch else None,
+                "traffic_note": (f"ncu DRAM bytes of one {t_iters}-iteration launch, scaled per iteration to the "
+                                 f"timed solves' {statistics.mean(iters):.2f} iterations") if t_iters else None,
                 "algorithmic_bytes_per_launch": statistics.mean(solve_bytes), "note": note}
     solver_desc = {
         "pcg": "plain PCG (Jacobi, FP64 vectors)",
@@ -279,7 +302,10 @@ def run_ours(args, rank, local, world):
                       "l2": f"inputs larger than L2 (particle arrays 2 x {np_ * 16 / 1e6:.0f} MB + face grids "
                             f"{24 * (args.n + 1) * args.n ** 2 / 1e6:.0f} MB per step)"},
            "ns_per_particle_step": round(ms_step * 1e6 / np_, 3),
-           "clocks": clk, "gpu_launches": int(launches), "roofline": roofline, "phases": phases}
+           "clocks": clk, "gpu_launches": int(launches), "roofline": roofline, "phases": phases,
+           "roofline_step": {"bound": "hbm", "algorithmic_bytes": round(sb), "achieved": round(step_gbs, 1),
+                             "peak": peak, "unit": "GB/s", "frac": round(step_gbs / peak, 4),
+                             "note": "84 Np + 96 Nc + 41 Nf iters + 17 Nf outer bytes per step over ms_per_step"}}
 
     # ---- PCG time-to-1e-6 of each solver on the same scene, all from x = 0 (the
     # learned one from its network guess), and MG warm-started as in the step ----
@@ -333,6 +359,16 @@ def run_ours(args, rank, local, world):
                       "h2d_bytes_per_step": int(np_ * 24), "d2h_bytes_per_step": int(np_ * 24), "steps": k,
                       "path": "fp_set_particles(pinned host pos, vel) + fp_step + fp_get_particles"}
 
+    # ---- the configuration's whole run (200 steps from the seeded state) and
+    # the 16 ppc variant (7.66 M particles, the configuration's "~8 M") ----
+    if not args.no_extra and rank == 0:
+        out["run_200_steps"] = timed_run(lab, local, args, 200, 0, args.ppc)
+        out["ppc16"] = timed_run(lab, local, args, 20, 5, 16)
+
+    # ---- parity of the timed scene against the FP64 oracle (rank 0, N = 1) ----
+    if not args.no_parity and rank == 0 and world == 1:
+        out["parity"] = parity_leg(lab, local, args)
+
     # ---- frame output of fp_run (optional) ----
     if args.frames > 0 and rank == 0:
         out["frame_output"] = frame_output(s, args.frames)
@@ -348,6 +384,54 @@ def run_ours(args, rank, local, world):
     s.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def timed_run(lab, device, args, steps, warmup, ppc):
+    """Device time of `steps` consecutive steps of a fresh solver (after
+    `warmup` steps), on the solver's stream."""
+    s = new_solver(lab, device, args.solver, args.n, ppc)
+    stream, Ev = event_timer(s.stream)
+    if warmup:
+        s.step(warmup)
+    e0, e1 = Ev(), Ev()
+    e0.record(stream)
+    s.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = s.stats()
+    n = s.num_particles
+    s.close()
+    return {"steps": steps, "warmup": warmup, "ppc": ppc, "particles": int(n), "ms": round(ms, 3),
+            "steps_per_s": round(steps / (ms / 1000.0), 2), "ns_per_particle_step": round(ms * 1e6 / steps / n, 4),
+            "last_step_pcg_iters": st["pcg_iters"], "last_step_residual": st["residual"]}
+
+
+def parity_leg(lab, device, args):
+    """The timed configuration against the FP64 oracle (oracle/parity.py):
+    step 1 from the seeded state as a whole step (each side its own solver:
+    the GPU's MG-PCG to 1e-6, the oracle's FP64 Jacobi PCG to 1e-12), then
+    step 2 phase by phase from identical inputs."""
+    from oracle import oracle as O
+    from oracle import parity
+    n = args.n
+    s = new_solver(lab, device, args.solver, n, args.ppc)
+    o = O.Sim3(n, n, n, 1.0 / n, DT, fp64=True, pic_weight=PIC, tol=1e-12, rk2=True)
+    o.set_labels(lab)
+    o.set_particles(*s.particles())
+    whole = parity.full_step(s, o)
+    o.set_particles(*s.particles())
+    ph = parity.step_phases(s, o, 1.0 / n)
+    s.close()
+    o.close()
+    r = lambda x: float(f"{x:.3e}")
+    return {"labels_bitexact": whole["labels_bitexact"] and ph["labels_bitexact"],
+            "u_rel_l2": r(whole["u_rel_l2"]), "v_rel_l2": r(whole["v_rel_l2"]), "w_rel_l2": r(whole["w_rel_l2"]),
+            "p_rel_l2": r(whole["p_rel_l2"]), "vel_rel_l2": r(whole["vel_rel_l2"]),
+            "pos_rel_l2": r(whole["pos_rel_l2"]),
+            "what": "step 1 of the timed scene (GPU MG-PCG to 1e-6) against the oracle's FP64 step (FP64 Jacobi PCG "
+                    "to 1e-12); relative L2 over whole arrays",
+            "step2_phases": {k: (r(v) if isinstance(v, float) else v) for k, v in ph.items()}}
 
 
 def frame_output(s, frames):

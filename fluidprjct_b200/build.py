@@ -1,4 +1,6 @@
-"""Build the native library ``fluidprjct_b200/_lib/libfluidprjct_b200.so``.
+"""Build the native library ``fluidprjct_b200/_lib/libfluidprjct_b200.so`` and
+the ``FluidGPU`` driver executable beside it (``_lib/FluidGPU``, the reference's
+``main.cpp`` over the C ABI, linked to the library with an ``$ORIGIN`` rpath).
 
 Every CUDA source is compiled for sm_100a only
 (``-gencode arch=compute_100a,code=sm_100a``) with IEEE division and square
@@ -16,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libfluidprjct_b200.so")
+DRIVER = os.path.join(LIBDIR, "FluidGPU")
 BUILD = os.path.join(HERE, "_build")
 
 SOURCES = [
@@ -78,6 +81,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if force or _stale(LIB, objs):
         cmd = [nvcc, "-ccbin", _host_cxx(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-ldl",
                "-lpthread"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    main = os.path.join(CSRC, "fluidgpu_main.cpp")
+    header = os.path.join(HERE, "..", "include", "fluidprjct.h")
+    if force or _stale(DRIVER, [main, header, LIB]):
+        cmd = [_host_cxx(), "-O2", "-std=c++17", "-Wall", main, "-o", DRIVER, "-L" + LIBDIR, "-lfluidprjct_b200",
+               "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -21,6 +21,7 @@ SOLVER_PCG, SOLVER_PCG_MIXED, SOLVER_PCG_MG, SOLVER_PCG_LEARNED = 0, 1, 2, 3
 ADVECT_RK3REF, ADVECT_RK2 = 0, 1
 SCHEME_DEFAULT, SCHEME_REF2D = 0, 1
 BODY_FORCES_FACE_FRACTION, BODY_FORCES_REFERENCE = 0, 1
+COLLISION_LABELS, COLLISION_SDF = 0, 1
 GRID_U, GRID_V, GRID_W, GRID_U_SAVED, GRID_V_SAVED, GRID_W_SAVED, GRID_P, GRID_RHS = range(8)
 (PHASE_LABEL, PHASE_P2G, PHASE_SAVE, PHASE_FORCES, PHASE_PRESSURE, PHASE_PROJECT, PHASE_BODY, PHASE_G2P,
  PHASE_ADVECT, PHASE_CLEANUP) = range(10)
@@ -39,6 +40,8 @@ class FpConfig(C.Structure):
         ("device", C.c_int), ("scheme", C.c_int), ("extrapolate", C.c_int), ("body_forces", C.c_int),
         ("mg_sweeps", C.c_int),
         ("warm_start", C.c_int),
+        ("collision", C.c_int),
+        ("body_sdf", C.c_char * 256),
     ]
 
 
@@ -122,6 +125,7 @@ _SIGS = {
     "fp_set_body_state": (C.c_int, [_P, _P, _P, _P]),
     "fp_stats": (C.c_int, [_P, _P]),
     "fp_cuda_stream": (C.c_void_p, [_P]),
+    "fp_set_wait_limit": (C.c_int, [_P, C.c_int64]),
     "fp_pressure_solve": (C.c_int, [_P, _P, _P, C.c_int64, _P, _P]),
     "fp_solve_csr_upper": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, C.c_double, C.c_int, _P, _P]),
     "fp_solve_csr_upper_noalloc": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, C.c_double, C.c_int, _P, _P, _P]),
@@ -169,8 +173,8 @@ def default_config(**kw) -> FpConfig:
     cfg = FpConfig()
     lib().fp_config_default(C.byref(cfg))
     for k, v in kw.items():
-        if k == "output_template":
-            cfg.output_template = v.encode()
+        if k in ("output_template", "body_sdf"):
+            setattr(cfg, k, v.encode())
         elif k == "body_pos":
             cfg.body_pos[:] = list(v)
         elif k == "solver" and isinstance(v, str):
@@ -179,6 +183,8 @@ def default_config(**kw) -> FpConfig:
             cfg.advection = {"rk3ref": ADVECT_RK3REF, "rk2": ADVECT_RK2}[v]
         elif k == "scheme" and isinstance(v, str):
             cfg.scheme = {"default": SCHEME_DEFAULT, "ref2d": SCHEME_REF2D}[v]
+        elif k == "collision" and isinstance(v, str):
+            cfg.collision = {"labels": COLLISION_LABELS, "sdf": COLLISION_SDF}[v]
         elif k == "body_forces" and isinstance(v, str):
             cfg.body_forces = {"face_fraction": BODY_FORCES_FACE_FRACTION, "reference": BODY_FORCES_REFERENCE}[v]
         else:
@@ -337,6 +343,11 @@ class Solver:
     def stream(self) -> int:
         """The solver's cudaStream_t as an integer handle."""
         return lib().fp_cuda_stream(self._h) or 0
+
+    def set_wait_limit(self, polls: int):
+        """Polls after which a grid-barrier wait of the pressure solvers gives
+        up (FP_ERR_TIMEOUT); 0 restores the default."""
+        return self._check(lib().fp_set_wait_limit(self._h, int(polls)))
 
     def stats(self) -> dict:
         st = FpStepStats()

@@ -143,6 +143,87 @@ struct BodyShape {
     const float* sdf;    // device SDF values, i fastest
 };
 
+// Voxel of the SDF grid that holds world point x (nearest-lower voxel in body
+// coordinates: local = R^T (x - pos) + local_com, voxel (local - origin) /
+// cell); false outside the SDF box.
+__device__ __forceinline__ bool body_voxel(const BodyShape& b, float3 x, int& i, int& j, int& k) {
+    const float3 d = make_float3(x.x - b.com.x, x.y - b.com.y, x.z - b.com.z);
+    const float lx = b.rot[0] * d.x + b.rot[3] * d.y + b.rot[6] * d.z + b.local_com.x;
+    const float ly = b.rot[1] * d.x + b.rot[4] * d.y + b.rot[7] * d.z + b.local_com.y;
+    const float lz = b.rot[2] * d.x + b.rot[5] * d.y + b.rot[8] * d.z + b.local_com.z;
+    const float sx = (lx - b.origin.x) / b.cell, sy = (ly - b.origin.y) / b.cell, sz = (lz - b.origin.z) / b.cell;
+    if (sx < 0.0f || sx >= float(b.nx) || sy < 0.0f || sy >= float(b.ny) || sz < 0.0f || sz >= float(b.nz))
+        return false;
+    i = min(int(sx), b.nx - 1); j = min(int(sy), b.ny - 1); k = min(int(sz), b.nz - 1);
+    return true;
+}
+
+// Signed distance of world point x to the body (negative inside): the
+// analytic sphere |x - c| - r, the paddle's x - x_p, or the voxel SDF
+// (Utility::contains, utility.cu:163-206; 1e30 outside its box).  The sphere
+// is explicitly rounded (no contraction) so BODY marks match a CPU
+// evaluation bit for bit.
+__device__ __forceinline__ float body_sdf(const BodyShape& b, float3 x) {
+    const float3 d = make_float3(x.x - b.com.x, x.y - b.com.y, x.z - b.com.z);
+    if (b.kind == BODY_SPHERE)
+        return sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(d.x, d.x), __fmul_rn(d.y, d.y)), __fmul_rn(d.z, d.z))) - b.radius;
+    if (b.kind == BODY_PADDLE) return d.x;  // signed distance to the paddle face x = com.x
+    int i, j, k;
+    if (!body_voxel(b, x, i, j, k)) return 1e30f;
+    return __ldg(b.sdf + i + j * b.nx + k * b.nx * b.ny);
+}
+
+// SDF collision projection: a point with phi(x) < eps is moved along the
+// outward normal to phi = eps.  Sphere: radially to r + eps from the centre
+// (straight up if it sits at the centre); paddle: to x_p + eps; voxel SDF:
+// x += (eps - phi) n with n the normalised central-difference gradient of the
+// voxel values, rotated into the world, repeated up to four times because
+// the nearest-voxel SDF is piecewise constant.  Returns false if the point
+// was inside and could not be moved (a voxel with zero gradient).
+__device__ __forceinline__ bool sdf_push_out(const BodyShape& b, float3& x, float eps) {
+    if (b.kind == BODY_SPHERE) {
+        const float3 d = make_float3(__fsub_rn(x.x, b.com.x), __fsub_rn(x.y, b.com.y), __fsub_rn(x.z, b.com.z));
+        const float r = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(d.x, d.x), __fmul_rn(d.y, d.y)), __fmul_rn(d.z, d.z)));
+        const float target = __fadd_rn(b.radius, eps);
+        if (!(__fsub_rn(r, b.radius) < eps)) return true;
+        if (r > 0.0f) {
+            const float sc = __fdiv_rn(target, r);
+            x = make_float3(__fadd_rn(b.com.x, __fmul_rn(d.x, sc)), __fadd_rn(b.com.y, __fmul_rn(d.y, sc)),
+                            __fadd_rn(b.com.z, __fmul_rn(d.z, sc)));
+        } else {
+            x = make_float3(b.com.x, __fadd_rn(b.com.y, target), b.com.z);
+        }
+        return true;
+    }
+    if (b.kind == BODY_PADDLE) {
+        if (__fsub_rn(x.x, b.com.x) < eps) x.x = __fadd_rn(b.com.x, eps);
+        return true;
+    }
+    for (int it = 0; it < 4; ++it) {
+        int i, j, k;
+        if (!body_voxel(b, x, i, j, k)) return true;
+        const float* s = b.sdf;
+        const int sx = 1, sy = b.nx, sz = b.nx * b.ny;
+        const int c = i + j * sy + k * sz;
+        const float phi = __ldg(s + c);
+        if (!(phi < eps)) return true;
+        // central differences (one-sided at the box faces), in voxel units
+        const int i0 = max(i - 1, 0), i1 = min(i + 1, b.nx - 1), j0 = max(j - 1, 0), j1 = min(j + 1, b.ny - 1),
+                  k0 = max(k - 1, 0), k1 = min(k + 1, b.nz - 1);
+        const float gx = i1 > i0 ? (__ldg(s + c + (i1 - i) * sx) - __ldg(s + c + (i0 - i) * sx)) / float(i1 - i0) : 0.0f;
+        const float gy = j1 > j0 ? (__ldg(s + c + (j1 - j) * sy) - __ldg(s + c + (j0 - j) * sy)) / float(j1 - j0) : 0.0f;
+        const float gz = k1 > k0 ? (__ldg(s + c + (k1 - k) * sz) - __ldg(s + c + (k0 - k) * sz)) / float(k1 - k0) : 0.0f;
+        const float gn = sqrtf(gx * gx + gy * gy + gz * gz);
+        if (!(gn > 0.0f)) return false;
+        const float lx = gx / gn, ly = gy / gn, lz = gz / gn;  // local normal
+        const float step = eps - phi;
+        x.x += step * (b.rot[0] * lx + b.rot[1] * ly + b.rot[2] * lz);
+        x.y += step * (b.rot[3] * lx + b.rot[4] * ly + b.rot[5] * lz);
+        x.z += step * (b.rot[6] * lx + b.rot[7] * ly + b.rot[8] * lz);
+    }
+    return true;
+}
+
 // Labels with out-of-domain cells reading as SOLID.
 __device__ __forceinline__ uint8_t label_at(const uint8_t* __restrict__ lab, const Dims& g, int i, int j, int k) {
     if (i < 0 || i >= g.W || j < 0 || j >= g.H || k < 0 || k >= g.D) return SOLID;
@@ -151,5 +232,16 @@ __device__ __forceinline__ uint8_t label_at(const uint8_t* __restrict__ lab, con
 
 // Device status word written by kernels that can fail without trapping.
 enum : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_NAN = 2, DEV_BREAKDOWN = 3, DEV_MAXIT = 4 };
+
+// True when the pressure solve whose status word is *status failed in a way
+// that makes the step return an error (a grid barrier gave up, or NaN).  The
+// kernels queued after the solve then leave the face velocities and the
+// particles as they are, so a failed step changes no particle.  A null
+// pointer means "no guard".
+__device__ __forceinline__ bool solve_failed(const int* status) {
+    if (!status) return false;
+    const int s = *status;
+    return s == DEV_TIMEOUT || s == DEV_NAN;
+}
 
 }  // namespace fp

@@ -422,6 +422,7 @@ bool load_config_json(const std::string& path, fp_config& cfg, std::string* labe
         std::snprintf(cfg.output_template, sizeof cfg.output_template, "%s", s.c_str());
     }
     if (label_path && strv("inputLabelData", s)) *label_path = s;
+    if (strv("body_sdf", s)) std::snprintf(cfg.body_sdf, sizeof cfg.body_sdf, "%s", s.c_str());
     if (frames) num("frameAmount", *frames);
     num("activeBody", cfg.active_body);
     num("body_x", cfg.body_pos[0]);
@@ -444,6 +445,11 @@ bool load_config_json(const std::string& path, fp_config& cfg, std::string* labe
         else if (s == "pcg_mg") cfg.solver = FP_SOLVER_PCG_MG;
         else if (s == "pcg_learned") cfg.solver = FP_SOLVER_PCG_LEARNED;
         else { err = "unknown solver " + s; return false; }
+    }
+    if (strv("collision", s)) {
+        if (s == "labels") cfg.collision = FP_COLLISION_LABELS;
+        else if (s == "sdf") cfg.collision = FP_COLLISION_SDF;
+        else { err = "unknown collision " + s; return false; }
     }
     if (strv("advection", s)) {
         if (s == "rk3ref") cfg.advection = FP_ADVECT_RK3REF;

@@ -14,6 +14,10 @@ struct GridBar {
     unsigned gen;
 };
 
+// Polls after which a grid-barrier wait of the persistent solvers gives up
+// and reports DEV_TIMEOUT (fp_set_wait_limit lowers it for tests).
+constexpr long long kDefaultWaitPolls = 1ll << 27;
+
 struct PcgOut {
     int iters;
     int status;     // DEV_*
@@ -87,7 +91,7 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStrea
 // ||rhs||^2 (FP64) to pb.red.
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
                   const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0 = nullptr, int nu0 = 2,
-                  const float* pprev = nullptr, float* pout = nullptr);
+                  const float* pprev = nullptr, float* pout = nullptr, long long wait_polls = kDefaultWaitPolls);
 
 // -------- labelling and the particle sort (kernels_sort.cu) --------
 // counts[nc] must be zero on entry.  Writes key/rank per particle.
@@ -116,7 +120,8 @@ void launch_pressure_setup(const uint8_t* labels, const float* u, const float* v
 // FP64 (fp64 = 1) or FP32 (0), reductions always FP64.  Solution in pb.X,
 // diagnostics in pb.out.  The padded work grids must be zero on entry;
 // launch_pcg_clear restores that after a solve.
-int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, int fp64, double tol, int maxit, cudaStream_t st);
+int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, int fp64, double tol, int maxit, cudaStream_t st,
+               long long wait_polls = kDefaultWaitPolls);
 void launch_pcg_clear(PressureBufs& pb, int fp64, int with_invd, cudaStream_t st);
 int pcg_max_blocks();
 // p[cell] = X[n] (src 0: FP32 X, 1: FP64 X, 2: x64).
@@ -129,13 +134,18 @@ void launch_ir_residual(PressureBufs& pb, Dims g, cudaStream_t st);
 void launch_ir_update(PressureBufs& pb, Dims g, cudaStream_t st);
 
 // -------- projection (kernels_pressure.cu) --------
+// guard: the status word of the solve that produced p, or null; the kernel
+// does nothing when that solve failed (solve_failed).
 void launch_project(float* u, float* v, float* w, const float* p, const uint8_t* labels, Dims g, float dt, BodyKin b,
-                    cudaStream_t st);
+                    cudaStream_t st, const int* guard = nullptr);
 
 // -------- G2P + advection (kernels_advect.cu) --------
 void launch_g2p_advect(float4* pos, float4* vel, int64_t np, const float* u, const float* v, const float* w,
                        const float* us, const float* vs, const float* ws, const uint8_t* labels, Dims g, float alpha,
-                       float dt, float cfl, int do_g2p, int do_advect, int rk2, cudaStream_t st);
+                       float dt, float cfl, int do_g2p, int do_advect, int rk2, cudaStream_t st,
+                       const int* guard = nullptr, const BodyShape* collide = nullptr);
+// collide: the body for SDF collision projection (sdf_push_out, eps = dx/4),
+// or null for the reference's label search alone.
 
 // -------- rigid body (kernels_body.cu) --------
 // mark[c] = 1 where the cell centre is inside the body (SDF <= 0).

@@ -12,6 +12,10 @@
 //        [0, (N-1)*dx]; a particle that lands in SOLID/BODY is nudged half a
 //        cell toward the nearest FLUID cell centre among 34 offsets
 //        (projectParticleDevice3D, :1161-1239); at most 1000 substeps.
+//        With SDF collision (fp_config.collision) a particle whose body SDF
+//        is below eps = 0.25 dx is first projected along the SDF normal to
+//        phi = eps (sdf_push_out), and the label search is kept for SOLID
+//        cells only.
 #include "kernels.hpp"
 
 namespace fp {
@@ -56,9 +60,10 @@ __global__ void __launch_bounds__(256) k_g2p_advect(float4* __restrict__ pos, fl
                                                     const float* __restrict__ w, const float* __restrict__ us,
                                                     const float* __restrict__ vs, const float* __restrict__ ws,
                                                     const uint8_t* __restrict__ lab, Dims g, float alpha, float dt,
-                                                    float C, int do_g2p, int do_advect, int rk2) {
+                                                    float C, int do_g2p, int do_advect, int rk2,
+                                                    const int* __restrict__ guard, BodyShape body, int sdf_collide) {
     const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (q >= np) return;
+    if (q >= np || solve_failed(guard)) return;
     const float4 P = pos[q];
     float3 p = make_float3(P.x, P.y, P.z);
     const float dx = g.dx;
@@ -107,10 +112,16 @@ __global__ void __launch_bounds__(256) k_g2p_advect(float4* __restrict__ pos, fl
         p.x = fminf(fmaxf(p.x, 0.0f), xmax);
         p.y = fminf(fmaxf(p.y, 0.0f), ymax);
         p.z = fminf(fmaxf(p.z, 0.0f), zmax);
+        if (sdf_collide) {
+            if (!sdf_push_out(body, p, __fmul_rn(0.25f, dx))) break;
+            p.x = fminf(fmaxf(p.x, 0.0f), xmax);
+            p.y = fminf(fmaxf(p.y, 0.0f), ymax);
+            p.z = fminf(fmaxf(p.z, 0.0f), zmax);
+        }
         const int cx = int(floorf(p.x / dx)), cy = int(floorf(p.y / dx)), cz = int(floorf(p.z / dx));
         if (cx >= 0 && cx < g.W && cy >= 0 && cy < g.H && cz >= 0 && cz < g.D) {
             const uint8_t l = __ldg(lab + cx + cy * g.W + cz * g.W * g.H);
-            if (l == SOLID || l == BODY) {
+            if (l == SOLID || (l == BODY && !sdf_collide)) {
                 if (!project_particle(p, lab, g)) break;
             }
         }
@@ -158,10 +169,13 @@ __global__ void k_pack(const float* __restrict__ pos, const float* __restrict__ 
 
 void launch_g2p_advect(float4* pos, float4* vel, int64_t np, const float* u, const float* v, const float* w,
                        const float* us, const float* vs, const float* ws, const uint8_t* labels, Dims g, float alpha,
-                       float dt, float cfl, int do_g2p, int do_advect, int rk2, cudaStream_t st) {
+                       float dt, float cfl, int do_g2p, int do_advect, int rk2, cudaStream_t st, const int* guard,
+                       const BodyShape* collide) {
     if (np == 0) return;
+    BodyShape b{};
+    if (collide) b = *collide;
     k_g2p_advect<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, u, v, w, us, vs, ws, labels, g, alpha, dt,
-                                                             cfl, do_g2p, do_advect, rk2);
+                                                             cfl, do_g2p, do_advect, rk2, guard, b, collide ? 1 : 0);
 }
 
 void launch_unsort(const float4* pos, const float4* vel, int64_t np, float* pos_out, float* vel_out, cudaStream_t st) {

@@ -24,28 +24,12 @@ namespace fp {
 
 namespace {
 
-__device__ __forceinline__ float sdf_at(const BodyShape& b, float3 x) {
-    const float3 d = make_float3(x.x - b.com.x, x.y - b.com.y, x.z - b.com.z);
-    // Explicitly rounded (no contraction) so BODY marks match a CPU evaluation bit for bit.
-    if (b.kind == BODY_SPHERE)
-        return sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(d.x, d.x), __fmul_rn(d.y, d.y)), __fmul_rn(d.z, d.z))) - b.radius;
-    if (b.kind == BODY_PADDLE) return d.x;  // signed distance to the paddle face x = com.x
-    // Voxel SDF: local = R^T (x - pos) + local_com; coordinate (local - origin)/cell.
-    const float lx = b.rot[0] * d.x + b.rot[3] * d.y + b.rot[6] * d.z + b.local_com.x;
-    const float ly = b.rot[1] * d.x + b.rot[4] * d.y + b.rot[7] * d.z + b.local_com.y;
-    const float lz = b.rot[2] * d.x + b.rot[5] * d.y + b.rot[8] * d.z + b.local_com.z;
-    const float sx = (lx - b.origin.x) / b.cell, sy = (ly - b.origin.y) / b.cell, sz = (lz - b.origin.z) / b.cell;
-    if (sx < 0.0f || sx >= float(b.nx) || sy < 0.0f || sy >= float(b.ny) || sz < 0.0f || sz >= float(b.nz)) return 1e30f;
-    const int i = min(int(sx), b.nx - 1), j = min(int(sy), b.ny - 1), k = min(int(sz), b.nz - 1);
-    return __ldg(b.sdf + i + j * b.nx + k * b.nx * b.ny);
-}
-
 __global__ void k_mark_body(uint8_t* __restrict__ mark, Dims g, BodyShape b) {
     const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c >= g.nc()) return;
     const int i = int(c % g.W), j = int((c / g.W) % g.H), k = int(c / (int64_t(g.W) * g.H));
     const float3 x = make_float3((float(i) + 0.5f) * g.dx, (float(j) + 0.5f) * g.dx, (float(k) + 0.5f) * g.dx);
-    mark[c] = sdf_at(b, x) <= 0.0f ? 1 : 0;
+    mark[c] = body_sdf(b, x) <= 0.0f ? 1 : 0;
 }
 
 // Pressure with BODY cells extended by the mean of their FLUID/AIR neighbours
@@ -87,7 +71,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_body_force(const float* __res
             const float3 xf = make_float3(ax == 0 ? float(i) * dx : (float(i) + 0.5f) * dx,
                                           ax == 1 ? float(j) * dx : (float(j) + 0.5f) * dx,
                                           ax == 2 ? float(k) * dx : (float(k) + 0.5f) * dx);
-            const float theta = clamp01(0.5f - sdf_at(b, xf) / dx);
+            const float theta = clamp01(0.5f - body_sdf(b, xf) / dx);
             if (theta <= 0.0f) continue;
             float pl, pr;
             const int li = i - (ax == 0), lj = j - (ax == 1), lk = k - (ax == 2);

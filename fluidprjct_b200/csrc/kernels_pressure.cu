@@ -166,6 +166,7 @@ struct PcgArgs {
     PcgOut* out;
     double tol;
     int maxit;
+    long long wait_polls;  // grid-barrier poll limit
 };
 
 // Jacobi-preconditioned conjugate gradients in the Chronopoulos-Gear form
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
         a.P[n] = T(0);
         a.X[n] = T(0);
     }
-    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+    if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
     // Init 2: u0 = M^-1 r0, w0 = A u0; partials (r,u), (w,u), (r,r).
     {
         double g_l = 0.0, d_l = 0.0, rr_l = 0.0;
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
         double* pp = a.part + 3 * nb;  // parity 1
         if (threadIdx.x == 0) { pp[blockIdx.x] = bs.x; pp[nb + blockIdx.x] = bs.y; pp[2 * nb + blockIdx.x] = bs.z; }
     }
-    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+    if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
     double3 tot = grid_sum3(a.part + 3 * nb, nb);
     double gam = tot.x, del = tot.y, rr = tot.z;
     const double bb = tot.z;
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
         double3 bs = block_sum3(g_l, d_l, rr_l);
         double* pp = a.part + (it & 1) * 3 * nb;
         if (threadIdx.x == 0) { pp[blockIdx.x] = bs.x; pp[nb + blockIdx.x] = bs.y; pp[2 * nb + blockIdx.x] = bs.z; }
-        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
+        if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
         tot = grid_sum3(pp, nb);
         ++it;
         if (isnan(tot.x) || isnan(tot.y) || isnan(tot.z)) { st = DEV_NAN; rr = tot.z; break; }
@@ -392,7 +393,8 @@ __device__ __forceinline__ float p_at(const float* __restrict__ p, const Dims& g
 
 __global__ void k_project(float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
                           const float* __restrict__ p, const uint8_t* __restrict__ lab, Dims g, float scale, float inv,
-                          BodyKin body) {
+                          BodyKin body, const int* __restrict__ guard) {
+    if (solve_failed(guard)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -487,7 +489,8 @@ int pcg_max_blocks() {
 }
 
 template <class T>
-static int launch_pcg_t(Dims g, PressureBufs& pb, const float* rhs, double tol, int maxit, cudaStream_t st) {
+static int launch_pcg_t(Dims g, PressureBufs& pb, const float* rhs, double tol, int maxit, cudaStream_t st,
+                        long long wait_polls) {
     const int nb = pcg_max_blocks();
     int* status = &pb.out->status;
     k_reset_pcg<<<1, 1, 0, st>>>(pb.bar, status);
@@ -503,13 +506,16 @@ static int launch_pcg_t(Dims g, PressureBufs& pb, const float* rhs, double tol, 
     a.X = static_cast<T*>(pb.X);
     a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;
     a.tol = tol; a.maxit = maxit;
+    a.wait_polls = wait_polls;
     void* args[] = {&a};
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_cg<T>, dim3(nb), dim3(PCG_THREADS), args, 0, st);
     return e == cudaSuccess ? 0 : int(e);
 }
 
-int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, int fp64, double tol, int maxit, cudaStream_t st) {
-    return fp64 ? launch_pcg_t<double>(g, pb, rhs, tol, maxit, st) : launch_pcg_t<float>(g, pb, rhs, tol, maxit, st);
+int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, int fp64, double tol, int maxit, cudaStream_t st,
+               long long wait_polls) {
+    return fp64 ? launch_pcg_t<double>(g, pb, rhs, tol, maxit, st, wait_polls)
+                : launch_pcg_t<float>(g, pb, rhs, tol, maxit, st, wait_polls);
 }
 
 void launch_pcg_clear(PressureBufs& pb, int fp64, int with_invd, cudaStream_t st) {
@@ -560,12 +566,12 @@ void launch_ir_update(PressureBufs& pb, Dims g, cudaStream_t st) {
 }
 
 void launch_project(float* u, float* v, float* w, const float* p, const uint8_t* labels, Dims g, float dt, BodyKin b,
-                    cudaStream_t st) {
+                    cudaStream_t st, const int* guard) {
     const float scale = dt / (1000.0f * g.dx);  // dt/(rho*dx), FluidSolver3D.cu:2341
     const float inv = 1.0f / scale;
     dim3 blk(32, 8, 1);
     dim3 grd((g.W + 1 + 31) / 32, (g.H + 1 + 7) / 8, g.D + 1);
-    k_project<<<grd, blk, 0, st>>>(u, v, w, p, labels, g, scale, inv, b);
+    k_project<<<grd, blk, 0, st>>>(u, v, w, p, labels, g, scale, inv, b, guard);
 }
 
 int csr_cg_solve(int n, const int* offsets, const int* cols, const double* vals, const double* b, double* x, double tol,

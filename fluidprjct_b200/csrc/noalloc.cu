@@ -208,7 +208,7 @@ int solve_on_scratch(double* base, int n, const int* d_offsets, const int* d_col
         rz = rz2;
         ++it;
     }
-    if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return FP_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return FP_ERR_CUDA;
     if (iters) *iters = it;
     if (relres) *relres = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
     return FP_OK;
@@ -231,9 +231,17 @@ extern "C" int fp_solve_csr_upper_noalloc(int n, const int* d_offsets, const int
     if (const int rc = scratch_for_device(dev, &base)) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     std::lock_guard<std::mutex> lock(g_call_mutex[dev]);
-    const int rc = solve_on_scratch(base, n, d_offsets, d_cols, d_vals, d_b, d_x, tol, max_iters, iters, relres, st);
+    // A launch error of this call is one that appears during it: an error the
+    // calling thread left pending before the call is neither reported as this
+    // call's failure nor cleared.
+    const bool clean_before = cudaPeekAtLastError() == cudaSuccess;
+    int rc = solve_on_scratch(base, n, d_offsets, d_cols, d_vals, d_b, d_x, tol, max_iters, iters, relres, st);
     // An early error return may leave launches queued on st: let them finish
     // before the next call takes the scratch.
     if (rc != FP_OK) cudaStreamSynchronize(st);
+    if (clean_before && cudaPeekAtLastError() != cudaSuccess) {
+        cudaGetLastError();  // this call's launch error: report it and clear it
+        if (rc == FP_OK) rc = FP_ERR_CUDA;
+    }
     return rc;
 }

@@ -12,12 +12,13 @@ namespace {
 // Grid barrier for a cooperative launch on one 32-bit word: every block adds
 // 1 except block 0, which adds 2^31 - (nblocks - 1), so the word's top bit
 // flips exactly when the last block arrives and no reset is needed between
-// barriers.  The wait is bounded: after 2^27 polls the block records
+// barriers.  The wait is bounded: after `limit` polls (kDefaultWaitPolls =
+// 2^27 unless the solver's owner set another limit) the block records
 // DEV_TIMEOUT and leaves; callers check the status after every barrier and
 // return, so no block waits forever.  The arrival is a release atomic and the
 // poll an acquire load (the pattern of a release-acquire grid barrier), so
 // plain loads after it see every write made before it by any block.
-__device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* status) {
+__device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* status, long long limit) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -41,7 +42,7 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int
             unsigned cur;
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(cur) : "l"(&bar->count) : "memory");
             if (((old ^ cur) & 0x80000000u) != 0u) break;
-            if (++polls > (1ll << 27)) {
+            if (++polls >= limit) {
                 atomicExch(status, DEV_TIMEOUT);
                 ok = false;
                 break;

@@ -112,6 +112,7 @@ struct fp_solver {
     cudaEvent_t ev_pcg[2]{};
     int64_t launches = 0;   // kernels launched by this solver
     float pcg_ms = 0.0f;
+    long long wait_polls = kDefaultWaitPolls;  // grid-barrier poll limit (fp_set_wait_limit)
     bool have_grid = false;
 
     // grids
@@ -434,8 +435,8 @@ int solve_system(fp_solver* s, float* p_out, bool defer = false) {
         int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr, pb.b, tol,
                                    learned ? std::min(maxit, kLearnedMaxit) : maxit, s->st, x0,
                                    s->cfg.mg_sweeps > 0 ? s->cfg.mg_sweeps : 2,
-                                   s->cfg.warm_start && p_out == s->d_p ? p_out : nullptr, p_out)
-                   : launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st);
+                                   s->cfg.warm_start && p_out == s->d_p ? p_out : nullptr, p_out, s->wait_polls)
+                   : launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st, s->wait_polls);
         cudaEventRecord(s->ev_pcg[1], s->st);
         if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
         // FP64 solution to p, its true residual, then clear the work grids at
@@ -483,7 +484,7 @@ int solve_system(fp_solver* s, float* p_out, bool defer = false) {
                 // fallback: the plain FP64 PCG from x = 0
                 fallback = 1;
                 cudaEventRecord(s->ev_pcg[0], s->st);
-                e = launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st);
+                e = launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st, s->wait_polls);
                 cudaEventRecord(s->ev_pcg[1], s->st);
                 if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
                 ce = finish(true);
@@ -511,7 +512,7 @@ int solve_system(fp_solver* s, float* p_out, bool defer = false) {
             // not below what FP32 vectors can resolve.
             const double inner_tol = std::min(0.1, std::max(2e-4, 0.5 * tol / relres));
             cudaEventRecord(s->ev_pcg[0], s->st);
-            int e = launch_pcg(s->g, pb, pb.bin, 0, inner_tol, maxit - inner_total, s->st);
+            int e = launch_pcg(s->g, pb, pb.bin, 0, inner_tol, maxit - inner_total, s->st, s->wait_polls);
             cudaEventRecord(s->ev_pcg[1], s->st);
             if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
             launch_ir_update(pb, s->g, s->st);
@@ -598,10 +599,13 @@ int phase_pressure(fp_solver* s, bool defer = false) {
     return solve_system(s, s->d_p, defer);
 }
 
-void phase_project(fp_solver* s) {
+// guarded: the kernel reads the solve's device status word and does nothing
+// if that solve failed (one_step queues it before the status is known).
+void phase_project(fp_solver* s, bool guarded = false) {
     BodyKin b = body_kin(s);
     s->launches += 1;
-    launch_project(s->d_u, s->d_v, s->d_w, s->d_p, s->d_labels, s->g, s->cfg.dt, b, s->st);
+    launch_project(s->d_u, s->d_v, s->d_w, s->d_p, s->d_labels, s->g, s->cfg.dt, b, s->st,
+                   guarded ? &s->pb.out->status : nullptr);
 }
 
 // updateBody (FluidSolver3D.cu:2793-2846): fluid force and torque from the
@@ -705,11 +709,13 @@ int phase_body(fp_solver* s) {
     return FP_OK;
 }
 
-void phase_g2p_advect(fp_solver* s, int do_g2p, int do_adv) {
+void phase_g2p_advect(fp_solver* s, int do_g2p, int do_adv, bool guarded = false) {
     s->launches += 1;
+    const bool sdf = s->cfg.collision == FP_COLLISION_SDF && body_on(s);
+    const BodyShape b = sdf ? body_shape(s) : BodyShape{};
     launch_g2p_advect(s->d_pos, s->d_vel, s->np, s->d_u, s->d_v, s->d_w, s->d_us, s->d_vs, s->d_ws, s->d_labels, s->g,
                       s->cfg.pic_weight, s->cfg.dt, s->cfg.cfl, do_g2p, do_adv, s->cfg.advection == FP_ADVECT_RK2,
-                      s->st);
+                      s->st, guarded ? &s->pb.out->status : nullptr, sdf ? &b : nullptr);
     if (do_adv) s->sorted = false;
 }
 
@@ -893,23 +899,31 @@ int one_step(fp_solver* s, bool finish = true) {
     // The solve's statistics are read back only after the projection and
     // advection are issued (solve_finalize), so the GPU does not idle while
     // the host reads them; a failed solve is still reported by this call.
+    // The projection and G2P/advection kernels read the solve's device status
+    // and do nothing if it timed out or produced NaN, so such a step leaves
+    // the particles as they were; a body is integrated only after a good solve.
     int rc = phase_pressure(s, true);
     cudaEventRecord(s->ev[4], s->st);
     auto fail_after = [&](int rc0) { const int r = solve_finalize(s); return rc0 != FP_OK ? rc0 : r; };
     if (rc != FP_OK) return fail_after(rc);
-    phase_project(s);
+    phase_project(s, true);
     cudaEventRecord(s->ev[5], s->st);
+    if (body_on(s)) {
+        // the body phase waits for its own force anyway; finish the solve first
+        rc = solve_finalize(s);
+        if (rc != FP_OK) return rc;
+    }
     rc = phase_body(s);
     if (rc != FP_OK) return fail_after(rc);
     cudaEventRecord(s->ev[6], s->st);
     cudaEventRecord(s->ev[7], s->st);
     if (s->cfg.extrapolate > 0) {
-        phase_g2p_advect(s, 1, 0);
+        phase_g2p_advect(s, 1, 0, true);
         rc = extrapolate_3d(s);
         if (rc != FP_OK) return fail_after(rc);
-        phase_g2p_advect(s, 0, 1);
+        phase_g2p_advect(s, 0, 1, true);
     } else {
-        phase_g2p_advect(s, 1, 1);
+        phase_g2p_advect(s, 1, 1, true);
     }
     cudaEventRecord(s->ev[8], s->st);
     rc = solve_finalize(s);
@@ -1027,6 +1041,8 @@ int fp_config_default(fp_config* c) {
     c->body_density = 0.5f;
     c->device = -1;
     c->warm_start = 1;
+    c->collision = FP_COLLISION_LABELS;
+    std::snprintf(c->body_sdf, sizeof c->body_sdf, "%s", "InputData/ball.sdf");  // FluidSolver3D.cu:158
     return FP_OK;
 }
 
@@ -1055,6 +1071,10 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     }
     if (s->cfg.extrapolate < 0 ||
         (s->cfg.body_forces != FP_BODY_FORCES_FACE_FRACTION && s->cfg.body_forces != FP_BODY_FORCES_REFERENCE)) {
+        delete s;
+        return FP_ERR_ARG;
+    }
+    if (s->cfg.collision != FP_COLLISION_LABELS && s->cfg.collision != FP_COLLISION_SDF) {
         delete s;
         return FP_ERR_ARG;
     }
@@ -1640,6 +1660,12 @@ int fp_stats(const fp_solver* s, fp_step_stats* out) {
 }
 
 void* fp_cuda_stream(const fp_solver* s) { return s ? static_cast<void*>(s->st) : nullptr; }
+
+int fp_set_wait_limit(fp_solver* s, int64_t polls) {
+    if (!s || polls < 0) return s ? s->fail(FP_ERR_ARG, "negative wait limit") : FP_ERR_ARG;
+    s->wait_polls = polls == 0 ? kDefaultWaitPolls : static_cast<long long>(polls);
+    return FP_OK;
+}
 
 int fp_pressure_solve(fp_solver* s, const float* rhs, float* x, int64_t n, int* iters, double* relres) {
     if (!s || !rhs || !x) return FP_ERR_ARG;

@@ -81,6 +81,9 @@ enum { FP_ADVECT_RK3REF = 0, FP_ADVECT_RK2 = 1 };
  * cfl are unused (the reference fixes Euler and C = 1). */
 enum { FP_SCHEME_DEFAULT = 0, FP_SCHEME_REF2D = 1 };
 
+/* Collision of advected particles with the rigid body (fp_config.collision). */
+enum { FP_COLLISION_LABELS = 0, FP_COLLISION_SDF = 1 };
+
 /* Fluid force on the rigid body.  FP_BODY_FORCES_FACE_FRACTION (default):
  * the pressure integral over SDF face fractions, an FP64 reduction.
  * FP_BODY_FORCES_REFERENCE: the reference's panel drag and lift
@@ -143,6 +146,19 @@ typedef struct fp_config {
                                       previous step, scaled by its energy-optimal
                                       factor; the stopping test stays relative
                                       to ||b||.  0: from x = 0                  */
+    int      collision;            /* particles that advection moves into the body:
+                                      FP_COLLISION_LABELS (default) nudges them
+                                      half a cell toward the nearest FLUID cell
+                                      centre (projectParticleDevice3D,
+                                      FluidSolver3D.cu:1161-1239);
+                                      FP_COLLISION_SDF projects them along the
+                                      body SDF's normal to phi = dx/4 (SOLID
+                                      cells keep the label search)              */
+    char     body_sdf[256];        /* "body_sdf": SDF file of the body that the
+                                      FluidGPU driver loads when activeBody is
+                                      set and body_radius is 0 (the reference's
+                                      fixed InputData/ball.sdf,
+                                      FluidSolver3D.cu:158)                     */
 } fp_config;
 
 /* Per-step statistics: the reference's cudaEvent phase timers
@@ -267,6 +283,15 @@ int fp_stats(const fp_solver* s, fp_step_stats* out);
  * own events or order their own work after the solver's. */
 void* fp_cuda_stream(const fp_solver* s);
 
+/* Diagnostics (no counterpart in the reference): the number of polls after
+ * which a grid-barrier wait of the persistent pressure solvers gives up and
+ * the step returns FP_ERR_TIMEOUT (default 2^27, about a minute; 0 restores
+ * it).  A small limit makes the timeout path run without any fault, so a
+ * caller can test its error handling: after FP_ERR_TIMEOUT the particles and
+ * the body are as before the step, and the next step with the default limit
+ * solves normally. */
+int fp_set_wait_limit(fp_solver* s, int64_t polls);
+
 /* Pressure solve of the current labels for a caller right-hand side (dense,
  * W*H*D, zero off FLUID cells); x receives the dense solution.  Uses the
  * configured solver.  Reports iterations and the true relative residual. */
@@ -279,17 +304,24 @@ int fp_solve_csr_upper(int n, const int* offsets, const int* cols, const double*
                        double tol, int max_iters, int* iters, double* relres);
 
 /* Allocation-free variant of fp_solve_csr_upper; it has no counterpart in the
- * reference.  Same system, algorithm and status codes, but every pointer is a
- * DEVICE buffer owned by the caller (offsets n+1, cols/vals offsets[n], b and
- * x n doubles) and the work vectors live in one fixed device array, so the
- * call never allocates.  For hosts whose own pool allocator owns the GPU, and
- * for loops that cannot pay cudaMalloc's latency and device-wide sync.
- *   - n above FP_NOALLOC_MAX_N is rejected with FP_ERR_ARG;
+ * reference.  Same system and algorithm, but every pointer is a DEVICE buffer
+ * owned by the caller (offsets n+1, cols/vals offsets[n], b and x n doubles)
+ * and the work vectors live in one fixed device array, so the call never
+ * allocates.  For hosts whose own pool allocator owns the GPU, and for loops
+ * that cannot pay cudaMalloc's latency and device-wide sync.
+ *   - n above FP_NOALLOC_MAX_N is rejected with FP_ERR_ARG; so is a
+ *     malformed matrix, checked on the device before the solve: offsets[0]
+ *     must be 0, offsets must not decrease, columns must lie in [0, n);
+ *   - like fp_solve_csr_upper it returns FP_OK when CG stops at max_iters or
+ *     breaks down: check *relres against tol;
+ *   - the call is synchronous (it reads scalars back every iteration and
+ *     drains its stream before returning), so it must not be issued on a
+ *     stream that is being captured;
  *   - all calls on a device share the array, so they take turns: a call
  *     holds a per-device host lock until its stream has drained, and calls
  *     from several host threads are serialised;
  *   - the first call on a device, with that device current, looks up the
- *     array's address; make it before any stream capture on that device.
+ *     array's address.
  * stream may be NULL (the legacy default stream). */
 #define FP_NOALLOC_MAX_N (1 << 18)
 int fp_solve_csr_upper_noalloc(int n, const int* d_offsets, const int* d_cols, const double* d_vals,

@@ -115,6 +115,7 @@ template <class R> struct Sim3 {
     R alpha = R(0.05);      // PIC_WEIGHT
     R cfl = R(0.1);         // advectParticles(0.1), FluidSolver3D.cu:3092
     int rk2 = 0;            // 1: midpoint RK2 in place of the reference's RK3
+    int sdf_collide = 0;    // 1: SDF collision projection against the body (not the reference's)
     double tol = 1e-12;     // relative residual of the FP64 solve
     int maxit = 100000;
     BodyKin<R> body;
@@ -509,6 +510,30 @@ template <class R> struct Sim3 {
         return true;
     }
 
+    // ---- SDF collision projection (an addition beside projectParticleDevice3D,
+    // the same arithmetic as the GPU's sdf_push_out): a point whose body SDF is
+    // below eps moves along the SDF normal to phi = eps -- radially to r + eps
+    // for the sphere, to x_p + eps for the paddle. ----
+    void sdf_push_out(V3<R>& x, R eps) const {
+        if (ob.paddle) {
+            const R xp = R(float(ob.pos[0]));
+            if (x.x - xp < eps) x.x = xp + eps;
+            return;
+        }
+        const R cx = R(float(ob.pos[0])), cy = R(float(ob.pos[1])), cz = R(float(ob.pos[2]));
+        const R rad = R(float(ob.radius));
+        const R ex = x.x - cx, ey = x.y - cy, ez = x.z - cz;
+        const R r = std::sqrt((ex * ex + ey * ey) + ez * ez);
+        if (!(r - rad < eps)) return;
+        const R target = rad + eps;
+        if (r > R(0)) {
+            const R sc = target / r;
+            x = mk(cx + ex * sc, cy + ey * sc, cz + ez * sc);
+        } else {
+            x = mk(cx, cy + target, cz);
+        }
+    }
+
     // ---- AdvectParticlesFunctor (:1241-1330): adaptive substeps, Ralston RK3 ----
     void advect_one(R& x, R& y, R& z) const {
         V3<R> pos = mk(x, y, z);
@@ -537,10 +562,17 @@ template <class R> struct Sim3 {
             pos.x = std::min(std::max(pos.x, R(0)), xmax);
             pos.y = std::min(std::max(pos.y, R(0)), ymax);
             pos.z = std::min(std::max(pos.z, R(0)), zmax);
+            const bool sdf = sdf_collide && ob.loaded;
+            if (sdf) {
+                sdf_push_out(pos, R(0.25f) * dx);
+                pos.x = std::min(std::max(pos.x, R(0)), xmax);
+                pos.y = std::min(std::max(pos.y, R(0)), ymax);
+                pos.z = std::min(std::max(pos.z, R(0)), zmax);
+            }
             int cx = int(std::floor(pos.x / dx)), cy = int(std::floor(pos.y / dx)), cz = int(std::floor(pos.z / dx));
             if (cx >= 0 && cx < W && cy >= 0 && cy < H && cz >= 0 && cz < D) {
                 uint8_t l = labels[cidx(cx, cy, cz)];
-                if (l == SOLID || l == BODY) {
+                if (l == SOLID || (l == BODY && !sdf)) {
                     if (!project_particle(pos)) break;  // the reference retries once, then stops (:1313-1317)
                 }
             }
@@ -1006,6 +1038,9 @@ void or3_set_extrap(void* p, int layers) {
 }
 void or3_set_rk2(void* p, int rk2) {
     with(static_cast<Handle*>(p), [&](auto& s) { s.rk2 = rk2; return 0; });
+}
+void or3_set_collision(void* p, int sdf) {
+    with(static_cast<Handle*>(p), [&](auto& s) { s.sdf_collide = sdf; return 0; });
 }
 void or3_set_body(void* p, const double* vel, const double* omega, const double* com) {
     with(static_cast<Handle*>(p), [&](auto& s) {

@@ -54,6 +54,7 @@ def lib():
         L.or3_set_params.argtypes = [P, D, D, D, I]
         L.or3_set_body.argtypes = [P, P, P, P]
         L.or3_set_rk2.argtypes = [P, I]
+        L.or3_set_collision.argtypes = [P, I]
         L.or3_set_sphere.argtypes = [P, P, D, D]
         L.or3_set_paddle.argtypes = [P, D, D, D]
         L.or3_set_extrap.argtypes = [P, I]
@@ -208,6 +209,11 @@ class Sim3:
 
     def set_paddle(self, x_rest, amplitude, period):
         lib().or3_set_paddle(self.h, x_rest, amplitude, period)
+
+    def set_collision(self, sdf):
+        """SDF collision projection against the body (True) or the
+        reference's label search alone (False)."""
+        lib().or3_set_collision(self.h, int(bool(sdf)))
 
     def set_extrapolate(self, layers):
         """Velocity extrapolation layers between G2P and advection (0 = off)."""

@@ -9,6 +9,18 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+# Root of a checkout of the reference (Ship-Vano/FluidPrjct), when one is at
+# hand: tests that read its files directly use it, the others read the
+# committed fixtures that tests/golden/make_golden.py made from it.
+REFERENCE = os.environ.get("FLUIDPRJCT_REFERENCE", "")
+
+
+def reference_file(*parts):
+    """Path of a file of the reference checkout, or None without one."""
+    if not REFERENCE:
+        return None
+    p = os.path.join(REFERENCE, *parts)
+    return p if os.path.exists(p) else None
 
 
 def pytest_configure(config):

@@ -95,4 +95,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FLUIDPRJCT_REFERENCE", "")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout>  (or set FLUIDPRJCT_REFERENCE)")
+    main(root)

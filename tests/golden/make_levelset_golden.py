@@ -6,9 +6,9 @@ DistrGen/fluidLabels.py (generate_combined_labels_simple) at a small size and
 copies their output files into tests/golden/levelsets/.  The functions are
 taken from the reference sources by name (their modules also run plotting and
 full-size generation at import, which is skipped).  Run from the repository
-root with the reference checkout at REF (default /root/reference):
+root with the reference checkout named by FLUIDPRJCT_REFERENCE:
 
-    python tests/golden/make_levelset_golden.py
+    FLUIDPRJCT_REFERENCE=<checkout> python tests/golden/make_levelset_golden.py
 """
 import ast
 import os
@@ -16,7 +16,9 @@ import shutil
 import sys
 import tempfile
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("FLUIDPRJCT_REFERENCE", "")
+if not REF:
+    sys.exit("set FLUIDPRJCT_REFERENCE to the root of a reference checkout")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "levelsets")
 
 

@@ -7,7 +7,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, ROOT
+from conftest import GOLDEN, ROOT, reference_file
 
 HEADER = os.path.join(ROOT, "include", "fluidprjct.h")
 
@@ -90,8 +90,8 @@ def test_config_json(tmp_path):
 def test_host_label_reader(golden_labels, name, dim, tmp_path):
     from fluidprjct_b200 import capi, scenes
     exp = golden_labels[name]
-    path = os.path.join("/root/reference/InputData", name + ".txt")
-    if not os.path.exists(path):
+    path = reference_file("InputData", name + ".txt")
+    if path is None:
         path = str(tmp_path / "l.txt")
         (scenes.write_labels3d if dim == 3 else scenes.write_labels2d)(path, exp)
     assert np.array_equal(capi.read_label_file(path, dim), exp)
@@ -121,8 +121,9 @@ def test_ply_reader_ascii_and_binary(golden_particles, tmp_path):
         np.savetxt(f, pos, fmt="%.9g")
     p2, v2 = capi.read_ply_file(a)
     assert v2 is None and np.array_equal(p2, pos)
-    if os.path.exists("/root/reference/InputData/particles_-1.ply"):
-        p3, _ = capi.read_ply_file("/root/reference/InputData/particles_-1.ply")
+    ref_ply = reference_file("InputData", "particles_-1.ply")
+    if ref_ply:
+        p3, _ = capi.read_ply_file(ref_ply)
         assert np.array_equal(p3, pos)
     # binary little endian with velocities and an extra double property
     rng = np.random.default_rng(1)

@@ -1,0 +1,143 @@
+"""GPU parity at the benchmark configurations' full sizes, against the FP64 oracle.
+
+Each test runs one step of a full-size scene phase by phase from identical
+inputs (oracle/parity.py: every phase of both sides starts from the GPU's
+output of the phase before), with the oracle in FP64 mode and its pressure
+solved by FP64 Jacobi PCG to 1e-12 (the stand-in for the reference's direct
+solve).  The step compared is the second one: after one step from the seeded
+state, whose velocities are zero, every phase has non-trivial input.
+
+Bars (from the reference's own contract for this path):
+  * cell labels: bit-exact;
+  * face velocities after P2G, forces and projection: relative L2 <= 1e-5;
+  * pressure of a solve to tol 1e-9: relative L2 <= 1e-5 against the FP64
+    solve, and FP64 residual ||b - A p|| / ||b|| <= 1e-8 with the oracle's own
+    right-hand side and operator;
+  * particle velocities after G2P: relative L2 <= 1e-5;
+  * positions after advection: 99.9 % within 1e-5 dx (a substep boundary can
+    flip on a rounding), relative L2 <= 1e-6.
+The whole step of the timed configuration (tol 1e-6) is also compared with
+the oracle's whole step from the same seeded state.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_phases(r, tol_solve=1e-9, exact=True):
+    print({k: (f"{v:.3e}" if isinstance(v, float) else v) for k, v in r.items()})
+    assert r["labels_bitexact"]
+    for ph in ("p2g", "forces", "project"):
+        for c in "uvw":
+            assert r[f"{ph}_{c}_rel_l2"] <= 1e-5, (ph, c, r[f"{ph}_{c}_rel_l2"])
+    assert r["rhs_rel_l2"] <= 1e-5
+    assert r["solve_residual"] <= tol_solve
+    if exact:
+        assert r["p_rel_l2"] <= 1e-5, r["p_rel_l2"]
+    assert r["p_fp64_residual"] <= 10 * tol_solve, r["p_fp64_residual"]
+    assert r["g2p_vel_rel_l2"] <= 1e-5
+    assert r["advect_frac_within_1e-5dx"] >= 0.999
+    assert r["advect_pos_rel_l2"] <= 1e-6
+
+
+def _dam_break(O, tol):
+    from fluidprjct_b200 import capi, scenes
+    n = 128
+    lab = scenes.dam_break_3d(n)
+    s = capi.Solver(dx=1.0 / n, dt=0.002, pic_weight=0.05, advection="rk2", solver="pcg_mg", tol=tol,
+                    output_format=capi.OUT_NONE)
+    s.set_labels(lab)
+    s.seed_particles(8, 1)
+    assert s.num_particles == 3830400
+    o = O.Sim3(n, n, n, 1.0 / n, 0.002, fp64=True, pic_weight=0.05, tol=1e-12, rk2=True)
+    o.set_labels(lab)
+    o.set_particles(*s.particles())
+    return s, o
+
+
+def test_dam_break_128_phases_against_fp64_oracle(O):
+    """The 128^3 dam break (3,830,400 particles, seed 1, dt 0.002, FLIP 0.95,
+    RK2), step 2 phase by phase."""
+    from oracle import parity
+    s, o = _dam_break(O, 1e-9)
+    s.step(1)
+    o.set_particles(*s.particles())
+    r = parity.step_phases(s, o, 1.0 / 128)
+    _check_phases(r)
+
+
+def test_dam_break_128_whole_step_against_fp64_oracle(O):
+    """The timed configuration's own step (MG-PCG to 1e-6, warm start) from the
+    seeded state against the oracle's FP64 step: labels bit-exact, velocity
+    grids and particle velocities within 1e-5, the pressure within the error a
+    1e-6 residual allows."""
+    from oracle import parity
+    s, o = _dam_break(O, 1e-6)
+    r = parity.full_step(s, o)
+    print(r)
+    assert r["labels_bitexact"]
+    for c in "uvw":
+        assert r[f"{c}_rel_l2"] <= 1e-5, (c, r)
+    assert r["p_rel_l2"] <= 1e-4, r
+    assert r["vel_rel_l2"] <= 1e-5 and r["pos_rel_l2"] <= 1e-6, r
+
+
+def test_pool_160_with_sphere_phases_against_fp64_oracle(O):
+    """The rigid-body drop at full size: 160^3 pool to y < 0.35 (8 ppc, seed 2,
+    10,982,800 particles), sphere r = 0.12 at half density.  The sphere is
+    placed half submerged at (0.5, 0.35, 0.5) so that the body terms of the
+    right-hand side, the projection and the face-fraction force all act;
+    BODY marks are bit-exact and the force and torque of the same pressure
+    agree with the oracle's FP64 sums."""
+    from fluidprjct_b200 import capi, scenes
+    from oracle import parity
+    n, c, r_ = 160, (0.5, 0.35, 0.5), 0.12
+    lab = scenes.pool_3d(n, 0.35)
+    s = capi.Solver(dx=1.0 / n, dt=0.002, pic_weight=0.05, advection="rk2", solver="pcg_mg", tol=1e-9,
+                    body_radius=r_, body_density=0.5, body_pos=c, active_body=1, output_format=capi.OUT_NONE)
+    s.set_labels(lab)
+    s.load_sdf(None)
+    s.seed_particles(8, 2)
+    o = O.Sim3(n, n, n, 1.0 / n, 0.002, fp64=True, pic_weight=0.05, tol=1e-12, rk2=True)
+    o.set_labels(lab)
+    r32 = float(np.float32(r_))
+    mass = float(np.float32(0.5)) * 1000.0 * 4.0 / 3.0 * np.pi * r32 ** 3
+    o.set_sphere(np.array(c, np.float64), r_, mass)
+    s.step(1)
+    o.set_particles(*s.particles())
+    st = s.stats()
+    o.set_body(st["body_vel"], st["body_omega"], st["body_pos"])  # the body as it is after step 1
+    res = parity.step_phases(s, o, 1.0 / n, body_mass=mass)
+    _check_phases(res)
+    assert res["body_force_rel"] <= 1e-6 and res["body_torque_abs_over_force"] <= 1e-6, res
+
+
+def test_seabed_paddle_one_step_phases_against_fp64_oracle(O):
+    """The large seabed scene (256 x 128 x 256, seabed 0.15 + 0.05 noise(seed 4),
+    water to y < 0.45, 8 ppc), one step with the paddle's BODY region, phase
+    by phase.  The pressure is checked through its FP64 residual with the
+    oracle's own right-hand side and operator (an exact FP64 solve at this
+    size takes minutes on the host)."""
+    from fluidprjct_b200 import capi, scenes
+    from oracle import parity
+    W, H, D, dx = 256, 128, 256, 1.0 / 128
+    s = capi.Solver(dx=dx, dt=0.001, pic_weight=0.05, advection="rk2", solver="pcg_mg", tol=1e-9,
+                    output_format=capi.OUT_NONE)
+    s.scene_seabed(W, H, D, level=0.45, bed_base=0.15, bed_amp=0.05, seed=4, water_xmin=0.1)
+    s.set_paddle(0.1, 0.05, 1.0)
+    lab = s.labels()
+    s.seed_particles(8, 4)
+    o = O.Sim3(W, H, D, dx, 0.001, fp64=True, pic_weight=0.05, tol=1e-12, rk2=True)
+    base = lab.copy()
+    base[base == capi.BODY] = capi.AIR
+    o.set_labels(base)
+    o.set_paddle(0.1, 0.05, 1.0)
+    s.step(1)
+    o.set_particles(*s.particles())
+    st = s.stats()
+    o.set_body(st["body_vel"], st["body_omega"], st["body_pos"])  # the paddle as it is after step 1
+    res = parity.step_phases(s, o, dx, exact_solve=False)
+    _check_phases(res, exact=False)

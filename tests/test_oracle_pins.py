@@ -13,9 +13,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, rel_l2
-
-REF = "/root/reference/InputData"
+from conftest import GOLDEN, reference_file, rel_l2
 
 
 def test_particles_m1_binning(O, golden, golden_particles):
@@ -35,8 +33,8 @@ def test_particles_m1_binning(O, golden, golden_particles):
 @pytest.mark.parametrize("name", ["labels_simple3d", "labels_3d_sphere", "labels_bathymetry"])
 def test_label_reader_3d(O, golden, golden_labels, name, tmp_path):
     exp = golden_labels[name]
-    path = os.path.join(REF, name + ".txt")
-    if not os.path.exists(path):  # away from the reference checkout: rebuild the file in its format
+    path = reference_file("InputData", name + ".txt")
+    if path is None:  # away from the reference checkout: rebuild the file in its format
         from fluidprjct_b200.scenes import write_labels3d
         path = str(tmp_path / (name + ".txt"))
         write_labels3d(path, exp)
@@ -49,8 +47,8 @@ def test_label_reader_3d(O, golden, golden_labels, name, tmp_path):
 @pytest.mark.parametrize("name", ["labels_simple", "labels_colimn"])
 def test_label_reader_2d(O, golden, golden_labels, name, tmp_path):
     exp = golden_labels[name]
-    path = os.path.join(REF, name + ".txt")
-    if not os.path.exists(path):
+    path = reference_file("InputData", name + ".txt")
+    if path is None:
         from fluidprjct_b200.scenes import write_labels2d
         path = str(tmp_path / (name + ".txt"))
         write_labels2d(path, exp)

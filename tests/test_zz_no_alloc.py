@@ -72,6 +72,29 @@ def test_noalloc_matches_allocating_solve_on_two_calls(O, golden):
 
 
 @pytest.mark.gpu
+def test_noalloc_leaves_device_free_memory_unchanged(O):
+    """The call allocates nothing: after a first call (which looks up the
+    scratch array's address), the device's free memory is the same after
+    each of three more calls as before them."""
+    import torch
+    off, cols, vals = _poisson(O, 30, 28, 26, obstacle=True)
+    b = np.random.default_rng(3).standard_normal(len(off) - 1)
+    _device_solve(off, cols, vals, b, 1e-10)
+    dev = torch.device("cuda:0")
+    t = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (off, cols, vals, b)]
+    t_x = torch.zeros_like(t[3])
+    torch.cuda.synchronize(dev)
+    from fluidprjct_b200 import capi
+    free0, _ = torch.cuda.mem_get_info(dev)
+    for _ in range(3):
+        capi.solve_csr_upper_noalloc(len(b), t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), t[3].data_ptr(),
+                                     t_x.data_ptr(), tol=1e-10, max_iters=20000,
+                                     stream=torch.cuda.current_stream(dev).cuda_stream)
+        free1, _ = torch.cuda.mem_get_info(dev)
+        assert free1 == free0, (free0, free1)
+
+
+@pytest.mark.gpu
 def test_noalloc_rejects_oversize_and_malformed():
     import torch
     from fluidprjct_b200 import capi
