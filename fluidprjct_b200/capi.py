@@ -11,7 +11,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libfluidprjct_b200.so")
+# FLUIDPRJCT_LIB may name another build of the same library (for example one
+# built with different tuning macros); by default the in-tree build is used.
+LIB_PATH = os.environ.get("FLUIDPRJCT_LIB") or os.path.join(HERE, "_lib", "libfluidprjct_b200.so")
 
 FP_OK, FP_ERR_ARG, FP_ERR_IO, FP_ERR_CUDA, FP_ERR_STATE, FP_ERR_NO_FLUID, FP_ERR_SOLVER, FP_ERR_TIMEOUT = (
     0, -1, -2, -3, -4, -5, -6, -7)

@@ -13,10 +13,13 @@ namespace fp {
 
 constexpr uint8_t SOLID = 0, FLUID = 1, AIR = 2, BODY = 3;
 
-// Grid geometry passed by value to every kernel.
+// Grid geometry passed by value to every kernel.  idx = 1/dx when dx is a
+// power of two (then x * idx is exactly x / dx, so the cheap multiply gives
+// the reference's quotient bit for bit), else 0 (divide).
 struct Dims {
     int W, H, D;
     float dx;
+    float idx = 0.0f;
     __host__ __device__ int64_t nc() const { return int64_t(W) * H * D; }
     __host__ __device__ int64_t nu() const { return int64_t(W + 1) * H * D; }
     __host__ __device__ int64_t nv() const { return int64_t(W) * (H + 1) * D; }
@@ -30,13 +33,16 @@ struct BodyKin {
     int active;
 };
 
+// x / dx, by the exact reciprocal multiply when dx is a power of two.
+__device__ __forceinline__ float over_dx(float x, const Dims& g) { return g.idx != 0.0f ? x * g.idx : x / g.dx; }
+
 __device__ __forceinline__ int clampi(int a, int lo, int hi) { return min(max(a, lo), hi); }
 __device__ __forceinline__ float clamp01(float f) { return fminf(fmaxf(f, 0.0f), 1.0f); }
 
 // Cell of a particle: floorf(p/dx) clamped to the grid (MarkFluidCellsFunctor,
 // FluidSolver3D.cu:316-331).
 __device__ __forceinline__ int cell_key(float x, float y, float z, const Dims& g) {
-    int i = int(floorf(x / g.dx)), j = int(floorf(y / g.dx)), k = int(floorf(z / g.dx));
+    int i = int(floorf(over_dx(x, g))), j = int(floorf(over_dx(y, g))), k = int(floorf(over_dx(z, g)));
     i = clampi(i, 0, g.W - 1);
     j = clampi(j, 0, g.H - 1);
     k = clampi(k, 0, g.D - 1);
@@ -119,7 +125,7 @@ __device__ __forceinline__ int sxy_v(const Dims& g) { return g.D > 1 ? g.W * (g.
 
 __device__ __forceinline__ float3 interp_vel(const float* __restrict__ u, const float* __restrict__ v,
                                              const float* __restrict__ w, const Dims& g, float3 pos) {
-    float rx = pos.x / g.dx, ry = pos.y / g.dx, rz = pos.z / g.dx;
+    const float rx = over_dx(pos.x, g), ry = over_dx(pos.y, g), rz = over_dx(pos.z, g);
     return make_float3(sample(u, stencil_u(rx, ry, rz, g), g.W + 1, sxy_u(g)),
                        sample(v, stencil_v(rx, ry, rz, g), g.W, sxy_v(g)),
                        sample(w, stencil_w(rx, ry, rz, g), g.W, g.W * g.H));

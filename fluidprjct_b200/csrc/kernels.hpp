@@ -11,12 +11,13 @@ namespace fp {
 // Scratch of the persistent PCG kernel: a grid barrier and FP64 partials.
 struct GridBar {
     unsigned count;
-    unsigned gen;
+    unsigned limit;  // polls after which a wait gives up (set at launch)
 };
 
 // Polls after which a grid-barrier wait of the persistent solvers gives up
-// and reports DEV_TIMEOUT (fp_set_wait_limit lowers it for tests).
-constexpr long long kDefaultWaitPolls = 1ll << 27;
+// and reports DEV_TIMEOUT (fp_set_wait_limit lowers it for tests).  Each
+// launch stores it in its GridBar, where the polling thread reads it.
+constexpr unsigned kDefaultWaitPolls = 1u << 27;
 
 struct PcgOut {
     int iters;
@@ -91,7 +92,7 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStrea
 // ||rhs||^2 (FP64) to pb.red.
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
                   const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0 = nullptr, int nu0 = 2,
-                  const float* pprev = nullptr, float* pout = nullptr, long long wait_polls = kDefaultWaitPolls);
+                  const float* pprev = nullptr, float* pout = nullptr, unsigned wait_polls = kDefaultWaitPolls);
 
 // -------- labelling and the particle sort (kernels_sort.cu) --------
 // counts[nc] must be zero on entry.  Writes key/rank per particle.
@@ -121,8 +122,11 @@ void launch_pressure_setup(const uint8_t* labels, const float* u, const float* v
 // diagnostics in pb.out.  The padded work grids must be zero on entry;
 // launch_pcg_clear restores that after a solve.
 int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, int fp64, double tol, int maxit, cudaStream_t st,
-               long long wait_polls = kDefaultWaitPolls);
+               unsigned wait_polls = kDefaultWaitPolls);
 void launch_pcg_clear(PressureBufs& pb, int fp64, int with_invd, cudaStream_t st);
+// Barrier word to zero with its poll limit, status word to DEV_OK (before
+// every persistent-solver launch).
+void launch_reset_barrier(GridBar* bar, int* status, unsigned wait_polls, cudaStream_t st);
 int pcg_max_blocks();
 // p[cell] = X[n] (src 0: FP32 X, 1: FP64 X, 2: x64).
 void launch_scatter_p(const PressureBufs& pb, float* p, int src, Dims g, cudaStream_t st);
@@ -143,9 +147,12 @@ void launch_project(float* u, float* v, float* w, const float* p, const uint8_t*
 void launch_g2p_advect(float4* pos, float4* vel, int64_t np, const float* u, const float* v, const float* w,
                        const float* us, const float* vs, const float* ws, const uint8_t* labels, Dims g, float alpha,
                        float dt, float cfl, int do_g2p, int do_advect, int rk2, cudaStream_t st,
-                       const int* guard = nullptr, const BodyShape* collide = nullptr);
+                       const int* guard = nullptr, const BodyShape* collide = nullptr,
+                       const int* cell_start = nullptr);
 // collide: the body for SDF collision projection (sdf_push_out, eps = dx/4),
-// or null for the reference's label search alone.
+// or null for the reference's label search alone.  cell_start: the cell
+// offsets of the current (cell-sorted) particle order, or null; with it, a 3D
+// grid is processed brick by brick from shared-memory tiles of the faces.
 
 // -------- rigid body (kernels_body.cu) --------
 // mark[c] = 1 where the cell centre is inside the body (SDF <= 0).

@@ -74,7 +74,6 @@ struct MgArgs {
     PcgOut* out;
     double tol;
     int maxit;
-    long long wait_polls;        // grid-barrier poll limit
 };
 
 __device__ __forceinline__ int lv_diag(const MgLevel& L, int c) {
@@ -534,7 +533,7 @@ __device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
     auto sweep = [&](int l, int color) {
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, color, t0, st);
         else op_sweep(a.lv[l], color, t0, st);
-        return grid_barrier(a.bar, nb, a.status, a.wait_polls);
+        return grid_barrier(a.bar, nb, a.status);
     };
     for (int l = 0; l < G; ++l) {
         // pre-smoothing (red, black)^nu (nu = nu0 on level 0, else 1); the first
@@ -543,17 +542,17 @@ __device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
         for (int e = 1; e < (l == 0 ? a.nu0 : 1); ++e)
             if (!sweep(l, 0) || !sweep(l, 1)) return false;
         op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st);
-        if (!grid_barrier(a.bar, nb, a.status, a.wait_polls)) return false;
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
     if (blockIdx.x == 0) {
         if (a.smem) block_vcycle_smem(a, G, nl, S);
         else block_vcycle_global(a, G);
     }
-    if (!grid_barrier(a.bar, nb, a.status, a.wait_polls)) return false;
+    if (!grid_barrier(a.bar, nb, a.status)) return false;
     if (G > 0) {  // level G's last red sweep, fused with its prolongation into level G - 1
         if (G == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
         else op_prolong_red(a.lv[G - 1], a.lv[G], a.omega, t0, st);
-        if (!grid_barrier(a.bar, nb, a.status, a.wait_polls)) return false;
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
     for (int l = G - 1; l >= 0; --l) {
         // post-smoothing (black, red)^nu, the reverse of the pre-smoothing; the
@@ -565,7 +564,7 @@ __device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 0, t0, st);
         else if (l == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
         else op_prolong_red(a.lv[l - 1], a.lv[l], a.omega, t0, st);
-        if (!grid_barrier(a.bar, nb, a.status, a.wait_polls)) return false;
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
     return true;
 }
@@ -661,7 +660,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         // Scale the guess by its energy-optimal factor alpha = (x0, b) / (x0, A x0):
         // the A-norm error of alpha x0 is never above that of x = 0.  Then r = b - A x.
         if (a.x0) {
-            if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
+            if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
             for (int n = t0; n < nf; n += st) {
                 const int c = a.fidx[n];
                 const double* xp = a.xs + c;
@@ -673,7 +672,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
             }
         }
         partial(xb, xq, rrl);
-        if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
         const double3 t = total();
         const double alpha = (t.y > 0.0 && isfinite(t.x / t.y)) ? t.x / t.y : 0.0;
         bb_warm = t.z;  // all reads of x ended before the barrier above
@@ -702,7 +701,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         }
     }
     partial(rrl, 0.0, 0.0);
-    if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
+    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
     double rr = total().x;
     const double bb = guess ? bb_warm : rr;
     const double rr0 = rr;
@@ -752,7 +751,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
             }
         }
         partial(gl, dl, sl);
-        if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
         const double3 t = total();
         gam = t.x;
         if (isnan(t.x) || isnan(t.y) || isnan(t.z)) { stt = DEV_NAN; break; }
@@ -794,7 +793,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
             }
         }
         partial(rrl, 0.0, 0.0);
-        if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
         rr = total().x;
         ++it;
         if (isnan(rr)) { stt = DEV_NAN; break; }
@@ -805,7 +804,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     // The true residual of the FP64 solution, ||rhs - A x||^2 and ||rhs||^2,
     // then the compact and dense solution; zero the level-0 work grids at the
     // FLUID cells so the next solve starts from zero whatever cells are fluid.
-    if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
+    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
     {
         double e2 = 0.0, b2 = 0.0;
         for (int n = t0; n < nf; n += st) {
@@ -819,7 +818,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         }
         partial(e2, b2, 0.0);
     }
-    if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
+    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
     {
         const double3 t = total();
         if (blockIdx.x == 0 && threadIdx.x == 0) { a.red[0] = t.x; a.red[1] = t.y; }
@@ -926,11 +925,10 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStrea
 
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
                   const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0, int nu0,
-                  const float* pprev, float* pout, long long wait_polls) {
+                  const float* pprev, float* pout, unsigned wait_polls) {
     const int nb = mg_max_blocks();
     int* status = &pb.out->status;
-    cudaMemsetAsync(pb.bar, 0, sizeof(GridBar), st);
-    cudaMemsetAsync(status, 0, sizeof(int), st);
+    launch_reset_barrier(pb.bar, status, wait_polls, st);
     MgArgs a;
     a.L = L;
     a.G = mg_split(lv, L, &a.smem);
@@ -952,7 +950,6 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     a.red = pb.red;
     a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;
     a.tol = tol; a.maxit = maxit;
-    a.wait_polls = wait_polls;
     void* args[] = {&a};
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_mg, dim3(nb), dim3(MG_THREADS), args, size_t(a.smem), st);
     return e == cudaSuccess ? 0 : int(e);

@@ -21,90 +21,221 @@ namespace fp {
 
 namespace {
 
-// Slot weights along one axis: slot m is face s0 + m; the particle's two
-// corners are faces base (weight 1 - f) and base + 1 (weight f).
-template <int NS>
-__device__ __forceinline__ void axis_weights(int s0, int base, float f, float (&w)[NS]) {
-#pragma unroll
-    for (int m = 0; m < NS; ++m) {
-        const int face = s0 + m;
-        w[m] = face == base ? 1.0f - f : (face == base + 1 ? f : 0.0f);
-    }
+// Packed FP32 pairs (sm_100's f32x2 FMA/mul/add): two lanes of one 64-bit
+// register, each an IEEE FP32 operation rounded to nearest.
+__device__ __forceinline__ float2 f2_fma(float2 a, float2 b, float2 c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)),
+          "l"(*reinterpret_cast<unsigned long long*>(&c)));
+    return *reinterpret_cast<float2*>(&d);
+}
+__device__ __forceinline__ float2 f2_mul(float2 a, float2 b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)));
+    return *reinterpret_cast<float2*>(&d);
+}
+__device__ __forceinline__ float2 f2_add(float2 a, float2 b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)));
+    return *reinterpret_cast<float2*>(&d);
+}
+
+// Weights of the three face slots s0, s0+1, s0+2 along a non-staggered axis:
+// the particle's corners are faces base (1 - f) and base + 1 (f), with base
+// s0 or s0 + 1.
+__device__ __forceinline__ void axis3(int s0, int base, float f, float (&w)[3]) {
+    const bool lo = base == s0;
+    w[0] = lo ? 1.0f - f : 0.0f;
+    w[1] = lo ? f : 1.0f - f;
+    w[2] = lo ? 0.0f : f;
 }
 
 // Accumulates one velocity component of the particles [q0, q1) of cell
-// (ci, cj, ck) over the faces that cell can reach -- NX x NY x NZ slots whose
-// first face is (sx0, sy0, sz0) -- and adds the owned ones into shared memory.
-// COMP selects the component and its base-index rules (AccumulateVelocities,
-// FluidSolver3D.cu:465-574); weights are (wx*wy)*wz and contributions
-// vel*wgt, rounded as in the reference.
-template <int COMP, int NX, int NY, int NZ>
+// (ci, cj, ck) over the 2 x 3 x 3 faces that cell can reach (2 along the
+// component's own axis, whose base face is always the cell's), and adds the
+// owned ones into shared memory.  COMP selects the component and its
+// base-index rules (AccumulateVelocities, FluidSolver3D.cu:465-574).  Weights
+// are (wx*wy)*wz as in the reference; the two faces along the component's
+// axis are one packed pair, so each particle costs 12 packed multiplies and
+// 9 packed FMAs and adds per component.  num accumulates vel*wgt with one
+// fused multiply-add (the reference rounds the product first; its float
+// atomics already leave the last bits of the sums order-dependent).
+// MA, MB: which of the three slots of the other two axes (in the order x, y,
+// z without the component's own axis) hold owned faces; slots outside the
+// masks are neither computed nor added (halo cells reach only a one-slot-wide
+// slab of the brick's faces).
+template <int COMP, int MA = 7, int MB = 7>
 __device__ __forceinline__ void splat_cell(const float4* __restrict__ pos, const float4* __restrict__ vel, int q0,
                                            int q1, int ci, int cj, int ck, const Dims& g, float* s_num, float* s_den,
                                            int fx0, int fx1, int fy0, int fy1, int fz0, int fz1, int lsx, int lsy) {
     const int W = g.W, H = g.H, D = g.D;
+    // first face of each axis' slot range: the cell's own face on the
+    // component's axis, the face below the cell on the other two
     const int sx0 = COMP == 0 ? ci : ci - 1, sy0 = COMP == 1 ? cj : cj - 1, sz0 = COMP == 2 ? ck : ck - 1;
-    float an[NX * NY * NZ], ad[NX * NY * NZ];
+    float2 an[9], ad[9];  // pair = the component axis' two faces; index = the other two axes' slots
 #pragma unroll
-    for (int m = 0; m < NX * NY * NZ; ++m) { an[m] = 0.0f; ad[m] = 0.0f; }
-    const float dx = g.dx;
+    for (int m = 0; m < 9; ++m) { an[m] = make_float2(0.0f, 0.0f); ad[m] = make_float2(0.0f, 0.0f); }
     for (int q = q0; q < q1; ++q) {
         const float4 P = pos[q];
-        const float4 V = vel[q];
-        const float rx = P.x / dx, ry = P.y / dx, rz = P.z / dx;
+        const float rx = over_dx(P.x, g), ry = over_dx(P.y, g), rz = over_dx(P.z, g);
         int bi, bj, bk;
         float fx, fy, fz, vc;
         if (COMP == 0) {
             bi = clampi(int(floorf(rx)), 0, W); bj = clampi(int(floorf(ry - 0.5f)), 0, H - 1);
             bk = clampi(int(floorf(rz - 0.5f)), 0, D - 1);
             fx = clamp01(rx - float(bi)); fy = clamp01((ry - 0.5f) - float(bj)); fz = clamp01((rz - 0.5f) - float(bk));
-            vc = V.x;
+            vc = vel[q].x;
         } else if (COMP == 1) {
             bi = clampi(int(floorf(rx - 0.5f)), 0, W - 1); bj = clampi(int(floorf(ry)), 0, H);
             bk = clampi(int(floorf(rz - 0.5f)), 0, D - 1);
             fx = clamp01((rx - 0.5f) - float(bi)); fy = clamp01(ry - float(bj)); fz = clamp01((rz - 0.5f) - float(bk));
-            vc = V.y;
+            vc = vel[q].y;
         } else {
             bi = clampi(int(floorf(rx - 0.5f)), 0, W - 1); bj = clampi(int(floorf(ry - 0.5f)), 0, H - 1);
             bk = clampi(int(floorf(rz)), 0, D);
             fx = clamp01((rx - 0.5f) - float(bi)); fy = clamp01((ry - 0.5f) - float(bj)); fz = clamp01(rz - float(bk));
-            vc = V.z;
+            vc = vel[q].z;
         }
-        float wx[NX], wy[NY], wz[NZ];
-        axis_weights<NX>(sx0, bi, fx, wx);
-        axis_weights<NY>(sy0, bj, fy, wy);
-        axis_weights<NZ>(sz0, bk, fz, wz);
+        const float2 vv = make_float2(vc, vc);
+        if (COMP == 0) {
+            // faces along the component's axis: the base is the cell's own face,
+            // or the next one for a particle beyond the grid's far edge (whose
+            // cell key is clamped); the other two axes' bases are always the
+            // face below the cell or the cell's own (axis3)
+            const float2 wa = bi == sx0 ? make_float2(1.0f - fx, fx) : make_float2(0.0f, 1.0f - fx);
+            float wy[3], wz[3];
+            axis3(sy0, bj, fy, wy);
+            axis3(sz0, bk, fz, wz);
 #pragma unroll
-        for (int c = 0; c < NZ; ++c)
+            for (int b = 0; b < 3; ++b) {
+                if (!((MA >> b) & 1)) continue;
+                const float2 wab = f2_mul(wa, make_float2(wy[b], wy[b]));
 #pragma unroll
-            for (int b = 0; b < NY; ++b)
-#pragma unroll
-                for (int a = 0; a < NX; ++a) {
-                    const float wgt = wx[a] * wy[b] * wz[c];
-                    const int m = a + NX * (b + NY * c);
-                    an[m] += __fmul_rn(vc, wgt);
-                    ad[m] += wgt;
+                for (int c = 0; c < 3; ++c) {
+                    if (!((MB >> c) & 1)) continue;
+                    const float2 wgt = f2_mul(wab, make_float2(wz[c], wz[c]));
+                    an[b + 3 * c] = f2_fma(vv, wgt, an[b + 3 * c]);
+                    ad[b + 3 * c] = f2_add(ad[b + 3 * c], wgt);
                 }
-    }
-#pragma unroll
-    for (int c = 0; c < NZ; ++c)
-#pragma unroll
-        for (int b = 0; b < NY; ++b)
-#pragma unroll
-            for (int a = 0; a < NX; ++a) {
-                const int m = a + NX * (b + NY * c);
-                const int fi = sx0 + a, fj = sy0 + b, fk = sz0 + c;
-                if (ad[m] == 0.0f || fi < fx0 || fi > fx1 || fj < fy0 || fj > fy1 || fk < fz0 || fk > fz1) continue;
-                const int sidx = (fi - fx0) + lsx * ((fj - fy0) + lsy * (fk - fz0));
-                atomicAdd(&s_num[sidx], an[m]);
-                atomicAdd(&s_den[sidx], ad[m]);
             }
+        } else if (COMP == 1) {
+            const float2 wb = bj == sy0 ? make_float2(1.0f - fy, fy) : make_float2(0.0f, 1.0f - fy);
+            float wx[3], wz[3];
+            axis3(sx0, bi, fx, wx);
+            axis3(sz0, bk, fz, wz);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (!((MA >> a) & 1)) continue;
+                const float2 wab = f2_mul(make_float2(wx[a], wx[a]), wb);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    if (!((MB >> c) & 1)) continue;
+                    const float2 wgt = f2_mul(wab, make_float2(wz[c], wz[c]));
+                    an[a + 3 * c] = f2_fma(vv, wgt, an[a + 3 * c]);
+                    ad[a + 3 * c] = f2_add(ad[a + 3 * c], wgt);
+                }
+            }
+        } else {
+            const float2 wc = bk == sz0 ? make_float2(1.0f - fz, fz) : make_float2(0.0f, 1.0f - fz);
+            float wx[3], wy[3];
+            axis3(sx0, bi, fx, wx);
+            axis3(sy0, bj, fy, wy);
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    if (!((MA >> a) & 1) || !((MB >> b) & 1)) continue;
+                    const float wab = wx[a] * wy[b];
+                    const float2 wgt = f2_mul(make_float2(wab, wab), wc);
+                    an[a + 3 * b] = f2_fma(vv, wgt, an[a + 3 * b]);
+                    ad[a + 3 * b] = f2_add(ad[a + 3 * b], wgt);
+                }
+        }
+    }
+    // owned faces into shared memory: slot m of the pair is face +0 / +1 along
+    // the component's axis
+#pragma unroll
+    for (int m = 0; m < 9; ++m)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int o1 = m % 3, o2 = m / 3;
+            if (!((MA >> o1) & 1) || !((MB >> o2) & 1)) continue;
+            const float num = e ? an[m].y : an[m].x, den = e ? ad[m].y : ad[m].x;
+            const int fi = COMP == 0 ? sx0 + e : sx0 + o1;
+            const int fj = COMP == 1 ? sy0 + e : sy0 + (COMP == 0 ? o1 : o2);
+            const int fk = COMP == 2 ? sz0 + e : sz0 + o2;
+            if (den == 0.0f || fi < fx0 || fi > fx1 || fj < fy0 || fj > fy1 || fk < fz0 || fk > fz1) continue;
+            const int sidx = (fi - fx0) + lsx * ((fj - fy0) + lsy * (fk - fz0));
+            atomicAdd(&s_num[sidx], num);
+            atomicAdd(&s_den[sidx], den);
+        }
 }
 
-// Three CTAs per SM: 80 registers and no spills, against 126 registers and
-// two CTAs unbounded; the walk over a cell's particles is latency-bound.
+// Cell regions of a brick's walk.  R_FULL: the brick's own cells (and the
+// halo's edges and corners), every slot.  A halo cell on one face of the
+// brick reaches only the brick faces next to it: on the low side of axis a
+// the last slot of each non-staggered component along a and the upper face
+// of the component staggered along a; on the high side the first slot, and
+// nothing of the staggered component.
+enum : int { R_FULL = 0, R_XLO, R_XHI, R_YLO, R_YHI, R_ZLO, R_ZHI };
+__host__ __device__ constexpr int region_axis(int R) {
+    return (R == R_XLO || R == R_XHI) ? 0 : (R == R_YLO || R == R_YHI) ? 1 : (R == R_ZLO || R == R_ZHI) ? 2 : -1;
+}
+__host__ __device__ constexpr bool region_low(int R) { return R == R_XLO || R == R_YLO || R == R_ZLO; }
+// axis (0 x, 1 y, 2 z) of component COMP's first (which = 0) or second
+// non-staggered axis
+__host__ __device__ constexpr int other_axis(int COMP, int which) {
+    return COMP == 0 ? 1 + which : (COMP == 1 ? 2 * which : which);
+}
+// slot mask of that axis in region R: all three slots, the last (low side)
+// or the first (high side)
+__host__ __device__ constexpr int region_mask(int R, int COMP, int which) {
+    return region_axis(R) != other_axis(COMP, which) ? 7 : (region_low(R) ? 4 : 1);
+}
+
+// Owned face ranges of a brick (inclusive): cells [i0, ie] x [j0, je] x
+// [k0, ke]; the staggered component of an axis also owns the far boundary
+// face in the last brick of that axis (iue, jve, kwe).
+struct Owned {
+    int i0, ie, iue, j0, je, jve, k0, ke, kwe;
+};
+
+// All three components of one cell's particles in region R.
+template <int R, int BX, int BY, int BZ>
+__device__ __forceinline__ void splat_region(const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                             const int* __restrict__ start, int ci, int cj, int ck, const Dims& g,
+                                             float* s_num, float* s_den, const Owned& o) {
+    constexpr int NU = (BX + 1) * BY * BZ, NV = BX * (BY + 1) * BZ;
+    const int c = ci + cj * g.W + ck * g.W * g.H;
+    const int q0 = start[c], q1 = start[c + 1];
+    if (q0 == q1) return;
+    if (!(R == R_XHI))
+        splat_cell<0, region_mask(R, 0, 0), region_mask(R, 0, 1)>(pos, vel, q0, q1, ci, cj, ck, g, s_num, s_den, o.i0,
+                                                                 o.iue, o.j0, o.je, o.k0, o.ke, BX + 1, BY);
+    if (!(R == R_YHI))
+        splat_cell<1, region_mask(R, 1, 0), region_mask(R, 1, 1)>(pos, vel, q0, q1, ci, cj, ck, g, s_num + NU,
+                                                                 s_den + NU, o.i0, o.ie, o.j0, o.jve, o.k0, o.ke, BX,
+                                                                 BY + 1);
+    if (!(R == R_ZHI))
+        splat_cell<2, region_mask(R, 2, 0), region_mask(R, 2, 1)>(pos, vel, q0, q1, ci, cj, ck, g, s_num + NU + NV,
+                                                                 s_den + NU + NV, o.i0, o.ie, o.j0, o.je, o.k0, o.kwe,
+                                                                 BX, BY);
+}
+
+// CTAs per SM that the register budget must allow (P2G_MIN_BLOCKS, a build
+// tunable): 3 gives 80 registers, 2 gives up to 128; the walk over a cell's
+// particles is latency-bound, so occupancy and spills trade against each other.
+#ifndef P2G_MIN_BLOCKS
+#define P2G_MIN_BLOCKS 3
+#endif
 template <int BX, int BY, int BZ, int NT>
-__global__ void __launch_bounds__(NT, 3) k_p2g(const float4* __restrict__ pos, const float4* __restrict__ vel,
+__global__ void __launch_bounds__(NT, P2G_MIN_BLOCKS) k_p2g(const float4* __restrict__ pos, const float4* __restrict__ vel,
                                             const int* __restrict__ start, Dims g, float dt, float3 grav,
                                             float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
                                             float* __restrict__ us, float* __restrict__ vs, float* __restrict__ ws,
@@ -128,21 +259,44 @@ __global__ void __launch_bounds__(NT, 3) k_p2g(const float4* __restrict__ pos, c
     const int kwe = (k0 + BZ >= D) ? D : ke;
     __syncthreads();
 
-    // Cells whose particles reach an owned face: the brick plus one halo cell.
-    const int ilo = max(i0 - 1, 0), ihi = min(i0 + BX, W - 1);
-    const int jlo = max(j0 - 1, 0), jhi = min(j0 + BY, H - 1);
-    const int klo = max(k0 - 1, 0), khi = min(k0 + BZ, D - 1);
-    const int ni = ihi - ilo + 1, nj = jhi - jlo + 1, ncell = ni * nj * (khi - klo + 1);
-    for (int t = threadIdx.x; t < ncell; t += NT) {
-        const int ci = ilo + t % ni, cj = jlo + (t / ni) % nj, ck = klo + t / (ni * nj);
-        const int c = ci + cj * W + ck * W * H;
-        const int q0 = start[c], q1 = start[c + 1];
-        if (q0 == q1) continue;
-        splat_cell<0, 2, 3, 3>(pos, vel, q0, q1, ci, cj, ck, g, s_num, s_den, i0, iue, j0, je, k0, ke, BX + 1, BY);
-        splat_cell<1, 3, 2, 3>(pos, vel, q0, q1, ci, cj, ck, g, s_num + NU, s_den + NU, i0, ie, j0, jve, k0, ke, BX,
-                               BY + 1);
-        splat_cell<2, 3, 3, 2>(pos, vel, q0, q1, ci, cj, ck, g, s_num + NU + NV, s_den + NU + NV, i0, ie, j0, je, k0,
-                               kwe, BX, BY);
+    // Cells whose particles reach an owned face: the brick plus one halo
+    // cell.  The brick's cells first, then each face of the halo shell with
+    // the slots it can reach (a region per loop, so a warp's cells share
+    // their region), then the shell's edges and corners with every slot.
+    const Owned own{i0, ie, iue, j0, je, jve, k0, ke, kwe};
+    const int bxe = ie - i0 + 1, bye = je - j0 + 1, bze = ke - k0 + 1;
+    for (int t = threadIdx.x; t < bxe * bye * bze; t += NT)
+        splat_region<R_FULL, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + (t / bxe) % bye, k0 + t / (bxe * bye), g,
+                                         s_num, s_den, own);
+    if (i0 > 0)
+        for (int t = threadIdx.x; t < bye * bze; t += NT)
+            splat_region<R_XLO, BX, BY, BZ>(pos, vel, start, i0 - 1, j0 + t % bye, k0 + t / bye, g, s_num, s_den, own);
+    if (ie + 1 < W)
+        for (int t = threadIdx.x; t < bye * bze; t += NT)
+            splat_region<R_XHI, BX, BY, BZ>(pos, vel, start, ie + 1, j0 + t % bye, k0 + t / bye, g, s_num, s_den, own);
+    if (j0 > 0)
+        for (int t = threadIdx.x; t < bxe * bze; t += NT)
+            splat_region<R_YLO, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 - 1, k0 + t / bxe, g, s_num, s_den, own);
+    if (je + 1 < H)
+        for (int t = threadIdx.x; t < bxe * bze; t += NT)
+            splat_region<R_YHI, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, je + 1, k0 + t / bxe, g, s_num, s_den, own);
+    if (k0 > 0)
+        for (int t = threadIdx.x; t < bxe * bye; t += NT)
+            splat_region<R_ZLO, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + t / bxe, k0 - 1, g, s_num, s_den, own);
+    if (ke + 1 < D)
+        for (int t = threadIdx.x; t < bxe * bye; t += NT)
+            splat_region<R_ZHI, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + t / bxe, ke + 1, g, s_num, s_den, own);
+    {
+        const int ilo = max(i0 - 1, 0), ihi = min(ie + 1, W - 1);
+        const int jlo = max(j0 - 1, 0), jhi = min(je + 1, H - 1);
+        const int klo = max(k0 - 1, 0), khi = min(ke + 1, D - 1);
+        const int ni = ihi - ilo + 1, nj = jhi - jlo + 1, ncell = ni * nj * (khi - klo + 1);
+        for (int t = threadIdx.x; t < ncell; t += NT) {
+            const int ci = ilo + t % ni, cj = jlo + (t / ni) % nj, ck = klo + t / (ni * nj);
+            const int outside = (ci < i0 || ci > ie) + (cj < j0 || cj > je) + (ck < k0 || ck > ke);
+            if (outside < 2) continue;  // the brick's cells and the halo faces are done
+            splat_region<R_FULL, BX, BY, BZ>(pos, vel, start, ci, cj, ck, g, s_num, s_den, own);
+        }
     }
     __syncthreads();
 

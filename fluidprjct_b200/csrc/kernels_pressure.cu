@@ -166,7 +166,6 @@ struct PcgArgs {
     PcgOut* out;
     double tol;
     int maxit;
-    long long wait_polls;  // grid-barrier poll limit
 };
 
 // Jacobi-preconditioned conjugate gradients in the Chronopoulos-Gear form
@@ -201,7 +200,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
         a.P[n] = T(0);
         a.X[n] = T(0);
     }
-    if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
+    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
     // Init 2: u0 = M^-1 r0, w0 = A u0; partials (r,u), (w,u), (r,r).
     {
         double g_l = 0.0, d_l = 0.0, rr_l = 0.0;
@@ -224,7 +223,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
         double* pp = a.part + 3 * nb;  // parity 1
         if (threadIdx.x == 0) { pp[blockIdx.x] = bs.x; pp[nb + blockIdx.x] = bs.y; pp[2 * nb + blockIdx.x] = bs.z; }
     }
-    if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
+    if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
     double3 tot = grid_sum3(a.part + 3 * nb, nb);
     double gam = tot.x, del = tot.y, rr = tot.z;
     const double bb = tot.z;
@@ -273,7 +272,7 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
         double3 bs = block_sum3(g_l, d_l, rr_l);
         double* pp = a.part + (it & 1) * 3 * nb;
         if (threadIdx.x == 0) { pp[blockIdx.x] = bs.x; pp[nb + blockIdx.x] = bs.y; pp[2 * nb + blockIdx.x] = bs.z; }
-        if (!grid_barrier(a.bar, unsigned(nb), a.status, a.wait_polls)) return;
+        if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
         tot = grid_sum3(pp, nb);
         ++it;
         if (isnan(tot.x) || isnan(tot.y) || isnan(tot.z)) { st = DEV_NAN; rr = tot.z; break; }
@@ -295,9 +294,9 @@ __global__ void __launch_bounds__(PCG_THREADS) k_pcg_cg(PcgArgs<T> a) {
     }
 }
 
-__global__ void k_reset_pcg(GridBar* bar, int* status) {
+__global__ void k_reset_pcg(GridBar* bar, int* status, unsigned limit) {
     bar->count = 0;
-    bar->gen = 0;
+    bar->limit = limit;
     *status = DEV_OK;
 }
 
@@ -490,10 +489,10 @@ int pcg_max_blocks() {
 
 template <class T>
 static int launch_pcg_t(Dims g, PressureBufs& pb, const float* rhs, double tol, int maxit, cudaStream_t st,
-                        long long wait_polls) {
+                        unsigned wait_polls) {
     const int nb = pcg_max_blocks();
     int* status = &pb.out->status;
-    k_reset_pcg<<<1, 1, 0, st>>>(pb.bar, status);
+    k_reset_pcg<<<1, 1, 0, st>>>(pb.bar, status, wait_polls);
     PcgArgs<T> a;
     a.g = g; a.nf = pb.nf; a.fidx = pb.fidx; a.diag = pb.diag; a.b = rhs;
     for (int i = 0; i < 2; ++i) {
@@ -506,14 +505,17 @@ static int launch_pcg_t(Dims g, PressureBufs& pb, const float* rhs, double tol, 
     a.X = static_cast<T*>(pb.X);
     a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;
     a.tol = tol; a.maxit = maxit;
-    a.wait_polls = wait_polls;
     void* args[] = {&a};
     cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_cg<T>, dim3(nb), dim3(PCG_THREADS), args, 0, st);
     return e == cudaSuccess ? 0 : int(e);
 }
 
+void launch_reset_barrier(GridBar* bar, int* status, unsigned wait_polls, cudaStream_t st) {
+    k_reset_pcg<<<1, 1, 0, st>>>(bar, status, wait_polls);
+}
+
 int launch_pcg(Dims g, PressureBufs& pb, const float* rhs, int fp64, double tol, int maxit, cudaStream_t st,
-               long long wait_polls) {
+               unsigned wait_polls) {
     return fp64 ? launch_pcg_t<double>(g, pb, rhs, tol, maxit, st, wait_polls)
                 : launch_pcg_t<float>(g, pb, rhs, tol, maxit, st, wait_polls);
 }

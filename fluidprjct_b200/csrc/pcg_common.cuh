@@ -12,13 +12,13 @@ namespace {
 // Grid barrier for a cooperative launch on one 32-bit word: every block adds
 // 1 except block 0, which adds 2^31 - (nblocks - 1), so the word's top bit
 // flips exactly when the last block arrives and no reset is needed between
-// barriers.  The wait is bounded: after `limit` polls (kDefaultWaitPolls =
+// barriers.  The wait is bounded: after bar->limit polls (kDefaultWaitPolls =
 // 2^27 unless the solver's owner set another limit) the block records
 // DEV_TIMEOUT and leaves; callers check the status after every barrier and
 // return, so no block waits forever.  The arrival is a release atomic and the
 // poll an acquire load (the pattern of a release-acquire grid barrier), so
 // plain loads after it see every write made before it by any block.
-__device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* status, long long limit) {
+__device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* status) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -34,15 +34,18 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int
                      : "=r"(old)
                      : "l"(&bar->count), "r"(inc)
                      : "memory");
-        long long polls = 0;
         bool ok = st0 == DEV_OK;
-        for (;;) {
+        // polls left before giving up (at least 1), read when the first poll
+        // finds the barrier still closed
+        unsigned left = 0;
+        for (bool first = true;; first = false) {
             // acquire load: writes published by the other blocks' arrivals are
             // visible to this block once the top bit has flipped
             unsigned cur;
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(cur) : "l"(&bar->count) : "memory");
             if (((old ^ cur) & 0x80000000u) != 0u) break;
-            if (++polls >= limit) {
+            if (first) left = *(volatile unsigned*)&bar->limit;
+            if (--left == 0u) {
                 atomicExch(status, DEV_TIMEOUT);
                 ok = false;
                 break;

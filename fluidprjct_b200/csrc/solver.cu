@@ -112,7 +112,7 @@ struct fp_solver {
     cudaEvent_t ev_pcg[2]{};
     int64_t launches = 0;   // kernels launched by this solver
     float pcg_ms = 0.0f;
-    long long wait_polls = kDefaultWaitPolls;  // grid-barrier poll limit (fp_set_wait_limit)
+    unsigned wait_polls = kDefaultWaitPolls;  // grid-barrier poll limit (fp_set_wait_limit)
     bool have_grid = false;
 
     // grids
@@ -236,6 +236,11 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     free_grid(s);
     s->W = W; s->H = H; s->D = D;
     s->g = Dims{W, H, D, s->cfg.dx};
+    {
+        // dx a power of two: its reciprocal is exact, and x * (1/dx) == x / dx
+        int ex = 0;
+        if (std::frexp(double(s->cfg.dx), &ex) == 0.5) s->g.idx = float(1.0 / double(s->cfg.dx));
+    }
     const int64_t nc = s->g.nc();
     s->padded = int64_t(W + 2) * (H + 2) * (D + 2);
     const int ntiles = int((nc + 4095) / 4096) + 1;
@@ -715,7 +720,8 @@ void phase_g2p_advect(fp_solver* s, int do_g2p, int do_adv, bool guarded = false
     const BodyShape b = sdf ? body_shape(s) : BodyShape{};
     launch_g2p_advect(s->d_pos, s->d_vel, s->np, s->d_u, s->d_v, s->d_w, s->d_us, s->d_vs, s->d_ws, s->d_labels, s->g,
                       s->cfg.pic_weight, s->cfg.dt, s->cfg.cfl, do_g2p, do_adv, s->cfg.advection == FP_ADVECT_RK2,
-                      s->st, guarded ? &s->pb.out->status : nullptr, sdf ? &b : nullptr);
+                      s->st, guarded ? &s->pb.out->status : nullptr, sdf ? &b : nullptr,
+                      s->sorted ? s->d_start : nullptr);
     if (do_adv) s->sorted = false;
 }
 
@@ -1663,7 +1669,8 @@ void* fp_cuda_stream(const fp_solver* s) { return s ? static_cast<void*>(s->st) 
 
 int fp_set_wait_limit(fp_solver* s, int64_t polls) {
     if (!s || polls < 0) return s ? s->fail(FP_ERR_ARG, "negative wait limit") : FP_ERR_ARG;
-    s->wait_polls = polls == 0 ? kDefaultWaitPolls : static_cast<long long>(polls);
+    if (polls > 0xFFFFFFFFll) return s->fail(FP_ERR_ARG, "wait limit above 2^32 - 1 polls");
+    s->wait_polls = polls == 0 ? kDefaultWaitPolls : static_cast<unsigned>(polls);
     return FP_OK;
 }
 
