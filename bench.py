@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--frames", type=int, default=0,
                     help="also time fp_run's frame output (binary and ASCII PLY) over this many frames")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
-    ap.add_argument("--solver", default="pcg_mg", choices=["pcg", "pcg_mixed", "pcg_mg", "pcg_learned"],
+    ap.add_argument("--solver", default="pcg_mg", choices=["pcg", "pcg_mixed", "pcg_mg", "pcg_learned",
+                                                           "pcg_learned_mixed"],
                     help="pressure solver of the timed steps")
     ap.add_argument("--no-parity", action="store_true", help="skip the parity leg against the FP64 oracle")
     ap.add_argument("--no-extra", action="store_true", help="skip the 200-step run and the 16 ppc variant")
@@ -148,7 +149,7 @@ def new_solver(lab, device, solver="pcg", n=N_GRID, ppc=PPC, warm_start=1):
     s = capi.Solver(dx=1.0 / n, dt=DT, pic_weight=PIC, advection="rk2", solver=solver, tol=1e-6, max_iters=20000,
                     device=device, output_format=capi.OUT_NONE, warm_start=warm_start)
     s.set_labels(lab)
-    if solver == "pcg_learned":
+    if solver in ("pcg_learned", "pcg_learned_mixed"):
         from fluidprjct_b200.learned import DEFAULT_WEIGHTS
         s.load_learned(DEFAULT_WEIGHTS)
     s.seed_particles(ppc, SEED)
@@ -288,7 +289,10 @@ def run_ours(args, rank, local, world):
         "pcg_mixed": "pcg_mixed (Jacobi PCG, FP32 stencil/vectors, FP64 reductions, FP64 refinement)",
         "pcg_mg": "pcg_mg (flexible PCG with an FP32 multigrid V-cycle preconditioner, FP64 Krylov vectors and "
                   "reductions, warm-started from the previous step's pressure)",
-        "pcg_learned": "pcg_learned (U-Net initial guess + pcg_mg, plain PCG fallback)",
+        "pcg_learned": "pcg_learned (flexible PCG: the U-Net as the first preconditioner application, the MG "
+                       "V-cycle after it; plain PCG fallback)",
+        "pcg_learned_mixed": "pcg_learned_mixed (the U-Net's scaled guess starts pcg_mixed's FP64 refinement; "
+                             "plain PCG fallback)",
     }[args.solver]
 
     out = {"metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": args.steps,
@@ -312,7 +316,8 @@ def run_ours(args, rank, local, world):
     if not args.no_variants and rank == 0:
         var = {}
         for name, solver, warm in (("pcg", "pcg", 0), ("pcg_mixed", "pcg_mixed", 0), ("pcg_mg", "pcg_mg", 0),
-                                   ("pcg_learned", "pcg_learned", 0), ("pcg_mg_warm", "pcg_mg", 1)):
+                                   ("pcg_learned", "pcg_learned", 0), ("pcg_learned_mixed", "pcg_learned_mixed", 0),
+                                   ("pcg_mg_warm", "pcg_mg", 1)):
             try:
                 v = new_solver(lab, local, solver, args.n, args.ppc, warm)
             except Exception as e:  # variant not available in this build

@@ -19,7 +19,7 @@ FP_OK, FP_ERR_ARG, FP_ERR_IO, FP_ERR_CUDA, FP_ERR_STATE, FP_ERR_NO_FLUID, FP_ERR
     0, -1, -2, -3, -4, -5, -6, -7)
 SOLID, FLUID, AIR, BODY = 0, 1, 2, 3
 OUT_PLY, OUT_OFF, OUT_PLY_BINARY, OUT_NONE = 0, 1, 2, 3
-SOLVER_PCG, SOLVER_PCG_MIXED, SOLVER_PCG_MG, SOLVER_PCG_LEARNED = 0, 1, 2, 3
+SOLVER_PCG, SOLVER_PCG_MIXED, SOLVER_PCG_MG, SOLVER_PCG_LEARNED, SOLVER_PCG_LEARNED_MIXED = 0, 1, 2, 3, 4
 ADVECT_RK3REF, ADVECT_RK2 = 0, 1
 SCHEME_DEFAULT, SCHEME_REF2D = 0, 1
 BODY_FORCES_FACE_FRACTION, BODY_FORCES_REFERENCE = 0, 1
@@ -29,7 +29,7 @@ GRID_U, GRID_V, GRID_W, GRID_U_SAVED, GRID_V_SAVED, GRID_W_SAVED, GRID_P, GRID_R
  PHASE_ADVECT, PHASE_CLEANUP) = range(10)
 
 SOLVER_NAMES = {"pcg": SOLVER_PCG, "pcg_mixed": SOLVER_PCG_MIXED, "pcg_mg": SOLVER_PCG_MG,
-                "pcg_learned": SOLVER_PCG_LEARNED}
+                "pcg_learned": SOLVER_PCG_LEARNED, "pcg_learned_mixed": SOLVER_PCG_LEARNED_MIXED}
 
 
 class FpConfig(C.Structure):

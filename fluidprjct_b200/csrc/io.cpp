@@ -444,6 +444,7 @@ bool load_config_json(const std::string& path, fp_config& cfg, std::string* labe
         else if (s == "pcg_mixed") cfg.solver = FP_SOLVER_PCG_MIXED;
         else if (s == "pcg_mg") cfg.solver = FP_SOLVER_PCG_MG;
         else if (s == "pcg_learned") cfg.solver = FP_SOLVER_PCG_LEARNED;
+        else if (s == "pcg_learned_mixed") cfg.solver = FP_SOLVER_PCG_LEARNED_MIXED;
         else { err = "unknown solver " + s; return false; }
     }
     if (strv("collision", s)) {

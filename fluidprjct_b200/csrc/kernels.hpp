@@ -136,6 +136,9 @@ void launch_true_residual(PressureBufs& pb, int fp64, Dims g, cudaStream_t st);
 // pb.red; x64 += X (FP32) and its padded copy xd.
 void launch_ir_residual(PressureBufs& pb, Dims g, cudaStream_t st);
 void launch_ir_update(PressureBufs& pb, Dims g, cudaStream_t st);
+// Scales the refinement's starting point x64 (and xd) by its energy-optimal
+// factor (x, b) / (x, A x), computed in FP64 on the device (3 launches).
+void launch_guess_scale(PressureBufs& pb, Dims g, cudaStream_t st);
 
 // -------- projection (kernels_pressure.cu) --------
 // guard: the status word of the solve that produced p, or null; the kernel

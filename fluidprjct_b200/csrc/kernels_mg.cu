@@ -656,6 +656,14 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     }
     const bool guess = a.x0 || a.pprev;
     double bb_warm = 0.0;  // ||b||^2 when started from a guess
+    // With a guess g the solve's first flexible-CG step uses g as its
+    // preconditioned residual: z0 = g (the network's output N(b), or the
+    // previous pressure), p0 = z0, alpha0 = (r0, z0) / (p0, A p0) -- the
+    // energy-optimal scaling -- and x1 = alpha0 g.  p0, A p0, gamma0 = (r0, z0)
+    // and (p0, A p0) stay in the recurrence, so the next direction (from the
+    // V-cycle) is made A-conjugate to g by the Polak-Ribiere beta.
+    bool dir0 = false;
+    double gam0 = 0.0, alpha0 = 0.0, den0 = 0.0;
     if (guess) {
         // Scale the guess by its energy-optimal factor alpha = (x0, b) / (x0, A x0):
         // the A-norm error of alpha x0 is never above that of x = 0.  Then r = b - A x.
@@ -675,6 +683,8 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
         const double3 t = total();
         const double alpha = (t.y > 0.0 && isfinite(t.x / t.y)) ? t.x / t.y : 0.0;
+        dir0 = alpha != 0.0;
+        gam0 = t.x; alpha0 = alpha; den0 = t.y;
         bb_warm = t.z;  // all reads of x ended before the barrier above
         rrl = 0.0;
         for (int base = t0, q0 = 0; base < nf; base += UI * st, q0 += UI) {
@@ -692,6 +702,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
                 if (!k.ok[u]) continue;
                 const int c = k.c[u];
                 a.xs[c] = xv[u] * alpha;
+                a.p[c] = xv[u];  // p0 = g; q holds A p0
                 const double rv = rv0[u] - alpha * qc[u];
                 r[c] = rv;
                 b0[c] = float(rv);
@@ -718,7 +729,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     // compact X buffer (the solution is written there only at the end); s
     // lives in q.
     double* w = a.X;
-    double gam = 0.0, gam_old = 0.0, alpha_old = 1.0, den_old = 1.0;
+    double gam = 0.0, gam_old = gam0, alpha_old = dir0 ? alpha0 : 1.0, den_old = dir0 ? den0 : 1.0;
     int it = 0, stt = DEV_OK;
     while (rr > thr && bb > 0.0) {
         if (it >= a.maxit) { stt = DEV_MAXIT; break; }
@@ -755,8 +766,9 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         const double3 t = total();
         gam = t.x;
         if (isnan(t.x) || isnan(t.y) || isnan(t.z)) { stt = DEV_NAN; break; }
-        const double beta = it > 0 ? -alpha_old * t.z / gam_old : 0.0;
-        const double den = it > 0 ? t.y + beta * (2.0 * t.z + beta * den_old) : t.y;
+        const bool coupled = it > 0 || dir0;  // a previous direction to conjugate against
+        const double beta = coupled ? -alpha_old * t.z / gam_old : 0.0;
+        const double den = coupled ? t.y + beta * (2.0 * t.z + beta * den_old) : t.y;
         if (!(den > 0.0)) { stt = DEV_BREAKDOWN; break; }
         const double alpha = gam / den;
         rrl = 0.0;
@@ -780,8 +792,8 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
             for (int u = 0; u < U2; ++u) {
                 if (!k.ok[u]) continue;
                 const int c = k.c[u];
-                const double pn = it > 0 ? double(zc[u]) + beta * pv[u] : double(zc[u]);
-                const double sn = it > 0 ? wv[u] + beta * sv[u] : wv[u];
+                const double pn = coupled ? double(zc[u]) + beta * pv[u] : double(zc[u]);
+                const double sn = coupled ? wv[u] + beta * sv[u] : wv[u];
                 a.p[c] = pn;
                 a.q[c] = sn;
                 a.xs[c] = xv[u] + alpha * pn;

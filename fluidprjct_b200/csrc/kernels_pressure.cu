@@ -360,6 +360,38 @@ __global__ void k_sum_partials(const double2* __restrict__ part, int nb, double*
     if (threadIdx.x == 0) { out[0] = s.x; out[1] = s.y; }
 }
 
+// Partials of (x, b) and (x, A x) over the padded dense guess xd (FP64).
+__global__ void __launch_bounds__(256) k_guess_dots(const int* __restrict__ nf_p, const int* __restrict__ fidx,
+                                                    const uint8_t* __restrict__ diag, const float* __restrict__ b,
+                                                    const double* __restrict__ xd, Dims g, double2* __restrict__ part) {
+    const int nf = *nf_p;
+    const int sy = g.W + 2, sz = (g.W + 2) * (g.H + 2);
+    double xb = 0.0, xax = 0.0;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) {
+        const double* x = xd + fidx[n];
+        const double ax = double(diag[n] & 0x7F) * x[0] - ((x[1] + x[-1]) + (x[sy] + x[-sy]) + (x[sz] + x[-sz]));
+        xb += x[0] * double(b[n]);
+        xax += x[0] * ax;
+    }
+    double2 s = block_sum2(xb, xax);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// x64 and its padded copy xd scaled by alpha = (x, b) / (x, A x) (red[0..1]),
+// 0 when (x, A x) is not positive: the A-norm error of alpha x is never above
+// that of x = 0.
+__global__ void k_scale_guess(const int* __restrict__ nf_p, const int* __restrict__ fidx, const double* __restrict__ red,
+                              double* __restrict__ x64, double* __restrict__ xd) {
+    const int nf = *nf_p;
+    const double d = red[1];
+    const double alpha = (d > 0.0 && isfinite(red[0] / d)) ? red[0] / d : 0.0;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < nf; n += gridDim.x * blockDim.x) {
+        const double v = x64[n] * alpha;
+        x64[n] = v;
+        xd[fidx[n]] = v;
+    }
+}
+
 __global__ void k_ir_update(const int* __restrict__ nf_p, const int* __restrict__ fidx, const float* __restrict__ c,
                             double* __restrict__ x64, double* __restrict__ xd) {
     const int nf = *nf_p;
@@ -560,6 +592,14 @@ void launch_ir_residual(PressureBufs& pb, Dims g, cudaStream_t st) {
     auto* part = reinterpret_cast<double2*>(pb.part);
     k_residual<double><<<nb, 256, 0, st>>>(pb.nf, pb.fidx, pb.diag, pb.b, pb.xd, g, part, pb.bin, nullptr);
     k_sum_partials<<<1, 32, 0, st>>>(part, nb, pb.red);
+}
+
+void launch_guess_scale(PressureBufs& pb, Dims g, cudaStream_t st) {
+    const int nb = 592;
+    auto* part = reinterpret_cast<double2*>(pb.part);
+    k_guess_dots<<<nb, 256, 0, st>>>(pb.nf, pb.fidx, pb.diag, pb.b, pb.xd, g, part);
+    k_sum_partials<<<1, 32, 0, st>>>(part, nb, pb.red);
+    k_scale_guess<<<592, 256, 0, st>>>(pb.nf, pb.fidx, pb.red, pb.x64, pb.xd);
 }
 
 void launch_ir_update(PressureBufs& pb, Dims g, cudaStream_t st) {

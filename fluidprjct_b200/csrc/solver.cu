@@ -266,7 +266,8 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     ck(dalloc(&pb.bar, 1)); ck(dalloc(&pb.out, 1)); ck(dalloc(&pb.red, 2));
     pb.tile_sums = s->d_tiles;
     ck(dalloc(&s->d_rhs_dense, nc));
-    if (s->cfg.solver == FP_SOLVER_PCG_LEARNED) ck(dalloc(&s->d_x0c, nc));
+    if (s->cfg.solver == FP_SOLVER_PCG_LEARNED || s->cfg.solver == FP_SOLVER_PCG_LEARNED_MIXED)
+        ck(dalloc(&s->d_x0c, nc));
     if (s->cfg.solver == FP_SOLVER_PCG_MG || s->cfg.solver == FP_SOLVER_PCG_LEARNED) {
         s->mgL = mg_levels_for(W, H, D, s->mg);
         for (int l = 0; l < s->mgL && e == cudaSuccess; ++l) {
@@ -503,15 +504,38 @@ int solve_system(fp_solver* s, float* p_out, bool defer = false) {
             }
         }
     } else {
+        // FP_SOLVER_PCG_MIXED, or FP_SOLVER_PCG_LEARNED_MIXED: the same
+        // refinement started from the network's guess (energy-optimally scaled)
+        const bool learned = s->cfg.solver == FP_SOLVER_PCG_LEARNED_MIXED;
+        if (learned && !s->net) return s->fail(FP_ERR_STATE, "learned solver: no weights loaded (fp_load_learned)");
         cudaMemsetAsync(pb.x64, 0, sizeof(double) * s->g.nc(), s->st);
-        launch_ir_residual(pb, s->g, s->st);  // x64 = 0: bin = b
+        if (learned) {
+            cudaEventRecord(s->ev_pcg[0], s->st);
+            const unet::Lvl real{s->W, s->H, s->D};
+            unet::launch_rhs_dense(pb.nf, pb.fidx, real, pb.b, s->d_rhs_dense, s->st);
+            if (unet::forward_on(s->net, s->d_labels, s->d_rhs_dense, s->st))
+                return s->cuda_fail(cudaGetLastError(), "U-Net forward");
+            unet::launch_output_compact(pb.nf, pb.fidx, real, unet::net_level0(s->net), unet::net_out(s->net),
+                                        unet::net_scal(s->net), s->d_x0c, s->st);
+            // x64 = xd = guess (xd is zero between solves), then scaled by (x, b) / (x, A x)
+            cudaMemcpyAsync(pb.X, s->d_x0c, sizeof(float) * size_t(s->g.nc()), cudaMemcpyDeviceToDevice, s->st);
+            launch_ir_update(pb, s->g, s->st);
+            launch_guess_scale(pb, s->g, s->st);
+            cudaEventRecord(s->ev_net, s->st);
+            s->launches += 1 + 16 + 1 + 1 + 3;  // rhs scatter, network, guess, copy-in, scaling
+            cudaMemcpyAsync(s->h_bad, unet::net_status(s->net), sizeof(int), cudaMemcpyDeviceToHost, s->st);
+        }
+        launch_ir_residual(pb, s->g, s->st);  // bin = b - A x64 (= b from x64 = 0)
         s->launches += 3;
         cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
         cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
         ce = cudaStreamSynchronize(s->st);
         if (ce != cudaSuccess) return s->cuda_fail(ce, "refinement residual");
+        if (learned && *s->h_bad) return s->fail(FP_ERR_TIMEOUT, "U-Net forward: a bounded tensor-core wait gave up");
+        if (learned) cudaEventElapsedTime(&learned_ms, s->ev_pcg[0], s->ev_net);
         const double bb = s->h_red[1];
         double relres = bb > 0 ? std::sqrt(s->h_red[0] / bb) : 0.0;
+        if (learned) guess_relres = float(relres);
         while (relres > tol && outer < 12 && inner_total < maxit) {
             // Inner accuracy: enough to land below tol after this update, but
             // not below what FP32 vectors can resolve.
@@ -546,6 +570,29 @@ int solve_system(fp_solver* s, float* p_out, bool defer = false) {
         if (relres > tol && dev_status == DEV_OK) dev_status = DEV_MAXIT;
         // xd must be zero at the start of the next solve
         cudaMemsetAsync(pb.xd, 0, sizeof(double) * size_t(s->padded), s->st);
+        pcg_ms += learned_ms;
+        if (learned && *s->h_nf > 0 && dev_status != DEV_TIMEOUT && dev_status != DEV_OK) {
+            // the refinement from the learned guess stalled: plain FP64 PCG from zero
+            fallback = 1;
+            cudaEventRecord(s->ev_pcg[0], s->st);
+            const int e = launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st, s->wait_polls);
+            cudaEventRecord(s->ev_pcg[1], s->st);
+            if (e) return s->cuda_fail(cudaError_t(e), "cooperative PCG launch");
+            launch_scatter_p(pb, p_out, 1, s->g, s->st);
+            launch_true_residual(pb, 1, s->g, s->st);
+            launch_pcg_clear(pb, 1, 1, s->st);
+            s->launches += 1 + 1 + 1 + 3 + 1;
+            cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
+            cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
+            ce = cudaStreamSynchronize(s->st);
+            if (ce != cudaSuccess) return s->cuda_fail(ce, "pressure solve (fallback)");
+            inner_total += s->h_out->iters;
+            dev_status = s->h_out->status;
+            ++outer;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, s->ev_pcg[0], s->ev_pcg[1]);
+            pcg_ms += ms;
+        }
     }
     return solve_tail(s, inner_total, outer, dev_status, pcg_ms, learned_ms, guess_relres, fallback);
 }
@@ -1070,7 +1117,7 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     if (!s) return FP_ERR_ARG;
     if (cfg) s->cfg = *cfg; else fp_config_default(&s->cfg);
     if (!(s->cfg.dx > 0) || !(s->cfg.dt > 0) || (s->cfg.dim != 2 && s->cfg.dim != 3)) { delete s; return FP_ERR_ARG; }
-    if (s->cfg.solver < FP_SOLVER_PCG || s->cfg.solver > FP_SOLVER_PCG_LEARNED) {
+    if (s->cfg.solver < FP_SOLVER_PCG || s->cfg.solver > FP_SOLVER_PCG_LEARNED_MIXED) {
         std::fprintf(stderr, "fp_create: solver %d is not available in this build\n", s->cfg.solver);
         delete s;
         return FP_ERR_ARG;

@@ -112,7 +112,7 @@ def compare_solvers(labels, rhs, weights, tol=1e-6, dx=None, repeats=3, names=("
     for name in names:
         s = capi.Solver(dim=3, dx=dx, dt=0.002, solver=name, tol=tol, output_format=capi.OUT_NONE)
         s.set_labels(labels)
-        if name == "pcg_learned":
+        if name in ("pcg_learned", "pcg_learned_mixed"):
             s.load_learned(weights)
         times, its = [], []
         for _ in range(repeats):

@@ -61,12 +61,18 @@ enum { FP_OUT_PLY = 0, FP_OUT_OFF = 1, FP_OUT_PLY_BINARY = 2, FP_OUT_NONE = 3 };
  *   FP_SOLVER_PCG_MIXED   FP32 stencil and vectors with FP64 reductions, inside
  *                         an FP64 iterative-refinement loop (true residual
  *                         recomputed in FP64);
- *   FP_SOLVER_PCG_MG      FP32 geometric-multigrid V-cycle preconditioner, FP64
- *                         Krylov vectors and reductions; warm-started from the
- *                         previous step's pressure (warm_start);
- *   FP_SOLVER_PCG_LEARNED a learned U-Net's pressure guess as the initial
- *                         iterate of the MG solve, plain PCG fallback. */
-enum { FP_SOLVER_PCG = 0, FP_SOLVER_PCG_MIXED = 1, FP_SOLVER_PCG_MG = 2, FP_SOLVER_PCG_LEARNED = 3 };
+ *   FP_SOLVER_PCG_MG      flexible PCG with an FP32 geometric-multigrid V-cycle
+ *                         preconditioner, FP64 Krylov vectors and reductions;
+ *                         its first direction is the previous step's pressure
+ *                         (warm_start);
+ *   FP_SOLVER_PCG_LEARNED flexible PCG whose first preconditioner application
+ *                         is a learned U-Net (z0 = N(b)) and whose later ones
+ *                         are the V-cycle; plain PCG fallback;
+ *   FP_SOLVER_PCG_LEARNED_MIXED the U-Net's guess, energy-optimally scaled, as
+ *                         the starting point of FP_SOLVER_PCG_MIXED's FP64
+ *                         refinement ("learned + mixed"); plain PCG fallback. */
+enum { FP_SOLVER_PCG = 0, FP_SOLVER_PCG_MIXED = 1, FP_SOLVER_PCG_MG = 2, FP_SOLVER_PCG_LEARNED = 3,
+       FP_SOLVER_PCG_LEARNED_MIXED = 4 };
 
 /* Advection: the reference's adaptive Ralston RK3 (AdvectParticlesFunctor,
  * FluidSolver3D.cu:1241-1330) or midpoint RK2 with the same substepping. */

@@ -179,7 +179,8 @@ def test_committed_weights_gain_on_a_heldout_128_scene(tmp_path):
     held = learned.generate(n=128, scenes=1, steps_per_scene=16, seed=4242)
     lab = held[0][15].cpu().numpy()
     rhs = held[1][15].cpu().numpy()
-    r = learned.compare_solvers(lab, rhs, learned.DEFAULT_WEIGHTS, repeats=1)
+    r = learned.compare_solvers(lab, rhs, learned.DEFAULT_WEIGHTS, repeats=1,
+                                names=("pcg", "pcg_mg", "pcg_learned", "pcg_mixed", "pcg_learned_mixed"))
     untrained = tmp_path / "untrained.bin"
     capi.UNet(8, 8, 8, seed=9).save(untrained)
     r0 = learned.compare_solvers(lab, rhs, str(untrained), repeats=1, names=("pcg_learned",))
@@ -188,4 +189,8 @@ def test_committed_weights_gain_on_a_heldout_128_scene(tmp_path):
         assert v["status"] == 0 and v["residual"] <= 1e-6 and v["fallback"] == 0
     assert r["pcg_learned"]["guess_relres"] < 0.6
     assert r0["pcg_learned"]["guess_relres"] > 0.8
+    # the network as the first flexible-CG preconditioner saves MG iterations ...
     assert r["pcg_learned"]["iters"] < r["pcg_mg"]["iters"]
+    # ... and, as the start of the mixed-precision refinement, inner FP32 iterations
+    assert r["pcg_learned_mixed"]["guess_relres"] < 0.6
+    assert r["pcg_learned_mixed"]["iters"] < r["pcg_mixed"]["iters"]
