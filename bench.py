@@ -369,6 +369,7 @@ def run_ours(args, rank, local, world):
     if not args.no_extra and rank == 0:
         out["run_200_steps"] = timed_run(lab, local, args, 200, 0, args.ppc)
         out["ppc16"] = timed_run(lab, local, args, 20, 5, 16)
+        out["other_configs"] = other_configs(local)
 
     # ---- parity of the timed scene against the FP64 oracle (rank 0, N = 1) ----
     if not args.no_parity and rank == 0 and world == 1:
@@ -410,6 +411,55 @@ def timed_run(lab, device, args, steps, warmup, ppc):
     return {"steps": steps, "warmup": warmup, "ppc": ppc, "particles": int(n), "ms": round(ms, 3),
             "steps_per_s": round(steps / (ms / 1000.0), 2), "ns_per_particle_step": round(ms * 1e6 / steps / n, 4),
             "last_step_pcg_iters": st["pcg_iters"], "last_step_residual": st["residual"]}
+
+
+def _time_steps(s, steps, warmup):
+    stream, Ev = event_timer(s.stream)
+    s.step(warmup)
+    e0, e1 = Ev(), Ev()
+    e0.record(stream)
+    s.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = s.stats()
+    return {"steps": steps, "warmup": warmup, "particles": int(s.num_particles), "ms_per_step": round(ms / steps, 4),
+            "steps_per_s": round(steps / (ms / 1000.0), 2), "last_pcg_iters": st["pcg_iters"],
+            "last_residual": st["residual"], "solve_status": st["solve_status"]}
+
+
+def other_configs(device):
+    """Device-timed steps of the other configurations of the benchmark table
+    (each from its seeded state; the warm-up steps are not timed):
+    the 2D dam break (64^2, 4 ppc seed 0, dt 0.005, FLIP 0.95, the reference's
+    2D step), the rigid-body drop (160^3 pool to y < 0.35, 8 ppc seed 2, sphere
+    r 0.12 at half density from (0.5, 0.7, 0.5), SDF collision) and the seabed
+    scene (256 x 128 x 256, paddle amplitude 0.05 period 1 s, 8 ppc seed 4,
+    dt 0.001)."""
+    from fluidprjct_b200 import capi, scenes
+    res = {}
+    s = capi.Solver(dim=2, dx=1 / 64, dt=0.005, pic_weight=0.05, solver="pcg_mg", tol=1e-6, scheme="ref2d",
+                    device=device, output_format=capi.OUT_NONE)
+    s.set_labels(scenes.dam_break_2d(64))
+    s.seed_particles(4, 0)
+    res["dam_break_2d_64"] = _time_steps(s, 100, 0)
+    s.close()
+    s = capi.Solver(dx=1 / 160, dt=0.002, pic_weight=0.05, solver="pcg_mg", tol=1e-6, body_radius=0.12,
+                    body_density=0.5, body_pos=(0.5, 0.7, 0.5), active_body=1, advection="rk2", collision="sdf",
+                    device=device, output_format=capi.OUT_NONE)
+    s.set_labels(scenes.pool_3d(160, 0.35))
+    s.load_sdf(None)
+    s.seed_particles(8, 2)
+    res["pool_160_sphere"] = _time_steps(s, 20, 3)
+    s.close()
+    s = capi.Solver(dx=1 / 128, dt=0.001, pic_weight=0.05, solver="pcg_mg", tol=1e-6, advection="rk2", device=device,
+                    output_format=capi.OUT_NONE)
+    s.scene_seabed(256, 128, 256, level=0.45, bed_base=0.15, bed_amp=0.05, seed=4, water_xmin=0.1)
+    s.set_paddle(0.1, 0.05, 1.0)
+    s.seed_particles(8, 4)
+    res["seabed_256x128x256_paddle"] = _time_steps(s, 20, 3)
+    s.close()
+    return res
 
 
 def parity_leg(lab, device, args):

@@ -128,6 +128,9 @@ _SIGS = {
     "fp_stats": (C.c_int, [_P, _P]),
     "fp_cuda_stream": (C.c_void_p, [_P]),
     "fp_set_wait_limit": (C.c_int, [_P, C.c_int64]),
+    "fp_set_step_log": (C.c_int, [_P, C.c_char_p]),
+    "fp_save_state": (C.c_int, [_P, C.c_char_p]),
+    "fp_load_state": (C.c_int, [_P, C.c_char_p]),
     "fp_pressure_solve": (C.c_int, [_P, _P, _P, C.c_int64, _P, _P]),
     "fp_solve_csr_upper": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, C.c_double, C.c_int, _P, _P]),
     "fp_solve_csr_upper_noalloc": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, C.c_double, C.c_int, _P, _P, _P]),
@@ -345,6 +348,16 @@ class Solver:
     def stream(self) -> int:
         """The solver's cudaStream_t as an integer handle."""
         return lib().fp_cuda_stream(self._h) or 0
+
+    def set_step_log(self, path=None):
+        """One JSON line of statistics per step to path (None closes the log)."""
+        return self._check(lib().fp_set_step_log(self._h, None if path is None else str(path).encode()))
+
+    def save_state(self, path):
+        return self._check(lib().fp_save_state(self._h, str(path).encode()))
+
+    def load_state(self, path):
+        return self._check(lib().fp_load_state(self._h, str(path).encode()))
 
     def set_wait_limit(self, polls: int):
         """Polls after which a grid-barrier wait of the pressure solvers gives

@@ -21,6 +21,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/fluidprjct.h"
 #include "io.hpp"
 #include "kernels.hpp"
@@ -31,6 +33,16 @@ using namespace fp;
 namespace {
 
 constexpr float kGravity[3] = {0.0f, -9.81f, 0.0f};  // FluidSolver3D.cuh:78
+
+// NVTX range over a scope (the phases of a step, as the reference's
+// cudaEvent timers of frameStep, FluidSolver3D.cu:3030-3098, delimit them);
+// a no-op unless a profiler is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 template <class T>
 cudaError_t dalloc(T** p, size_t n) {
@@ -162,6 +174,7 @@ struct fp_solver {
     // stats
     fp_step_stats stats{};
     int64_t steps = 0;
+    FILE* step_log = nullptr;  // one JSON line per step (fp_set_step_log)
 
     int fail(int code, const std::string& m) {
         err = m;
@@ -942,11 +955,12 @@ int check_ready(fp_solver* s) {
 // all but the last of its steps, so the host goes on issuing the next step
 // while the GPU completes this one (the solve's own read-back still waits).
 int one_step(fp_solver* s, bool finish = true) {
+    NvtxRange step_range("fp_step");
     if (ref2d(s)) return one_step_ref2d(s);
     cudaEventRecord(s->ev[0], s->st);
-    phase_label(s);
+    { NvtxRange r("label"); phase_label(s); }
     cudaEventRecord(s->ev[1], s->st);
-    phase_p2g(s, 1);  // P2G + save + forces
+    { NvtxRange r("p2g+save+forces"); phase_p2g(s, 1); }  // P2G + save + forces
     cudaEventRecord(s->ev[2], s->st);
     cudaEventRecord(s->ev[3], s->st);
     // The solve's statistics are read back only after the projection and
@@ -955,21 +969,23 @@ int one_step(fp_solver* s, bool finish = true) {
     // The projection and G2P/advection kernels read the solve's device status
     // and do nothing if it timed out or produced NaN, so such a step leaves
     // the particles as they were; a body is integrated only after a good solve.
-    int rc = phase_pressure(s, true);
+    int rc;
+    { NvtxRange r("pressure"); rc = phase_pressure(s, true); }
     cudaEventRecord(s->ev[4], s->st);
     auto fail_after = [&](int rc0) { const int r = solve_finalize(s); return rc0 != FP_OK ? rc0 : r; };
     if (rc != FP_OK) return fail_after(rc);
-    phase_project(s, true);
+    { NvtxRange r("project"); phase_project(s, true); }
     cudaEventRecord(s->ev[5], s->st);
     if (body_on(s)) {
         // the body phase waits for its own force anyway; finish the solve first
         rc = solve_finalize(s);
         if (rc != FP_OK) return rc;
     }
-    rc = phase_body(s);
+    { NvtxRange r("body"); rc = phase_body(s); }
     if (rc != FP_OK) return fail_after(rc);
     cudaEventRecord(s->ev[6], s->st);
     cudaEventRecord(s->ev[7], s->st);
+    NvtxRange adv_range("g2p+advect");
     if (s->cfg.extrapolate > 0) {
         phase_g2p_advect(s, 1, 0, true);
         rc = extrapolate_3d(s);
@@ -1001,6 +1017,42 @@ int one_step(fp_solver* s, bool finish = true) {
     cudaEventElapsedTime(&s->stats.t_total, s->ev[0], s->ev[8]);
     return FP_OK;
 }
+
+// One JSON line of the last step's statistics to the step log.
+void write_step_log(fp_solver* s) {
+    if (!s->step_log) return;
+    const fp_step_stats& t = s->stats;
+    std::fprintf(s->step_log,
+                 "{\"step\": %lld, \"particles\": %lld, \"fluid_cells\": %d, \"pcg_iters\": %d, \"outer_iters\": %d, "
+                 "\"residual\": %.9g, \"solve_status\": %d, \"fallback\": %d, \"guess_relres\": %.6g, "
+                 "\"t_label\": %.6g, \"t_p2g\": %.6g, \"t_pressure\": %.6g, \"t_pcg\": %.6g, \"t_learned\": %.6g, "
+                 "\"t_project\": %.6g, \"t_body\": %.6g, \"t_advect\": %.6g, \"t_total\": %.6g, "
+                 "\"body_pos\": [%.9g, %.9g, %.9g], \"body_vel\": [%.9g, %.9g, %.9g], \"kernel_launches\": %lld}\n",
+                 (long long)t.step, (long long)t.num_particles, t.num_fluid_cells, t.pcg_iters, t.outer_iters,
+                 t.residual, t.solve_status, t.fallback, double(t.guess_relres), double(t.t_label), double(t.t_p2g),
+                 double(t.t_pressure), double(t.t_pcg), double(t.t_learned), double(t.t_project), double(t.t_body),
+                 double(t.t_advect), double(t.t_total), t.body_pos[0], t.body_pos[1], t.body_pos[2], t.body_vel[0],
+                 t.body_vel[1], t.body_vel[2], (long long)s->launches);
+    std::fflush(s->step_log);
+}
+
+// Binary state file (fp_save_state / fp_load_state): host-order values in
+// the order written; ok turns false on any short read or write.
+constexpr char kStateMagic[8] = {'F', 'P', 'S', 'T', 'A', 'T', 'E', '1'};
+
+struct StateFile {
+    FILE* f = nullptr;
+    bool ok = true;
+    ~StateFile() { if (f) std::fclose(f); }
+    template <class T>
+    void put(const T* p, size_t n) { if (ok && n && std::fwrite(p, sizeof(T), n, f) != n) ok = false; }
+    template <class T>
+    void put(const T& v) { put(&v, 1); }
+    template <class T>
+    void get(T* p, size_t n) { if (ok && n && std::fread(p, sizeof(T), n, f) != n) ok = false; }
+    template <class T>
+    void get(T& v) { get(&v, 1); }
+};
 
 std::string frame_dir(const std::string& tmpl) {
     size_t p = tmpl.find_last_of('/');
@@ -1161,6 +1213,7 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
 
 int fp_destroy(fp_solver* s) {
     if (!s) return FP_OK;
+    if (s->step_log) std::fclose(s->step_log);
     if (s->st) cudaStreamSynchronize(s->st);
     free_grid(s);
     free_particles(s);
@@ -1415,8 +1468,11 @@ int fp_step(fp_solver* s, int n) {
     int rc = check_ready(s);
     if (rc) return rc;
     for (int i = 0; i < n; ++i) {
-        rc = one_step(s, i + 1 == n);
+        // with a step log every step waits for its end, so that its phase
+        // times are its own
+        rc = one_step(s, i + 1 == n || s->step_log != nullptr);
         if (rc) return rc;
+        write_step_log(s);
     }
     return FP_OK;
 }
@@ -1537,6 +1593,7 @@ int fp_run(fp_solver* s, int frames) {
     for (int64_t i = 0; i <= last; ++i) {
         rc = one_step(s);
         if (rc) break;
+        write_step_log(s);
         if ((r2 || i % ipf == 0) && out) {
             const char* ext = s->cfg.output_format == FP_OUT_OFF ? ".off" : ".ply";
             rc = writer.submit(int(frame++ & 1), tmpl + std::to_string(r2 ? i : i / ipf) + ext);
@@ -1713,6 +1770,159 @@ int fp_stats(const fp_solver* s, fp_step_stats* out) {
 }
 
 void* fp_cuda_stream(const fp_solver* s) { return s ? static_cast<void*>(s->st) : nullptr; }
+
+int fp_set_step_log(fp_solver* s, const char* path) {
+    if (!s) return FP_ERR_ARG;
+    if (s->step_log) { std::fclose(s->step_log); s->step_log = nullptr; }
+    if (!path || !path[0]) return FP_OK;
+    s->step_log = std::fopen(path, "w");
+    if (!s->step_log) return s->fail(FP_ERR_IO, std::string("cannot open step log ") + path);
+    return FP_OK;
+}
+
+// ---------------------------------------------------------------- state snapshots
+
+int fp_save_state(fp_solver* s, const char* path) {
+    if (!s || !path) return FP_ERR_ARG;
+    if (!s->have_grid) return s->fail(FP_ERR_STATE, "no state: labels not loaded");
+    const size_t nc = size_t(s->g.nc()), nu = size_t(s->g.nu()), nv = size_t(s->g.nv()), nw = size_t(s->g.nw());
+    std::vector<uint8_t> base(nc), lab(nc);
+    std::vector<float> grids(2 * (nu + nv + nw) + nc);
+    std::vector<float> pos(size_t(s->np) * 3), vel(size_t(s->np) * 3);
+    cudaError_t e = cudaStreamSynchronize(s->st);
+    size_t off = 0;
+    for (auto [src, n] : {std::pair<const float*, size_t>{s->d_u, nu}, {s->d_v, nv}, {s->d_w, nw}, {s->d_us, nu},
+                          {s->d_vs, nv}, {s->d_ws, nw}, {s->d_p, nc}}) {
+        if (e == cudaSuccess) e = cudaMemcpy(grids.data() + off, src, sizeof(float) * n, cudaMemcpyDeviceToHost);
+        off += n;
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(base.data(), s->d_base, nc, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(lab.data(), s->d_labels, nc, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return s->cuda_fail(e, "state download");
+    if (s->np) {
+        const int rc = fp_get_particles(s, pos.data(), vel.data(), s->np);
+        if (rc) return rc;
+    }
+    StateFile sf;
+    sf.f = std::fopen(path, "wb");
+    if (!sf.f) return s->fail(FP_ERR_IO, std::string("cannot write state file ") + path);
+    sf.put(kStateMagic, 8);
+    sf.put(int32_t(1));
+    sf.put(int32_t(s->W)); sf.put(int32_t(s->H)); sf.put(int32_t(s->D));
+    sf.put(s->cfg.dx); sf.put(s->cfg.dt);
+    sf.put(int64_t(s->steps));
+    sf.put(base.data(), nc); sf.put(lab.data(), nc);
+    sf.put(grids.data(), grids.size());
+    sf.put(int64_t(s->np));
+    sf.put(pos.data(), pos.size()); sf.put(vel.data(), vel.size());
+    const HostBody& h = s->hb;
+    sf.put(int32_t(h.loaded ? 1 : 0));
+    sf.put(int32_t(s->cfg.active_body));
+    if (h.loaded) {
+        sf.put(int32_t(h.kind));
+        sf.put(h.pos, 3); sf.put(h.vel, 3); sf.put(h.omega, 3);
+        sf.put(h.theta); sf.put(h.psi); sf.put(h.phi);
+        sf.put(h.mass); sf.put(h.inertia); sf.put(h.radius);
+        sf.put(h.force, 3); sf.put(h.torque, 3);
+        sf.put(int32_t(h.nx)); sf.put(int32_t(h.ny)); sf.put(int32_t(h.nz));
+        sf.put(h.origin, 3); sf.put(h.cell); sf.put(h.local_com, 3);
+        sf.put(h.pad_x0); sf.put(h.pad_amp); sf.put(h.pad_period); sf.put(h.pad_t);
+        sf.put(int64_t(h.sdf_host.size()));
+        sf.put(h.sdf_host.data(), h.sdf_host.size());
+    }
+    if (!sf.ok) return s->fail(FP_ERR_IO, std::string("write error on state file ") + path);
+    return FP_OK;
+}
+
+int fp_load_state(fp_solver* s, const char* path) {
+    if (!s || !path) return FP_ERR_ARG;
+    StateFile sf;
+    sf.f = std::fopen(path, "rb");
+    if (!sf.f) return s->fail(FP_ERR_IO, std::string("cannot open state file ") + path);
+    char magic[8] = {};
+    int32_t ver = 0, W = 0, H = 0, D = 0;
+    float dx = 0, dt = 0;
+    int64_t steps = 0;
+    sf.get(magic, 8); sf.get(ver);
+    if (!sf.ok || std::memcmp(magic, kStateMagic, 8) != 0 || ver != 1)
+        return s->fail(FP_ERR_IO, std::string("not a state file: ") + path);
+    sf.get(W); sf.get(H); sf.get(D); sf.get(dx); sf.get(dt); sf.get(steps);
+    if (!sf.ok || W <= 0 || H <= 0 || D <= 0 || int64_t(W) * H * D > (int64_t(1) << 34))
+        return s->fail(FP_ERR_IO, "state file: bad grid header");
+    if (dx != s->cfg.dx || dt != s->cfg.dt) return s->fail(FP_ERR_ARG, "state file: dx or dt differ from the solver's");
+    const Dims gd{W, H, D, dx};
+    const size_t nc = size_t(gd.nc()), nu = size_t(gd.nu()), nv = size_t(gd.nv()), nw = size_t(gd.nw());
+    std::vector<uint8_t> base(nc), lab(nc);
+    std::vector<float> grids(2 * (nu + nv + nw) + nc);
+    sf.get(base.data(), nc); sf.get(lab.data(), nc);
+    sf.get(grids.data(), grids.size());
+    int64_t np = 0;
+    sf.get(np);
+    if (!sf.ok || np < 0 || np > 0x7F7F7F7FLL) return s->fail(FP_ERR_IO, "state file: truncated or bad particle count");
+    std::vector<float> pos(size_t(np) * 3), vel(size_t(np) * 3);
+    sf.get(pos.data(), pos.size()); sf.get(vel.data(), vel.size());
+    int32_t loaded = 0, active = 0;
+    sf.get(loaded); sf.get(active);
+    HostBody h;
+    if (sf.ok && loaded) {
+        int32_t kind = 0, nx = 0, ny = 0, nz = 0;
+        int64_t nsdf = 0;
+        sf.get(kind);
+        sf.get(h.pos, 3); sf.get(h.vel, 3); sf.get(h.omega, 3);
+        sf.get(h.theta); sf.get(h.psi); sf.get(h.phi);
+        sf.get(h.mass); sf.get(h.inertia); sf.get(h.radius);
+        sf.get(h.force, 3); sf.get(h.torque, 3);
+        sf.get(nx); sf.get(ny); sf.get(nz);
+        sf.get(h.origin, 3); sf.get(h.cell); sf.get(h.local_com, 3);
+        sf.get(h.pad_x0); sf.get(h.pad_amp); sf.get(h.pad_period); sf.get(h.pad_t);
+        sf.get(nsdf);
+        if (!sf.ok || kind < BODY_SPHERE || kind > BODY_PADDLE || nsdf < 0 || nsdf != int64_t(nx) * ny * nz ||
+            (kind == BODY_SDF && nsdf == 0))
+            return s->fail(FP_ERR_IO, "state file: bad body record");
+        h.kind = kind; h.nx = nx; h.ny = ny; h.nz = nz;
+        h.sdf_host.resize(size_t(nsdf));
+        sf.get(h.sdf_host.data(), h.sdf_host.size());
+        h.update_rotation();
+    }
+    if (!sf.ok) return s->fail(FP_ERR_IO, "state file: truncated");
+    // the grid, labels and fields
+    int rc = alloc_grid(s, W, H, D);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpy(s->d_base, base.data(), nc, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->d_labels, lab.data(), nc, cudaMemcpyHostToDevice);
+    size_t off = 0;
+    for (auto [dst, n] : {std::pair<float*, size_t>{s->d_u, nu}, {s->d_v, nv}, {s->d_w, nw}, {s->d_us, nu},
+                          {s->d_vs, nv}, {s->d_ws, nw}, {s->d_p, nc}}) {
+        if (e == cudaSuccess) e = cudaMemcpy(dst, grids.data() + off, sizeof(float) * n, cudaMemcpyHostToDevice);
+        off += n;
+    }
+    if (e != cudaSuccess) return s->cuda_fail(e, "state upload");
+    // the body
+    free_body(s);
+    if (loaded) {
+        h.loaded = false;
+        s->hb = std::move(h);
+        HostBody& hb = s->hb;
+        if (!hb.sdf_host.empty()) {
+            e = dalloc(&s->d_sdf, hb.sdf_host.size());
+            if (e == cudaSuccess)
+                e = cudaMemcpy(s->d_sdf, hb.sdf_host.data(), sizeof(float) * hb.sdf_host.size(), cudaMemcpyHostToDevice);
+        }
+        if (e == cudaSuccess) e = dalloc(&s->d_bpart, size_t(body_force_partials()));
+        if (e == cudaSuccess) e = dalloc(&s->d_bforce, 8);
+        if (e != cudaSuccess) { free_body(s); return s->cuda_fail(e, "state body upload"); }
+        hb.loaded = true;
+        fill_body_stats(s);
+    }
+    s->cfg.active_body = active;
+    // the particles, in their saved order
+    rc = fp_set_particles(s, np ? pos.data() : nullptr, np ? vel.data() : nullptr, np);
+    if (rc) return rc;
+    s->steps = steps;
+    s->stats.step = steps;
+    s->stats.num_particles = np;
+    return FP_OK;
+}
 
 int fp_set_wait_limit(fp_solver* s, int64_t polls) {
     if (!s || polls < 0) return s ? s->fail(FP_ERR_ARG, "negative wait limit") : FP_ERR_ARG;

@@ -289,6 +289,26 @@ int fp_stats(const fp_solver* s, fp_step_stats* out);
  * own events or order their own work after the solver's. */
 void* fp_cuda_stream(const fp_solver* s);
 
+/* Per-step log (the reference prints its phase timers at the end of run(),
+ * FluidSolver3D.cu:3149-3162): with a path, every step of fp_step / fp_run
+ * appends one JSON line of its fp_step_stats (step, particles, FLUID cells,
+ * PCG iterations, residual and status, phase times in ms, body position and
+ * velocity) to that file; each step then waits for its own end, so that its
+ * times are its own.  NULL or "" closes the log. */
+int fp_set_step_log(fp_solver* s, const char* path);
+
+/* Exact-resume snapshots (no counterpart in the reference): fp_save_state
+ * writes the grid dimensions, dx and dt, the step count, the SOLID map and
+ * labels, u, v, w, u*, v*, w* and p, the particles (in the order given) and
+ * the rigid body's full state (with its SDF); fp_load_state restores them on
+ * a solver created with the same dx and dt (FP_ERR_ARG otherwise; FP_ERR_IO
+ * for a missing, truncated or foreign file), re-sizing its grids.  The
+ * solver's own configuration (solver, advection, ...) is kept.  A loaded
+ * state steps on as the saved solver would, up to the order of P2G's
+ * floating-point sums. */
+int fp_save_state(fp_solver* s, const char* path);
+int fp_load_state(fp_solver* s, const char* path);
+
 /* Diagnostics (no counterpart in the reference): the number of polls after
  * which a grid-barrier wait of the persistent pressure solvers gives up and
  * the step returns FP_ERR_TIMEOUT (default 2^27, about a minute; 0 restores
