@@ -150,12 +150,9 @@ void launch_project(float* u, float* v, float* w, const float* p, const uint8_t*
 void launch_g2p_advect(float4* pos, float4* vel, int64_t np, const float* u, const float* v, const float* w,
                        const float* us, const float* vs, const float* ws, const uint8_t* labels, Dims g, float alpha,
                        float dt, float cfl, int do_g2p, int do_advect, int rk2, cudaStream_t st,
-                       const int* guard = nullptr, const BodyShape* collide = nullptr,
-                       const int* cell_start = nullptr);
+                       const int* guard = nullptr, const BodyShape* collide = nullptr);
 // collide: the body for SDF collision projection (sdf_push_out, eps = dx/4),
-// or null for the reference's label search alone.  cell_start: the cell
-// offsets of the current (cell-sorted) particle order, or null; with it, a 3D
-// grid is processed brick by brick from shared-memory tiles of the faces.
+// or null for the reference's label search alone.
 
 // -------- rigid body (kernels_body.cu) --------
 // mark[c] = 1 where the cell centre is inside the body (SDF <= 0).

@@ -16,7 +16,6 @@
 //        is below eps = 0.25 dx is first projected along the SDF normal to
 //        phi = eps (sdf_push_out), and the label search is kept for SOLID
 //        cells only.
-#include "device_memo.hpp"
 #include "kernels.hpp"
 
 namespace fp {
@@ -56,8 +55,11 @@ __device__ __forceinline__ bool project_particle(float3& pos, const uint8_t* __r
     return true;
 }
 
-// Face-grid samplers for the per-particle update.  GlobalSampler reads the
-// six face grids through L1 (trilinear corners as scalar loads).
+// Face-grid sampler of the per-particle update: the six face grids through
+// L1 (trilinear corners as scalar loads; particles in cell order make
+// neighbouring threads share lines).  A variant that staged each 8^3 brick's
+// faces in shared memory measured slower (0.355 against 0.294 ms at 128^3):
+// its index arithmetic and bank conflicts cost more than the L1 loads.
 struct GlobalSampler {
     const float *u, *v, *w, *us, *vs, *ws;
     Dims g;
@@ -70,105 +72,6 @@ struct GlobalSampler {
                           sample_delta(w, ws, sw, sxw, sxyw));
     }
     __device__ __forceinline__ float3 vel(float3 p) const { return interp_vel(u, v, w, g, p); }
-};
-
-// Base corner (i, j, k) and fractions of component COMP's stencil: the same
-// clamps and arithmetic as stencil_u / stencil_v / stencil_w.
-struct Corner {
-    int i, j, k;
-    float fx, fy, fz;
-};
-template <int COMP>
-__device__ __forceinline__ Corner corner(float rx, float ry, float rz, const Dims& g) {
-    Corner c;
-    if (COMP == 0) {
-        c.i = clampi(int(floorf(rx)), 0, g.W - 1); c.j = clampi(int(floorf(ry - 0.5f)), 0, g.H - 2);
-        c.k = clampi(int(floorf(rz - 0.5f)), 0, max(g.D - 2, 0));
-        c.fx = clamp01(rx - float(c.i)); c.fy = clamp01((ry - 0.5f) - float(c.j)); c.fz = clamp01((rz - 0.5f) - float(c.k));
-    } else if (COMP == 1) {
-        c.i = clampi(int(floorf(rx - 0.5f)), 0, g.W - 2); c.j = clampi(int(floorf(ry)), 0, g.H - 1);
-        c.k = clampi(int(floorf(rz - 0.5f)), 0, max(g.D - 2, 0));
-        c.fx = clamp01((rx - 0.5f) - float(c.i)); c.fy = clamp01(ry - float(c.j)); c.fz = clamp01((rz - 0.5f) - float(c.k));
-    } else {
-        c.i = clampi(int(floorf(rx - 0.5f)), 0, g.W - 2); c.j = clampi(int(floorf(ry - 0.5f)), 0, g.H - 2);
-        c.k = clampi(int(floorf(rz)), 0, g.D - 1);
-        c.fx = clamp01((rx - 0.5f) - float(c.i)); c.fy = clamp01((ry - 0.5f) - float(c.j)); c.fz = clamp01(rz - float(c.k));
-    }
-    return c;
-}
-
-// Shared-memory tile of one brick of BX x BY x BZ cells and HL halo cells:
-// for each face grid f (u, v, w) an array of entries (f[i], f[i+1], f*[i],
-// f*[i+1]) over the stencil bases that particles inside the brick and halo
-// can have, so that one 16-byte load gives both x corners of f and f*.
-// Tile extents and origins (in face indices) per component:
-//   u: x BX+2HL from i0-HL, y BY+2HL+2 from j0-HL-1, z BZ+2HL+2 from k0-HL-1
-//   v: x BX+2HL+1 from i0-HL-1, y BY+2HL+1 from j0-HL, z as u
-//   w: x as v, y as u, z BZ+2HL+1 from k0-HL
-template <int BX, int BY, int BZ, int HL>
-struct Tile {
-    static __host__ __device__ constexpr int nx(int comp) { return comp == 0 ? BX + 2 * HL : BX + 2 * HL + 1; }
-    static __host__ __device__ constexpr int ny(int comp) { return comp == 1 ? BY + 2 * HL + 1 : BY + 2 * HL + 2; }
-    static __host__ __device__ constexpr int nz(int comp) { return comp == 2 ? BZ + 2 * HL + 1 : BZ + 2 * HL + 2; }
-    static __host__ __device__ constexpr int n(int comp) { return nx(comp) * ny(comp) * nz(comp); }
-    static constexpr int TOTAL = n(0) + n(1) + n(2);
-    static __host__ __device__ constexpr int offset(int comp) { return comp == 0 ? 0 : (comp == 1 ? n(0) : n(0) + n(1)); }
-    // origin of component comp's tile for the brick at (i0, j0, k0)
-    static __device__ __forceinline__ int ox(int comp, int i0) { return comp == 0 ? i0 - HL : i0 - HL - 1; }
-    static __device__ __forceinline__ int oy(int comp, int j0) { return comp == 1 ? j0 - HL : j0 - HL - 1; }
-    static __device__ __forceinline__ int oz(int comp, int k0) { return comp == 2 ? k0 - HL : k0 - HL - 1; }
-};
-
-// TileSampler reads the staged tile when the whole stencil lies in it, and
-// the global grids otherwise (particles that left the brick and its halo).
-// The values and the arithmetic are the same either way, so the result does
-// not depend on which path a sample takes.
-template <int BX, int BY, int BZ, int HL>
-struct TileSampler {
-    using T = Tile<BX, BY, BZ, HL>;
-    GlobalSampler G;
-    const float4* t;  // the staged tile (shared memory)
-    int i0, j0, k0;   // brick origin
-
-    template <int COMP>
-    __device__ __forceinline__ int entry(const Corner& c) const {
-        const int li = c.i - T::ox(COMP, i0), lj = c.j - T::oy(COMP, j0), lk = c.k - T::oz(COMP, k0);
-        if (unsigned(li) >= unsigned(T::nx(COMP)) || unsigned(lj) >= unsigned(T::ny(COMP) - 1) ||
-            unsigned(lk) >= unsigned(T::nz(COMP) - 1))
-            return -1;
-        return T::offset(COMP) + li + T::nx(COMP) * (lj + T::ny(COMP) * lk);
-    }
-    // PIC and FLIP samples of component COMP from entry e (4 tile loads)
-    template <int COMP>
-    __device__ __forceinline__ void both(int e, const Corner& c, float& pic, float& dlt) const {
-        const int sy = T::nx(COMP), sz = T::nx(COMP) * T::ny(COMP);
-        const float4 a = t[e], b = t[e + sy], d = t[e + sz], f = t[e + sy + sz];  // (y,z): a 00, b 10, d 01, f 11
-        pic = trilin(c.fx, c.fy, c.fz, a.x, a.y, d.x, d.y, b.x, b.y, f.x, f.y);
-        dlt = trilin(c.fx, c.fy, c.fz, a.x - a.z, a.y - a.w, d.x - d.z, d.y - d.w, b.x - b.z, b.y - b.w, f.x - f.z,
-                     f.y - f.w);
-    }
-    template <int COMP>
-    __device__ __forceinline__ float one(int e, const Corner& c) const {
-        const int sy = T::nx(COMP), sz = T::nx(COMP) * T::ny(COMP);
-        const float2* t2 = reinterpret_cast<const float2*>(t);  // the (f[i], f[i+1]) half of each entry
-        const float2 a = t2[2 * e], b = t2[2 * (e + sy)], d = t2[2 * (e + sz)], f = t2[2 * (e + sy + sz)];
-        return trilin(c.fx, c.fy, c.fz, a.x, a.y, d.x, d.y, b.x, b.y, f.x, f.y);
-    }
-    __device__ __forceinline__ void g2p(float rx, float ry, float rz, float3& pic, float3& dlt) const {
-        const Corner cu = corner<0>(rx, ry, rz, G.g), cv = corner<1>(rx, ry, rz, G.g), cw = corner<2>(rx, ry, rz, G.g);
-        const int eu = entry<0>(cu), ev = entry<1>(cv), ew = entry<2>(cw);
-        if (eu < 0 || ev < 0 || ew < 0) { G.g2p(rx, ry, rz, pic, dlt); return; }
-        both<0>(eu, cu, pic.x, dlt.x);
-        both<1>(ev, cv, pic.y, dlt.y);
-        both<2>(ew, cw, pic.z, dlt.z);
-    }
-    __device__ __forceinline__ float3 vel(float3 p) const {
-        const float rx = over_dx(p.x, G.g), ry = over_dx(p.y, G.g), rz = over_dx(p.z, G.g);
-        const Corner cu = corner<0>(rx, ry, rz, G.g), cv = corner<1>(rx, ry, rz, G.g), cw = corner<2>(rx, ry, rz, G.g);
-        const int eu = entry<0>(cu), ev = entry<1>(cv), ew = entry<2>(cw);
-        if (eu < 0 || ev < 0 || ew < 0) return G.vel(p);
-        return make_float3(one<0>(eu, cu), one<1>(ev, cv), one<2>(ew, cw));
-    }
 };
 
 struct AdvectParams {
@@ -256,87 +159,6 @@ __global__ void __launch_bounds__(256) k_g2p_advect(float4* __restrict__ pos, fl
     particle_update(smp, pos, vel, q, lab, smp.g, a);
 }
 
-// Cell-sorted particles, one CTA per brick of cells (3D grids): the CTA
-// stages the brick's six face grids with a one-cell halo in shared memory
-// (Tile), then its threads update the brick's particles, which are BY*BZ
-// contiguous ranges (one per row of cells along x) of the cell-sorted order.
-// Bricks without particles return before staging.
-// G2P_TILED (a build tunable, default 1) selects this kernel for sorted 3D
-// particles; 0 keeps the particle-parallel kernel everywhere.
-#ifndef G2P_TILED
-#define G2P_TILED 1
-#endif
-constexpr int G2P_BX = 8, G2P_BY = 8, G2P_BZ = 8, G2P_HL = 1, G2P_NT = 256;
-using G2PTile = Tile<G2P_BX, G2P_BY, G2P_BZ, G2P_HL>;
-
-__global__ void __launch_bounds__(G2P_NT) k_g2p_advect_tiled(float4* __restrict__ pos, float4* __restrict__ vel,
-                                                            const int* __restrict__ start, GlobalSampler G,
-                                                            const uint8_t* __restrict__ lab, AdvectParams a,
-                                                            const int* __restrict__ guard) {
-    extern __shared__ float4 s_tile[];
-    constexpr int NR = G2P_BY * G2P_BZ;
-    __shared__ int s_row0[NR + 1];  // prefix of the rows' particle counts
-    __shared__ int s_q0[NR];        // first particle of each row
-    const Dims& g = G.g;
-    const int W = g.W, H = g.H, D = g.D;
-    const int nbx = (W + G2P_BX - 1) / G2P_BX, nby = (H + G2P_BY - 1) / G2P_BY;
-    const int bid = blockIdx.x;
-    const int i0 = (bid % nbx) * G2P_BX, j0 = ((bid / nbx) % nby) * G2P_BY, k0 = (bid / (nbx * nby)) * G2P_BZ;
-    const int bxe = min(G2P_BX, W - i0), bye = min(G2P_BY, H - j0), bze = min(G2P_BZ, D - k0);
-    if (threadIdx.x < NR) {
-        const int r = threadIdx.x, j = j0 + r % G2P_BY, k = k0 + r / G2P_BY;
-        int q0 = 0, n = 0;
-        if (r % G2P_BY < bye && r / G2P_BY < bze) {
-            const int c0 = i0 + j * W + k * W * H;
-            q0 = start[c0];
-            n = start[c0 + bxe] - q0;
-        }
-        s_q0[r] = q0;
-        s_row0[r + 1] = n;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        s_row0[0] = 0;
-        for (int r = 1; r <= NR; ++r) { acc += s_row0[r]; s_row0[r] = acc; }
-    }
-    __syncthreads();
-    const int total = s_row0[NR];
-    if (total == 0 || solve_failed(guard)) return;
-    // stage the three tiles: entry (li, lj, lk) of component f holds
-    // f[i], f[i+1], f*[i], f*[i+1] at face (i, j, k) = origin + (li, lj, lk),
-    // zero outside the face grid
-    for (int e = threadIdx.x; e < G2PTile::TOTAL; e += G2P_NT) {
-        int comp = e < G2PTile::n(0) ? 0 : (e < G2PTile::n(0) + G2PTile::n(1) ? 1 : 2);
-        const int le = e - G2PTile::offset(comp);
-        const int nx = G2PTile::nx(comp), ny = G2PTile::ny(comp);
-        const int i = G2PTile::ox(comp, i0) + le % nx, j = G2PTile::oy(comp, j0) + (le / nx) % ny,
-                  k = G2PTile::oz(comp, k0) + le / (nx * ny);
-        const int fw = W + (comp == 0), fh = H + (comp == 1), fd = D + (comp == 2);
-        const float* f = comp == 0 ? G.u : (comp == 1 ? G.v : G.w);
-        const float* fs = comp == 0 ? G.us : (comp == 1 ? G.vs : G.ws);
-        float4 val = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (j >= 0 && j < fh && k >= 0 && k < fd) {
-            const int64_t row = (int64_t(k) * fh + j) * fw;
-            if (i >= 0 && i < fw) { val.x = __ldg(f + row + i); val.z = __ldg(fs + row + i); }
-            if (i + 1 >= 0 && i + 1 < fw) { val.y = __ldg(f + row + i + 1); val.w = __ldg(fs + row + i + 1); }
-        }
-        s_tile[e] = val;
-    }
-    __syncthreads();
-    TileSampler<G2P_BX, G2P_BY, G2P_BZ, G2P_HL> smp{G, s_tile, i0, j0, k0};
-    for (int t = threadIdx.x; t < total; t += G2P_NT) {
-        // the row holding the t-th particle of the brick
-        int lo = 0, hi = NR - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (s_row0[mid] <= t) lo = mid; else hi = mid - 1;
-        }
-        const int64_t q = int64_t(s_q0[lo]) + (t - s_row0[lo]);
-        particle_update(smp, pos, vel, q, lab, g, a);
-    }
-}
-
 __global__ void k_unsort(const float4* __restrict__ pos, const float4* __restrict__ vel, int64_t np,
                          float* __restrict__ pos_out, float* __restrict__ vel_out) {
     const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -377,24 +199,13 @@ __global__ void k_pack(const float* __restrict__ pos, const float* __restrict__ 
 void launch_g2p_advect(float4* pos, float4* vel, int64_t np, const float* u, const float* v, const float* w,
                        const float* us, const float* vs, const float* ws, const uint8_t* labels, Dims g, float alpha,
                        float dt, float cfl, int do_g2p, int do_advect, int rk2, cudaStream_t st, const int* guard,
-                       const BodyShape* collide, const int* cell_start) {
+                       const BodyShape* collide) {
     if (np == 0) return;
     AdvectParams a{};
     a.alpha = alpha; a.dt = dt; a.C = cfl;
     a.do_g2p = do_g2p; a.do_advect = do_advect; a.rk2 = rk2; a.sdf_collide = collide ? 1 : 0;
     if (collide) a.body = *collide;
     const GlobalSampler G{u, v, w, us, vs, ws, g};
-    if (G2P_TILED && cell_start && g.D > 1) {
-        static DeviceMemo memo;
-        constexpr int smem = int(sizeof(float4)) * G2PTile::TOTAL;
-        memo.get([](int) {
-            cudaFuncSetAttribute(k_g2p_advect_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            return 1;
-        });
-        const int nb = ((g.W + G2P_BX - 1) / G2P_BX) * ((g.H + G2P_BY - 1) / G2P_BY) * ((g.D + G2P_BZ - 1) / G2P_BZ);
-        k_g2p_advect_tiled<<<nb, G2P_NT, smem, st>>>(pos, vel, cell_start, G, labels, a, guard);
-        return;
-    }
     k_g2p_advect<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, G, labels, a, guard);
 }
 

@@ -657,11 +657,13 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     const bool guess = a.x0 || a.pprev;
     double bb_warm = 0.0;  // ||b||^2 when started from a guess
     // With a guess g the solve's first flexible-CG step uses g as its
-    // preconditioned residual: z0 = g (the network's output N(b), or the
-    // previous pressure), p0 = z0, alpha0 = (r0, z0) / (p0, A p0) -- the
-    // energy-optimal scaling -- and x1 = alpha0 g.  p0, A p0, gamma0 = (r0, z0)
-    // and (p0, A p0) stay in the recurrence, so the next direction (from the
-    // V-cycle) is made A-conjugate to g by the Polak-Ribiere beta.
+    // preconditioned residual: z0 = g, p0 = z0, alpha0 = (r0, z0) / (p0, A p0)
+    // -- the energy-optimal scaling -- and x1 = alpha0 g.  For the network's
+    // guess N(b) (the learned preconditioner), p0, A p0, gamma0 = (r0, z0) and
+    // (p0, A p0) stay in the recurrence, so the next direction (from the
+    // V-cycle) is made A-conjugate to p0 by the Polak-Ribiere beta.  The
+    // previous step's pressure restarts the recurrence instead: kept in it, it
+    // cost iterations (11.2 against 10.8 per warm-started solve at 128^3).
     bool dir0 = false;
     double gam0 = 0.0, alpha0 = 0.0, den0 = 0.0;
     if (guess) {
@@ -683,7 +685,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         if (!grid_barrier(a.bar, unsigned(nb), a.status)) return;
         const double3 t = total();
         const double alpha = (t.y > 0.0 && isfinite(t.x / t.y)) ? t.x / t.y : 0.0;
-        dir0 = alpha != 0.0;
+        dir0 = alpha != 0.0 && a.x0 != nullptr;  // the learned guess only (see above)
         gam0 = t.x; alpha0 = alpha; den0 = t.y;
         bb_warm = t.z;  // all reads of x ended before the barrier above
         rrl = 0.0;

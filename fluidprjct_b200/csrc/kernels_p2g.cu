@@ -265,37 +265,60 @@ __global__ void __launch_bounds__(NT, P2G_MIN_BLOCKS) k_p2g(const float4* __rest
     // their region), then the shell's edges and corners with every slot.
     const Owned own{i0, ie, iue, j0, je, jve, k0, ke, kwe};
     const int bxe = ie - i0 + 1, bye = je - j0 + 1, bze = ke - k0 + 1;
-    for (int t = threadIdx.x; t < bxe * bye * bze; t += NT)
-        splat_region<R_FULL, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + (t / bxe) % bye, k0 + t / (bxe * bye), g,
-                                         s_num, s_den, own);
-    if (i0 > 0)
-        for (int t = threadIdx.x; t < bye * bze; t += NT)
-            splat_region<R_XLO, BX, BY, BZ>(pos, vel, start, i0 - 1, j0 + t % bye, k0 + t / bye, g, s_num, s_den, own);
-    if (ie + 1 < W)
-        for (int t = threadIdx.x; t < bye * bze; t += NT)
-            splat_region<R_XHI, BX, BY, BZ>(pos, vel, start, ie + 1, j0 + t % bye, k0 + t / bye, g, s_num, s_den, own);
-    if (j0 > 0)
-        for (int t = threadIdx.x; t < bxe * bze; t += NT)
-            splat_region<R_YLO, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 - 1, k0 + t / bxe, g, s_num, s_den, own);
-    if (je + 1 < H)
-        for (int t = threadIdx.x; t < bxe * bze; t += NT)
-            splat_region<R_YHI, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, je + 1, k0 + t / bxe, g, s_num, s_den, own);
-    if (k0 > 0)
-        for (int t = threadIdx.x; t < bxe * bye; t += NT)
-            splat_region<R_ZLO, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + t / bxe, k0 - 1, g, s_num, s_den, own);
-    if (ke + 1 < D)
-        for (int t = threadIdx.x; t < bxe * bye; t += NT)
-            splat_region<R_ZHI, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + t / bxe, ke + 1, g, s_num, s_den, own);
-    {
-        const int ilo = max(i0 - 1, 0), ihi = min(ie + 1, W - 1);
-        const int jlo = max(j0 - 1, 0), jhi = min(je + 1, H - 1);
-        const int klo = max(k0 - 1, 0), khi = min(ke + 1, D - 1);
-        const int ni = ihi - ilo + 1, nj = jhi - jlo + 1, ncell = ni * nj * (khi - klo + 1);
-        for (int t = threadIdx.x; t < ncell; t += NT) {
-            const int ci = ilo + t % ni, cj = jlo + (t / ni) % nj, ck = klo + t / (ni * nj);
-            const int outside = (ci < i0 || ci > ie) + (cj < j0 || cj > je) + (ck < k0 || ck > ke);
-            if (outside < 2) continue;  // the brick's cells and the halo faces are done
-            splat_region<R_FULL, BX, BY, BZ>(pos, vel, start, ci, cj, ck, g, s_num, s_den, own);
+    const int ilo = max(i0 - 1, 0), ihi = min(ie + 1, W - 1);
+    const int jlo = max(j0 - 1, 0), jhi = min(je + 1, H - 1);
+    const int klo = max(k0 - 1, 0), khi = min(ke + 1, D - 1);
+    const int ni = ihi - ilo + 1, nj = jhi - jlo + 1;
+    // One flat, evenly shared list of work items: the brick's cells, each
+    // halo face (a segment per region, so a warp's cells share their region:
+    // the segment sizes are multiples of 32 for a full brick), then every cell
+    // of the halo box, of which only the edges and corners are walked.
+    const int n_int = bxe * bye * bze, n_x = bye * bze, n_y = bxe * bze, n_z = bxe * bye;
+    const int seg[8] = {n_int, i0 > 0 ? n_x : 0, ie + 1 < W ? n_x : 0, j0 > 0 ? n_y : 0, je + 1 < H ? n_y : 0,
+                        k0 > 0 ? n_z : 0, ke + 1 < D ? n_z : 0, ni * nj * (khi - klo + 1)};
+    int total = 0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) total += seg[r];
+    for (int t0 = threadIdx.x; t0 < total; t0 += NT) {
+        int r = 0, t = t0;
+#pragma unroll
+        for (int q = 0; q < 7; ++q)  // constant indices keep seg[] in registers
+            if (r == q && t >= seg[q]) { t -= seg[q]; r = q + 1; }
+        switch (r) {
+            case 0:
+                splat_region<R_FULL, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + (t / bxe) % bye,
+                                                 k0 + t / (bxe * bye), g, s_num, s_den, own);
+                break;
+            case 1:
+                splat_region<R_XLO, BX, BY, BZ>(pos, vel, start, i0 - 1, j0 + t % bye, k0 + t / bye, g, s_num, s_den,
+                                                own);
+                break;
+            case 2:
+                splat_region<R_XHI, BX, BY, BZ>(pos, vel, start, ie + 1, j0 + t % bye, k0 + t / bye, g, s_num, s_den,
+                                                own);
+                break;
+            case 3:
+                splat_region<R_YLO, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 - 1, k0 + t / bxe, g, s_num, s_den,
+                                                own);
+                break;
+            case 4:
+                splat_region<R_YHI, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, je + 1, k0 + t / bxe, g, s_num, s_den,
+                                                own);
+                break;
+            case 5:
+                splat_region<R_ZLO, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + t / bxe, k0 - 1, g, s_num, s_den,
+                                                own);
+                break;
+            case 6:
+                splat_region<R_ZHI, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + t / bxe, ke + 1, g, s_num, s_den,
+                                                own);
+                break;
+            default: {
+                const int ci = ilo + t % ni, cj = jlo + (t / ni) % nj, ck = klo + t / (ni * nj);
+                const int outside = (ci < i0 || ci > ie) + (cj < j0 || cj > je) + (ck < k0 || ck > ke);
+                if (outside >= 2)  // the brick's cells and the halo faces are done above
+                    splat_region<R_FULL, BX, BY, BZ>(pos, vel, start, ci, cj, ck, g, s_num, s_den, own);
+            }
         }
     }
     __syncthreads();

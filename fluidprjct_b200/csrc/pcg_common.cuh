@@ -22,10 +22,12 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        // The status load is issued before the arrival so that its latency
-        // overlaps the atomic; a timeout recorded by another block is seen at
-        // this or the next barrier, and every wait below is bounded.
+        // The status and limit loads are issued before the arrival so that
+        // their latency overlaps the atomic; a timeout recorded by another
+        // block is seen at this or the next barrier, and every wait below is
+        // bounded.
         const int st0 = *(volatile int*)status;
+        const unsigned limit = *(volatile unsigned*)&bar->limit;  // at least 1
         const unsigned inc = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
         // arrival with release semantics: after the block barrier above it
         // publishes every write this block made before the grid barrier
@@ -35,17 +37,14 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int
                      : "l"(&bar->count), "r"(inc)
                      : "memory");
         bool ok = st0 == DEV_OK;
-        // polls left before giving up (at least 1), read when the first poll
-        // finds the barrier still closed
-        unsigned left = 0;
-        for (bool first = true;; first = false) {
+        unsigned polls = 0;
+        for (;;) {
             // acquire load: writes published by the other blocks' arrivals are
             // visible to this block once the top bit has flipped
             unsigned cur;
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(cur) : "l"(&bar->count) : "memory");
             if (((old ^ cur) & 0x80000000u) != 0u) break;
-            if (first) left = *(volatile unsigned*)&bar->limit;
-            if (--left == 0u) {
+            if (++polls >= limit) {
                 atomicExch(status, DEV_TIMEOUT);
                 ok = false;
                 break;

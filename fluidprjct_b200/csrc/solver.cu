@@ -780,8 +780,7 @@ void phase_g2p_advect(fp_solver* s, int do_g2p, int do_adv, bool guarded = false
     const BodyShape b = sdf ? body_shape(s) : BodyShape{};
     launch_g2p_advect(s->d_pos, s->d_vel, s->np, s->d_u, s->d_v, s->d_w, s->d_us, s->d_vs, s->d_ws, s->d_labels, s->g,
                       s->cfg.pic_weight, s->cfg.dt, s->cfg.cfl, do_g2p, do_adv, s->cfg.advection == FP_ADVECT_RK2,
-                      s->st, guarded ? &s->pb.out->status : nullptr, sdf ? &b : nullptr,
-                      s->sorted ? s->d_start : nullptr);
+                      s->st, guarded ? &s->pb.out->status : nullptr, sdf ? &b : nullptr);
     if (do_adv) s->sorted = false;
 }
 
