@@ -151,7 +151,13 @@ __device__ __forceinline__ void particle_update(const S& smp, float4* __restrict
 }
 
 // One thread per particle, any particle order (also 2D grids).
-__global__ void __launch_bounds__(256) k_g2p_advect(float4* __restrict__ pos, float4* __restrict__ vel, int64_t np,
+// G2P_MIN_BLOCKS (a build tunable) bounds registers for that many CTAs per SM.
+#ifdef G2P_MIN_BLOCKS
+#define G2P_BOUNDS __launch_bounds__(256, G2P_MIN_BLOCKS)
+#else
+#define G2P_BOUNDS __launch_bounds__(256)
+#endif
+__global__ void G2P_BOUNDS k_g2p_advect(float4* __restrict__ pos, float4* __restrict__ vel, int64_t np,
                                                     GlobalSampler smp, const uint8_t* __restrict__ lab,
                                                     AdvectParams a, const int* __restrict__ guard) {
     const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
