@@ -21,6 +21,16 @@ namespace fp {
 
 namespace {
 
+// P2G_UNROLL (a build tunable): unroll factor of the walk over a cell's
+// particles (more loads in flight against more registers).
+#define P2G_PRAGMA_(x) _Pragma(#x)
+#define P2G_PRAGMA(x) P2G_PRAGMA_(x)
+#ifdef P2G_UNROLL
+#define P2G_WALK_UNROLL P2G_PRAGMA(unroll P2G_UNROLL)
+#else
+#define P2G_WALK_UNROLL
+#endif
+
 // Packed FP32 pairs (sm_100's f32x2 FMA/mul/add): two lanes of one 64-bit
 // register, each an IEEE FP32 operation rounded to nearest.
 __device__ __forceinline__ float2 f2_fma(float2 a, float2 b, float2 c) {
@@ -66,11 +76,7 @@ __device__ __forceinline__ void axis3(int s0, int base, float f, float (&w)[3]) 
 // 9 packed FMAs and adds per component.  num accumulates vel*wgt with one
 // fused multiply-add (the reference rounds the product first; its float
 // atomics already leave the last bits of the sums order-dependent).
-// MA, MB: which of the three slots of the other two axes (in the order x, y,
-// z without the component's own axis) hold owned faces; slots outside the
-// masks are neither computed nor added (halo cells reach only a one-slot-wide
-// slab of the brick's faces).
-template <int COMP, int MA = 7, int MB = 7>
+template <int COMP>
 __device__ __forceinline__ void splat_cell(const float4* __restrict__ pos, const float4* __restrict__ vel, int q0,
                                            int q1, int ci, int cj, int ck, const Dims& g, float* s_num, float* s_den,
                                            int fx0, int fx1, int fy0, int fy1, int fz0, int fz1, int lsx, int lsy) {
@@ -81,6 +87,7 @@ __device__ __forceinline__ void splat_cell(const float4* __restrict__ pos, const
     float2 an[9], ad[9];  // pair = the component axis' two faces; index = the other two axes' slots
 #pragma unroll
     for (int m = 0; m < 9; ++m) { an[m] = make_float2(0.0f, 0.0f); ad[m] = make_float2(0.0f, 0.0f); }
+    P2G_WALK_UNROLL
     for (int q = q0; q < q1; ++q) {
         const float4 P = pos[q];
         const float rx = over_dx(P.x, g), ry = over_dx(P.y, g), rz = over_dx(P.z, g);
@@ -114,11 +121,9 @@ __device__ __forceinline__ void splat_cell(const float4* __restrict__ pos, const
             axis3(sz0, bk, fz, wz);
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-                if (!((MA >> b) & 1)) continue;
                 const float2 wab = f2_mul(wa, make_float2(wy[b], wy[b]));
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    if (!((MB >> c) & 1)) continue;
                     const float2 wgt = f2_mul(wab, make_float2(wz[c], wz[c]));
                     an[b + 3 * c] = f2_fma(vv, wgt, an[b + 3 * c]);
                     ad[b + 3 * c] = f2_add(ad[b + 3 * c], wgt);
@@ -131,11 +136,9 @@ __device__ __forceinline__ void splat_cell(const float4* __restrict__ pos, const
             axis3(sz0, bk, fz, wz);
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                if (!((MA >> a) & 1)) continue;
                 const float2 wab = f2_mul(make_float2(wx[a], wx[a]), wb);
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    if (!((MB >> c) & 1)) continue;
                     const float2 wgt = f2_mul(wab, make_float2(wz[c], wz[c]));
                     an[a + 3 * c] = f2_fma(vv, wgt, an[a + 3 * c]);
                     ad[a + 3 * c] = f2_add(ad[a + 3 * c], wgt);
@@ -150,7 +153,6 @@ __device__ __forceinline__ void splat_cell(const float4* __restrict__ pos, const
             for (int a = 0; a < 3; ++a)
 #pragma unroll
                 for (int b = 0; b < 3; ++b) {
-                    if (!((MA >> a) & 1) || !((MB >> b) & 1)) continue;
                     const float wab = wx[a] * wy[b];
                     const float2 wgt = f2_mul(make_float2(wab, wab), wc);
                     an[a + 3 * b] = f2_fma(vv, wgt, an[a + 3 * b]);
@@ -165,7 +167,6 @@ __device__ __forceinline__ void splat_cell(const float4* __restrict__ pos, const
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
             const int o1 = m % 3, o2 = m / 3;
-            if (!((MA >> o1) & 1) || !((MB >> o2) & 1)) continue;
             const float num = e ? an[m].y : an[m].x, den = e ? ad[m].y : ad[m].x;
             const int fi = COMP == 0 ? sx0 + e : sx0 + o1;
             const int fj = COMP == 1 ? sy0 + e : sy0 + (COMP == 0 ? o1 : o2);
@@ -177,28 +178,6 @@ __device__ __forceinline__ void splat_cell(const float4* __restrict__ pos, const
         }
 }
 
-// Cell regions of a brick's walk.  R_FULL: the brick's own cells (and the
-// halo's edges and corners), every slot.  A halo cell on one face of the
-// brick reaches only the brick faces next to it: on the low side of axis a
-// the last slot of each non-staggered component along a and the upper face
-// of the component staggered along a; on the high side the first slot, and
-// nothing of the staggered component.
-enum : int { R_FULL = 0, R_XLO, R_XHI, R_YLO, R_YHI, R_ZLO, R_ZHI };
-__host__ __device__ constexpr int region_axis(int R) {
-    return (R == R_XLO || R == R_XHI) ? 0 : (R == R_YLO || R == R_YHI) ? 1 : (R == R_ZLO || R == R_ZHI) ? 2 : -1;
-}
-__host__ __device__ constexpr bool region_low(int R) { return R == R_XLO || R == R_YLO || R == R_ZLO; }
-// axis (0 x, 1 y, 2 z) of component COMP's first (which = 0) or second
-// non-staggered axis
-__host__ __device__ constexpr int other_axis(int COMP, int which) {
-    return COMP == 0 ? 1 + which : (COMP == 1 ? 2 * which : which);
-}
-// slot mask of that axis in region R: all three slots, the last (low side)
-// or the first (high side)
-__host__ __device__ constexpr int region_mask(int R, int COMP, int which) {
-    return region_axis(R) != other_axis(COMP, which) ? 7 : (region_low(R) ? 4 : 1);
-}
-
 // Owned face ranges of a brick (inclusive): cells [i0, ie] x [j0, je] x
 // [k0, ke]; the staggered component of an axis also owns the far boundary
 // face in the last brick of that axis (iue, jve, kwe).
@@ -206,26 +185,20 @@ struct Owned {
     int i0, ie, iue, j0, je, jve, k0, ke, kwe;
 };
 
-// All three components of one cell's particles in region R.
-template <int R, int BX, int BY, int BZ>
-__device__ __forceinline__ void splat_region(const float4* __restrict__ pos, const float4* __restrict__ vel,
+// All three components of one cell's particles.
+template <int BX, int BY, int BZ>
+__device__ __forceinline__ void splat_all(const float4* __restrict__ pos, const float4* __restrict__ vel,
                                              const int* __restrict__ start, int ci, int cj, int ck, const Dims& g,
                                              float* s_num, float* s_den, const Owned& o) {
     constexpr int NU = (BX + 1) * BY * BZ, NV = BX * (BY + 1) * BZ;
     const int c = ci + cj * g.W + ck * g.W * g.H;
     const int q0 = start[c], q1 = start[c + 1];
     if (q0 == q1) return;
-    if (!(R == R_XHI))
-        splat_cell<0, region_mask(R, 0, 0), region_mask(R, 0, 1)>(pos, vel, q0, q1, ci, cj, ck, g, s_num, s_den, o.i0,
-                                                                 o.iue, o.j0, o.je, o.k0, o.ke, BX + 1, BY);
-    if (!(R == R_YHI))
-        splat_cell<1, region_mask(R, 1, 0), region_mask(R, 1, 1)>(pos, vel, q0, q1, ci, cj, ck, g, s_num + NU,
-                                                                 s_den + NU, o.i0, o.ie, o.j0, o.jve, o.k0, o.ke, BX,
-                                                                 BY + 1);
-    if (!(R == R_ZHI))
-        splat_cell<2, region_mask(R, 2, 0), region_mask(R, 2, 1)>(pos, vel, q0, q1, ci, cj, ck, g, s_num + NU + NV,
-                                                                 s_den + NU + NV, o.i0, o.ie, o.j0, o.je, o.k0, o.kwe,
-                                                                 BX, BY);
+    splat_cell<0>(pos, vel, q0, q1, ci, cj, ck, g, s_num, s_den, o.i0, o.iue, o.j0, o.je, o.k0, o.ke, BX + 1, BY);
+    splat_cell<1>(pos, vel, q0, q1, ci, cj, ck, g, s_num + NU, s_den + NU, o.i0, o.ie, o.j0, o.jve, o.k0, o.ke, BX,
+                  BY + 1);
+    splat_cell<2>(pos, vel, q0, q1, ci, cj, ck, g, s_num + NU + NV, s_den + NU + NV, o.i0, o.ie, o.j0, o.je, o.k0,
+                  o.kwe, BX, BY);
 }
 
 // CTAs per SM that the register budget must allow (P2G_MIN_BLOCKS, a build
@@ -234,6 +207,7 @@ __device__ __forceinline__ void splat_region(const float4* __restrict__ pos, con
 #ifndef P2G_MIN_BLOCKS
 #define P2G_MIN_BLOCKS 3
 #endif
+
 template <int BX, int BY, int BZ, int NT>
 __global__ void __launch_bounds__(NT, P2G_MIN_BLOCKS) k_p2g(const float4* __restrict__ pos, const float4* __restrict__ vel,
                                             const int* __restrict__ start, Dims g, float dt, float3 grav,
@@ -260,67 +234,18 @@ __global__ void __launch_bounds__(NT, P2G_MIN_BLOCKS) k_p2g(const float4* __rest
     __syncthreads();
 
     // Cells whose particles reach an owned face: the brick plus one halo
-    // cell.  The brick's cells first, then each face of the halo shell with
-    // the slots it can reach (a region per loop, so a warp's cells share
-    // their region), then the shell's edges and corners with every slot.
+    // cell, each with its full 2 x 3 x 3 window per component.  (Splats
+    // specialised to the few slots a halo cell reaches, one per face of the
+    // halo shell, made the kernel 2.7x larger and slower: instruction-cache
+    // misses became its largest stall.)
     const Owned own{i0, ie, iue, j0, je, jve, k0, ke, kwe};
-    const int bxe = ie - i0 + 1, bye = je - j0 + 1, bze = ke - k0 + 1;
     const int ilo = max(i0 - 1, 0), ihi = min(ie + 1, W - 1);
     const int jlo = max(j0 - 1, 0), jhi = min(je + 1, H - 1);
     const int klo = max(k0 - 1, 0), khi = min(ke + 1, D - 1);
     const int ni = ihi - ilo + 1, nj = jhi - jlo + 1;
-    // One flat, evenly shared list of work items: the brick's cells, each
-    // halo face (a segment per region, so a warp's cells share their region:
-    // the segment sizes are multiples of 32 for a full brick), then every cell
-    // of the halo box, of which only the edges and corners are walked.
-    const int n_int = bxe * bye * bze, n_x = bye * bze, n_y = bxe * bze, n_z = bxe * bye;
-    const int seg[8] = {n_int, i0 > 0 ? n_x : 0, ie + 1 < W ? n_x : 0, j0 > 0 ? n_y : 0, je + 1 < H ? n_y : 0,
-                        k0 > 0 ? n_z : 0, ke + 1 < D ? n_z : 0, ni * nj * (khi - klo + 1)};
-    int total = 0;
-#pragma unroll
-    for (int r = 0; r < 8; ++r) total += seg[r];
-    for (int t0 = threadIdx.x; t0 < total; t0 += NT) {
-        int r = 0, t = t0;
-#pragma unroll
-        for (int q = 0; q < 7; ++q)  // constant indices keep seg[] in registers
-            if (r == q && t >= seg[q]) { t -= seg[q]; r = q + 1; }
-        switch (r) {
-            case 0:
-                splat_region<R_FULL, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + (t / bxe) % bye,
-                                                 k0 + t / (bxe * bye), g, s_num, s_den, own);
-                break;
-            case 1:
-                splat_region<R_XLO, BX, BY, BZ>(pos, vel, start, i0 - 1, j0 + t % bye, k0 + t / bye, g, s_num, s_den,
-                                                own);
-                break;
-            case 2:
-                splat_region<R_XHI, BX, BY, BZ>(pos, vel, start, ie + 1, j0 + t % bye, k0 + t / bye, g, s_num, s_den,
-                                                own);
-                break;
-            case 3:
-                splat_region<R_YLO, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 - 1, k0 + t / bxe, g, s_num, s_den,
-                                                own);
-                break;
-            case 4:
-                splat_region<R_YHI, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, je + 1, k0 + t / bxe, g, s_num, s_den,
-                                                own);
-                break;
-            case 5:
-                splat_region<R_ZLO, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + t / bxe, k0 - 1, g, s_num, s_den,
-                                                own);
-                break;
-            case 6:
-                splat_region<R_ZHI, BX, BY, BZ>(pos, vel, start, i0 + t % bxe, j0 + t / bxe, ke + 1, g, s_num, s_den,
-                                                own);
-                break;
-            default: {
-                const int ci = ilo + t % ni, cj = jlo + (t / ni) % nj, ck = klo + t / (ni * nj);
-                const int outside = (ci < i0 || ci > ie) + (cj < j0 || cj > je) + (ck < k0 || ck > ke);
-                if (outside >= 2)  // the brick's cells and the halo faces are done above
-                    splat_region<R_FULL, BX, BY, BZ>(pos, vel, start, ci, cj, ck, g, s_num, s_den, own);
-            }
-        }
-    }
+    for (int t = threadIdx.x; t < ni * nj * (khi - klo + 1); t += NT)
+        splat_all<BX, BY, BZ>(pos, vel, start, ilo + t % ni, jlo + (t / ni) % nj, klo + t / (ni * nj), g, s_num, s_den,
+                              own);
     __syncthreads();
 
     // Epilogue: num/den (ComputeVelocityFunc :598-605), u* <- u, u += dt*g.
