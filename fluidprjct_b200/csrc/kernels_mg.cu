@@ -704,7 +704,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
                 if (!k.ok[u]) continue;
                 const int c = k.c[u];
                 a.xs[c] = xv[u] * alpha;
-                a.p[c] = xv[u];  // p0 = g; q holds A p0
+                if (a.x0) a.p[c] = xv[u];  // the learned guess: p0 = g; q holds A p0
                 const double rv = rv0[u] - alpha * qc[u];
                 r[c] = rv;
                 b0[c] = float(rv);
