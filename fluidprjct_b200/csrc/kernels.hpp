@@ -105,8 +105,10 @@ void launch_scatter(const float4* pos, const float4* vel, const int* key, const 
                     float4* pos2, float4* vel2, cudaStream_t st);
 
 // -------- P2G with the fused normalise / save / gravity epilogue (kernels_p2g.cu) --------
-void launch_p2g(const float4* pos, const float4* vel, const int* start, Dims g, float dt, float3 gravity, float* u,
-                float* v, float* w, float* us, float* vs, float* ws, int fused_forces, cudaStream_t st);
+// acc: [nu + nv + nw] (num, den) pairs, zero on entry and left zero (four launches).
+void launch_p2g(const float4* pos, const float4* vel, const int* start, Dims g, float dt, float3 gravity,
+                float2* acc, float* u, float* v, float* w, float* us, float* vs, float* ws, int fused_forces,
+                cudaStream_t st);
 void launch_forces(float* u, float* v, float* w, Dims g, float dt, float3 gravity, cudaStream_t st);
 void launch_copy(const float* src, float* dst, int64_t n, cudaStream_t st);
 

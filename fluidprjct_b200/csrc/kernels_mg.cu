@@ -845,7 +845,8 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
             const int i = c % sy - 1, j = (c / sy) % (F.H + 2) - 1, k = c / sz - 1;
             a.pout[(int64_t(k) * F.H + j) * F.W + i] = float(xv);
         }
-        a.xs[c] = 0.0; a.p[c] = 0.0; a.q[c] = 0.0; r[c] = 0.0; b0[c] = 0.0f; z[c] = 0.0f; F.code[c] = 0;
+        a.xs[c] = fmin(fabs(xv), 0.0);  // +0 computed from the load (a constant store would wait on it)
+        a.p[c] = 0.0; a.q[c] = 0.0; r[c] = 0.0; b0[c] = 0.0f; z[c] = 0.0f; F.code[c] = 0;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.out->iters = it;

@@ -131,6 +131,7 @@ struct fp_solver {
     uint8_t *d_base = nullptr, *d_labels = nullptr, *d_bodymark = nullptr;
     float *d_u = nullptr, *d_v = nullptr, *d_w = nullptr, *d_us = nullptr, *d_vs = nullptr, *d_ws = nullptr,
           *d_p = nullptr, *d_scratch = nullptr, *d_scratch2 = nullptr;
+    float2* d_acc = nullptr;  // P2G (num, den) pairs of every face; zero between steps
     int *d_counts = nullptr, *d_start = nullptr, *d_tiles = nullptr;
     // particles (cell order; pid in pos.w)
     float4 *d_pos = nullptr, *d_vel = nullptr, *d_pos2 = nullptr, *d_vel2 = nullptr;
@@ -196,6 +197,7 @@ void free_r2(fp_solver* s) {
 void free_grid(fp_solver* s) {
     dfree(s->d_base); dfree(s->d_labels); dfree(s->d_bodymark);
     dfree(s->d_u); dfree(s->d_v); dfree(s->d_w); dfree(s->d_us); dfree(s->d_vs); dfree(s->d_ws);
+    dfree(s->d_acc);
     dfree(s->d_p); dfree(s->d_scratch); dfree(s->d_scratch2);
     dfree(s->d_counts); dfree(s->d_start); dfree(s->d_tiles);
     PressureBufs& pb = s->pb;
@@ -264,6 +266,7 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     ck(dalloc(&s->d_u, s->g.nu())); ck(dalloc(&s->d_us, s->g.nu()));
     ck(dalloc(&s->d_v, s->g.nv())); ck(dalloc(&s->d_vs, s->g.nv()));
     ck(dalloc(&s->d_w, s->g.nw())); ck(dalloc(&s->d_ws, s->g.nw()));
+    ck(dalloc(&s->d_acc, s->g.nu() + s->g.nv() + s->g.nw()));
     ck(dalloc(&s->d_p, nc)); ck(dalloc(&s->d_scratch, nc)); ck(dalloc(&s->d_scratch2, nc));
     ck(dalloc(&s->d_counts, nc + 1)); ck(dalloc(&s->d_start, nc + 1)); ck(dalloc(&s->d_tiles, ntiles));
     PressureBufs& pb = s->pb;
@@ -303,6 +306,7 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     for (float* a : {s->d_u, s->d_us}) ck(cudaMemsetAsync(a, 0, sizeof(float) * s->g.nu(), s->st));
     for (float* a : {s->d_v, s->d_vs}) ck(cudaMemsetAsync(a, 0, sizeof(float) * s->g.nv(), s->st));
     for (float* a : {s->d_w, s->d_ws}) ck(cudaMemsetAsync(a, 0, sizeof(float) * s->g.nw(), s->st));
+    ck(cudaMemsetAsync(s->d_acc, 0, sizeof(float2) * (s->g.nu() + s->g.nv() + s->g.nw()), s->st));
     ck(cudaMemsetAsync(s->d_p, 0, sizeof(float) * nc, s->st));
     ck(cudaMemsetAsync(s->d_bodymark, 0, nc, s->st));
     for (int i = 0; i < 2; ++i) {
@@ -394,9 +398,9 @@ void phase_label(fp_solver* s) {
 
 void phase_p2g(fp_solver* s, int fused) {
     if (!s->sorted) phase_label(s);
-    s->launches += 1;
-    launch_p2g(s->d_pos, s->d_vel, s->d_start, s->g, s->cfg.dt, gravity3(), s->d_u, s->d_v, s->d_w, s->d_us, s->d_vs,
-               s->d_ws, fused, s->st);
+    s->launches += 4;
+    launch_p2g(s->d_pos, s->d_vel, s->d_start, s->g, s->cfg.dt, gravity3(), s->d_acc, s->d_u, s->d_v, s->d_w,
+               s->d_us, s->d_vs, s->d_ws, fused, s->st);
 }
 
 void phase_save(fp_solver* s) {
