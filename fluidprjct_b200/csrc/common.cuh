@@ -35,14 +35,20 @@ struct BodyKin {
 
 // x / dx, by the exact reciprocal multiply when dx is a power of two.
 __device__ __forceinline__ float over_dx(float x, const Dims& g) { return g.idx != 0.0f ? x * g.idx : x / g.dx; }
+// The same with the choice made at compile time (P2: dx is a power of two and
+// Dims.idx = 1/dx).  Hot kernels take P2 as a template argument: a run-time
+// choice lets the compiler evaluate the division on every path.
+template <bool P2>
+__device__ __forceinline__ float to_grid(float x, const Dims& g) { return P2 ? x * g.idx : x / g.dx; }
 
 __device__ __forceinline__ int clampi(int a, int lo, int hi) { return min(max(a, lo), hi); }
 __device__ __forceinline__ float clamp01(float f) { return fminf(fmaxf(f, 0.0f), 1.0f); }
 
 // Cell of a particle: floorf(p/dx) clamped to the grid (MarkFluidCellsFunctor,
 // FluidSolver3D.cu:316-331).
+template <bool P2>
 __device__ __forceinline__ int cell_key(float x, float y, float z, const Dims& g) {
-    int i = int(floorf(over_dx(x, g))), j = int(floorf(over_dx(y, g))), k = int(floorf(over_dx(z, g)));
+    int i = int(floorf(to_grid<P2>(x, g))), j = int(floorf(to_grid<P2>(y, g))), k = int(floorf(to_grid<P2>(z, g)));
     i = clampi(i, 0, g.W - 1);
     j = clampi(j, 0, g.H - 1);
     k = clampi(k, 0, g.D - 1);
@@ -123,9 +129,10 @@ __device__ __forceinline__ float sample_delta(const float* __restrict__ f, const
 __device__ __forceinline__ int sxy_u(const Dims& g) { return g.D > 1 ? (g.W + 1) * g.H : 0; }
 __device__ __forceinline__ int sxy_v(const Dims& g) { return g.D > 1 ? g.W * (g.H + 1) : 0; }
 
+template <bool P2>
 __device__ __forceinline__ float3 interp_vel(const float* __restrict__ u, const float* __restrict__ v,
                                              const float* __restrict__ w, const Dims& g, float3 pos) {
-    const float rx = over_dx(pos.x, g), ry = over_dx(pos.y, g), rz = over_dx(pos.z, g);
+    const float rx = to_grid<P2>(pos.x, g), ry = to_grid<P2>(pos.y, g), rz = to_grid<P2>(pos.z, g);
     return make_float3(sample(u, stencil_u(rx, ry, rz, g), g.W + 1, sxy_u(g)),
                        sample(v, stencil_v(rx, ry, rz, g), g.W, sxy_v(g)),
                        sample(w, stencil_w(rx, ry, rz, g), g.W, g.W * g.H));

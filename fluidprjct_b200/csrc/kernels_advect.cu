@@ -34,9 +34,11 @@ __constant__ signed char c_off[34][3] = {
     {-2, -1, 0}, {0, -1, -2}, {-2, -2, 0}, {0, -2, -2},
     {-2, -2, -2}, {-2, 0, -2}, {2, -1, 0}, {0, -1, 2}};
 
+template <bool P2>
 __device__ __forceinline__ bool project_particle(float3& pos, const uint8_t* __restrict__ lab, const Dims& g) {
     const float dx = g.dx;
-    const int cx = int(floorf(over_dx(pos.x, g))), cy = int(floorf(over_dx(pos.y, g))), cz = int(floorf(over_dx(pos.z, g)));
+    const int cx = int(floorf(to_grid<P2>(pos.x, g))), cy = int(floorf(to_grid<P2>(pos.y, g))),
+              cz = int(floorf(to_grid<P2>(pos.z, g)));
     float best = 1e10f;
     int bn = -1;
 #pragma unroll 2
@@ -71,7 +73,8 @@ struct GlobalSampler {
         dlt = make_float3(sample_delta(u, us, su, sxu, sxyu), sample_delta(v, vs, sv, sxv, sxyv),
                           sample_delta(w, ws, sw, sxw, sxyw));
     }
-    __device__ __forceinline__ float3 vel(float3 p) const { return interp_vel(u, v, w, g, p); }
+    template <bool P2>
+    __device__ __forceinline__ float3 vel(float3 p) const { return interp_vel<P2>(u, v, w, g, p); }
 };
 
 struct AdvectParams {
@@ -81,8 +84,9 @@ struct AdvectParams {
 };
 
 // G2P and advection of particle q (GridToParticleFunctor :803-980,
-// AdvectParticlesFunctor :1241-1330), with face samples from S.
-template <class S>
+// AdvectParticlesFunctor :1241-1330), with face samples from S; P2: dx is a
+// power of two (to_grid).
+template <class S, bool P2>
 __device__ __forceinline__ void particle_update(const S& smp, float4* __restrict__ pos, float4* __restrict__ vel,
                                                 int64_t q, const uint8_t* __restrict__ lab, const Dims& g,
                                                 const AdvectParams& a) {
@@ -92,7 +96,7 @@ __device__ __forceinline__ void particle_update(const S& smp, float4* __restrict
     if (a.do_g2p) {
         const float4 V = vel[q];
         float3 pic, dlt;
-        smp.g2p(over_dx(p.x, g), over_dx(p.y, g), over_dx(p.z, g), pic, dlt);
+        smp.g2p(to_grid<P2>(p.x, g), to_grid<P2>(p.y, g), to_grid<P2>(p.z, g), pic, dlt);
         const float alpha = a.alpha;
         float4 out;
         out.x = alpha * pic.x + (1.0f - alpha) * (V.x + dlt.x);
@@ -109,20 +113,20 @@ __device__ __forceinline__ void particle_update(const S& smp, float4* __restrict
     const float floor_speed = sqrtf((5.0f * dx) * 9.8f);
     const float xmax = float(g.W - 1) * dx, ymax = float(g.H - 1) * dx, zmax = float(g.D - 1) * dx;
     while (!finished && iter++ < 1000) {
-        const float3 vel0 = smp.vel(p);
+        const float3 vel0 = smp.template vel<P2>(p);
         const float speed = sqrtf(vel0.x * vel0.x + vel0.y * vel0.y + vel0.z * vel0.z) + 1e-37f + floor_speed;
         float dT = (a.C * dx) / speed;
         if (subT + dT >= dt) { dT = dt - subT; finished = true; }
         else if (subT + 2.0f * dT >= dt) { dT *= 0.5f; }
         if (a.rk2) {
             const float3 mid = make_float3(p.x + (vel0.x * 0.5f) * dT, p.y + (vel0.y * 0.5f) * dT, p.z + (vel0.z * 0.5f) * dT);
-            const float3 k2 = smp.vel(mid);
+            const float3 k2 = smp.template vel<P2>(mid);
             p = make_float3(p.x + k2.x * dT, p.y + k2.y * dT, p.z + k2.z * dT);
         } else {
             const float3 k1 = vel0;
-            const float3 k2 = smp.vel(make_float3(p.x + (k1.x * 0.5f) * dT, p.y + (k1.y * 0.5f) * dT,
+            const float3 k2 = smp.template vel<P2>(make_float3(p.x + (k1.x * 0.5f) * dT, p.y + (k1.y * 0.5f) * dT,
                                                   p.z + (k1.z * 0.5f) * dT));
-            const float3 k3 = smp.vel(make_float3(p.x + (k2.x * 0.75f) * dT, p.y + (k2.y * 0.75f) * dT,
+            const float3 k3 = smp.template vel<P2>(make_float3(p.x + (k2.x * 0.75f) * dT, p.y + (k2.y * 0.75f) * dT,
                                                   p.z + (k2.z * 0.75f) * dT));
             const float a1 = (2.0f / 9.0f) * dT, a2 = (3.0f / 9.0f) * dT, a3 = (4.0f / 9.0f) * dT;
             p = make_float3(p.x + k1.x * a1 + k2.x * a2 + k3.x * a3, p.y + k1.y * a1 + k2.y * a2 + k3.y * a3,
@@ -138,11 +142,12 @@ __device__ __forceinline__ void particle_update(const S& smp, float4* __restrict
             p.y = fminf(fmaxf(p.y, 0.0f), ymax);
             p.z = fminf(fmaxf(p.z, 0.0f), zmax);
         }
-        const int cx = int(floorf(over_dx(p.x, g))), cy = int(floorf(over_dx(p.y, g))), cz = int(floorf(over_dx(p.z, g)));
+        const int cx = int(floorf(to_grid<P2>(p.x, g))), cy = int(floorf(to_grid<P2>(p.y, g))),
+                  cz = int(floorf(to_grid<P2>(p.z, g)));
         if (cx >= 0 && cx < g.W && cy >= 0 && cy < g.H && cz >= 0 && cz < g.D) {
             const uint8_t l = __ldg(lab + cx + cy * g.W + cz * g.W * g.H);
             if (l == SOLID || (l == BODY && !a.sdf_collide)) {
-                if (!project_particle(p, lab, g)) break;
+                if (!project_particle<P2>(p, lab, g)) break;
             }
         }
         if (p.x < 0.0f || p.y < 0.0f || p.z < 0.0f || isnan(p.x) || isnan(p.y) || isnan(p.z)) break;
@@ -150,19 +155,24 @@ __device__ __forceinline__ void particle_update(const S& smp, float4* __restrict
     pos[q] = make_float4(p.x, p.y, p.z, P.w);
 }
 
-// One thread per particle, any particle order (also 2D grids).
-// G2P_MIN_BLOCKS (a build tunable) bounds registers for that many CTAs per SM.
-#ifdef G2P_MIN_BLOCKS
-#define G2P_BOUNDS __launch_bounds__(256, G2P_MIN_BLOCKS)
-#else
-#define G2P_BOUNDS __launch_bounds__(256)
+// One thread per particle, any particle order (also 2D grids).  G2P_THREADS
+// and G2P_MIN_BLOCKS (build tunables) set the CTA size and bound registers
+// for that many CTAs per SM.
+#ifndef G2P_THREADS
+#define G2P_THREADS 384
 #endif
+#ifdef G2P_MIN_BLOCKS
+#define G2P_BOUNDS __launch_bounds__(G2P_THREADS, G2P_MIN_BLOCKS)
+#else
+#define G2P_BOUNDS __launch_bounds__(G2P_THREADS)
+#endif
+template <bool P2>
 __global__ void G2P_BOUNDS k_g2p_advect(float4* __restrict__ pos, float4* __restrict__ vel, int64_t np,
                                                     GlobalSampler smp, const uint8_t* __restrict__ lab,
                                                     AdvectParams a, const int* __restrict__ guard) {
     const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (q >= np || solve_failed(guard)) return;
-    particle_update(smp, pos, vel, q, lab, smp.g, a);
+    particle_update<GlobalSampler, P2>(smp, pos, vel, q, lab, smp.g, a);
 }
 
 __global__ void k_unsort(const float4* __restrict__ pos, const float4* __restrict__ vel, int64_t np,
@@ -212,7 +222,9 @@ void launch_g2p_advect(float4* pos, float4* vel, int64_t np, const float* u, con
     a.do_g2p = do_g2p; a.do_advect = do_advect; a.rk2 = rk2; a.sdf_collide = collide ? 1 : 0;
     if (collide) a.body = *collide;
     const GlobalSampler G{u, v, w, us, vs, ws, g};
-    k_g2p_advect<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, vel, np, G, labels, a, guard);
+    const unsigned nb = unsigned((np + G2P_THREADS - 1) / G2P_THREADS);
+    if (g.idx != 0.0f) k_g2p_advect<true><<<nb, G2P_THREADS, 0, st>>>(pos, vel, np, G, labels, a, guard);
+    else k_g2p_advect<false><<<nb, G2P_THREADS, 0, st>>>(pos, vel, np, G, labels, a, guard);
 }
 
 void launch_unsort(const float4* pos, const float4* vel, int64_t np, float* pos_out, float* vel_out, cudaStream_t st) {

@@ -150,7 +150,7 @@ __device__ void ref_panel(int i, int j, int k, int dir, const float* u, const fl
     const float3 off = mul3(nrm, 0.5f);  // face offset (+-0.5 along the normal)
     const float3 fc = add3(cc, mul3(off, dx));
     const float3 r = sub3(fc, cm);
-    const float3 up = interp_vel(u, v, w, g, fc);
+    const float3 up = interp_vel<false>(u, v, w, g, fc);
     const float3 ur = sub3(bvel, up);
     const float ua = __fsqrt_rn(dot3(ur, ur));
     const float alpha_s = 0.5f;

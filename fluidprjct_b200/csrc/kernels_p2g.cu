@@ -74,11 +74,6 @@ __device__ __forceinline__ void axis3(int s0, int base, float f, float (&w)[3]) 
 // packed FMAs and adds per component.  num accumulates vel*wgt with one fused
 // multiply-add (the reference rounds the product first; its float atomics
 // already leave the last bits of the sums order-dependent).
-// x / dx: the exact reciprocal multiply when dx is a power of two (P2), else
-// the IEEE division (a kernel template argument, so no path is predicated).
-template <bool P2>
-__device__ __forceinline__ float to_grid(float x, const Dims& g) { return P2 ? x * g.idx : x / g.dx; }
-
 // The particle's velocity component COMP.
 template <int COMP>
 __device__ __forceinline__ float comp_of(const float4& v) { return COMP == 0 ? v.x : (COMP == 1 ? v.y : v.z); }

@@ -17,12 +17,13 @@ constexpr int SCAN_BLOCK = 1024;
 constexpr int SCAN_ITEMS = 4;
 constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
 
+template <bool P2>
 __global__ void k_bin(const float4* __restrict__ pos, int64_t np, Dims g, int* __restrict__ counts,
                       int* __restrict__ key, int* __restrict__ rank) {
     int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (q >= np) return;
     float4 p = pos[q];
-    int c = cell_key(p.x, p.y, p.z, g);
+    int c = cell_key<P2>(p.x, p.y, p.z, g);
     key[q] = c;
     rank[q] = atomicAdd(&counts[c], 1);
 }
@@ -105,7 +106,9 @@ __global__ void k_scan_single_block(int* data, int n, int* total) {
 
 void launch_bin(const float4* pos, int64_t np, Dims g, int* counts, int* key, int* rank, cudaStream_t st) {
     if (np == 0) return;
-    k_bin<<<unsigned((np + 255) / 256), 256, 0, st>>>(pos, np, g, counts, key, rank);
+    const unsigned nb = unsigned((np + 255) / 256);
+    if (g.idx != 0.0f) k_bin<true><<<nb, 256, 0, st>>>(pos, np, g, counts, key, rank);
+    else k_bin<false><<<nb, 256, 0, st>>>(pos, np, g, counts, key, rank);
 }
 
 void launch_label_scan(const uint8_t* base, const uint8_t* body_mark, const int* counts, uint8_t* labels, int* start,
