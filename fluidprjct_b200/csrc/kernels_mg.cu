@@ -19,10 +19,16 @@
 //     so restriction sums the red children.  The coarse correction is scaled
 //     by omega.  Level 0 works on the compact FLUID list.
 // Levels with more than MG_BLOCK_CELLS cells are swept by the whole grid with a
-// grid barrier between sweeps; the remaining coarse levels are done by block 0
-// alone with __syncthreads, on shared-memory copies (labels coarsened there at
-// kernel start; the first block level's b and x copied in and its x copied
-// back out per cycle).  The whole PCG (flexible, in the Chronopoulos-Gear
+// grid barrier between sweeps; every block then does the remaining coarse
+// levels on its own shared-memory copy with __syncthreads only (labels
+// coarsened there at kernel start; the first block level's b and x copied in
+// per cycle) and prolongs from that copy, so the stage costs no grid barrier
+// of its own (one block alone, with a copy-out and a barrier, was 1.5 us per
+// iteration slower at 128^3).  Block levels take MG_NU_BLOCK sweep pairs:
+// two instead of one took the 128^3 dam break from 10.85 to 10.1 iterations
+// per warm-started solve (1.030 to 0.985 ms); two pairs on the grid-wide
+// levels as well reached 8.9 iterations, but their extra grid barriers made
+// the solve slower (1.067 ms).  The whole PCG (flexible, in the Chronopoulos-Gear
 // form, optionally started from a guess) runs in one persistent cooperative
 // launch with the bounded grid barrier.  Precision split: the V-cycle works in FP32; the
 // Krylov vectors (x, r, p, s) and all dot products are FP64, so the
@@ -39,6 +45,15 @@ namespace fp {
 namespace {
 
 constexpr int MG_THREADS = 1024;
+// Red-black sweep pairs before and after the coarse correction on the
+// grid-wide levels below the finest (MG_NU_GRID) and on the block levels
+// above the coarsest (MG_NU_BLOCK); build tunables.
+#ifndef MG_NU_GRID
+#define MG_NU_GRID 1
+#endif
+#ifndef MG_NU_BLOCK
+#define MG_NU_BLOCK 2
+#endif
 // Over-relaxation of every red-black Gauss-Seidel update (pre- and
 // post-smoothing alike, so the cycle stays symmetric): x <- x + w (y - x),
 // y = (b + neighbours) / d.  1 is plain Gauss-Seidel; 1.1 took a 128^3 dam
@@ -53,7 +68,9 @@ struct MgArgs {
     float rscale;                // restriction scale (1/4 in 3D, 1/2 in 2D)
     float omega;                 // over-relaxation of the coarse-grid correction
     int nu_coarse;               // symmetric sweep pairs on the coarsest level
-    int nu0;                     // red-black sweep pairs before and after on level 0 (coarser: 1)
+    int nu0;                     // red-black sweep pairs before and after on level 0
+    int nu_grid;                 // ... on the other grid-wide levels
+    int nu_block;                // ... on the block levels above the coarsest
     MgLevel lv[MG_MAX_LEVELS];
     double* p;                   // level-0 padded dense Krylov vectors (FP64)
     double* q;
@@ -280,7 +297,7 @@ __device__ __forceinline__ void coarsen_cell(const MgLevel& F, const MgLevel& Cl
     Cl.lab[cc] = air ? AIR : (fluid ? FLUID : SOLID);
 }
 
-// ---- the block stage: levels [G, L) solved by block 0 alone ----
+// ---- the block stage: levels [G, L) solved by each block on its own copy ----
 // Shared-memory form.  Per level: x, b and rs (the red cells' residuals) as
 // FP32 padded grids; lab (labels, used while setting up) and code (FLUID:
 // 1 + diagonal, else 0) as bytes; ent, the level's FLUID cells (red ones from
@@ -317,7 +334,7 @@ __host__ __device__ __forceinline__ int mg_smem_bytes(const MgLevel* lv, int G, 
 
 extern __shared__ __align__(16) unsigned char mg_smem[];
 
-// Block 0 at kernel start.  Returns the number of levels that carry FLUID
+// Each block at kernel start.  Returns the number of levels that carry FLUID
 // cells (at least G + 1): the deepest of them is the cycle's coarsest level.
 __device__ int block_levels_init(const MgArgs& a, BlkLevel* S) {
     const int G = a.G, L = a.L, t0 = threadIdx.x, st = blockDim.x;
@@ -429,12 +446,12 @@ __device__ void bl_prolong(const BlkLevel& F, const BlkLevel& C, float omega, in
     }
 }
 
-// V-cycle over the shared-memory levels [l0, nl) by block 0 (nl from
+// V-cycle over the shared-memory levels [l0, nl) by one block (nl from
 // block_levels_init).  Level l0's first sweep is already done: the grid-wide
 // restriction wrote its b and x, which are copied in.  The stage stops after
-// level l0's last black sweep and copies its x back out: the final red sweep
-// of level l0 is the grid-wide prolongation into level l0 - 1, which
-// recomputes it from that copy.
+// level l0's last black sweep: the final red sweep of level l0 is the
+// grid-wide prolongation into level l0 - 1, which recomputes it from this
+// block's copy.
 __device__ void block_vcycle_smem(const MgArgs& a, int l0, int nl, const BlkLevel* S) {
     const int t0 = threadIdx.x, st = blockDim.x;
     const BlkLevel& B0 = S[l0];
@@ -448,6 +465,10 @@ __device__ void block_vcycle_smem(const MgArgs& a, int l0, int nl, const BlkLeve
     const int lc = nl - 1;
     for (int l = l0; l < lc; ++l) {
         bl_sweep(S[l], 1, t0, st); __syncthreads();
+        for (int e = 1; e < a.nu_block; ++e) {
+            bl_sweep(S[l], 0, t0, st); __syncthreads();
+            bl_sweep(S[l], 1, t0, st); __syncthreads();
+        }
         bl_residual(S[l], t0, st); __syncthreads();
         bl_restrict(S[l], S[l + 1], a.rscale, t0, st); __syncthreads();
     }
@@ -467,17 +488,17 @@ __device__ void block_vcycle_smem(const MgArgs& a, int l0, int nl, const BlkLeve
         }
     }
     for (int l = lc - 1; l >= l0; --l) {
+        for (int e = 1; e < a.nu_block; ++e) {
+            bl_sweep(S[l], 1, t0, st); __syncthreads();
+            bl_sweep(S[l], 0, t0, st); __syncthreads();
+        }
         bl_sweep(S[l], 1, t0, st); __syncthreads();
         if (l > l0) {
             bl_sweep(S[l], 0, t0, st); __syncthreads();
             bl_prolong(S[l - 1], S[l], a.omega, t0, st); __syncthreads();
         }
     }
-    // the grid barrier that follows begins with __syncthreads
-    for (int t = t0; t < B0.nred + B0.nblack; t += st) {
-        const int c = int(B0.ent[bl_slot(B0, t)] & 0xFFFFu);
-        a.lv[l0].x[c] = B0.m.x[c];
-    }
+    // the prolongation that follows reads level l0 from this block's copy
 }
 
 // Global-memory form (the block levels do not fit in shared memory, or the
@@ -490,6 +511,10 @@ __device__ void block_vcycle_global(const MgArgs& a, int l0) {
     const int t0 = threadIdx.x, st = blockDim.x;
     for (int l = l0; l < a.L - 1; ++l) {
         op_sweep(a.lv[l], 1, t0, st); __syncthreads();
+        for (int e = 1; e < (l == 0 ? a.nu0 : a.nu_block); ++e) {
+            op_sweep(a.lv[l], 0, t0, st); __syncthreads();
+            op_sweep(a.lv[l], 1, t0, st); __syncthreads();
+        }
         op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st); __syncthreads();
     }
     const int lc = a.L - 1;
@@ -508,6 +533,10 @@ __device__ void block_vcycle_global(const MgArgs& a, int l0) {
         }
     }
     for (int l = lc - 1; l >= l0; --l) {
+        for (int e = 1; e < (l == 0 ? a.nu0 : a.nu_block); ++e) {
+            op_sweep(a.lv[l], 1, t0, st); __syncthreads();
+            op_sweep(a.lv[l], 0, t0, st); __syncthreads();
+        }
         op_sweep(a.lv[l], 1, t0, st); __syncthreads();
         if (l == 0) {
             op_sweep(a.lv[0], 0, t0, st); __syncthreads();
@@ -536,30 +565,39 @@ __device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
         return grid_barrier(a.bar, nb, a.status);
     };
     for (int l = 0; l < G; ++l) {
-        // pre-smoothing (red, black)^nu (nu = nu0 on level 0, else 1); the first
-        // red sweep is fused upstream
+        // pre-smoothing (red, black)^nu (nu = nu0 on level 0, else nu_grid); the
+        // first red sweep is fused upstream
         if (!sweep(l, 1)) return false;
-        for (int e = 1; e < (l == 0 ? a.nu0 : 1); ++e)
+        for (int e = 1; e < (l == 0 ? a.nu0 : a.nu_grid); ++e)
             if (!sweep(l, 0) || !sweep(l, 1)) return false;
         op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
-    if (blockIdx.x == 0) {
-        if (a.smem) block_vcycle_smem(a, G, nl, S);
-        else block_vcycle_global(a, G);
-    }
-    if (!grid_barrier(a.bar, nb, a.status)) return false;
-    if (G > 0) {  // level G's last red sweep, fused with its prolongation into level G - 1
-        if (G == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
-        else op_prolong_red(a.lv[G - 1], a.lv[G], a.omega, t0, st);
+    if (a.smem) {
+        // Every block runs the block levels on its own shared-memory copy (the
+        // same arithmetic, so the same bits) and prolongs from that copy: no
+        // grid barrier and no copy-out between the stage and the prolongation.
+        block_vcycle_smem(a, G, nl, S);
+        MgLevel cg = S[G].m;  // level G in this block's shared memory
+        cg.code = S[G].code;
+        if (G == 1) op0_prolong_red(a.lv[0], cg, a.omega, a.fidx, nf, t0, st);
+        else op_prolong_red(a.lv[G - 1], cg, a.omega, t0, st);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
+    } else {
+        if (blockIdx.x == 0) block_vcycle_global(a, G);
+        if (!grid_barrier(a.bar, nb, a.status)) return false;
+        if (G > 0) {  // level G's last red sweep, fused with its prolongation into level G - 1
+            if (G == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
+            else op_prolong_red(a.lv[G - 1], a.lv[G], a.omega, t0, st);
+            if (!grid_barrier(a.bar, nb, a.status)) return false;
+        }
     }
     for (int l = G - 1; l >= 0; --l) {
         // post-smoothing (black, red)^nu, the reverse of the pre-smoothing; the
         // first red sweep was fused with the prolongation, the last red sweep
         // with the next prolongation
         if (!sweep(l, 1)) return false;
-        for (int e = 1; e < (l == 0 ? a.nu0 : 1); ++e)
+        for (int e = 1; e < (l == 0 ? a.nu0 : a.nu_grid); ++e)
             if (!sweep(l, 0) || !sweep(l, 1)) return false;
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 0, t0, st);
         else if (l == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
@@ -591,8 +629,8 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     };
     auto total = [&]() { double3 t = grid_sum3(a.part + (red & 1) * 3 * nb, nb); ++red; return t; };
     const int sy = F.sy, sz = F.sz;
-    __shared__ BlkLevel s_lv[MG_MAX_LEVELS];  // block 0: the shared-memory block levels
-    const int nl = (blockIdx.x == 0 && a.smem) ? block_levels_init(a, s_lv) : a.L;
+    __shared__ BlkLevel s_lv[MG_MAX_LEVELS];  // the shared-memory block levels
+    const int nl = a.smem ? block_levels_init(a, s_lv) : a.L;  // every block: its own copy
 
     // level codes: level 0 on its FLUID cells (zero elsewhere, restored at the
     // end), the dense grid-wide levels (and, without shared-memory copies, the
@@ -959,6 +997,8 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     a.omega = 1.8f;
     a.nu_coarse = 2;
     a.nu0 = std::max(1, nu0);
+    a.nu_grid = MG_NU_GRID;
+    a.nu_block = MG_NU_BLOCK;
     a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.pprev = x0 ? nullptr : pprev; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
     a.X = static_cast<double*>(pb.X);
     a.pout = pout;
