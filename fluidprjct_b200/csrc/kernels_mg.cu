@@ -13,8 +13,8 @@
 //     multiple of R^T.
 //   * Smoother: red-black Gauss-Seidel over-relaxed by MG_SOR, red then black
 //     going down, black then red coming up (two pairs on the finest level by
-//     default, one on the others); the coarsest level does the same symmetric
-//     sweeps.  The V-cycle is therefore a symmetric positive definite
+//     default, one on the other grid-wide levels, two on the block levels);
+//     the coarsest level does the same symmetric sweeps.  The V-cycle is therefore a symmetric positive definite
 //     preconditioner.  After the black sweep only red cells carry a residual,
 //     so restriction sums the red children.  The coarse correction is scaled
 //     by omega.  Level 0 works on the compact FLUID list.
@@ -54,12 +54,21 @@ constexpr int MG_THREADS = 1024;
 #ifndef MG_NU_BLOCK
 #define MG_NU_BLOCK 2
 #endif
+// Scale of the coarse-grid correction (build tunable).
+#ifndef MG_OMEGA
+#define MG_OMEGA 1.7f
+#endif
 // Over-relaxation of every red-black Gauss-Seidel update (pre- and
 // post-smoothing alike, so the cycle stays symmetric): x <- x + w (y - x),
-// y = (b + neighbours) / d.  1 is plain Gauss-Seidel; 1.1 took a 128^3 dam
-// break from 13.6 to 12.2 iterations per solve (1.05: 12.8, 1.15: 12.1 but
-// more from x = 0, 1.2: 12.4, 1.3: 14.0).
-constexpr float MG_SOR = 1.1f;
+// y = (b + neighbours) / d.  1 is plain Gauss-Seidel.  With two sweep pairs
+// on the block levels, 1.2 (and a coarse correction scaled by 1.7) took the
+// 128^3 dam break from 10.83 to 10.35 iterations per warm-started solve and
+// from 12.9 to 12.1 from x = 0 (mean of 40 steps), against 1.1 and 1.8; 1.15
+// gave 10.48 and 12.5, 1.25 (with 1.8) 11.1.
+#ifndef MG_SOR_VALUE
+#define MG_SOR_VALUE 1.2f
+#endif
+constexpr float MG_SOR = MG_SOR_VALUE;
 __device__ __forceinline__ float sor(float x, float y) { return MG_SOR == 1.0f ? y : x + MG_SOR * (y - x); }
 
 struct MgArgs {
@@ -992,9 +1001,11 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     // 31 -> 14 at 256^2 in a float64 model of this V-cycle).  Any omega > 0
     // keeps the preconditioner symmetric; in that model PCG converged for
     // every omega up to 2 on dam-break, pool and random-box scenes.  With the
-    // over-relaxed smoother, 1.8 is as fast as 1.9 on the dam break and
-    // faster on random boxes (14 against 15 iterations).
-    a.omega = 1.8f;
+    // over-relaxed smoother, 1.8 was as fast as 1.9 on the dam break and
+    // faster on random boxes (14 against 15 iterations); with two sweep pairs
+    // on the block levels and SOR 1.2, 1.7 is best (1.9: 10.55, 2.0: 10.75
+    // iterations per warm-started solve at 128^3).
+    a.omega = MG_OMEGA;
     a.nu_coarse = 2;
     a.nu0 = std::max(1, nu0);
     a.nu_grid = MG_NU_GRID;
