@@ -77,6 +77,68 @@ struct GlobalSampler {
     __device__ __forceinline__ float3 vel(float3 p) const { return interp_vel<P2>(u, v, w, g, p); }
 };
 
+// The eight trilinear corners of one face grid at one stencil base, in the
+// order trilin() takes them, kept in registers across one particle's samples.
+struct Corners {
+    int base;
+    float c[8];
+};
+__device__ __forceinline__ void load_corners(const float* __restrict__ f, int base, int sx, int sxy, Corners& k) {
+    const float* b = f + base;
+    k.c[0] = __ldg(b); k.c[1] = __ldg(b + 1); k.c[2] = __ldg(b + sxy); k.c[3] = __ldg(b + 1 + sxy);
+    k.c[4] = __ldg(b + sx); k.c[5] = __ldg(b + 1 + sx); k.c[6] = __ldg(b + sx + sxy); k.c[7] = __ldg(b + 1 + sx + sxy);
+    k.base = base;
+}
+__device__ __forceinline__ float trilin_k(const Stencil& s, const Corners& k) {
+    return trilin(s.fx, s.fy, s.fz, k.c[0], k.c[1], k.c[2], k.c[3], k.c[4], k.c[5], k.c[6], k.c[7]);
+}
+// Sample of f at stencil s, loading the corners only when the base moved.
+__device__ __forceinline__ float sample_cached(const float* __restrict__ f, const Stencil& s, int sx, int sxy,
+                                               Corners& k) {
+    if (s.base != k.base) load_corners(f, s.base, sx, sxy, k);
+    return trilin_k(s, k);
+}
+// FLIP delta sample from the u corners already loaded in k and u*.
+__device__ __forceinline__ float delta_k(const float* __restrict__ g, const Stencil& s, int sx, int sxy,
+                                         const Corners& k) {
+    const float* b = g + s.base;
+    return trilin(s.fx, s.fy, s.fz, k.c[0] - __ldg(b), k.c[1] - __ldg(b + 1), k.c[2] - __ldg(b + sxy),
+                  k.c[3] - __ldg(b + 1 + sxy), k.c[4] - __ldg(b + sx), k.c[5] - __ldg(b + 1 + sx),
+                  k.c[6] - __ldg(b + sx + sxy), k.c[7] - __ldg(b + 1 + sx + sxy));
+}
+
+// The same samples with each face grid's eight corners cached per particle:
+// a particle moves a small fraction of a cell per substep (C = 0.1), so its
+// G2P sample and most of its advection samples share stencil bases, and the
+// corners are loaded again only when a base changes.  The values and the
+// arithmetic are those of GlobalSampler, so the results are identical.
+struct CachedSampler {
+    GlobalSampler s;
+    Corners cu, cv, cw;
+    __device__ __forceinline__ explicit CachedSampler(const GlobalSampler& g) : s(g) {
+        cu.base = cv.base = cw.base = -1;
+    }
+    __device__ __forceinline__ void g2p(float rx, float ry, float rz, float3& pic, float3& dlt) {
+        const Dims& g = s.g;
+        const Stencil su = stencil_u(rx, ry, rz, g), sv = stencil_v(rx, ry, rz, g), sw = stencil_w(rx, ry, rz, g);
+        const int sxu = g.W + 1, sxyu = sxy_u(g), sxv = g.W, sxyv = sxy_v(g), sxw = g.W, sxyw = g.W * g.H;
+        load_corners(s.u, su.base, sxu, sxyu, cu);
+        load_corners(s.v, sv.base, sxv, sxyv, cv);
+        load_corners(s.w, sw.base, sxw, sxyw, cw);
+        pic = make_float3(trilin_k(su, cu), trilin_k(sv, cv), trilin_k(sw, cw));
+        dlt = make_float3(delta_k(s.us, su, sxu, sxyu, cu), delta_k(s.vs, sv, sxv, sxyv, cv),
+                          delta_k(s.ws, sw, sxw, sxyw, cw));
+    }
+    template <bool P2>
+    __device__ __forceinline__ float3 vel(float3 p) {
+        const Dims& g = s.g;
+        const float rx = to_grid<P2>(p.x, g), ry = to_grid<P2>(p.y, g), rz = to_grid<P2>(p.z, g);
+        return make_float3(sample_cached(s.u, stencil_u(rx, ry, rz, g), g.W + 1, sxy_u(g), cu),
+                           sample_cached(s.v, stencil_v(rx, ry, rz, g), g.W, sxy_v(g), cv),
+                           sample_cached(s.w, stencil_w(rx, ry, rz, g), g.W, g.W * g.H, cw));
+    }
+};
+
 struct AdvectParams {
     float alpha, dt, C;
     int do_g2p, do_advect, rk2, sdf_collide;
@@ -87,7 +149,7 @@ struct AdvectParams {
 // AdvectParticlesFunctor :1241-1330), with face samples from S; P2: dx is a
 // power of two (to_grid).
 template <class S, bool P2>
-__device__ __forceinline__ void particle_update(const S& smp, float4* __restrict__ pos, float4* __restrict__ vel,
+__device__ __forceinline__ void particle_update(S& smp, float4* __restrict__ pos, float4* __restrict__ vel,
                                                 int64_t q, const uint8_t* __restrict__ lab, const Dims& g,
                                                 const AdvectParams& a) {
     const float4 P = pos[q];
@@ -158,8 +220,12 @@ __device__ __forceinline__ void particle_update(const S& smp, float4* __restrict
 // One thread per particle, any particle order (also 2D grids).  G2P_THREADS
 // and G2P_MIN_BLOCKS (build tunables) set the CTA size and bound registers
 // for that many CTAs per SM.
+// Per-particle corner cache of the face samples (a build tunable).
+#ifndef G2P_CORNER_CACHE
+#define G2P_CORNER_CACHE 1
+#endif
 #ifndef G2P_THREADS
-#define G2P_THREADS 384
+#define G2P_THREADS 128
 #endif
 #ifdef G2P_MIN_BLOCKS
 #define G2P_BOUNDS __launch_bounds__(G2P_THREADS, G2P_MIN_BLOCKS)
@@ -172,7 +238,13 @@ __global__ void G2P_BOUNDS k_g2p_advect(float4* __restrict__ pos, float4* __rest
                                                     AdvectParams a, const int* __restrict__ guard) {
     const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (q >= np || solve_failed(guard)) return;
-    particle_update<GlobalSampler, P2>(smp, pos, vel, q, lab, smp.g, a);
+#if G2P_CORNER_CACHE
+    CachedSampler cs(smp);
+    particle_update<CachedSampler, P2>(cs, pos, vel, q, lab, smp.g, a);
+#else
+    GlobalSampler gs = smp;
+    particle_update<GlobalSampler, P2>(gs, pos, vel, q, lab, smp.g, a);
+#endif
 }
 
 __global__ void k_unsort(const float4* __restrict__ pos, const float4* __restrict__ vel, int64_t np,
