@@ -77,20 +77,54 @@ struct GlobalSampler {
     __device__ __forceinline__ float3 vel(float3 p) const { return interp_vel<P2>(u, v, w, g, p); }
 };
 
-// The eight trilinear corners of one face grid at one stencil base, in the
-// order trilin() takes them, kept in registers across one particle's samples.
+// Packed FP32 pairs (sm_100's f32x2 FMA/mul): two lanes of one 64-bit
+// register, each an IEEE FP32 operation rounded to nearest.
+__device__ __forceinline__ float2 f2_fma(float2 a, float2 b, float2 c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)),
+          "l"(*reinterpret_cast<unsigned long long*>(&c)));
+    return *reinterpret_cast<float2*>(&d);
+}
+__device__ __forceinline__ float2 f2_mul(float2 a, float2 b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)));
+    return *reinterpret_cast<float2*>(&d);
+}
+
+// The eight trilinear corners of one face grid at one stencil base, kept in
+// registers across one particle's samples, as z pairs: z0 = (c000, c001),
+// z1 = (c100, c101), z2 = (c010, c011), z3 = (c110, c111), the first index
+// along x, the second along y (row stride sx), the third along z (slice
+// stride sxy).
 struct Corners {
     int base;
-    float c[8];
+    float2 z0, z1, z2, z3;
 };
 __device__ __forceinline__ void load_corners(const float* __restrict__ f, int base, int sx, int sxy, Corners& k) {
     const float* b = f + base;
-    k.c[0] = __ldg(b); k.c[1] = __ldg(b + 1); k.c[2] = __ldg(b + sxy); k.c[3] = __ldg(b + 1 + sxy);
-    k.c[4] = __ldg(b + sx); k.c[5] = __ldg(b + 1 + sx); k.c[6] = __ldg(b + sx + sxy); k.c[7] = __ldg(b + 1 + sx + sxy);
+    k.z0 = make_float2(__ldg(b), __ldg(b + sxy));
+    k.z1 = make_float2(__ldg(b + 1), __ldg(b + 1 + sxy));
+    k.z2 = make_float2(__ldg(b + sx), __ldg(b + sx + sxy));
+    k.z3 = make_float2(__ldg(b + 1 + sx), __ldg(b + 1 + sx + sxy));
     k.base = base;
 }
+// trilinearInterpolation (FluidSolver3D.cu:783-801) on z pairs: the four x
+// lerps as two packed ones, the two y lerps as one, then the z lerp.
+__device__ __forceinline__ float trilin_pairs(float xd, float yd, float zd, float2 z0, float2 z1, float2 z2,
+                                              float2 z3) {
+    const float2 ox = make_float2(1.0f - xd, 1.0f - xd), wx = make_float2(xd, xd);
+    const float2 y0 = f2_fma(z1, wx, f2_mul(z0, ox));  // (c00, c01)
+    const float2 y1 = f2_fma(z3, wx, f2_mul(z2, ox));  // (c10, c11)
+    const float2 oy = make_float2(1.0f - yd, 1.0f - yd), wy = make_float2(yd, yd);
+    const float2 c = f2_fma(y1, wy, f2_mul(y0, oy));   // (c0, c1)
+    return c.x * (1.0f - zd) + c.y * zd;
+}
 __device__ __forceinline__ float trilin_k(const Stencil& s, const Corners& k) {
-    return trilin(s.fx, s.fy, s.fz, k.c[0], k.c[1], k.c[2], k.c[3], k.c[4], k.c[5], k.c[6], k.c[7]);
+    return trilin_pairs(s.fx, s.fy, s.fz, k.z0, k.z1, k.z2, k.z3);
 }
 // Sample of f at stencil s, loading the corners only when the base moved.
 __device__ __forceinline__ float sample_cached(const float* __restrict__ f, const Stencil& s, int sx, int sxy,
@@ -98,20 +132,25 @@ __device__ __forceinline__ float sample_cached(const float* __restrict__ f, cons
     if (s.base != k.base) load_corners(f, s.base, sx, sxy, k);
     return trilin_k(s, k);
 }
-// FLIP delta sample from the u corners already loaded in k and u*.
+// FLIP delta sample from the u corners already loaded in k and u*: each
+// corner is u* * (-1) + u in one fused step, which rounds as u - u* does.
 __device__ __forceinline__ float delta_k(const float* __restrict__ g, const Stencil& s, int sx, int sxy,
                                          const Corners& k) {
     const float* b = g + s.base;
-    return trilin(s.fx, s.fy, s.fz, k.c[0] - __ldg(b), k.c[1] - __ldg(b + 1), k.c[2] - __ldg(b + sxy),
-                  k.c[3] - __ldg(b + 1 + sxy), k.c[4] - __ldg(b + sx), k.c[5] - __ldg(b + 1 + sx),
-                  k.c[6] - __ldg(b + sx + sxy), k.c[7] - __ldg(b + 1 + sx + sxy));
+    const float2 m1 = make_float2(-1.0f, -1.0f);
+    const float2 d0 = f2_fma(make_float2(__ldg(b), __ldg(b + sxy)), m1, k.z0);
+    const float2 d1 = f2_fma(make_float2(__ldg(b + 1), __ldg(b + 1 + sxy)), m1, k.z1);
+    const float2 d2 = f2_fma(make_float2(__ldg(b + sx), __ldg(b + sx + sxy)), m1, k.z2);
+    const float2 d3 = f2_fma(make_float2(__ldg(b + 1 + sx), __ldg(b + 1 + sx + sxy)), m1, k.z3);
+    return trilin_pairs(s.fx, s.fy, s.fz, d0, d1, d2, d3);
 }
 
 // The same samples with each face grid's eight corners cached per particle:
 // a particle moves a small fraction of a cell per substep (C = 0.1), so its
 // G2P sample and most of its advection samples share stencil bases, and the
-// corners are loaded again only when a base changes.  The values and the
-// arithmetic are those of GlobalSampler, so the results are identical.
+// corners are loaded again only when a base changes.  The interpolation is
+// the packed form of GlobalSampler's: the same products, the x and y lerps
+// two lanes at a time, each lerp one multiply and one fused multiply-add.
 struct CachedSampler {
     GlobalSampler s;
     Corners cu, cv, cw;
