@@ -54,6 +54,10 @@ constexpr int MG_THREADS = 1024;
 #ifndef MG_NU_BLOCK
 #define MG_NU_BLOCK 2
 #endif
+// Symmetric sweep pairs on the coarsest level (build tunable).
+#ifndef MG_NU_COARSE
+#define MG_NU_COARSE 2
+#endif
 // Scale of the coarse-grid correction (build tunable).
 #ifndef MG_OMEGA
 #define MG_OMEGA 1.7f
@@ -70,6 +74,12 @@ constexpr int MG_THREADS = 1024;
 #endif
 constexpr float MG_SOR = MG_SOR_VALUE;
 __device__ __forceinline__ float sor(float x, float y) { return MG_SOR == 1.0f ? y : x + MG_SOR * (y - x); }
+// The same on the coarser levels (build tunable MG_SOR_COARSE_VALUE).
+#ifndef MG_SOR_COARSE_VALUE
+#define MG_SOR_COARSE_VALUE MG_SOR_VALUE
+#endif
+constexpr float MG_SORC = MG_SOR_COARSE_VALUE;
+__device__ __forceinline__ float sorc(float x, float y) { return MG_SORC == 1.0f ? y : x + MG_SORC * (y - x); }
 
 struct MgArgs {
     int L, G;                    // levels; levels [0, G) are grid-wide
@@ -187,8 +197,8 @@ __device__ void op0_sweep(const MgLevel& L, const int* fidx, const uint8_t* dg, 
 // Gauss-Seidel update of one FLUID cell (code dc > 0).
 __device__ __forceinline__ void gs_update(const MgLevel& L, int c) {
     const int dc = L.code[c];
-    const float bv = L.b[c], nb = lv_nbsum(L, c), xo = MG_SOR == 1.0f ? 0.0f : L.x[c];
-    if (dc > 0) L.x[c] = dc > 1 ? sor(xo, (bv + nb) / float(dc - 1)) : 0.0f;
+    const float bv = L.b[c], nb = lv_nbsum(L, c), xo = MG_SORC == 1.0f ? 0.0f : L.x[c];
+    if (dc > 0) L.x[c] = dc > 1 ? sorc(xo, (bv + nb) / float(dc - 1)) : 0.0f;
 }
 // Gauss-Seidel update of the FLUID cells of one colour.  With an even width
 // the work items are the cells of that colour only: cell i2 of a row is
@@ -238,7 +248,7 @@ __device__ void op_restrict_first(const MgLevel& F, const MgLevel& Cl, float sca
             if (ii && kk) s += fine_residual(F, c0 + 1 + F.sz);
             if (jj && kk) s += fine_residual(F, c0 + F.sy + F.sz);
             s *= scale;
-            if (((I + J + K) & 1) == 0) xv = dc > 1 ? sor(0.0f, s / float(dc - 1)) : 0.0f;
+            if (((I + J + K) & 1) == 0) xv = dc > 1 ? sorc(0.0f, s / float(dc - 1)) : 0.0f;
         }
         Cl.b[cc] = s;
         Cl.x[cc] = xv;
@@ -257,7 +267,7 @@ __device__ __forceinline__ void prolong_one(const MgLevel& F, int c, const MgLev
     const int dc = Cl.code[cc];
     const float xc = Cl.x[cc], bc = Cl.b[cc], nb = lv_nbsum(Cl, cc), xf = F.x[c];
     if (dc == 0) return;
-    const float v = ((I + J + K) & 1) != 0 ? xc : (dc > 1 ? sor(xc, (bc + nb) / float(dc - 1)) : 0.0f);
+    const float v = ((I + J + K) & 1) != 0 ? xc : (dc > 1 ? sorc(xc, (bc + nb) / float(dc - 1)) : 0.0f);
     F.x[c] = xf + omega * v;
 }
 // ... over every cell of the fine level F (dense levels)
@@ -416,7 +426,7 @@ __device__ void bl_sweep(const BlkLevel& B, int color, int t0, int st) {
     for (int t = t0; t < n; t += st) {
         const int c = int(e[t] & 0xFFFFu);
         const int d = B.code[c] - 1;
-        B.m.x[c] = d > 0 ? sor(B.m.x[c], (B.m.b[c] + lv_nbsum(B.m, c)) / float(d)) : 0.0f;
+        B.m.x[c] = d > 0 ? sorc(B.m.x[c], (B.m.b[c] + lv_nbsum(B.m, c)) / float(d)) : 0.0f;
     }
 }
 // rs = b - A x on the red FLUID cells (after a black sweep the black ones vanish).
@@ -441,7 +451,7 @@ __device__ void bl_restrict(const BlkLevel& F, const BlkLevel& C, float scale, i
         s *= scale;
         C.m.b[cc] = s;
         const int d = C.code[cc] - 1;
-        C.m.x[cc] = (t < C.nred && d > 0) ? sor(0.0f, s / float(d)) : 0.0f;
+        C.m.x[cc] = (t < C.nred && d > 0) ? sorc(0.0f, s / float(d)) : 0.0f;
     }
 }
 // Prolongation: every FLUID cell of F adds omega * its parent's x when the
@@ -1006,7 +1016,7 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     // on the block levels and SOR 1.2, 1.7 is best (1.9: 10.55, 2.0: 10.75
     // iterations per warm-started solve at 128^3).
     a.omega = MG_OMEGA;
-    a.nu_coarse = 2;
+    a.nu_coarse = MG_NU_COARSE;
     a.nu0 = std::max(1, nu0);
     a.nu_grid = MG_NU_GRID;
     a.nu_block = MG_NU_BLOCK;
