@@ -129,7 +129,10 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_fluid_build(const uint8_t* __res
     for (int t = 0; t < SCAN_ITEMS; ++t) {
         if (lab[t] != FLUID) continue;
         int64_t e = e0 + t;
-        int i = int(e % g.W), j = int((e / g.W) % g.H), k = int(e / (int64_t(g.W) * g.H));
+        // 32-bit decode: cell indices fit in an int (the padded index does too)
+        const uint32_t eu = uint32_t(e), W = uint32_t(g.W), H = uint32_t(g.H);
+        const uint32_t ej = eu / W;
+        const int i = int(eu - ej * W), j = int(ej % H), k = int(ej / H);
         fidx[n] = int(padded_index(i, j, k, g));
         int d = 0;
         const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
@@ -433,21 +436,27 @@ __global__ void k_project(float* __restrict__ u, float* __restrict__ v, float* _
     if (i > W || j > H || k > D) return;
     const float dx = g.dx;
     const uint8_t lc = label_at(lab, g, i, j, k);
+    // A face between two AIR cells keeps its velocity exactly (the pressure is
+    // zero off the fluid: vel - scale * (0 - 0) is vel), so it is neither read
+    // nor written; in a dam break most faces are such.
+    const uint8_t lx = label_at(lab, g, i - 1, j, k), ly = label_at(lab, g, i, j - 1, k),
+                  lz = label_at(lab, g, i, j, k - 1);
+    const bool air = lc == AIR;
     const float pc = p_at(p, g, i, j, k);
-    if (j < H && k < D) {
+    if (j < H && k < D && !(air && lx == AIR)) {
         int64_t id = int64_t(i) + int64_t(j) * (W + 1) + int64_t(k) * (W + 1) * H;
         float vb = body.active ? body_vel_at(body, make_float3(float(i) * dx, (float(j) + 0.5f) * dx, (float(k) + 0.5f) * dx)).x : 0.0f;
-        u[id] = project_face(u[id], label_at(lab, g, i - 1, j, k), lc, p_at(p, g, i - 1, j, k), pc, vb, scale, inv);
+        u[id] = project_face(u[id], lx, lc, p_at(p, g, i - 1, j, k), pc, vb, scale, inv);
     }
-    if (i < W && k < D) {
+    if (i < W && k < D && !(air && ly == AIR)) {
         int64_t id = int64_t(i) + int64_t(j) * W + int64_t(k) * W * (H + 1);
         float vb = body.active ? body_vel_at(body, make_float3((float(i) + 0.5f) * dx, float(j) * dx, (float(k) + 0.5f) * dx)).y : 0.0f;
-        v[id] = project_face(v[id], label_at(lab, g, i, j - 1, k), lc, p_at(p, g, i, j - 1, k), pc, vb, scale, inv);
+        v[id] = project_face(v[id], ly, lc, p_at(p, g, i, j - 1, k), pc, vb, scale, inv);
     }
-    if (i < W && j < H) {
+    if (i < W && j < H && !(air && lz == AIR)) {
         int64_t id = int64_t(i) + int64_t(j) * W + int64_t(k) * W * H;
         float vb = body.active ? body_vel_at(body, make_float3((float(i) + 0.5f) * dx, (float(j) + 0.5f) * dx, float(k) * dx)).z : 0.0f;
-        w[id] = project_face(w[id], label_at(lab, g, i, j, k - 1), lc, p_at(p, g, i, j, k - 1), pc, vb, scale, inv);
+        w[id] = project_face(w[id], lz, lc, p_at(p, g, i, j, k - 1), pc, vb, scale, inv);
     }
 }
 
