@@ -17,15 +17,31 @@ constexpr int SCAN_BLOCK = 1024;
 constexpr int SCAN_ITEMS = 4;
 constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
 
+// Particles arrive nearly in cell order (sorted last step, moved less than a
+// cell), so a warp's lanes share a few cells: one atomic per distinct cell of
+// the warp (lanes grouped by __match_any_sync), each lane's rank the group's
+// base plus its place among the group's lanes.  The order of a cell's
+// particles is arbitrary either way.  Every lane of every warp reaches the
+// match (the block size is a multiple of 32; lanes past np carry key -1).
 template <bool P2>
 __global__ void k_bin(const float4* __restrict__ pos, int64_t np, Dims g, int* __restrict__ counts,
                       int* __restrict__ key, int* __restrict__ rank) {
-    int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (q >= np) return;
-    float4 p = pos[q];
-    int c = cell_key<P2>(p.x, p.y, p.z, g);
-    key[q] = c;
-    rank[q] = atomicAdd(&counts[c], 1);
+    const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool ok = q < np;
+    int c = -1;
+    if (ok) {
+        const float4 p = pos[q];
+        c = cell_key<P2>(p.x, p.y, p.z, g);
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, c);
+    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    int base = 0;
+    if (ok && lane == leader) base = atomicAdd(&counts[c], __popc(grp));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (ok) {
+        key[q] = c;
+        rank[q] = base + __popc(grp & ((1u << lane) - 1u));
+    }
 }
 
 __device__ __forceinline__ uint8_t label_of(uint8_t base, uint8_t body, int count) {
