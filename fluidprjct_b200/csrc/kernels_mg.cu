@@ -998,7 +998,10 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStrea
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
                   const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0, int nu0,
                   const float* pprev, float* pout, unsigned wait_polls) {
-    const int nb = mg_max_blocks();
+    // One block per 4096 cells (each thread's UNR cells per trip), at most one
+    // per SM: a small grid waits at cheaper barriers (one block: __syncthreads).
+    const int64_t want = (g.nc() + int64_t(MG_THREADS) * UNR - 1) / (int64_t(MG_THREADS) * UNR);
+    const int nb = int(std::max<int64_t>(1, std::min<int64_t>(mg_max_blocks(), want)));
     int* status = &pb.out->status;
     launch_reset_barrier(pb.bar, status, wait_polls, st);
     MgArgs a;

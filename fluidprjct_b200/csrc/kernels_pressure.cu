@@ -531,7 +531,10 @@ int pcg_max_blocks() {
 template <class T>
 static int launch_pcg_t(Dims g, PressureBufs& pb, const float* rhs, double tol, int maxit, cudaStream_t st,
                         unsigned wait_polls) {
-    const int nb = pcg_max_blocks();
+    // One block per four cells per thread, at most the resident maximum: a
+    // small grid waits at cheaper barriers (one block: __syncthreads).
+    const int64_t want = (g.nc() + int64_t(PCG_THREADS) * 4 - 1) / (int64_t(PCG_THREADS) * 4);
+    const int nb = int(std::max<int64_t>(1, std::min<int64_t>(pcg_max_blocks(), want)));
     int* status = &pb.out->status;
     k_reset_pcg<<<1, 1, 0, st>>>(pb.bar, status, wait_polls);
     PcgArgs<T> a;

@@ -21,6 +21,9 @@ namespace {
 __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* status) {
     __shared__ int s_ok;
     __syncthreads();
+    // A one-block launch (a small grid) has no other block to wait for: the
+    // block barrier alone orders its threads' global writes and reads.
+    if (nblocks == 1u) return true;
     if (threadIdx.x == 0) {
         // The status and limit loads are issued before the arrival so that
         // their latency overlaps the atomic; a timeout recorded by another
