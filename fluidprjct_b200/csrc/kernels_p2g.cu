@@ -191,10 +191,12 @@ struct Reach {
 };
 
 // CTAs per SM that the register budget must allow (P2G_MIN_BLOCKS, a build
-// tunable): 3 gives 80 registers, 2 gives up to 128; the walk over a cell's
-// particles is latency-bound, so occupancy and spills trade against each other.
+// tunable): the walk over a cell's particles is latency-bound, so occupancy
+// and spills trade against each other.  With 8 x 8 x 8 bricks at 128^3, 4
+// (64 registers, a 12-byte spill) took the phase to 0.186 ms; 3 (78
+// registers) gave 0.202, 2 0.220, and 5 and 6 spilled (0.30, 0.49 ms).
 #ifndef P2G_MIN_BLOCKS
-#define P2G_MIN_BLOCKS 3
+#define P2G_MIN_BLOCKS 4
 #endif
 
 // Pass 1: one CTA per brick.  acc holds (num, den) pairs for the u, v and w
