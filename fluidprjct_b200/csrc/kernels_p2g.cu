@@ -16,10 +16,12 @@
 // (num, den) pairs into a global FP32 pair array with one vector reduction
 // per face, so every particle is walked once (a brick that instead re-walks
 // a one-cell halo to own its faces outright walks each particle 1.76 times
-// on average for 16 x 8 x 8 bricks); empty bricks return at once.  Bricks of
-// 8 x 8 x 8 cells (two per thread) balance the SMs better than 16 x 8 x 8:
-// the dam break's ~640 full bricks of that size filled 1.4 waves of three
-// CTAs per SM (0.198 against 0.232 ms for the phase at 128^3).  A second,
+// on average for 16 x 8 x 8 bricks); empty bricks return at once.  Small
+// bricks balance the SMs: the dam break's ~640 full 16 x 8 x 8 bricks filled
+// 1.4 waves of three CTAs per SM (0.232 ms for the phase at 128^3, 0.198 with
+// 8 x 8 x 8).  The default is 8 x 8 x 4 cells, one per thread of a 128-thread
+// CTA, eight CTAs per SM (0.180 ms; 8 x 8 x 8 with 256 threads at four per SM
+// 0.186, 8 x 4 x 4 0.182).  A second,
 // elementwise kernel divides, saves and adds gravity, and zeroes the pair
 // array for the next step.
 #include "kernels.hpp"
@@ -192,11 +194,12 @@ struct Reach {
 
 // CTAs per SM that the register budget must allow (P2G_MIN_BLOCKS, a build
 // tunable): the walk over a cell's particles is latency-bound, so occupancy
-// and spills trade against each other.  With 8 x 8 x 8 bricks at 128^3, 4
-// (64 registers, a 12-byte spill) took the phase to 0.186 ms; 3 (78
-// registers) gave 0.202, 2 0.220, and 5 and 6 spilled (0.30, 0.49 ms).
+// and spills trade against each other.  With 256-thread 8 x 8 x 8 bricks at
+// 128^3, four per SM (64 registers, a 12-byte spill) took the phase to 0.186
+// ms; three (78 registers) gave 0.202, two 0.220, and five and six spilled
+// (0.30, 0.49 ms).  The default is 64 registers for the 128-thread CTAs.
 #ifndef P2G_MIN_BLOCKS
-#define P2G_MIN_BLOCKS 4
+#define P2G_MIN_BLOCKS 8
 #endif
 
 // Pass 1: one CTA per brick.  acc holds (num, den) pairs for the u, v and w
@@ -313,8 +316,8 @@ __global__ void k_copy(const float* __restrict__ s, float* __restrict__ d, int64
 #ifndef P2G_BRICK_X
 #define P2G_BRICK_X 8
 #define P2G_BRICK_Y 8
-#define P2G_BRICK_Z 8
-#define P2G_THREADS 256
+#define P2G_BRICK_Z 4
+#define P2G_THREADS 128
 #endif
 constexpr int P2G_BX = P2G_BRICK_X, P2G_BY = P2G_BRICK_Y, P2G_BZ = P2G_BRICK_Z, P2G_NT = P2G_THREADS;
 
