@@ -113,6 +113,35 @@ def test_fused_p2g_epilogue_matches_phases(O):
         assert rel_l2(a.grid(g), b.grid(g)) <= 1e-6
 
 
+def test_p2g_leaves_its_pair_array_clear(O):
+    """P2G adds each brick's face sums into a device array of (num, den) pairs,
+    and its finish pass clears that array for the next transfer.  A second
+    transfer of other velocities must equal a fresh solver's transfer of those
+    velocities.  (A stale sum from the same velocities would cancel in num/den,
+    so the second transfer uses different ones.)"""
+    from fluidprjct_b200 import capi
+    dx, dt = 0.05, 0.004
+    lab, pos, vel = _scene(O)
+    vel2 = (-0.5 * vel + 0.1).astype(np.float32)
+    a = _solver(dx=dx, dt=dt, pic_weight=0.05)
+    a.set_labels(lab)
+    a.set_particles(pos, vel)
+    a.phase(capi.PHASE_LABEL)
+    a.phase(capi.PHASE_P2G)
+    a.set_particles(pos, vel2)
+    a.phase(capi.PHASE_LABEL)
+    a.phase(capi.PHASE_P2G)
+    b = _solver(dx=dx, dt=dt, pic_weight=0.05)
+    b.set_labels(lab)
+    b.set_particles(pos, vel2)
+    b.phase(capi.PHASE_LABEL)
+    b.phase(capi.PHASE_P2G)
+    for g in (capi.GRID_U, capi.GRID_V, capi.GRID_W):
+        assert rel_l2(a.grid(g), b.grid(g)) <= 1e-6, g
+    a.close()
+    b.close()
+
+
 def _prepare_pressure(O, solver="pcg", tol=1e-6):
     from fluidprjct_b200 import capi
     dx, dt = 0.05, 0.004
