@@ -60,6 +60,21 @@ cudaError_t dalloc_bytes(void** p, size_t bytes) {
     return cudaMalloc(p, bytes ? bytes : 1);
 }
 
+// The solve's read-back block, on the device and pinned on the host: PcgOut,
+// then the true residual's two FP64 sums, then the FLUID count, so that one
+// copy per step brings all three back (three small copies each took their
+// own turn on the stream).
+constexpr size_t kRbRed = (sizeof(PcgOut) + 7) & ~size_t(7);
+constexpr size_t kRbNf = kRbRed + 2 * sizeof(double);
+constexpr size_t kRbBytes = (kRbNf + sizeof(int) + 15) & ~size_t(15);
+template <class Out, class Red, class Nf>
+void readback_views(void* base, Out*& out, Red*& red, Nf*& nf) {
+    char* b = static_cast<char*>(base);
+    out = reinterpret_cast<Out*>(b);
+    red = b ? reinterpret_cast<Red*>(b + kRbRed) : nullptr;
+    nf = b ? reinterpret_cast<Nf*>(b + kRbNf) : nullptr;
+}
+
 }  // namespace
 
 // Rigid body state on the host (RigidBody, utility.cuh:195-491): position,
@@ -201,10 +216,11 @@ void free_grid(fp_solver* s) {
     dfree(s->d_p); dfree(s->d_scratch); dfree(s->d_scratch2);
     dfree(s->d_counts); dfree(s->d_start); dfree(s->d_tiles);
     PressureBufs& pb = s->pb;
-    dfree(pb.nf); dfree(pb.fidx); dfree(pb.diag); dfree(pb.b); dfree(pb.bin);
+    pb.nf = nullptr; pb.red = nullptr;  // inside the read-back block (pb.out)
+    dfree(pb.fidx); dfree(pb.diag); dfree(pb.b); dfree(pb.bin);
     for (int i = 0; i < 2; ++i) { dfree(pb.R[i]); dfree(pb.Wv[i]); dfree(pb.S[i]); }
     dfree(pb.invd); dfree(pb.P); dfree(pb.X);
-    dfree(pb.x64); dfree(pb.xd); dfree(pb.part); dfree(pb.bar); dfree(pb.out); dfree(pb.red);
+    dfree(pb.x64); dfree(pb.xd); dfree(pb.part); dfree(pb.bar); dfree(pb.out);
     for (int l = 0; l < s->mgL; ++l) {
         dfree(s->mg[l].lab); dfree(s->mg[l].x); dfree(s->mg[l].b); dfree(s->mg[l].code);
     }
@@ -270,7 +286,12 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     ck(dalloc(&s->d_p, nc)); ck(dalloc(&s->d_scratch, nc)); ck(dalloc(&s->d_scratch2, nc));
     ck(dalloc(&s->d_counts, nc + 1)); ck(dalloc(&s->d_start, nc + 1)); ck(dalloc(&s->d_tiles, ntiles));
     PressureBufs& pb = s->pb;
-    ck(dalloc(&pb.nf, 1)); ck(dalloc(&pb.fidx, nc)); ck(dalloc(&pb.diag, nc)); ck(dalloc(&pb.b, nc));
+    {
+        void* rb = nullptr;
+        ck(dalloc_bytes(&rb, kRbBytes));
+        readback_views(rb, pb.out, pb.red, pb.nf);
+    }
+    ck(dalloc(&pb.fidx, nc)); ck(dalloc(&pb.diag, nc)); ck(dalloc(&pb.b, nc));
     ck(dalloc(&pb.bin, nc));
     const size_t pbytes = sizeof(double) * size_t(s->padded), cbytes = sizeof(double) * size_t(nc);
     for (int i = 0; i < 2; ++i) {
@@ -279,7 +300,7 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
     ck(dalloc_bytes(&pb.invd, pbytes)); ck(dalloc_bytes(&pb.P, cbytes)); ck(dalloc_bytes(&pb.X, cbytes));
     ck(dalloc(&pb.x64, nc)); ck(dalloc(&pb.xd, s->padded));
     ck(dalloc(&pb.part, size_t(6) * std::max(maxb, 1024)));
-    ck(dalloc(&pb.bar, 1)); ck(dalloc(&pb.out, 1)); ck(dalloc(&pb.red, 2));
+    ck(dalloc(&pb.bar, 1));
     pb.tile_sums = s->d_tiles;
     ck(dalloc(&s->d_rhs_dense, nc));
     if (s->cfg.solver == FP_SOLVER_PCG_LEARNED || s->cfg.solver == FP_SOLVER_PCG_LEARNED_MIXED)
@@ -474,9 +495,7 @@ int solve_system(fp_solver* s, float* p_out, bool defer = false) {
             } else {
                 s->launches += 1;  // the MG kernel
             }
-            cudaMemcpyAsync(s->h_out, pb.out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s->st);
-            cudaMemcpyAsync(s->h_red, pb.red, sizeof(double) * 2, cudaMemcpyDeviceToHost, s->st);
-            cudaMemcpyAsync(s->h_nf, pb.nf, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+            cudaMemcpyAsync(s->h_out, pb.out, kRbBytes, cudaMemcpyDeviceToHost, s->st);  // out, red and nf
         };
         auto finish = [&](bool jacobi) -> cudaError_t {
             finish_launch(jacobi);
@@ -1198,9 +1217,11 @@ int fp_create(const fp_config* cfg, fp_solver** out) {
     for (auto& ev : s->ev) if (e == cudaSuccess) e = cudaEventCreate(&ev);
     for (auto& ev : s->ev_pcg) if (e == cudaSuccess) e = cudaEventCreate(&ev);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev_net);
-    if (e == cudaSuccess) e = cudaMallocHost(&s->h_out, sizeof(PcgOut));
-    if (e == cudaSuccess) e = cudaMallocHost(&s->h_red, sizeof(double) * 2);
-    if (e == cudaSuccess) e = cudaMallocHost(&s->h_nf, sizeof(int));
+    if (e == cudaSuccess) {
+        void* rb = nullptr;
+        e = cudaMallocHost(&rb, kRbBytes);
+        if (e == cudaSuccess) readback_views(rb, s->h_out, s->h_red, s->h_nf);
+    }
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_bad, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&s->d_bad, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_bforce, sizeof(double) * 8);
@@ -1226,9 +1247,7 @@ int fp_destroy(fp_solver* s) {
     for (auto& ev : s->ev) if (ev) cudaEventDestroy(ev);
     for (auto& ev : s->ev_pcg) if (ev) cudaEventDestroy(ev);
     if (s->ev_net) cudaEventDestroy(s->ev_net);
-    if (s->h_out) cudaFreeHost(s->h_out);
-    if (s->h_red) cudaFreeHost(s->h_red);
-    if (s->h_nf) cudaFreeHost(s->h_nf);
+    if (s->h_out) cudaFreeHost(s->h_out);  // h_red and h_nf lie inside it
     if (s->h_bad) cudaFreeHost(s->h_bad);
     if (s->d_bad) cudaFree(s->d_bad);
     if (s->st) cudaStreamDestroy(s->st);
