@@ -74,9 +74,10 @@ int mg_max_blocks();
 // copies take (0: the block levels stay in global memory).
 int mg_split(const MgLevel* lv, int L, int* smem_bytes);
 // Level labels from the cell labels (per solve): the grid-wide coarse levels;
-// the solver kernel coarsens the shared-memory levels itself.  Returns the
-// number of launches.
-int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStream_t st);
+// the solver kernel coarsens the shared-memory levels itself.  With l1list
+// (room for level 1's W*H*D cells) it also lists level 1's FLUID cells there
+// and their number in *l1n.  Returns the number of launches.
+int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, int* l1list, int* l1n, cudaStream_t st);
 // MG-preconditioned PCG (FP32 V-cycle, FP64 Krylov vectors and reductions) for
 // A x = rhs (compact) to ||r||/||rhs|| <= tol; solution in pb.X (FP64
 // compact).  p, q, xs, r are level-0 padded dense FP64 work grids, zero at
@@ -89,9 +90,10 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStrea
 // gathered at the FLUID cells and scaled like x0; null to start from zero.
 // pout: the dense W x H x D pressure out (its non-FLUID cells must be zero),
 // or null.  The kernel also writes the true residual's ||rhs - A x||^2 and
-// ||rhs||^2 (FP64) to pb.red.
-int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
-                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0 = nullptr, int nu0 = 2,
+// ||rhs||^2 (FP64) to pb.red.  l1list / l1n: level 1's FLUID cells from
+// launch_mg_setup (or null), whose x and b the kernel leaves zero again.
+int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, const int* l1list, const int* l1n, double* p,
+                  double* q, double* xs, double* r, const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0 = nullptr, int nu0 = 2,
                   const float* pprev = nullptr, float* pout = nullptr, unsigned wait_polls = kDefaultWaitPolls);
 
 // -------- labelling and the particle sort (kernels_sort.cu) --------

@@ -101,6 +101,8 @@ struct MgArgs {
     const int* fidx;             // compact FLUID list (level-0 padded index)
     const uint8_t* diag;         // compact diagonal, bit 7 = red/black colour
     const int* nf;
+    const int* l1list;           // level 1's FLUID cells (padded indices, any order), or null
+    const int* l1n;              // their number
     double* X;                   // compact solution out (FP64)
     float* pout;                 // dense W x H x D pressure out (zero off the fluid already), or null
     double* red;                 // [2] out: ||rhs - A x||^2 and ||rhs||^2 of the solution, in FP64
@@ -277,6 +279,38 @@ __device__ void op_prolong_red(const MgLevel& F, const MgLevel& Cl, float omega,
         int i, j, k;
         const int c = lv_cell(F, t, i, j, k);
         if (F.code[c] != 0) prolong_one(F, c, Cl, omega, i, j, k);
+    }
+}
+// The same two operations over a list of the coarse (restriction) or fine
+// (prolongation) level's FLUID cells: the cells whose results the dense forms
+// compute, with the same arithmetic.  A thread's loads do not wait on the
+// cell's code, and one trip covers a level whose FLUID cells are fewer than
+// the grid's threads (at 128^3, level 1 has about 60 K of 262 K).  The other
+// cells' x and b stay zero: only FLUID cells are written, and the solve
+// clears them at its end.
+__device__ void op_restrict_first_list(const MgLevel& F, const MgLevel& Cl, float scale, const int* list, int n,
+                                       int t0, int stride) {
+    for (int t = t0; t < n; t += stride) {
+        const int cc = list[t];
+        const int I = cc % Cl.sy - 1, J = (cc / Cl.sy) % (Cl.H + 2) - 1, K = cc / Cl.sz - 1;
+        const int dc = Cl.code[cc];
+        const bool ii = 2 * I + 1 < F.W, jj = 2 * J + 1 < F.H, kk = 2 * K + 1 < F.D;
+        const int c0 = (2 * I + 1) + (2 * J + 1) * F.sy + (2 * K + 1) * F.sz;
+        float s = fine_residual(F, c0);
+        if (ii && jj) s += fine_residual(F, c0 + 1 + F.sy);
+        if (ii && kk) s += fine_residual(F, c0 + 1 + F.sz);
+        if (jj && kk) s += fine_residual(F, c0 + F.sy + F.sz);
+        s *= scale;
+        Cl.b[cc] = s;
+        Cl.x[cc] = ((I + J + K) & 1) == 0 && dc > 1 ? sorc(0.0f, s / float(dc - 1)) : 0.0f;
+    }
+}
+__device__ void op_prolong_red_list(const MgLevel& F, const MgLevel& Cl, float omega, const int* list, int n, int t0,
+                                    int stride) {
+    for (int t = t0; t < n; t += stride) {
+        const int c = list[t];
+        const int i = c % F.sy - 1, j = (c / F.sy) % (F.H + 2) - 1, k = c / F.sz - 1;
+        prolong_one(F, c, Cl, omega, i, j, k);
     }
 }
 // ... over the level-0 FLUID list
@@ -572,11 +606,22 @@ __device__ void block_vcycle_global(const MgArgs& a, int l0) {
 // sweep pair (level 0 two more per extra pair): black sweep, restriction (with
 // the next level's first sweep), black sweep, red sweep (with the
 // prolongation into the finer level).  nl: the levels that hold FLUID cells.
-__device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
+// n1: the number of level 1's listed FLUID cells (a.l1list), or -1 for none.
+__device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl, int n1) {
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
     const unsigned nb = gridDim.x;
     const int G = min(a.G, a.L - 1);
     const int nf = *a.nf;
+    // restriction from level l and prolongation into level lf >= 1, level 1
+    // over its FLUID list when there is one
+    auto restrict_first = [&](int l) {
+        if (l == 0 && n1 >= 0) op_restrict_first_list(a.lv[0], a.lv[1], a.rscale, a.l1list, n1, t0, st);
+        else op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st);
+    };
+    auto prolong_into = [&](int lf, const MgLevel& Cl) {
+        if (lf == 1 && n1 >= 0) op_prolong_red_list(a.lv[1], Cl, a.omega, a.l1list, n1, t0, st);
+        else op_prolong_red(a.lv[lf], Cl, a.omega, t0, st);
+    };
     // one grid-wide sweep of level l (colour 0 red, 1 black) and a barrier
     auto sweep = [&](int l, int color) {
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, color, t0, st);
@@ -589,7 +634,7 @@ __device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
         if (!sweep(l, 1)) return false;
         for (int e = 1; e < (l == 0 ? a.nu0 : a.nu_grid); ++e)
             if (!sweep(l, 0) || !sweep(l, 1)) return false;
-        op_restrict_first(a.lv[l], a.lv[l + 1], a.rscale, t0, st);
+        restrict_first(l);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
     if (a.smem) {
@@ -600,14 +645,14 @@ __device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
         MgLevel cg = S[G].m;  // level G in this block's shared memory
         cg.code = S[G].code;
         if (G == 1) op0_prolong_red(a.lv[0], cg, a.omega, a.fidx, nf, t0, st);
-        else op_prolong_red(a.lv[G - 1], cg, a.omega, t0, st);
+        else prolong_into(G - 1, cg);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
     } else {
         if (blockIdx.x == 0) block_vcycle_global(a, G);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
         if (G > 0) {  // level G's last red sweep, fused with its prolongation into level G - 1
             if (G == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
-            else op_prolong_red(a.lv[G - 1], a.lv[G], a.omega, t0, st);
+            else prolong_into(G - 1, a.lv[G]);
             if (!grid_barrier(a.bar, nb, a.status)) return false;
         }
     }
@@ -620,7 +665,7 @@ __device__ bool vcycle(const MgArgs& a, const BlkLevel* S, int nl) {
             if (!sweep(l, 0) || !sweep(l, 1)) return false;
         if (l == 0) op0_sweep(a.lv[0], a.fidx, a.diag, nf, 0, t0, st);
         else if (l == 1) op0_prolong_red(a.lv[0], a.lv[1], a.omega, a.fidx, nf, t0, st);
-        else op_prolong_red(a.lv[l - 1], a.lv[l], a.omega, t0, st);
+        else prolong_into(l - 1, a.lv[l]);
         if (!grid_barrier(a.bar, nb, a.status)) return false;
     }
     return true;
@@ -637,6 +682,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     const int nb = int(gridDim.x);
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x, st = nb * blockDim.x;
     const MgLevel& F = a.lv[0];
+    const int n1 = a.l1list && a.L > 1 ? *a.l1n : -1;  // level 1's listed FLUID cells
     float* b0 = F.b;  // FP32 copy of r: the V-cycle's right-hand side
     float* z = F.x;   // FP32 preconditioned residual
     double* r = a.r;
@@ -792,7 +838,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
     int it = 0, stt = DEV_OK;
     while (rr > thr && bb > 0.0) {
         if (it >= a.maxit) { stt = DEV_MAXIT; break; }
-        if (!vcycle(a, s_lv, nl)) return;  // z = M^-1 r
+        if (!vcycle(a, s_lv, nl, n1)) return;  // z = M^-1 r
         double gl = 0.0, dl = 0.0, sl = 0.0;
         constexpr int U3 = 3;  // three cells in flight fit the register budget with FP64 sums
         for (int base = t0, q0 = 0; base < nf; base += U3 * st, q0 += U3) {
@@ -905,6 +951,11 @@ __global__ void __launch_bounds__(MG_THREADS) k_pcg_mg(MgArgs a) {
         a.xs[c] = fmin(fabs(xv), 0.0);  // +0 computed from the load (a constant store would wait on it)
         a.p[c] = 0.0; a.q[c] = 0.0; r[c] = 0.0; b0[c] = 0.0f; z[c] = 0.0f; F.code[c] = 0;
     }
+    for (int t = t0; t < n1; t += st) {  // level 1's FLUID cells: x and b back to zero
+        const int c = a.l1list[t];
+        a.lv[1].x[c] = 0.0f;
+        a.lv[1].b[c] = 0.0f;
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.out->iters = it;
         atomicCAS(a.status, DEV_OK, stt);
@@ -925,22 +976,48 @@ __global__ void k_coarsen(MgLevel F, MgLevel Cl) {
 // Level 1 straight from the cell labels, by the same rule (BODY, like SOLID,
 // is neither AIR nor FLUID); level 0 itself needs no padded label copy, as
 // its operations read the FLUID list's diagonal bytes and codes.
-__global__ void k_coarsen_cells(const uint8_t* __restrict__ lab, Dims g, MgLevel Cl) {
+// It also appends level 1's FLUID cells (padded indices) to list, one atomic
+// per block, in no fixed order: every use of the list treats its cells
+// independently.  *nlist must be zero before the launch; at most cap entries
+// are written.
+constexpr int COARSEN_THREADS = 256;
+__global__ void __launch_bounds__(COARSEN_THREADS) k_coarsen_cells(const uint8_t* __restrict__ lab, Dims g, MgLevel Cl,
+                                                                   int* __restrict__ list, int* __restrict__ nlist,
+                                                                   int cap) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= Cl.W * Cl.H * Cl.D) return;
-    int I, J, K;
-    const int cc = lv_cell(Cl, t, I, J, K);
-    bool air = false, fluid = false;
-    for (int c3 = 0; c3 < 2; ++c3)
-        for (int b3 = 0; b3 < 2; ++b3)
-            for (int a3 = 0; a3 < 2; ++a3) {
-                const int i = 2 * I + a3, j = 2 * J + b3, k = 2 * K + c3;
-                if (i >= g.W || j >= g.H || k >= g.D) continue;
-                const uint8_t l = lab[int64_t(i) + int64_t(j) * g.W + int64_t(k) * g.W * g.H];
-                air |= l == AIR;
-                fluid |= l == FLUID;
-            }
-    Cl.lab[cc] = air ? AIR : (fluid ? FLUID : SOLID);
+    bool listed = false;
+    int cc = 0;
+    if (t < Cl.W * Cl.H * Cl.D) {
+        int I, J, K;
+        cc = lv_cell(Cl, t, I, J, K);
+        bool air = false, fluid = false;
+        for (int c3 = 0; c3 < 2; ++c3)
+            for (int b3 = 0; b3 < 2; ++b3)
+                for (int a3 = 0; a3 < 2; ++a3) {
+                    const int i = 2 * I + a3, j = 2 * J + b3, k = 2 * K + c3;
+                    if (i >= g.W || j >= g.H || k >= g.D) continue;
+                    const uint8_t l = lab[int64_t(i) + int64_t(j) * g.W + int64_t(k) * g.W * g.H];
+                    air |= l == AIR;
+                    fluid |= l == FLUID;
+                }
+        Cl.lab[cc] = air ? AIR : (fluid ? FLUID : SOLID);
+        listed = fluid && !air;
+    }
+    if (!list) return;  // uniform across the block
+    __shared__ int s_off[COARSEN_THREADS / 32];
+    __shared__ int s_base;
+    const unsigned m = __ballot_sync(0xffffffffu, listed);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) s_off[wid] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < COARSEN_THREADS / 32; ++w) { const int c = s_off[w]; s_off[w] = tot; tot += c; }
+        s_base = tot > 0 ? atomicAdd(nlist, tot) : 0;
+    }
+    __syncthreads();
+    const int slot = s_base + s_off[wid] + __popc(m & ((1u << lane) - 1u));
+    if (listed && slot < cap) list[slot] = cc;
 }
 
 }  // namespace
@@ -983,20 +1060,24 @@ int mg_split(const MgLevel* lv, int L, int* smem_bytes) {
     return L - 1;  // not even the coarsest level fits: the block levels stay in global memory
 }
 
-int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, cudaStream_t st) {
+int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, int* l1list, int* l1n, cudaStream_t st) {
     int smem = 0;
     const int G = mg_split(lv, L, &smem);
     const int last = smem ? G : L - 1;  // deeper shared-memory levels: coarsened by the solver kernel
     for (int l = 1; l <= last; ++l) {
         const int n = lv[l].W * lv[l].H * lv[l].D;
-        if (l == 1) k_coarsen_cells<<<(n + 255) / 256, 256, 0, st>>>(labels, g, lv[1]);
+        if (l == 1) {
+            if (l1list) cudaMemsetAsync(l1n, 0, sizeof(int), st);
+            k_coarsen_cells<<<(n + COARSEN_THREADS - 1) / COARSEN_THREADS, COARSEN_THREADS, 0, st>>>(labels, g, lv[1],
+                                                                                                   l1list, l1n, n);
+        }
         else k_coarsen<<<(n + 255) / 256, 256, 0, st>>>(lv[l - 1], lv[l]);
     }
     return last;
 }
 
-int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, double* q, double* xs, double* r,
-                  const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0, int nu0,
+int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, const int* l1list, const int* l1n, double* p,
+                  double* q, double* xs, double* r, const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0, int nu0,
                   const float* pprev, float* pout, unsigned wait_polls) {
     // One block per 4096 cells (each thread's UNR cells per trip), at most one
     // per SM: a small grid waits at cheaper barriers (one block: __syncthreads).
@@ -1024,6 +1105,7 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, double* p, doubl
     a.nu_grid = MG_NU_GRID;
     a.nu_block = MG_NU_BLOCK;
     a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.pprev = x0 ? nullptr : pprev; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
+    a.l1list = l1list; a.l1n = l1n;
     a.X = static_cast<double*>(pb.X);
     a.pout = pout;
     a.red = pb.red;

@@ -161,6 +161,7 @@ struct fp_solver {
     MgLevel mg[MG_MAX_LEVELS]{};
     int mgL = 0;
     double *d_mgp = nullptr, *d_mgq = nullptr, *d_mgx = nullptr, *d_mgr = nullptr;
+    int *d_l1list = nullptr, *d_l1n = nullptr;  // level 1's FLUID cells (multigrid)
     // learned initial guess
     fp_unet* net = nullptr;
     std::string learned_path;
@@ -226,6 +227,7 @@ void free_grid(fp_solver* s) {
     }
     s->mgL = 0;
     dfree(s->d_mgp); dfree(s->d_mgq); dfree(s->d_mgx); dfree(s->d_mgr);
+    dfree(s->d_l1list); dfree(s->d_l1n);
     dfree(s->d_rhs_dense); dfree(s->d_x0c);
     if (s->net) { fp_unet_destroy(s->net); s->net = nullptr; }
     free_r2(s);
@@ -317,6 +319,10 @@ int alloc_grid(fp_solver* s, int W, int H, int D) {
                 ck(cudaMemsetAsync(L.x, 0, np_ * sizeof(float), s->st));
                 ck(cudaMemsetAsync(L.b, 0, np_ * sizeof(float), s->st));
             }
+        }
+        if (s->mgL > 1) {
+            ck(dalloc(&s->d_l1list, size_t(s->mg[1].W) * s->mg[1].H * s->mg[1].D));
+            ck(dalloc(&s->d_l1n, 1));
         }
         ck(dalloc(&s->d_mgp, size_t(s->padded))); ck(dalloc(&s->d_mgq, size_t(s->padded)));
         ck(dalloc(&s->d_mgx, size_t(s->padded))); ck(dalloc(&s->d_mgr, size_t(s->padded)));
@@ -458,7 +464,7 @@ int solve_system(fp_solver* s, float* p_out, bool defer = false) {
         const bool mg = s->cfg.solver != FP_SOLVER_PCG;
         if (learned && !s->net) return s->fail(FP_ERR_STATE, "learned solver: no weights loaded (fp_load_learned)");
         if (mg) {
-            s->launches += launch_mg_setup(s->d_labels, s->g, s->mg, s->mgL, s->st);
+            s->launches += launch_mg_setup(s->d_labels, s->g, s->mg, s->mgL, s->d_l1list, s->d_l1n, s->st);
         }
         cudaEventRecord(s->ev_pcg[0], s->st);
         const float* x0 = nullptr;
@@ -476,7 +482,7 @@ int solve_system(fp_solver* s, float* p_out, bool defer = false) {
         // A learned solve that has not converged after kLearnedMaxit iterations
         // counts as stalled and hands over to the plain PCG.
         constexpr int kLearnedMaxit = 300;
-        int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr, pb.b, tol,
+        int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_l1list, s->d_l1n, s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr, pb.b, tol,
                                    learned ? std::min(maxit, kLearnedMaxit) : maxit, s->st, x0,
                                    s->cfg.mg_sweeps > 0 ? s->cfg.mg_sweeps : 2,
                                    s->cfg.warm_start && p_out == s->d_p ? p_out : nullptr, p_out, s->wait_polls)
