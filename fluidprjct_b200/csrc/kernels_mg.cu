@@ -1077,8 +1077,8 @@ int launch_mg_setup(const uint8_t* labels, Dims g, MgLevel* lv, int L, int* l1li
 }
 
 int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, const int* l1list, const int* l1n, double* p,
-                  double* q, double* xs, double* r, const float* rhs, double tol, int maxit, cudaStream_t st, const float* x0, int nu0,
-                  const float* pprev, float* pout, unsigned wait_polls) {
+                  double* q, double* xs, double* r, const float* rhs, double tol, int maxit, cudaStream_t st,
+                  const float* x0, int nu0, const float* pprev, float* pout, unsigned wait_polls) {
     // One block per 4096 cells (each thread's UNR cells per trip), at most one
     // per SM: a small grid waits at cheaper barriers (one block: __syncthreads).
     const int64_t want = (g.nc() + int64_t(MG_THREADS) * UNR - 1) / (int64_t(MG_THREADS) * UNR);
@@ -1104,7 +1104,8 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, const int* l1lis
     a.nu0 = std::max(1, nu0);
     a.nu_grid = MG_NU_GRID;
     a.nu_block = MG_NU_BLOCK;
-    a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.pprev = x0 ? nullptr : pprev; a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
+    a.p = p; a.q = q; a.xs = xs; a.r = r; a.rhs = rhs; a.x0 = x0; a.pprev = x0 ? nullptr : pprev;
+    a.fidx = pb.fidx; a.diag = pb.diag; a.nf = pb.nf;
     a.l1list = l1list; a.l1n = l1n;
     a.X = static_cast<double*>(pb.X);
     a.pout = pout;
@@ -1112,7 +1113,8 @@ int launch_pcg_mg(Dims g, PressureBufs& pb, MgLevel* lv, int L, const int* l1lis
     a.part = pb.part; a.bar = pb.bar; a.status = status; a.out = pb.out;
     a.tol = tol; a.maxit = maxit;
     void* args[] = {&a};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_mg, dim3(nb), dim3(MG_THREADS), args, size_t(a.smem), st);
+    cudaError_t e =
+        cudaLaunchCooperativeKernel((const void*)k_pcg_mg, dim3(nb), dim3(MG_THREADS), args, size_t(a.smem), st);
     return e == cudaSuccess ? 0 : int(e);
 }
 

@@ -482,8 +482,8 @@ int solve_system(fp_solver* s, float* p_out, bool defer = false) {
         // A learned solve that has not converged after kLearnedMaxit iterations
         // counts as stalled and hands over to the plain PCG.
         constexpr int kLearnedMaxit = 300;
-        int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_l1list, s->d_l1n, s->d_mgp, s->d_mgq, s->d_mgx, s->d_mgr, pb.b, tol,
-                                   learned ? std::min(maxit, kLearnedMaxit) : maxit, s->st, x0,
+        int e = mg ? launch_pcg_mg(s->g, pb, s->mg, s->mgL, s->d_l1list, s->d_l1n, s->d_mgp, s->d_mgq, s->d_mgx,
+                                   s->d_mgr, pb.b, tol, learned ? std::min(maxit, kLearnedMaxit) : maxit, s->st, x0,
                                    s->cfg.mg_sweeps > 0 ? s->cfg.mg_sweeps : 2,
                                    s->cfg.warm_start && p_out == s->d_p ? p_out : nullptr, p_out, s->wait_polls)
                    : launch_pcg(s->g, pb, pb.b, 1, tol, maxit, s->st, s->wait_polls);
