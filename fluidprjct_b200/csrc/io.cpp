@@ -309,17 +309,74 @@ struct JParser {
     std::string err;
     explicit JParser(const std::string& src) : s(src) {}
     void ws() { while (i < s.size() && std::isspace(static_cast<unsigned char>(s[i]))) ++i; }
+    // Four hex digits at s[at]; false if they are missing or not hex.
+    bool hex4(size_t at, uint32_t& v) const {
+        if (at + 4 > s.size()) return false;
+        v = 0;
+        for (size_t k = at; k < at + 4; ++k) {
+            const char c = s[k];
+            const int d = c >= '0' && c <= '9' ? c - '0' : c >= 'a' && c <= 'f' ? c - 'a' + 10
+                        : c >= 'A' && c <= 'F' ? c - 'A' + 10 : -1;
+            if (d < 0) return false;
+            v = v * 16 + uint32_t(d);
+        }
+        return true;
+    }
+    static void put_utf8(std::string& out, uint32_t cp) {
+        if (cp < 0x80) {
+            out += char(cp);
+        } else if (cp < 0x800) {
+            out += char(0xC0 | (cp >> 6));
+            out += char(0x80 | (cp & 0x3F));
+        } else if (cp < 0x10000) {
+            out += char(0xE0 | (cp >> 12));
+            out += char(0x80 | ((cp >> 6) & 0x3F));
+            out += char(0x80 | (cp & 0x3F));
+        } else {
+            out += char(0xF0 | (cp >> 18));
+            out += char(0x80 | ((cp >> 12) & 0x3F));
+            out += char(0x80 | ((cp >> 6) & 0x3F));
+            out += char(0x80 | (cp & 0x3F));
+        }
+    }
+    // A JSON string with the escapes of RFC 8259 (as jsoncpp, which the
+    // reference's driver uses, decodes them): \" \\ \/ \b \f \n \r \t and \uXXXX,
+    // a surrogate pair giving one code point, written as UTF-8.  Any other
+    // escape, or a lone surrogate, is an error.
     bool str(std::string& out) {
         if (i >= s.size() || s[i] != '"') return false;
         ++i;
         out.clear();
         while (i < s.size() && s[i] != '"') {
-            if (s[i] == '\\' && i + 1 < s.size()) {
-                char e = s[i + 1];
-                out += e == 'n' ? '\n' : e == 't' ? '\t' : e;
-                i += 2;
-            } else {
-                out += s[i++];
+            if (s[i] != '\\') { out += s[i++]; continue; }
+            if (i + 1 >= s.size()) return false;
+            const char e = s[i + 1];
+            i += 2;
+            switch (e) {
+                case '"': case '\\': case '/': out += e; break;
+                case 'b': out += '\b'; break;
+                case 'f': out += '\f'; break;
+                case 'n': out += '\n'; break;
+                case 'r': out += '\r'; break;
+                case 't': out += '\t'; break;
+                case 'u': {
+                    uint32_t cp = 0;
+                    if (!hex4(i, cp)) return false;
+                    i += 4;
+                    if (cp >= 0xD800 && cp < 0xDC00) {  // high surrogate: its low half must follow
+                        uint32_t lo = 0;
+                        if (i + 6 > s.size() || s[i] != '\\' || s[i + 1] != 'u' || !hex4(i + 2, lo) || lo < 0xDC00 ||
+                            lo >= 0xE000)
+                            return false;
+                        i += 6;
+                        cp = 0x10000 + ((cp - 0xD800) << 10) + (lo - 0xDC00);
+                    } else if (cp >= 0xDC00 && cp < 0xE000) {
+                        return false;
+                    }
+                    put_utf8(out, cp);
+                    break;
+                }
+                default: return false;
             }
         }
         if (i >= s.size()) return false;

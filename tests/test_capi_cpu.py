@@ -85,6 +85,57 @@ def test_config_json(tmp_path):
     assert capi.lib().fp_config_load_json(str(bad).encode(), C.byref(cfg), None, 0, None) == capi.FP_ERR_IO
 
 
+def _load_json(path, label_len=256):
+    from fluidprjct_b200 import capi
+    cfg = capi.default_config()
+    lab = C.create_string_buffer(label_len) if label_len else None
+    frames = C.c_int(-1)
+    rc = capi.lib().fp_config_load_json(str(path).encode(), C.byref(cfg), lab, label_len, C.byref(frames))
+    return rc, cfg, lab, frames.value
+
+
+def test_config_json_strings_and_formats(tmp_path):
+    """String escapes decode as jsoncpp decodes them (RFC 8259: \\" \\\\ \\/ \\b
+    \\f \\n \\r \\t and \\uXXXX with surrogate pairs, to UTF-8); outputFormat
+    maps "PLY" to PLY and anything else to OFF as main.cpp:25-31 does, plus this
+    library's PLY_BINARY and NONE; the label path is cut to the caller's
+    buffer."""
+    from fluidprjct_b200 import capi
+    p = tmp_path / "esc.json"
+    p.write_text('{"outputTemplate": "Out\\/d\\\\x\\"q\\tz\\u00e9\\ud83d\\ude00\\b\\f\\r\\n",'
+                 ' "inputLabelData": "InputData/labels_gaussian.txt", "outputFormat": "PLY_BINARY"}')
+    rc, cfg, lab, _ = _load_json(p)
+    assert rc == capi.FP_OK
+    assert cfg.output_template == 'Out/d\\x"q\tzé\U0001F600\b\f\r\n'.encode("utf-8")
+    assert cfg.output_format == capi.OUT_PLY_BINARY
+    rc, _, lab, _ = _load_json(p, label_len=10)
+    assert rc == capi.FP_OK and lab.value == b"InputData"
+    for fmt, want in (("PLY", capi.OUT_PLY), ("NONE", capi.OUT_NONE), ("OBJ", capi.OUT_OFF), ("ply", capi.OUT_OFF)):
+        p.write_text('{"outputFormat": "%s"}' % fmt)
+        rc, cfg, _, _ = _load_json(p)
+        assert rc == capi.FP_OK and cfg.output_format == want, fmt
+
+
+def test_config_json_rejects_malformed_input(tmp_path):
+    """Missing files, malformed JSON, bad escapes, lone surrogates and unknown
+    enumerated values are FP_ERR_IO.  A numeric key holding another type is
+    ignored and keeps its default (where jsoncpp's asFloat() would throw), and
+    nested values of any kind are skipped."""
+    from fluidprjct_b200 import capi
+    assert _load_json(tmp_path / "missing.json")[0] == capi.FP_ERR_IO
+    p = tmp_path / "c.json"
+    for text in ('{"dt": 0.1', '{"dt" 0.1}', '[1, 2]', '{"dt": }', '{"dt": 0.1,, "dx": 1}',
+                 '{"outputTemplate": "a\\qb"}', '{"outputTemplate": "\\ud83d"}', '{"outputTemplate": "\\ude00"}',
+                 '{"outputTemplate": "\\u12"}', '{"outputTemplate": "abc}',
+                 '{"collision": "mesh"}', '{"advection": "euler"}', '{"solver": "cg"}'):
+        p.write_text(text)
+        assert _load_json(p)[0] == capi.FP_ERR_IO, text
+    p.write_text('{"dt": "fast", "dx": 0.25, "nested": {"k": [true, false, null, "s", {"x": -1e-3}]}}')
+    rc, cfg, _, _ = _load_json(p)
+    d = capi.default_config()
+    assert rc == capi.FP_OK and cfg.dt == d.dt and cfg.dx == 0.25
+
+
 @pytest.mark.parametrize("name,dim", [("labels_simple3d", 3), ("labels_3d_sphere", 3), ("labels_bathymetry", 3),
                                       ("labels_simple", 2), ("labels_colimn", 2)])
 def test_host_label_reader(golden_labels, name, dim, tmp_path):
