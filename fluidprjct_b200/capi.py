@@ -175,9 +175,15 @@ def read_levelset_file(path) -> np.ndarray:
 
 
 def default_config(**kw) -> FpConfig:
+    """fp_config_default, then the given fields.  A name that is not a field of
+    fp_config raises TypeError (ctypes would otherwise keep it as a plain
+    attribute, and the setting would be lost without a word)."""
     cfg = FpConfig()
     lib().fp_config_default(C.byref(cfg))
+    fields = {f[0] for f in FpConfig._fields_}
     for k, v in kw.items():
+        if k not in fields:
+            raise TypeError(f"fp_config has no field {k!r}")
         if k in ("output_template", "body_sdf"):
             setattr(cfg, k, v.encode())
         elif k == "body_pos":

@@ -47,6 +47,12 @@ def test_config_defaults_match_reference():
     assert (c.warm_start, c.mg_sweeps) == (1, 0)
     # the ctypes mirrors have the C sizes (int64 + int32 x 2 appended to the stats)
     assert C.sizeof(capi.FpStepStats) % 8 == 0
+    # a misspelt field is an error, not a silently ignored attribute
+    with pytest.raises(TypeError, match="pic_wieght"):
+        capi.default_config(pic_wieght=0.1)
+    c = capi.default_config(pic_weight=0.25, body_pos=(0.1, 0.2, 0.3), solver="pcg_mg", output_template="o/p_")
+    assert c.pic_weight == 0.25 and list(c.body_pos) == pytest.approx([0.1, 0.2, 0.3])
+    assert c.solver == capi.SOLVER_PCG_MG and c.output_template == b"o/p_"
 
 
 def test_create_rejects_bad_schemes():
