@@ -25,9 +25,9 @@ class FluidSolver3D:
         # (main.cpp:21, FluidSolver3D.cu:88), exactly as in the reference.
         self.gridWidth, self.gridHeight, self.gridDepth = width, height, depth
         self.dx, self.dt = dx, dt
-        self.PIC_WEIGHT = 0.5       # FluidSolver3D.cuh:160
-        self.iterPerFrame = 10      # :161
-        self.outputFormat = "PLY"   # :162
+        self.PIC_WEIGHT = 0.5       # FluidSolver3D.cuh:156
+        self.iterPerFrame = 10      # :157
+        self.outputFormat = "PLY"   # :158
         self.outputTemplate = "InputData/particles_"
         self.activeBody = False
         self.initialBodyPos = (0.5, 0.5, 0.5)

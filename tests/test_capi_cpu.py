@@ -91,6 +91,36 @@ def test_config_json(tmp_path):
     assert capi.lib().fp_config_load_json(str(bad).encode(), C.byref(cfg), None, 0, None) == capi.FP_ERR_IO
 
 
+def test_reference_class_knobs_map_to_the_config():
+    """FluidSolver3D keeps the reference class's public knobs and defaults
+    (FluidSolver3D.cuh:156-166: PIC_WEIGHT 0.5, iterPerFrame 10, outputFormat
+    PLY, outputTemplate "InputData/particles_", four particles per cell at
+    :72) and forwards them, and its additions, to fp_config."""
+    from fluidprjct_b200 import capi
+    from fluidprjct_b200.solver import FluidSolver3D
+    f = FluidSolver3D(5, 5, 5, 0.02, 0.005)
+    c = f._config()
+    f32 = lambda x: float(np.float32(x))
+    assert (c.dx, c.dt, c.pic_weight, c.iter_per_frame, c.ppc) == (f32(0.02), f32(0.005), 0.5, 10, 4)
+    assert c.output_format == capi.OUT_PLY and c.output_template == b"InputData/particles_"
+    assert c.active_body == 0 and c.dim == 3
+    f.PIC_WEIGHT, f.iterPerFrame, f.outputTemplate = 0.001, 1, "OutputData/particles_"
+    f.activeBody, f.initialBodyPos, f.bodyMass = True, (0.5, 0.2, 0.5), 0.03
+    for fmt, want in (("PLY", capi.OUT_PLY), ("OFF", capi.OUT_OFF), ("PLY_BINARY", capi.OUT_PLY_BINARY),
+                      ("NONE", capi.OUT_NONE), ("OBJ", capi.OUT_OFF)):
+        f.outputFormat = fmt
+        assert f._config().output_format == want, fmt
+    c = f._config()
+    assert (c.pic_weight, c.iter_per_frame, c.active_body) == (f32(0.001), 1, 1)
+    assert c.output_template == b"OutputData/particles_" and c.body_mass == f32(0.03)
+    assert list(c.body_pos) == pytest.approx([0.5, 0.2, 0.5])
+    g = FluidSolver3D(dx=0.1, dt=0.02, solver="pcg_mg", advection="rk2", seed=9)
+    c = g._config()
+    assert (c.solver, c.advection, c.seed) == (capi.SOLVER_PCG_MG, capi.ADVECT_RK2, 9)
+    with pytest.raises(TypeError):
+        FluidSolver3D(dx=0.1, dt=0.02, sovler="pcg_mg")._config()
+
+
 def _load_json(path, label_len=256):
     from fluidprjct_b200 import capi
     cfg = capi.default_config()
