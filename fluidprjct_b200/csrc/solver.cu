@@ -1163,7 +1163,7 @@ int fp_config_default(fp_config* c) {
     c->active_body = 0;
     c->body_pos[0] = c->body_pos[1] = c->body_pos[2] = 0.5f;  // main.cpp:44-46
     c->body_mass = 50.0f;    // main.cpp:48
-    c->ppc = 4;              // FluidSolver3D.cuh:72
+    c->ppc = 4;              // FluidSolver3D.cuh:71
     c->seed = 0;
     c->solver = FP_SOLVER_PCG;
     c->advection = FP_ADVECT_RK3REF;

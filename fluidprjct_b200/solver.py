@@ -18,7 +18,7 @@ from . import capi
 class FluidSolver3D:
     """Drop-in for ``FluidSolver3D`` (same knobs, same call order)."""
 
-    PARTICLES_PER_CELL = 4  # FluidSolver3D.cuh:72
+    PARTICLES_PER_CELL = 4  # FluidSolver3D.cuh:71
 
     def __init__(self, width=5, height=5, depth=5, dx=0.1, dt=0.02, **extra):
         # The constructor's grid size is a placeholder overwritten by init()

@@ -110,7 +110,7 @@ enum { FP_PHASE_LABEL = 0, FP_PHASE_P2G = 1, FP_PHASE_SAVE = 2, FP_PHASE_FORCES 
        FP_PHASE_CLEANUP = 9 /* FP_SCHEME_REF2D only: cleanUpParticles, FluidSolver2D.cu:1171-1204 */ };
 
 /* Solver configuration.  Keys and defaults follow main.cpp:17-52 and the
- * member initialisers of FluidSolver3D.cuh:72-80,160-166; the fields after
+ * member initialisers of FluidSolver3D.cuh:71-79,156-166; the fields after
  * body_mass are additions whose defaults reproduce the reference's behaviour. */
 typedef struct fp_config {
     int      dim;                  /* 3 (FluidSolver3D) or 2 (FluidSolver2D)        */

@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol():
 def test_config_defaults_match_reference():
     from fluidprjct_b200 import capi
     c = capi.default_config()
-    # main.cpp:18-48 and FluidSolver3D.cuh:72, FluidSolver3D.cu:3092
+    # main.cpp:18-48 and FluidSolver3D.cuh:71, FluidSolver3D.cu:3092
     assert (c.dim, c.iter_per_frame, c.ppc) == (3, 1, 4)
     f32 = lambda x: float(np.float32(x))
     assert (c.dt, c.dx, c.pic_weight, c.cfl, c.body_mass) == (f32(0.02), f32(0.1), f32(0.01), f32(0.1), 50.0)
@@ -95,7 +95,7 @@ def test_reference_class_knobs_map_to_the_config():
     """FluidSolver3D keeps the reference class's public knobs and defaults
     (FluidSolver3D.cuh:156-166: PIC_WEIGHT 0.5, iterPerFrame 10, outputFormat
     PLY, outputTemplate "InputData/particles_", four particles per cell at
-    :72) and forwards them, and its additions, to fp_config."""
+    :71) and forwards them, and its additions, to fp_config."""
     from fluidprjct_b200 import capi
     from fluidprjct_b200.solver import FluidSolver3D
     f = FluidSolver3D(5, 5, 5, 0.02, 0.005)
