@@ -77,7 +77,7 @@ __device__ __forceinline__ float trilin(float xd, float yd, float zd, float c000
 // MAC sample stencil: base corner index and fractions.  Base indices are
 // clamped so that base+1 stays inside the face grid; for positions inside
 // [0, (N-1)*dx] (where advection keeps particles) these are the reference's
-// clamps of interpVelDevice3D (FluidSolver3D.cu:1059-1140).  A 2D grid is a
+// clamps of interpVelDevice3D (FluidSolver3D.cu:1052-1157).  A 2D grid is a
 // grid with D = 1: its z corner pairs collapse onto one slice (slice stride 0
 // in sample()) with weight 0 on the duplicate, which is exact bilinear
 // interpolation.

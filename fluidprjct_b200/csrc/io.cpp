@@ -176,7 +176,7 @@ const char* kBinaryHeader =
     "property float vz\nend_header\n";
 
 // ASCII PLY / OFF of positions pos[stride * q + 0..2]: "x y z" per line as an
-// ostream of floats prints them (saveParticlesToPLY, utility.cu:91-127), %g
+// ostream of floats prints them (save3dParticlesToPLY / save3dParticlesToOFF, utility.cu:91-127), %g
 // with 6 significant digits, i.e. std::to_chars in general format with
 // precision 6.  Chunks are formatted in parallel and written in order.
 bool write_ascii(const std::string& path, const float* pos, int stride, int64_t n, int format, std::string& err) {

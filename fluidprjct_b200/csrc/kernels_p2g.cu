@@ -70,7 +70,7 @@ __device__ __forceinline__ void axis3(int s0, int base, float f, float (&w)[3]) 
 // component's own axis, whose base face is always the cell's), and adds them
 // into the brick's shared-memory accumulators, whose face (ex0, ey0, ez0) is
 // slot 0 (strides lsx, lsy).  COMP selects the component and its base-index
-// rules (AccumulateVelocities, FluidSolver3D.cu:465-574).  Weights are
+// rules (AccumulateVelocities::operator(), FluidSolver3D.cu:469-574).  Weights are
 // (wx*wy)*wz as in the reference; the two faces along the component's axis
 // are one packed pair, so each particle costs 12 packed multiplies and 9
 // packed FMAs and adds per component.  num accumulates vel*wgt with one fused

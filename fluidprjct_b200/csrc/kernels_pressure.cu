@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_fluid_tiles(const uint8_t* __res
     if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
 
-// RHSCalculator3D (FluidSolver3D.cu:1371-1456) at FLUID cell (i,j,k).
+// RHSCalculator3D::operator() (FluidSolver3D.cu:1371-1456) at FLUID cell (i,j,k).
 __device__ __forceinline__ float rhs_at(const uint8_t* __restrict__ lab, const float* __restrict__ u,
                                         const float* __restrict__ v, const float* __restrict__ w, const Dims& g,
                                         int i, int j, int k, float scale, const BodyKin& body) {

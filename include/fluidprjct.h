@@ -398,7 +398,7 @@ int fp_unet_train_step(fp_unet* u, const uint8_t* d_labels, const float* d_rhs, 
 int fp_read_label_file(const char* path, int dim, int* dims, uint8_t* out);
 int fp_read_ply_file(const char* path, int64_t* n, float* pos, float* vel, int* has_vel);
 /* Writes n particles (pos, and vel for FP_OUT_PLY_BINARY; vel may be NULL) in
- * a frame format: ASCII PLY / OFF of positions as saveParticlesToPLY writes
+ * a frame format: ASCII PLY / OFF of positions as save3dParticlesToPLY / OFF write
  * them (utility.cu:91-127, %g), or binary little-endian PLY. */
 int fp_write_particle_file(const char* path, const float* pos, const float* vel, int64_t n, int format);
 

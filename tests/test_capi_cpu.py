@@ -255,7 +255,7 @@ def test_scene_file_round_trip(tmp_path):
 
 def test_particle_writer_formats(tmp_path):
     """ASCII PLY / OFF lines are "x y z" as an ostream of floats prints them
-    (saveParticlesToPLY, utility.cu:91-127): %g with six significant digits.
+    (save3dParticlesToPLY / save3dParticlesToOFF, utility.cu:91-127): %g with six significant digits.
     Binary PLY round-trips exactly through the reader."""
     from fluidprjct_b200 import capi
     rng = np.random.default_rng(0)
