@@ -32,6 +32,59 @@ def test_library_exports_every_declared_symbol():
     assert set(syms) <= exported
 
 
+C_CALLER = r"""
+#include <stdio.h>
+#include <string.h>
+#include "fluidprjct.h"
+int main(int argc, char** argv) {
+    fp_config c;
+    char labels[64];
+    int frames = 0;
+    float pos[6] = {0.1f, 0.2f, 0.3f, 0.4f, 0.5f, 0.6f}, back[6] = {0};
+    int64_t n = 2;
+    int has_vel = -1;
+    fp_solver* s = NULL;
+    if (argc < 3) return 2;
+    fp_config_default(&c);
+    printf("default %d %d %g\n", c.dim, c.ppc, (double)c.pic_weight);
+    if (fp_config_load_json(argv[1], &c, labels, sizeof labels, &frames) != FP_OK) return 3;
+    printf("json %g %d %s %s\n", (double)c.dt, frames, labels, c.output_template);
+    c.dim = 5;
+    printf("create %d %d\n", fp_create(&c, &s), s == NULL);
+    if (fp_write_particle_file(argv[2], pos, NULL, n, FP_OUT_PLY_BINARY) != FP_OK) return 4;
+    if (fp_read_ply_file(argv[2], &n, back, NULL, &has_vel) != FP_OK) return 5;
+    printf("ply %lld %d %d\n", (long long)n, has_vel, memcmp(pos, back, sizeof pos) == 0);
+    return 0;
+}
+"""
+
+
+def test_header_is_plain_c(tmp_path):
+    """The ABI is what a cgo / FFI binding would compile: a C99 caller built
+    with gcc -pedantic against include/fluidprjct.h links the library and
+    calls its host-side entry points (no GPU work)."""
+    import shutil
+    from fluidprjct_b200 import capi
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no gcc")
+    src = tmp_path / "caller.c"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(capi.LIB_PATH)
+    r = subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"),
+                        str(src), "-L", libdir, "-lfluidprjct_b200", "-Wl,-rpath," + libdir, "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    cfg = tmp_path / "config.json"
+    cfg.write_text('{"dt": 0.005, "frameAmount": 12, "inputLabelData": "InputData/labels.txt",'
+                   ' "outputTemplate": "OutputData/particles_"}')
+    r = subprocess.run([str(exe), str(cfg), str(tmp_path / "p.ply")], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, (r.stdout, r.stderr)
+    assert r.stdout.splitlines() == ["default 3 4 0.01", "json 0.005 12 InputData/labels.txt OutputData/particles_",
+                                     "create %d 1" % capi.FP_ERR_ARG, "ply 2 1 1"]  # binary PLY carries vel
+
+
 def test_config_defaults_match_reference():
     from fluidprjct_b200 import capi
     c = capi.default_config()
